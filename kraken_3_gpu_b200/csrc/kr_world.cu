@@ -1,0 +1,672 @@
+// kr_world.cu -- the gpuworld.js drop-in: handle, schedule and the plain
+// per-step kernel (one launch per env step, one warp per creature).
+//
+// Device buffers hold the reference's own AoS blocks (48 B bodies, 80 B
+// constraints, 16 B forces / collision points), so upload and download are
+// single copies and mirrorInto/packControls keep their exact field offsets.
+// The kernel stages each creature into shared memory as SoA for the launch.
+//
+// Schedule.  The reference runs one dispatch per colour class
+// (gpuworld.js:353-366); a colour class is body-disjoint, so the classes in
+// order are one valid sequential order of the solve list.  Here every
+// connected component of the constraint graph (a creature) gets its own
+// schedule: each constraint is placed on the first level after every earlier
+// constraint (in solve-list order) that shares one of its bodies.  Levels are
+// body-disjoint, and any order that keeps every pair of constraints sharing a
+// body in list order gives bit-identical results (the harness check
+// color-order-free, harness.js:1172-1193, pins this property for the
+// reference), so the warp's level sweep reproduces the list order exactly.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <numeric>
+#include <string>
+#include <vector>
+
+#include "../../include/kraken_b200.h"
+#include "kr_solver.cuh"
+
+namespace {
+
+thread_local std::string g_last_error;
+
+constexpr int kWarpsPerBlock = 4;
+
+// Per-island record, one int array of kIslandInts per island.
+enum {
+  I_BODY_OFF = 0, I_NB, I_CON_OFF, I_NC, I_PT_OFF, I_NP, I_LVL_OFF, I_NLV, I_ROUND_OFF,
+  I_NROUNDS, kIslandInts
+};
+
+struct DeviceTables {
+  const int *isl;          // nI x kIslandInts
+  const int *bodies;       // global body id per island body
+  const int *cons;         // global constraint index per schedule slot
+  const int *ab;           // local a | local b << 16 per schedule slot
+  const int *pts;          // global collision point index, local-body grouped
+  const int2 *bpt;         // per island body: (offset within island points, count)
+  const int *lvl;          // level offsets per island (nlv + 1 each)
+  const short *clane;      // collision lane table per island (nrounds x 32)
+};
+
+struct StepArgs {
+  kr::SolverConsts K;
+  float *bodies;           // nB x 12
+  uint32_t *cons;          // nC x 20
+  float *forces;           // nB x 4
+  const uint4 *coll;       // nP x 4 words
+  const float4 *rects;     // nR x (x, y, x+w, y+h)
+  int nR;
+  int nI;
+  int maxB, maxC, maxP;    // smem carve sizes (per warp)
+  DeviceTables T;
+};
+
+__host__ __device__ inline int warp_smem_words(int mb, int mc, int mp) {
+  return 16 * mb + 15 * mc + 3 * mp;
+}
+
+__device__ inline void carve(kr::Island &S, float *base, int mb, int mc, int mp) {
+  float *p = base;
+  S.px = p; p += mb; S.py = p; p += mb; S.ppx = p; p += mb; S.ppy = p; p += mb;
+  S.vx = p; p += mb; S.vy = p; p += mb; S.ang = p; p += mb; S.angP = p; p += mb;
+  S.av = p; p += mb; S.im = p; p += mb; S.ii = p; p += mb;
+  S.fx = p; p += mb; S.fy = p; p += mb; S.tq = p; p += mb;
+  S.boff = reinterpret_cast<int *>(p); p += mb;
+  S.bcnt = reinterpret_cast<int *>(p); p += mb;
+  S.ab = reinterpret_cast<int *>(p); p += mc;
+  S.tb = reinterpret_cast<int *>(p); p += mc;
+  S.lax = p; p += mc; S.lay = p; p += mc; S.lbx = p; p += mc; S.lby = p; p += mc;
+  S.comp = p; p += mc; S.rest = p; p += mc; S.tgt = p; p += mc; S.minA = p; p += mc;
+  S.maxA = p; p += mc; S.lamX = p; p += mc; S.lamY = p; p += mc; S.lam = p; p += mc;
+  S.brk = p; p += mc;
+  S.plx = p; p += mp; S.ply = p; p += mp; S.pr = p; p += mp;
+}
+
+__global__ void __launch_bounds__(32 * kWarpsPerBlock)
+plain_step_kernel(StepArgs A) {
+  extern __shared__ float smem[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int island = blockIdx.x * kWarpsPerBlock + warp;
+  if (island >= A.nI) return;
+  kr::Island S;
+  carve(S, smem + warp * warp_smem_words(A.maxB, A.maxC, A.maxP), A.maxB, A.maxC, A.maxP);
+  const int *rec = A.T.isl + island * kIslandInts;
+  const int bo = rec[I_BODY_OFF], co = rec[I_CON_OFF], po = rec[I_PT_OFF];
+  S.nb = rec[I_NB]; S.nc = rec[I_NC]; S.np = rec[I_NP];
+  S.nlv = rec[I_NLV]; S.nrounds = rec[I_NROUNDS];
+  S.lvl = A.T.lvl + rec[I_LVL_OFF];
+  S.clane = A.T.clane + rec[I_ROUND_OFF];
+
+  // stage bodies (48 B AoS -> SoA) and forces
+  for (int i = lane; i < S.nb; i += 32) {
+    const int g = A.T.bodies[bo + i];
+    const float4 *b4 = reinterpret_cast<const float4 *>(A.bodies + 12 * (size_t)g);
+    const float4 q0 = b4[0], q1 = b4[1], q2 = b4[2];
+    S.px[i] = q0.x; S.py[i] = q0.y; S.ppx[i] = q0.z; S.ppy[i] = q0.w;
+    S.vx[i] = q1.x; S.vy[i] = q1.y; S.ang[i] = q1.z; S.angP[i] = q1.w;
+    S.av[i] = q2.x; S.im[i] = q2.y; S.ii[i] = q2.z;
+    const float4 f = reinterpret_cast<const float4 *>(A.forces)[g];
+    S.fx[i] = f.x; S.fy[i] = f.y; S.tq[i] = f.z;
+    const int2 bp = A.T.bpt[bo + i];
+    S.boff[i] = bp.x; S.bcnt[i] = bp.y;
+  }
+  // stage constraints (80 B AoS -> SoA, schedule order)
+  for (int k = lane; k < S.nc; k += 32) {
+    const int g = A.T.cons[co + k];
+    const uint4 *c4 = reinterpret_cast<const uint4 *>(A.cons + 20 * (size_t)g);
+    const uint4 w0 = c4[0], w1 = c4[1], w2 = c4[2], w3 = c4[3], w4 = c4[4];
+    S.ab[k] = A.T.ab[co + k];
+    S.tb[k] = static_cast<int>(w0.z & 0xffu) | ((w4.y != 0u ? 1 : 0) << 8);
+    S.lax[k] = __uint_as_float(w1.x); S.lay[k] = __uint_as_float(w1.y);
+    S.lbx[k] = __uint_as_float(w1.z); S.lby[k] = __uint_as_float(w1.w);
+    S.comp[k] = __uint_as_float(w2.x); S.rest[k] = __uint_as_float(w2.y);
+    S.tgt[k] = __uint_as_float(w2.z); S.minA[k] = __uint_as_float(w2.w);
+    S.maxA[k] = __uint_as_float(w3.x); S.lamX[k] = __uint_as_float(w3.y);
+    S.lamY[k] = __uint_as_float(w3.z); S.lam[k] = __uint_as_float(w3.w);
+    S.brk[k] = __uint_as_float(w4.x);
+  }
+  // stage collision points
+  for (int p = lane; p < S.np; p += 32) {
+    const uint4 cp = A.coll[A.T.pts[po + p]];
+    S.plx[p] = __uint_as_float(cp.y); S.ply[p] = __uint_as_float(cp.z);
+    S.pr[p] = __uint_as_float(cp.w);
+  }
+  __syncwarp();
+
+  kr::island_step(A.K, S, A.rects, A.nR, lane);
+
+  // write back bodies, consumed forces and constraint multipliers / flags
+  for (int i = lane; i < S.nb; i += 32) {
+    const int g = A.T.bodies[bo + i];
+    float4 *b4 = reinterpret_cast<float4 *>(A.bodies + 12 * (size_t)g);
+    const float pad = A.bodies[12 * (size_t)g + 11];
+    b4[0] = make_float4(S.px[i], S.py[i], S.ppx[i], S.ppy[i]);
+    b4[1] = make_float4(S.vx[i], S.vy[i], S.ang[i], S.angP[i]);
+    b4[2] = make_float4(S.av[i], S.im[i], S.ii[i], pad);
+    if (!(S.im[i] == 0.f && S.ii[i] == 0.f)) {
+      float *f = A.forces + 4 * (size_t)g;
+      f[0] = 0.f; f[1] = 0.f; f[2] = 0.f;  // consumed, adhesion kept (solver.wgsl:204)
+    }
+  }
+  for (int k = lane; k < S.nc; k += 32) {
+    const int g = A.T.cons[co + k];
+    uint32_t *c = A.cons + 20 * (size_t)g;
+    c[13] = __float_as_uint(S.lamX[k]);
+    c[14] = __float_as_uint(S.lamY[k]);
+    c[15] = __float_as_uint(S.lam[k]);
+    c[17] = (S.tb[k] >> 8) != 0 ? 1u : 0u;
+  }
+}
+
+template <typename T>
+cudaError_t dev_upload(T **dptr, size_t *cap, const std::vector<T> &v) {
+  size_t n = std::max<size_t>(v.size(), 1);
+  if (*dptr == nullptr || *cap < n) {
+    if (*dptr) cudaFree(*dptr);
+    *dptr = nullptr;
+    cudaError_t e = cudaMalloc(reinterpret_cast<void **>(dptr), n * sizeof(T));
+    if (e != cudaSuccess) return e;
+    *cap = n;
+  }
+  if (v.empty()) return cudaSuccess;
+  return cudaMemcpy(*dptr, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice);
+}
+
+}  // namespace
+
+struct kr_world {
+  kr_solver_params p{};
+  kr::SolverConsts K{};
+  uint32_t nB = 0, nC = 0, nP = 0, nR = 0;
+  float *d_bodies = nullptr;
+  uint32_t *d_cons = nullptr;
+  uint32_t *d_stage = nullptr;          // staging copy of a control upload
+  size_t smem_bytes = 0;
+  float *d_forces = nullptr;
+  float4 *d_rects = nullptr;
+  uint4 *d_coll = nullptr;
+  std::vector<uint32_t> h_coll_range;   // 2 x nB
+  // island tables
+  int *d_isl = nullptr, *d_ibodies = nullptr, *d_icons = nullptr, *d_iab = nullptr,
+      *d_ipts = nullptr, *d_lvl = nullptr;
+  int2 *d_bpt = nullptr;
+  short *d_clane = nullptr;
+  size_t c_isl = 0, c_ibodies = 0, c_icons = 0, c_iab = 0, c_ipts = 0, c_lvl = 0, c_bpt = 0,
+         c_clane = 0;
+  int nI = 0, maxB = 1, maxC = 1, maxP = 1, maxLv = 0;
+  bool uploaded = false;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  std::string err;
+
+  int fail(int code, const std::string &msg) {
+    err = msg;
+    return code;
+  }
+  int cuda_fail(cudaError_t e, const char *what) {
+    err = std::string("CUDA error in ") + what + ": " + cudaGetErrorString(e);
+    return KR_ERR_CUDA;
+  }
+};
+
+extern "C" int kr_device_count(void) {
+  int n = 0;
+  cudaError_t e = cudaGetDeviceCount(&n);
+  if (e != cudaSuccess) {
+    g_last_error = std::string("cudaGetDeviceCount: ") + cudaGetErrorString(e);
+    cudaGetLastError();
+    return 0;
+  }
+  return n;
+}
+
+extern "C" const char *kr_last_error(const kr_world *w) {
+  if (w) return w->err.c_str();
+  return g_last_error.c_str();
+}
+
+extern "C" int kr_create(const kr_solver_params *params, uint32_t n_bodies, uint32_t n_constraints,
+                         const float *rects, uint32_t n_rects, const uint32_t *coll_pts,
+                         uint32_t n_coll_pts, const uint32_t *coll_range, kr_world **out) {
+  if (!out || !params) {
+    g_last_error = "kr_create: null argument";
+    return KR_ERR_INVALID;
+  }
+  *out = nullptr;
+  const kr_solver_params &p = *params;
+  // sanity guards of writeStatic (gpuworld.js:224-229), same bounds
+  if (!(p.iterations >= 1 && p.iterations <= 64)) {
+    g_last_error = "iterations implausible: " + std::to_string(p.iterations);
+    return KR_ERR_INVALID;
+  }
+  if (!(n_rects >= 1 && n_rects <= 100000)) {
+    g_last_error = "nRects implausible: " + std::to_string(n_rects);
+    return KR_ERR_INVALID;
+  }
+  if (!(n_bodies >= 1 && n_bodies <= 4000000)) {
+    g_last_error = "nBodies implausible: " + std::to_string(n_bodies);
+    return KR_ERR_INVALID;
+  }
+  const float hf = static_cast<float>(p.h);
+  if (!(hf > 0.f && hf < 1.f)) {
+    g_last_error = "h implausible: " + std::to_string(p.h);
+    return KR_ERR_INVALID;
+  }
+  if (p.substeps < 1 || p.substeps > 64) {
+    g_last_error = "substeps implausible: " + std::to_string(p.substeps);
+    return KR_ERR_INVALID;
+  }
+  if ((n_coll_pts > 0 && (!coll_pts || !coll_range)) || !rects) {
+    g_last_error = "kr_create: missing rects or collision points";
+    return KR_ERR_INVALID;
+  }
+  // collRange must cover the points exactly (gpuworld.js:193-199)
+  uint64_t acc = 0;
+  if (coll_range) {
+    for (uint32_t b = 0; b < n_bodies; b++) {
+      if (coll_range[b] != acc) {
+        g_last_error = "collRange offsets are not contiguous at body " + std::to_string(b);
+        return KR_ERR_INVALID;
+      }
+      acc += coll_range[n_bodies + b];
+    }
+    for (uint32_t i = 0; i < n_coll_pts; i++) {
+      if (coll_pts[4 * i] >= n_bodies) {
+        g_last_error = "collPt " + std::to_string(i) + " refers to body " +
+                       std::to_string(coll_pts[4 * i]) + " of " + std::to_string(n_bodies);
+        return KR_ERR_INDEX;
+      }
+    }
+  }
+  if (acc != n_coll_pts) {
+    g_last_error = "collRange covers " + std::to_string(acc) + " of " +
+                   std::to_string(n_coll_pts) + " points";
+    return KR_ERR_INVALID;
+  }
+  int dev_count = 0;
+  if (cudaGetDeviceCount(&dev_count) != cudaSuccess || dev_count == 0) {
+    cudaGetLastError();
+    g_last_error = "no CUDA device available";
+    return KR_ERR_NODEVICE;
+  }
+
+  kr_world *w = new kr_world();
+  w->p = p;
+  w->nB = n_bodies; w->nC = n_constraints; w->nP = n_coll_pts; w->nR = n_rects;
+  // f32 constants: writeStatic F[0], F[10], F[11] and f32solver.mjs:79-85
+  kr::SolverConsts &K = w->K;
+  K.h = hf;
+  K.invH = static_cast<float>(1.0 / p.h);
+  K.invH2 = static_cast<float>(1.0 / (p.h * p.h));
+  const float nl = -static_cast<float>(p.lin_drag), na = -static_cast<float>(p.ang_drag);
+  K.linDamp = static_cast<float>(std::exp(static_cast<double>(nl * hf)));
+  K.angDamp = static_cast<float>(std::exp(static_cast<double>(na * hf)));
+  K.maxSpeed = static_cast<float>(p.max_speed);
+  K.maxAngSpeed = static_cast<float>(p.max_ang_speed);
+  K.substeps = p.substeps;
+  K.iterations = p.iterations;
+
+  cudaError_t e;
+  auto cleanup_fail = [&](cudaError_t ce, const char *what) {
+    g_last_error = std::string("CUDA error in ") + what + ": " + cudaGetErrorString(ce);
+    kr_destroy(w);
+    return KR_ERR_CUDA;
+  };
+  if ((e = cudaStreamCreateWithFlags(&w->stream, cudaStreamNonBlocking)) != cudaSuccess)
+    return cleanup_fail(e, "cudaStreamCreate");
+  w->own_stream = true;
+  if ((e = cudaMalloc(&w->d_bodies, sizeof(float) * 12 * n_bodies)) != cudaSuccess)
+    return cleanup_fail(e, "cudaMalloc(bodies)");
+  if ((e = cudaMalloc(&w->d_cons, sizeof(uint32_t) * 20 * std::max<uint32_t>(n_constraints, 1))) !=
+      cudaSuccess)
+    return cleanup_fail(e, "cudaMalloc(cons)");
+  if ((e = cudaMalloc(&w->d_stage, sizeof(uint32_t) * 20 * std::max<uint32_t>(n_constraints, 1))) !=
+      cudaSuccess)
+    return cleanup_fail(e, "cudaMalloc(control staging)");
+  if ((e = cudaMalloc(&w->d_forces, sizeof(float) * 4 * n_bodies)) != cudaSuccess)
+    return cleanup_fail(e, "cudaMalloc(forces)");
+  if ((e = cudaMemset(w->d_forces, 0, sizeof(float) * 4 * n_bodies)) != cudaSuccess)
+    return cleanup_fail(e, "cudaMemset(forces)");
+  std::vector<float4> r4(n_rects);
+  for (uint32_t i = 0; i < n_rects; i++) {
+    const float x = rects[4 * i], y = rects[4 * i + 1], rw = rects[4 * i + 2], rh = rects[4 * i + 3];
+    r4[i] = make_float4(x, y, x + rw, y + rh);  // f32 sums, as solver.wgsl:120-121
+  }
+  if ((e = cudaMalloc(&w->d_rects, sizeof(float4) * n_rects)) != cudaSuccess)
+    return cleanup_fail(e, "cudaMalloc(rects)");
+  if ((e = cudaMemcpy(w->d_rects, r4.data(), sizeof(float4) * n_rects, cudaMemcpyHostToDevice)) !=
+      cudaSuccess)
+    return cleanup_fail(e, "cudaMemcpy(rects)");
+  if ((e = cudaMalloc(&w->d_coll, sizeof(uint4) * std::max<uint32_t>(n_coll_pts, 1))) != cudaSuccess)
+    return cleanup_fail(e, "cudaMalloc(collPts)");
+  if (n_coll_pts &&
+      (e = cudaMemcpy(w->d_coll, coll_pts, sizeof(uint4) * n_coll_pts, cudaMemcpyHostToDevice)) !=
+          cudaSuccess)
+    return cleanup_fail(e, "cudaMemcpy(collPts)");
+  w->h_coll_range.assign(2 * (size_t)n_bodies, 0u);
+  if (coll_range) std::memcpy(w->h_coll_range.data(), coll_range, sizeof(uint32_t) * 2 * n_bodies);
+  *out = w;
+  return KR_OK;
+}
+
+namespace {
+
+// Connected components, per-component levels and lane tables (see the file
+// comment).  Returns KR_OK or an error code with w->err set.
+int build_schedule(kr_world *w, const float *bodies, const uint32_t *cons) {
+  const uint32_t nB = w->nB, nC = w->nC;
+  std::vector<int> parent(nB);
+  std::iota(parent.begin(), parent.end(), 0);
+  auto find = [&](int x) {
+    while (parent[x] != x) { parent[x] = parent[parent[x]]; x = parent[x]; }
+    return x;
+  };
+  for (uint32_t k = 0; k < nC; k++) {
+    const uint32_t a = cons[20 * k], b = cons[20 * k + 1];
+    if (a >= nB || (b != 0xffffffffu && b >= nB)) {
+      return w->fail(KR_ERR_INDEX, "Constraint " + std::to_string(k) + ": body index " +
+                                       std::to_string(a) + "/" +
+                                       (b == 0xffffffffu ? std::string("-1") : std::to_string(b)) +
+                                       " outside of " + std::to_string(nB) +
+                                       " (an out-of-bounds read in the kernel)");
+    }
+    if (b != 0xffffffffu) {
+      int ra = find((int)a), rb = find((int)b);
+      if (ra != rb) parent[std::max(ra, rb)] = std::min(ra, rb);
+    }
+  }
+  // islands in order of their smallest body
+  std::vector<int> island_of(nB), local(nB);
+  std::vector<std::vector<int>> ib;  // bodies per island
+  std::vector<int> root_island(nB, -1);
+  for (uint32_t g = 0; g < nB; g++) {
+    int r = find((int)g);
+    if (root_island[r] < 0) { root_island[r] = (int)ib.size(); ib.emplace_back(); }
+    int I = root_island[r];
+    island_of[g] = I;
+    local[g] = (int)ib[I].size();
+    ib[I].push_back((int)g);
+  }
+  const int nI = (int)ib.size();
+  std::vector<std::vector<int>> ic(nI);  // constraints per island, list order
+  for (uint32_t k = 0; k < nC; k++) ic[island_of[cons[20 * k]]].push_back((int)k);
+
+  std::vector<int> isl(nI * (size_t)kIslandInts), h_bodies, h_cons, h_ab, h_pts, h_lvl;
+  std::vector<int2> h_bpt;
+  std::vector<short> h_clane;
+  h_bodies.reserve(nB); h_cons.reserve(nC); h_ab.reserve(nC);
+  int maxB = 1, maxC = 1, maxP = 1, maxLv = 0;
+  std::vector<int> last_level, level, order, cnt_per_level;
+  for (int I = 0; I < nI; I++) {
+    const auto &bl = ib[I];
+    const auto &cl = ic[I];
+    const int nb = (int)bl.size(), nc = (int)cl.size();
+    if (nb > KR_MAX_ISLAND_BODIES || nc > KR_MAX_ISLAND_CONSTRAINTS)
+      return w->fail(KR_ERR_CAPACITY, "connected component " + std::to_string(I) + " has " +
+                                          std::to_string(nb) + " bodies and " +
+                                          std::to_string(nc) + " constraints; the kernel holds " +
+                                          std::to_string(KR_MAX_ISLAND_BODIES) + " / " +
+                                          std::to_string(KR_MAX_ISLAND_CONSTRAINTS));
+    int *rec = &isl[I * (size_t)kIslandInts];
+    rec[I_BODY_OFF] = (int)h_bodies.size();
+    rec[I_NB] = nb;
+    for (int g : bl) h_bodies.push_back(g);
+    // levels: first level after every earlier constraint sharing a body
+    last_level.assign(nb, -1);
+    level.resize(nc);
+    int nlv = 0;
+    for (int q = 0; q < nc; q++) {
+      const uint32_t *c = cons + 20 * (size_t)cl[q];
+      const int a = local[c[0]];
+      const int b = c[1] == 0xffffffffu ? -1 : local[c[1]];
+      int L = last_level[a] + 1;
+      if (b >= 0) L = std::max(L, last_level[b] + 1);
+      level[q] = L;
+      last_level[a] = L;
+      if (b >= 0) last_level[b] = L;
+      nlv = std::max(nlv, L + 1);
+    }
+    if (nlv > KR_MAX_LEVELS)
+      return w->fail(KR_ERR_CAPACITY, "connected component " + std::to_string(I) + " needs " +
+                                          std::to_string(nlv) + " constraint levels; the kernel holds " +
+                                          std::to_string(KR_MAX_LEVELS));
+    cnt_per_level.assign(nlv + 1, 0);
+    for (int q = 0; q < nc; q++) cnt_per_level[level[q] + 1]++;
+    for (int L = 0; L < nlv; L++) cnt_per_level[L + 1] += cnt_per_level[L];
+    rec[I_LVL_OFF] = (int)h_lvl.size();
+    rec[I_NLV] = nlv;
+    for (int L = 0; L <= nlv; L++) h_lvl.push_back(cnt_per_level[L]);
+    order.assign(nc, 0);
+    {
+      std::vector<int> cur(cnt_per_level.begin(), cnt_per_level.end() - 1);
+      for (int q = 0; q < nc; q++) order[cur[level[q]]++] = q;  // stable within a level
+    }
+    rec[I_CON_OFF] = (int)h_cons.size();
+    rec[I_NC] = nc;
+    for (int s = 0; s < nc; s++) {
+      const int k = cl[order[s]];
+      const uint32_t *c = cons + 20 * (size_t)k;
+      const uint32_t a = (uint32_t)local[c[0]];
+      const uint32_t b = c[1] == 0xffffffffu ? 0xffffu : (uint32_t)local[c[1]];
+      h_cons.push_back(k);
+      h_ab.push_back((int)(a | (b << 16)));
+    }
+    // collision points in local body order
+    rec[I_PT_OFF] = (int)h_pts.size();
+    int np = 0;
+    std::vector<std::pair<int, int>> load_bodies;  // (count, local body)
+    for (int j = 0; j < nb; j++) {
+      const int g = bl[j];
+      const uint32_t off = w->h_coll_range[g], cnt = w->h_coll_range[nB + g];
+      h_bpt.push_back(make_int2(np, (int)cnt));
+      for (uint32_t q = 0; q < cnt; q++) h_pts.push_back((int)(off + q));
+      np += (int)cnt;
+      const float im = bodies[12 * (size_t)g + 9];
+      if (cnt > 0 && im != 0.f) load_bodies.emplace_back((int)cnt, j);
+    }
+    if (np > KR_MAX_ISLAND_COLLPTS)
+      return w->fail(KR_ERR_CAPACITY, "connected component " + std::to_string(I) + " has " +
+                                          std::to_string(np) + " collision points; the kernel holds " +
+                                          std::to_string(KR_MAX_ISLAND_COLLPTS));
+    rec[I_NP] = np;
+    // longest-first onto the least loaded lane
+    std::stable_sort(load_bodies.begin(), load_bodies.end(),
+                     [](const std::pair<int, int> &x, const std::pair<int, int> &y) {
+                       return x.first > y.first;
+                     });
+    std::vector<int> lane_load(32, 0);
+    std::vector<std::vector<int>> lane_q(32);
+    for (const auto &lb : load_bodies) {
+      int best = 0;
+      for (int l = 1; l < 32; l++)
+        if (lane_load[l] < lane_load[best]) best = l;
+      lane_load[best] += lb.first;
+      lane_q[best].push_back(lb.second);
+    }
+    int rounds = 0;
+    for (int l = 0; l < 32; l++) rounds = std::max(rounds, (int)lane_q[l].size());
+    rec[I_ROUND_OFF] = (int)h_clane.size();
+    rec[I_NROUNDS] = rounds;
+    for (int r = 0; r < rounds; r++)
+      for (int l = 0; l < 32; l++)
+        h_clane.push_back(r < (int)lane_q[l].size() ? (short)lane_q[l][r] : (short)-1);
+    maxB = std::max(maxB, nb);
+    maxC = std::max(maxC, nc);
+    maxP = std::max(maxP, np);
+    maxLv = std::max(maxLv, nlv);
+  }
+  cudaError_t e;
+  if ((e = dev_upload(&w->d_isl, &w->c_isl, isl)) != cudaSuccess) return w->cuda_fail(e, "upload(islands)");
+  if ((e = dev_upload(&w->d_ibodies, &w->c_ibodies, h_bodies)) != cudaSuccess) return w->cuda_fail(e, "upload(island bodies)");
+  if ((e = dev_upload(&w->d_icons, &w->c_icons, h_cons)) != cudaSuccess) return w->cuda_fail(e, "upload(island constraints)");
+  if ((e = dev_upload(&w->d_iab, &w->c_iab, h_ab)) != cudaSuccess) return w->cuda_fail(e, "upload(island ab)");
+  if ((e = dev_upload(&w->d_ipts, &w->c_ipts, h_pts)) != cudaSuccess) return w->cuda_fail(e, "upload(island points)");
+  if ((e = dev_upload(&w->d_bpt, &w->c_bpt, h_bpt)) != cudaSuccess) return w->cuda_fail(e, "upload(body point ranges)");
+  if ((e = dev_upload(&w->d_lvl, &w->c_lvl, h_lvl)) != cudaSuccess) return w->cuda_fail(e, "upload(levels)");
+  if ((e = dev_upload(&w->d_clane, &w->c_clane, h_clane)) != cudaSuccess) return w->cuda_fail(e, "upload(lane table)");
+  w->nI = nI;
+  // round up so every per-warp region keeps 16-byte alignment of its arrays
+  w->maxB = (maxB + 3) & ~3;
+  w->maxC = (maxC + 3) & ~3;
+  w->maxP = (maxP + 3) & ~3;
+  w->maxLv = maxLv;
+  w->smem_bytes =
+      sizeof(float) * kWarpsPerBlock * (size_t)warp_smem_words(w->maxB, w->maxC, w->maxP);
+  if ((e = cudaFuncSetAttribute(plain_step_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)w->smem_bytes)) != cudaSuccess)
+    return w->cuda_fail(e, "cudaFuncSetAttribute(plain_step_kernel)");
+  return KR_OK;
+}
+
+}  // namespace
+
+extern "C" int kr_upload(kr_world *w, const float *bodies, const uint32_t *cons, const float *forces,
+                         const uint32_t *color_info) {
+  if (!w) return KR_ERR_INVALID;
+  if (!bodies || (w->nC && !cons)) return w->fail(KR_ERR_INVALID, "kr_upload: null buffer");
+  if (color_info) {
+    uint32_t acc = 0;
+    for (int c = 0; c < 16; c++) {
+      if (color_info[c] != acc)
+        return w->fail(KR_ERR_INVALID, "colorInfo: colour " + std::to_string(c) +
+                                           " does not start where the previous one ends");
+      acc += color_info[16 + c];
+    }
+    if (acc != w->nC)
+      return w->fail(KR_ERR_INVALID, "colorInfo covers " + std::to_string(acc) + " of " +
+                                         std::to_string(w->nC) + " constraints");
+  }
+  int rc = build_schedule(w, bodies, cons);
+  if (rc != KR_OK) return rc;
+  cudaError_t e;
+  if ((e = cudaMemcpyAsync(w->d_bodies, bodies, sizeof(float) * 12 * w->nB, cudaMemcpyHostToDevice,
+                           w->stream)) != cudaSuccess)
+    return w->cuda_fail(e, "upload(bodies)");
+  if (w->nC && (e = cudaMemcpyAsync(w->d_cons, cons, sizeof(uint32_t) * 20 * w->nC,
+                                    cudaMemcpyHostToDevice, w->stream)) != cudaSuccess)
+    return w->cuda_fail(e, "upload(cons)");
+  if (forces) {
+    if ((e = cudaMemcpyAsync(w->d_forces, forces, sizeof(float) * 4 * w->nB, cudaMemcpyHostToDevice,
+                             w->stream)) != cudaSuccess)
+      return w->cuda_fail(e, "upload(forces)");
+  } else if ((e = cudaMemsetAsync(w->d_forces, 0, sizeof(float) * 4 * w->nB, w->stream)) !=
+             cudaSuccess) {
+    return w->cuda_fail(e, "upload(forces)");
+  }
+  if ((e = cudaStreamSynchronize(w->stream)) != cudaSuccess) return w->cuda_fail(e, "upload(sync)");
+  w->uploaded = true;
+  return KR_OK;
+}
+
+namespace {
+// Copies the control fields of the 80 B records (packControls, gpuworld.js:331-341).
+__global__ void controls_kernel(uint32_t *dst, const uint32_t *src, int nC) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= nC) return;
+  const uint32_t *s = src + 20 * (size_t)k;
+  uint32_t *d = dst + 20 * (size_t)k;
+  d[6] = s[6]; d[7] = s[7]; d[8] = s[8]; d[10] = s[10]; d[16] = s[16]; d[17] = s[17];
+}
+}  // namespace
+
+extern "C" int kr_upload_controls(kr_world *w, const uint32_t *cons) {
+  if (!w) return KR_ERR_INVALID;
+  if (!w->uploaded) return w->fail(KR_ERR_STATE, "uploadControls before upload");
+  if (!w->nC) return KR_OK;
+  if (!cons) return w->fail(KR_ERR_INVALID, "kr_upload_controls: null buffer");
+  // stage the whole block once, then scatter the six control words per record
+  cudaError_t e = cudaMemcpyAsync(w->d_stage, cons, sizeof(uint32_t) * 20 * w->nC,
+                                  cudaMemcpyHostToDevice, w->stream);
+  if (e != cudaSuccess) return w->cuda_fail(e, "uploadControls(copy)");
+  controls_kernel<<<(w->nC + 255) / 256, 256, 0, w->stream>>>(w->d_cons, w->d_stage, (int)w->nC);
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return w->cuda_fail(e, "uploadControls(scatter)");
+  return KR_OK;
+}
+
+extern "C" int kr_step(kr_world *w, int32_t n_steps) {
+  if (!w) return KR_ERR_INVALID;
+  if (!w->uploaded) return w->fail(KR_ERR_STATE, "step before upload");
+  if (n_steps < 0) return w->fail(KR_ERR_INVALID, "n_steps < 0");
+  if (n_steps == 0 || w->nI == 0) return KR_OK;
+  StepArgs A;
+  A.K = w->K;
+  A.bodies = w->d_bodies;
+  A.cons = w->d_cons;
+  A.forces = w->d_forces;
+  A.coll = w->d_coll;
+  A.rects = w->d_rects;
+  A.nR = (int)w->nR;
+  A.nI = w->nI;
+  A.maxB = w->maxB; A.maxC = w->maxC; A.maxP = w->maxP;
+  A.T = DeviceTables{w->d_isl, w->d_ibodies, w->d_icons, w->d_iab, w->d_ipts, w->d_bpt, w->d_lvl,
+                     w->d_clane};
+  const size_t smem = w->smem_bytes;
+  cudaError_t e;
+  const int grid = (w->nI + kWarpsPerBlock - 1) / kWarpsPerBlock;
+  for (int s = 0; s < n_steps; s++) {
+    plain_step_kernel<<<grid, 32 * kWarpsPerBlock, smem, w->stream>>>(A);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return w->cuda_fail(e, "plain_step_kernel launch");
+  }
+  return KR_OK;
+}
+
+extern "C" int kr_download(kr_world *w, float *bodies, uint32_t *cons) {
+  if (!w) return KR_ERR_INVALID;
+  if (!w->uploaded) return w->fail(KR_ERR_STATE, "download before upload");
+  cudaError_t e;
+  if (bodies && (e = cudaMemcpyAsync(bodies, w->d_bodies, sizeof(float) * 12 * w->nB,
+                                     cudaMemcpyDeviceToHost, w->stream)) != cudaSuccess)
+    return w->cuda_fail(e, "download(bodies)");
+  if (cons && w->nC && (e = cudaMemcpyAsync(cons, w->d_cons, sizeof(uint32_t) * 20 * w->nC,
+                                            cudaMemcpyDeviceToHost, w->stream)) != cudaSuccess)
+    return w->cuda_fail(e, "download(cons)");
+  if ((e = cudaStreamSynchronize(w->stream)) != cudaSuccess) return w->cuda_fail(e, "download(sync)");
+  return KR_OK;
+}
+
+extern "C" int kr_sync(kr_world *w) {
+  if (!w) return KR_ERR_INVALID;
+  cudaError_t e = cudaStreamSynchronize(w->stream);
+  if (e != cudaSuccess) return w->cuda_fail(e, "cudaStreamSynchronize");
+  return KR_OK;
+}
+
+extern "C" int kr_set_stream(kr_world *w, void *stream) {
+  if (!w) return KR_ERR_INVALID;
+  cudaError_t e = cudaStreamSynchronize(w->stream);
+  if (e != cudaSuccess) return w->cuda_fail(e, "cudaStreamSynchronize");
+  if (stream) {
+    if (w->own_stream) cudaStreamDestroy(w->stream);
+    w->own_stream = false;
+    w->stream = static_cast<cudaStream_t>(stream);
+  } else if (!w->own_stream) {
+    e = cudaStreamCreateWithFlags(&w->stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) return w->cuda_fail(e, "cudaStreamCreate");
+    w->own_stream = true;
+  }
+  return KR_OK;
+}
+
+extern "C" int kr_world_islands(const kr_world *w, int32_t *n_islands, int32_t *max_levels) {
+  if (!w) return KR_ERR_INVALID;
+  if (n_islands) *n_islands = w->nI;
+  if (max_levels) *max_levels = w->maxLv;
+  return KR_OK;
+}
+
+extern "C" void kr_destroy(kr_world *w) {
+  if (!w) return;
+  if (w->stream) cudaStreamSynchronize(w->stream);
+  void *ptrs[] = {w->d_bodies, w->d_cons, w->d_stage, w->d_forces, w->d_rects, w->d_coll, w->d_isl,
+                  w->d_ibodies, w->d_icons, w->d_iab, w->d_ipts, w->d_lvl, w->d_bpt, w->d_clane};
+  for (void *p : ptrs)
+    if (p) cudaFree(p);
+  if (w->own_stream && w->stream) cudaStreamDestroy(w->stream);
+  delete w;
+}

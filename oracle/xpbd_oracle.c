@@ -317,11 +317,21 @@ void or_world_stats(const or_world *w, double *maxSpeed, double *maxAngSpeed,
  * groupConstraintsByColor (core.js:276-288)
  * ==================================================================== */
 int or_assign_color(uint32_t *mask, int a, int b) {
-  uint32_t used = mask[a] | (b >= 0 ? mask[b] : 0u);
+  return or_assign_color_n(mask, 0x7fffffff, a, b);
+}
+
+/* assignColor over a mask of n entries with Uint32Array semantics: reads
+ * past the end give 0, writes past the end are dropped (createSim's mask
+ * has 1 << 16 entries, core.js:45) */
+int or_assign_color_n(uint32_t *mask, int n, int a, int b) {
+  uint32_t ma = a < n ? mask[a] : 0u;
+  uint32_t mb = (b >= 0 && b < n) ? mask[b] : 0u;
+  uint32_t used = ma | mb;
   int c = 0;
-  while (used & (1u << c)) c++;
-  mask[a] |= 1u << c;
-  if (b >= 0) mask[b] |= 1u << c;
+  while (c < 32 && (used & (1u << c))) c++;
+  if (c >= 32) c = 31;
+  if (a < n) mask[a] = ma | (1u << c);
+  if (b >= 0 && b < n) mask[b] = mb | (1u << c);
   return c;
 }
 
@@ -1246,7 +1256,7 @@ or_sim *or_sim_create(uint32_t seed, int creatures, double width, double height,
     or_spawn_kraken(s->w, x, y, ang, arms, segs, B_SPAWN_CURL, &s->cr[i].k);
     for (int id = 0; id < s->w->nC; id++) {
       orc_t *c = &s->w->cons[id];
-      if (c->color < 0) c->color = or_assign_color(mask, c->a, c->b >= 0 ? c->b : -1);
+      if (c->color < 0) c->color = or_assign_color_n(mask, 1 << 16, c->a, c->b >= 0 ? c->b : -1);
     }
     s->cr[i].tone = 0.5;
   }

@@ -81,6 +81,7 @@ void or_world_stats(const or_world *w, double *maxSpeed, double *maxAngSpeed,
                     int *nan, long *collisions, int *broken);
 
 int or_assign_color(uint32_t *mask, int a, int b);
+int or_assign_color_n(uint32_t *mask, int n, int a, int b);
 void or_ensure_colored(or_world *w);
 void or_group_by_color(or_world *w);
 
