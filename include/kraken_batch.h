@@ -1,0 +1,129 @@
+/*
+ * kraken_batch.h -- batched creature engine on B200 (sm_100a).
+ *
+ * Many independent creatures of uneven body shape, on many maps, each with
+ * its own horizon, advanced by one persistent kernel per call: one warp per
+ * creature, creatures of one body shape grouped per CTA, a device work queue
+ * over the groups.  The suction-cup reflex (applyControl, src/sim/core.js:
+ * 183-220) and the proprioception vector (readProprio, core.js:129-175) run
+ * on the device in f64, exactly as the reference's hybrid trainer runs them
+ * on the CPU over the f32 GPU state (src/sim/gputrain.js:72-128), so every
+ * creature behaves bit for bit like a one-creature gpuworld.js world driven
+ * by that loop.
+ *
+ * Per env step and creature: proprioception of the current state -> obs ring
+ * (optional) -> controls (device stream, host buffer or fused policy) ->
+ * reflex -> substeps x iterations of the XPBD step -> grip break.
+ *
+ * Plain pointers and sizes; every call returns KR_OK (0) or a KR_ERR_* code
+ * of kraken_b200.h; the handle is not thread-safe (one host thread, one
+ * stream).
+ */
+#ifndef KRAKEN_BATCH_H
+#define KRAKEN_BATCH_H
+#include <stdint.h>
+
+#include "kraken_b200.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define KR_BATCH_MAX_ARMS 8
+#define KR_BATCH_MAX_SEGS 9
+#define KR_OBS_STRIDE 56   /* 6 * arms + 6 proprio values (f32), ..., word 55 = grip flags */
+
+/* control sources */
+#define KR_CTRL_STREAM 0   /* per-creature mulberry32 stream, redrawn every period steps */
+#define KR_CTRL_BUFFER 1   /* host-provided buffer, one record per creature (kr_batch_set_controls) */
+#define KR_CTRL_POLICY 2   /* fused per-creature MLP on the proprioception vector */
+
+typedef struct kr_batch kr_batch;
+
+typedef struct kr_batch_desc {
+  kr_solver_params solver;     /* shared by all creatures */
+  int32_t n_maps;              /* >= 1 */
+  const float *rects;          /* every map's rects, x y w h (f32) */
+  const int32_t *map_rect_off; /* n_maps + 1 offsets into rects (in rects) */
+  int32_t capacity;            /* creature slots */
+  int32_t obs_ring;            /* steps kept in each creature's observation ring (0: none) */
+  double grip_slip_max;        /* px/s, core.js:30 */
+  double grip_cooldown;        /* s, core.js:31 */
+  int32_t control_mode;        /* KR_CTRL_* */
+  int32_t control_period;      /* KR_CTRL_STREAM: steps between redraws (>= 1) */
+} kr_batch_desc;
+
+int kr_batch_create(const kr_batch_desc *desc, kr_batch **out);
+
+/* Spawn (or respawn) creatures into slots [first, first + n): body shape
+ * arms x segs, the spawnKraken pose at (x, y, angle) (src/body/kraken.js:
+ * 64-101), zero velocity, every grip released, motor targets 0, muscle tone
+ * `tone` (compliance 1 / (2000 + tone * 398000), kraken.js:186-191), step
+ * counter 0 and the given horizon; control_seed seeds the slot's control
+ * stream (mulberry32, src/world/map.js:11-20).  Asynchronous. */
+int kr_batch_spawn(kr_batch *b, int32_t first, int32_t n, const int32_t *arms,
+                   const int32_t *segs, const int32_t *map_id, const double *x, const double *y,
+                   const double *angle, const int32_t *horizon, const uint32_t *control_seed,
+                   const float *tone);
+
+/* KR_CTRL_BUFFER: the control record of every slot, capacity x record floats,
+ * record = arms * segs motor targets (arm-major, shoulder first) then arms
+ * adhesion values, laid out at stride KR_BATCH_MAX_ARMS * (KR_BATCH_MAX_SEGS + 1).
+ * Copied host->device on the handle's stream; used by every following step
+ * until replaced. */
+int kr_batch_set_controls(kr_batch *b, const float *controls);
+
+/* KR_CTRL_POLICY: the fused controller of every slot.  weights holds
+ * n_individuals parameter vectors of n_params floats each; slot s uses
+ * vector slot_individual[s] (capacity entries).  Layout per vector, row-major
+ * with the bias last: W1 (KR_POLICY_HIDDEN x (n_in + 1)) then W2
+ * (n_out x (KR_POLICY_HIDDEN + 1)), n_in = 6 * arms + 6 (the proprioception
+ * vector), n_out = arms * segs motor targets (tanh) + arms adhesion values
+ * ((tanh + 1) / 2).  Copied host->device on the handle's stream. */
+#define KR_POLICY_HIDDEN 64
+int kr_batch_set_policy(kr_batch *b, const float *weights, int32_t n_individuals, int32_t n_params,
+                        const int32_t *slot_individual);
+
+/* Advance every live slot by min(max_steps, horizon - step) env steps with
+ * one persistent launch.  Asynchronous; returns once enqueued. */
+int kr_batch_run(kr_batch *b, int32_t max_steps);
+
+/* Capture `launches` consecutive kr_batch_run(max_steps) calls into one CUDA
+ * graph and replay it `replays` times. */
+int kr_batch_run_graph(kr_batch *b, int32_t max_steps, int32_t launches, int32_t replays);
+
+/* Number of slots whose step counter is below their horizon (synchronous). */
+int kr_batch_live(kr_batch *b, int32_t *live);
+
+/* Copy the state of slots [first, first + n) to the host (synchronous):
+ * bodies: n x (1 + 8 * 9) x 6 f32 (px py vx vy ang av per body, template
+ * body order), grips: n x 8 x 4 f32 (lbx lby breakForce broken), steps: n
+ * i32.  Any pointer may be NULL. */
+int kr_batch_read_state(kr_batch *b, int32_t first, int32_t n, float *bodies, float *grips,
+                        int32_t *steps);
+
+/* Copy the observation rings of slots [first, first + n) to the host
+ * (synchronous): n x obs_ring x KR_OBS_STRIDE f32, entry t % obs_ring holds
+ * the proprioception read at the start of env step t. */
+int kr_batch_read_obs(kr_batch *b, int32_t first, int32_t n, float *obs);
+
+/* Per-slot accumulators (synchronous): n x 4 f64 -- path length of the
+ * mantle, x and y of the mantle, attach events. */
+int kr_batch_read_fitness(kr_batch *b, int32_t first, int32_t n, double *out);
+
+/* Launch shape: warps (creatures) per CTA (1..16) and CTAs per SM
+ * (0 = as many as fit). */
+int kr_batch_set_launch(kr_batch *b, int32_t warps_per_cta, int32_t ctas_per_sm);
+
+/* Device time of the last kr_batch_run launch in ms (synchronous). */
+int kr_batch_last_ms(kr_batch *b, float *ms);
+
+int kr_batch_sync(kr_batch *b);
+int kr_batch_set_stream(kr_batch *b, void *stream);
+void kr_batch_destroy(kr_batch *b);
+const char *kr_batch_last_error(const kr_batch *b);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,205 @@
+"""Batched creature engine (include/kraken_batch.h) from Python.
+
+    eng = BatchEngine(maps, capacity=16384, obs_ring=0, control="stream")
+    eng.spawn(0, arms, segs, map_id, x, y, angle, horizon, seed)
+    eng.run(200)                      # one persistent launch, <= 200 steps each
+    state = eng.read_state(0, 16)     # bodies (px py vx vy ang av), grips, steps
+
+Every creature behaves like a one-creature gpuworld world driven by the
+reference's hybrid loop (readProprio -> controls -> applyControl reflex ->
+step, src/sim/gputrain.js:72-128), with the reflex and the proprioception on
+the device.  There is no CPU fallback: without the CUDA library every call
+raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _native
+
+MAX_ARMS = 8
+MAX_SEGS = 9
+MAX_BODIES = 1 + MAX_ARMS * MAX_SEGS
+OBS_STRIDE = 56
+CTRL_STRIDE = MAX_ARMS * (MAX_SEGS + 1)
+POLICY_HIDDEN = 64
+CONTROL_MODES = {"stream": 0, "buffer": 1, "policy": 2}
+
+_F32P = C.POINTER(C.c_float)
+_F64P = C.POINTER(C.c_double)
+_I32P = C.POINTER(C.c_int32)
+_U32P = C.POINTER(C.c_uint32)
+
+
+class BatchDesc(C.Structure):
+    _fields_ = [("solver", _native.SolverParams), ("n_maps", C.c_int32),
+                ("rects", _F32P), ("map_rect_off", _I32P), ("capacity", C.c_int32),
+                ("obs_ring", C.c_int32), ("grip_slip_max", C.c_double),
+                ("grip_cooldown", C.c_double), ("control_mode", C.c_int32),
+                ("control_period", C.c_int32)]
+
+
+_bound = False
+
+
+def _lib():
+    global _bound
+    L = _native.lib()
+    if _bound:
+        return L
+    vp, i32 = C.c_void_p, C.c_int32
+    sigs = {
+        "kr_batch_create": (C.c_int, [C.POINTER(BatchDesc), C.POINTER(vp)]),
+        "kr_batch_spawn": (C.c_int, [vp, i32, i32, _I32P, _I32P, _I32P, _F64P, _F64P, _F64P,
+                                     _I32P, _U32P, _F32P]),
+        "kr_batch_set_controls": (C.c_int, [vp, _F32P]),
+        "kr_batch_set_policy": (C.c_int, [vp, _F32P, i32, i32, _I32P]),
+        "kr_batch_run": (C.c_int, [vp, i32]),
+        "kr_batch_run_graph": (C.c_int, [vp, i32, i32, i32]),
+        "kr_batch_live": (C.c_int, [vp, _I32P]),
+        "kr_batch_read_state": (C.c_int, [vp, i32, i32, _F32P, _F32P, _I32P]),
+        "kr_batch_read_obs": (C.c_int, [vp, i32, i32, _F32P]),
+        "kr_batch_read_fitness": (C.c_int, [vp, i32, i32, _F64P]),
+        "kr_batch_set_launch": (C.c_int, [vp, i32, i32]),
+        "kr_batch_last_ms": (C.c_int, [vp, _F32P]),
+        "kr_batch_sync": (C.c_int, [vp]),
+        "kr_batch_set_stream": (C.c_int, [vp, vp]),
+        "kr_batch_destroy": (None, [vp]),
+        "kr_batch_last_error": (C.c_char_p, [vp]),
+    }
+    for name, (res, args) in sigs.items():
+        fn = getattr(L, name)
+        fn.restype = res
+        fn.argtypes = args
+    _bound = True
+    return L
+
+
+def _check(rc, handle):
+    if rc != _native.KR_OK:
+        msg = _lib().kr_batch_last_error(handle)
+        raise _native.KrError(rc, msg.decode() if msg else f"status {rc}")
+
+
+def _arr(a, dtype):
+    return np.ascontiguousarray(np.asarray(a), dtype=dtype)
+
+
+class BatchEngine:
+    """One batched engine handle (kr_batch)."""
+
+    def __init__(self, maps, capacity, obs_ring=0, control="stream", control_period=6,
+                 substeps=2, iterations=4, h=1 / 120, lin_drag=3.0, ang_drag=3.0,
+                 max_speed=360.0, max_ang_speed=18.0, grip_slip_max=150.0, grip_cooldown=0.05):
+        L = _lib()
+        rect_list = [np.asarray(m, dtype=np.float32).reshape(-1, 4) for m in maps]
+        off = np.zeros(len(rect_list) + 1, dtype=np.int32)
+        for i, r in enumerate(rect_list):
+            off[i + 1] = off[i] + len(r)
+        rects = np.ascontiguousarray(np.concatenate(rect_list) if rect_list else
+                                     np.zeros((0, 4), np.float32), dtype=np.float32)
+        self.capacity = int(capacity)
+        self.obs_ring = int(obs_ring)
+        self.control = control
+        d = BatchDesc(_native.SolverParams(h, substeps, iterations, lin_drag, ang_drag, max_speed,
+                                           max_ang_speed),
+                      len(rect_list), rects.ctypes.data_as(_F32P), off.ctypes.data_as(_I32P),
+                      self.capacity, self.obs_ring, grip_slip_max, grip_cooldown,
+                      CONTROL_MODES[control], control_period)
+        self.h = C.c_void_p()
+        rc = L.kr_batch_create(C.byref(d), C.byref(self.h))
+        _check(rc, None)
+        self.arms = np.zeros(self.capacity, dtype=np.int32)
+        self.segs = np.zeros(self.capacity, dtype=np.int32)
+
+    def close(self):
+        if getattr(self, "h", None) and self.h.value:
+            _lib().kr_batch_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def spawn(self, first, arms, segs, map_id, x, y, angle, horizon, seed=None, tone=None):
+        n = len(x)
+        arms, segs = _arr(arms, np.int32), _arr(segs, np.int32)
+        map_id, horizon = _arr(map_id, np.int32), _arr(horizon, np.int32)
+        x, y, angle = _arr(x, np.float64), _arr(y, np.float64), _arr(angle, np.float64)
+        seed = _arr(np.arange(first, first + n) if seed is None else seed, np.uint32)
+        tone = _arr(np.full(n, 0.5) if tone is None else tone, np.float32)
+        rc = _lib().kr_batch_spawn(self.h, first, n, arms.ctypes.data_as(_I32P),
+                                   segs.ctypes.data_as(_I32P), map_id.ctypes.data_as(_I32P),
+                                   x.ctypes.data_as(_F64P), y.ctypes.data_as(_F64P),
+                                   angle.ctypes.data_as(_F64P), horizon.ctypes.data_as(_I32P),
+                                   seed.ctypes.data_as(_U32P), tone.ctypes.data_as(_F32P))
+        _check(rc, self.h)
+        self.arms[first:first + n] = arms
+        self.segs[first:first + n] = segs
+
+    def set_controls(self, controls):
+        c = _arr(controls, np.float32).reshape(self.capacity, CTRL_STRIDE)
+        _check(_lib().kr_batch_set_controls(self.h, c.ctypes.data_as(_F32P)), self.h)
+
+    def set_policy(self, weights, slot_individual):
+        w = _arr(weights, np.float32)
+        w = w.reshape(w.shape[0], -1)
+        idx = _arr(slot_individual, np.int32)
+        _check(_lib().kr_batch_set_policy(self.h, w.ctypes.data_as(_F32P), w.shape[0], w.shape[1],
+                                          idx.ctypes.data_as(_I32P)), self.h)
+
+    def set_launch(self, warps_per_cta, ctas_per_sm=0):
+        _check(_lib().kr_batch_set_launch(self.h, warps_per_cta, ctas_per_sm), self.h)
+
+    def run(self, max_steps):
+        _check(_lib().kr_batch_run(self.h, max_steps), self.h)
+
+    def run_graph(self, max_steps, launches, replays=1):
+        _check(_lib().kr_batch_run_graph(self.h, max_steps, launches, replays), self.h)
+
+    def sync(self):
+        _check(_lib().kr_batch_sync(self.h), self.h)
+
+    def last_ms(self) -> float:
+        ms = C.c_float()
+        _check(_lib().kr_batch_last_ms(self.h, C.byref(ms)), self.h)
+        return ms.value
+
+    def live(self) -> int:
+        n = C.c_int32()
+        _check(_lib().kr_batch_live(self.h, C.byref(n)), self.h)
+        return n.value
+
+    def read_state(self, first=0, n=None):
+        n = self.capacity - first if n is None else n
+        bodies = np.zeros((n, MAX_BODIES, 6), dtype=np.float32)
+        grips = np.zeros((n, MAX_ARMS, 4), dtype=np.float32)
+        steps = np.zeros(n, dtype=np.int32)
+        _check(_lib().kr_batch_read_state(self.h, first, n, bodies.ctypes.data_as(_F32P),
+                                          grips.ctypes.data_as(_F32P),
+                                          steps.ctypes.data_as(_I32P)), self.h)
+        return {"px": bodies[..., 0], "py": bodies[..., 1], "vx": bodies[..., 2],
+                "vy": bodies[..., 3], "ang": bodies[..., 4], "av": bodies[..., 5],
+                "grips": grips, "steps": steps}
+
+    def read_obs(self, first=0, n=None):
+        n = self.capacity - first if n is None else n
+        out = np.zeros((n, self.obs_ring, OBS_STRIDE), dtype=np.float32)
+        _check(_lib().kr_batch_read_obs(self.h, first, n, out.ctypes.data_as(_F32P)), self.h)
+        return out
+
+    def read_fitness(self, first=0, n=None):
+        n = self.capacity - first if n is None else n
+        out = np.zeros((n, 4), dtype=np.float64)
+        _check(_lib().kr_batch_read_fitness(self.h, first, n, out.ctypes.data_as(_F64P)), self.h)
+        return out
+
+
+def policy_params(arms=6, segs=7) -> int:
+    """Parameter count of the fused controller for an arms x segs body."""
+    n_in, n_out = 6 * arms + 6, arms * segs + arms
+    return POLICY_HIDDEN * (n_in + 1) + n_out * (POLICY_HIDDEN + 1)

@@ -16,7 +16,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "libkraken_b200.so")
-SOURCES = ["kr_world.cu"]
+SOURCES = ["kr_world.cu", "kr_batch.cu", "kr_template.cpp"]
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
     "-lineinfo", "-O3", "-std=c++17", "-fmad=false",
@@ -32,7 +32,9 @@ def nvcc() -> str:
 def build(verbose: bool = False, force: bool = False) -> str:
     srcs = [os.path.join(CSRC, s) for s in SOURCES]
     deps = srcs + [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith(".cuh")]
-    deps.append(os.path.join(os.path.dirname(HERE), "include", "kraken_b200.h"))
+    deps += [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith(".h")]
+    inc = os.path.join(os.path.dirname(HERE), "include")
+    deps += [os.path.join(inc, f) for f in os.listdir(inc)]
     if not force and os.path.exists(OUT):
         t = os.path.getmtime(OUT)
         if all(os.path.getmtime(d) <= t for d in deps):

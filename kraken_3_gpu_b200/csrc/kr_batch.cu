@@ -1,0 +1,1071 @@
+// kr_batch.cu -- the batched creature engine (include/kraken_batch.h).
+//
+// Work unit: a group of up to W creatures of one body template.  A CTA of W
+// warps takes a group from a device queue, stages the template's static
+// arrays once in shared memory, and each warp advances one creature for the
+// whole run (up to max_steps env steps) with its state in shared memory and
+// registers.  Groups are queued longest-remaining-horizon first so the tail
+// of a run is short.  Per env step the warp computes the proprioception of
+// the current state (f64, lanes over arms), draws or reads the controls,
+// runs the suction-cup reflex (f64, lane per arm), then the XPBD step of
+// kr_solver.cuh (f32 in f32solver.mjs op order) and the grip break.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <string>
+#include <vector>
+
+#include "../../include/kraken_batch.h"
+#include "kr_solver.cuh"
+#include "kr_template.h"
+
+namespace {
+
+constexpr int kMaxW = 16;
+constexpr int kBodyPad = 76;                                   // >= kMaxTplBodies, /4
+constexpr int kStateStride = 6 * kBodyPad;                     // px py vx vy ang av
+constexpr int kCtrlStride = KR_BATCH_MAX_ARMS * (KR_BATCH_MAX_SEGS + 1);  // 80
+constexpr double kPiD = 3.141592653589793;
+constexpr double kSegHalf = 13.5 * 0.5;                        // tipPosition L
+
+struct TplDev {
+  int nb, nc, np, nlv, arms, segs;
+  float r_max;
+  float pad0;
+  double reach;
+  int o_b, o_c, o_l, o_p, o_a, o_s;
+};
+
+struct TplArrays {
+  const float *im, *ii;
+  const int *boff, *bcnt;
+  const int *ab, *type, *motor;
+  const float *lax, *lay, *lbx, *lby, *rest, *minA, *maxA;
+  const int *lvl;
+  const float *plx, *ply, *pr;
+  const int *pbody;
+  const int *arm_tip, *arm_grip, *arm_seg0, *arm_segs;
+};
+
+struct SlotMeta {
+  int tpl, map, horizon, step;
+  uint32_t rng;
+  float comp;       // muscle compliance (f32 as packControls writes it)
+  float tone;
+  int attach_events;
+  double prev_vx, prev_vy;
+  double path_len;
+  double last_x, last_y;
+};
+
+struct BatchArgs {
+  kr::SolverConsts K;
+  const TplDev *tpl;
+  TplArrays T;
+  float *state;          // capacity x kStateStride
+  float4 *grip;          // capacity x 8: lbx lby brk broken
+  float2 *glam;          // capacity x 8: grip lambda after the last substep
+  double *cd;            // capacity x 8
+  float *ctrl_cur;       // capacity x kCtrlStride: the controls in use
+  SlotMeta *meta;
+  const float4 *rects;   // x y x+w y+h
+  const int *map_off;    // n_maps + 1
+  const float *map_cull; // per map cull distance
+  const int *groups;     // n_groups x W slot ids, -1 = empty
+  int n_groups;
+  int W;
+  int *queue;            // group counter
+  int max_steps;
+  int ctrl_mode;
+  int ctrl_period;
+  float *obs;            // capacity x ring x KR_OBS_STRIDE
+  int obs_ring;
+  double slip_max, cooldown, inv_h64, dt;
+  // policy
+  const float *pw;       // n_individuals x n_params
+  const int *pw_idx;     // individual of each slot
+  int n_params;
+  // smem carve sizes
+  int mb, mc, mp;
+};
+
+// --- shared-memory layout -------------------------------------------------
+constexpr int kLvlWords = (kr::kMaxTplLevels + 1 + 3) & ~3;                 // 68
+constexpr int kArmWords = (3 * KR_BATCH_MAX_ARMS + KR_BATCH_MAX_ARMS * KR_BATCH_MAX_SEGS + 3) & ~3;
+constexpr int kPairDoubles = KR_BATCH_MAX_ARMS * (KR_BATCH_MAX_SEGS - 1);      // 64
+// every region a multiple of 4 words, so each region and each warp's base
+// stay 16-byte aligned (the f64 region included)
+__host__ __device__ inline int tpl_smem_words(int mb, int mc, int mp) {
+  return 5 * mb + 10 * mc + kLvlWords + 4 * mp + kArmWords;
+}
+__host__ __device__ inline int warp_smem_words(int mb, int mc, int mp) {
+  return 11 * mb + 8 * mc + 3 * mp + kr::kMaxCulled / 2 + kCtrlStride + 64 + 2 * kPairDoubles;
+}
+
+struct TplSmem {
+  float *im, *ii, *zero;
+  int *boff, *bcnt, *ab, *type, *motor;
+  float *lax, *lay, *lbx, *lby, *rest, *minA, *maxA;
+  int *lvl;
+  float *plx, *ply, *pr;
+  int *pbody;
+  int *arm_tip, *arm_grip, *arm_seg0, *arm_segs;
+};
+
+__device__ inline void carve_tpl(TplSmem &P, float *p, int mb, int mc, int mp) {
+  P.im = p; p += mb; P.ii = p; p += mb; P.zero = p; p += mb;
+  P.boff = reinterpret_cast<int *>(p); p += mb;
+  P.bcnt = reinterpret_cast<int *>(p); p += mb;
+  P.ab = reinterpret_cast<int *>(p); p += mc;
+  P.type = reinterpret_cast<int *>(p); p += mc;
+  P.motor = reinterpret_cast<int *>(p); p += mc;
+  P.lax = p; p += mc; P.lay = p; p += mc; P.lbx = p; p += mc; P.lby = p; p += mc;
+  P.rest = p; p += mc; P.minA = p; p += mc; P.maxA = p; p += mc;
+  P.lvl = reinterpret_cast<int *>(p); p += kLvlWords;
+  P.plx = p; p += mp; P.ply = p; p += mp; P.pr = p; p += mp;
+  P.pbody = reinterpret_cast<int *>(p); p += mp;
+  P.arm_tip = reinterpret_cast<int *>(p); p += KR_BATCH_MAX_ARMS;
+  P.arm_grip = reinterpret_cast<int *>(p); p += KR_BATCH_MAX_ARMS;
+  P.arm_seg0 = reinterpret_cast<int *>(p); p += KR_BATCH_MAX_ARMS;
+  P.arm_segs = reinterpret_cast<int *>(p);
+}
+
+struct WarpSmem {
+  float *ctrl;     // kCtrlStride
+  float *obs;      // 64
+  double *pair;    // kPairDoubles: atan2 terms of armCurl
+};
+
+__device__ inline void carve_warp(kr::Island &S, WarpSmem &X, const TplSmem &P, float *p, int mb,
+                                  int mc, int mp) {
+  S.px = p; p += mb; S.py = p; p += mb; S.ppx = p; p += mb; S.ppy = p; p += mb;
+  S.vx = p; p += mb; S.vy = p; p += mb; S.ang = p; p += mb; S.angP = p; p += mb;
+  S.av = p; p += mb; S.bs = p; p += mb; S.bc = p; p += mb;
+  S.tb = reinterpret_cast<int *>(p); p += mc;
+  S.lbx = p; p += mc; S.lby = p; p += mc; S.comp = p; p += mc; S.tgt = p; p += mc;
+  S.lamX = p; p += mc; S.lamY = p; p += mc; S.brk = p; p += mc;
+  S.lam = S.lamX;  // pins use lamX/lamY, angles lam: never both on one slot
+  S.pdx = p; p += mp; S.pdy = p; p += mp;
+  S.pflag = reinterpret_cast<int *>(p); p += mp;
+  S.cull = reinterpret_cast<short *>(p); p += kr::kMaxCulled / 2;
+  X.ctrl = p; p += kCtrlStride;
+  X.obs = p; p += 64;
+  X.pair = reinterpret_cast<double *>(p);
+  // statics shared by the CTA
+  S.im = P.im; S.ii = P.ii; S.fx = P.zero; S.fy = P.zero; S.tq = P.zero;
+  S.ab = P.ab; S.lax = P.lax; S.lay = P.lay; S.rest = P.rest; S.minA = P.minA; S.maxA = P.maxA;
+  S.plx = P.plx; S.ply = P.ply; S.pr = P.pr; S.pbody = P.pbody; S.boff = P.boff; S.bcnt = P.bcnt;
+  S.lvl = P.lvl;
+}
+
+__device__ inline double mulberry_next(uint32_t &s) {
+  s += 0x6D2B79F5u;
+  uint32_t t = s;
+  t = (t ^ (t >> 15)) * (t | 1u);
+  t ^= t + (t ^ (t >> 7)) * (t | 61u);
+  return (double)(t ^ (t >> 14)) / 4294967296.0;
+}
+
+__device__ inline double clamp_sym(double v, double m) { return v > m ? m : (v < -m ? -m : v); }
+
+// proprioception of the current state, readProprio (core.js:129-175), f64;
+// writes 6A+6 values into X.obs and returns the attached-arm bitmask
+__device__ unsigned proprio(const BatchArgs &A, const TplDev &td, const TplSmem &P, kr::Island &S,
+                            WarpSmem &X, SlotMeta &m, const float4 *grip_st, int lane) {
+  const int arms = td.arms, segs = td.segs;
+  const double cx = S.px[0], cy = S.py[0], cvx = S.vx[0], cvy = S.vy[0];
+  const double angle = S.ang[0], cav = S.av[0];
+  // armCurl terms: atan2(sin d, cos d) per adjacent segment pair
+  const int npair = arms * (segs - 1);
+  for (int q = lane; q < npair; q += 32) {
+    const int a = q / (segs - 1), i = q % (segs - 1) + 1;
+    const double d = (double)S.ang[P.arm_segs[a * segs + i]] - (double)S.ang[P.arm_segs[a * segs + i - 1]];
+    X.pair[q] = atan2(sin(d), cos(d));
+  }
+  __syncwarp();
+  double ext = 0.0, curl = 0.0, sh = 0.0, tx = 0.0, ty = 0.0;
+  bool attached = false;
+  if (lane < arms) {
+    const int a = lane;
+    double s = 0.0;
+    for (int i = 0; i < segs - 1; i++) s += X.pair[a * (segs - 1) + i];
+    curl = segs > 1 ? s / (segs - 1) : 0.0;
+    const int s0 = P.arm_seg0[a], tip = P.arm_tip[a];
+    const double d = (double)S.ang[s0] - angle;
+    sh = atan2(sin(d), cos(d));
+    const double ta = (double)S.ang[tip];
+    tx = (double)S.px[tip] + kSegHalf * cos(ta);
+    ty = (double)S.py[tip] + kSegHalf * sin(ta);
+    ext = fmin(1.0, hypot(tx - (double)S.px[s0], ty - (double)S.py[s0]) / fmax(1.0, td.reach));
+    attached = grip_st[a].w == 0.f;
+  }
+  const unsigned att = __ballot_sync(0xffffffffu, attached) & ((1u << arms) - 1u);
+  // sums in arm order, like the sequential loop
+  double ext_sum = 0.0;
+  for (int a = 0; a < arms; a++) ext_sum += __shfl_sync(0xffffffffu, ext, a);
+  const double ca = cos(-angle), sa = sin(-angle);
+  const double SL = kPiD * 0.62, JL = kPiD * 0.42;
+  if (lane < arms) {
+    const int a = lane;
+    X.obs[a] = (float)clamp_sym(sh / SL, 1.2);
+    X.obs[arms + a] = (float)clamp_sym(curl / JL, 1.2);
+    const double dx = tx - cx, dy = ty - cy;
+    X.obs[2 * arms + 2 * a] = (float)clamp_sym((dx * ca - dy * sa) / td.reach, 1.2);
+    X.obs[2 * arms + 2 * a + 1] = (float)clamp_sym((dx * sa + dy * ca) / td.reach, 1.2);
+    const float4 g = grip_st[a];
+    double force = 0.0;
+    if (g.w == 0.f) force = hypot((double)S.lamX[P.arm_grip[a]], (double)S.lamY[P.arm_grip[a]]) * A.inv_h64;
+    X.obs[4 * arms + a] = g.w != 0.f ? 0.f : (float)fmin(1.0, force / fmax(1.0, (double)g.z));
+    X.obs[5 * arms + a] = g.w != 0.f ? 0.f : 1.f;
+  }
+  if (lane == 0) {
+    const double ax = (cvx - m.prev_vx) / A.dt, ay = (cvy - m.prev_vy) / A.dt;
+    X.obs[6 * arms] = (float)fmax(-1.0, fmin(1.0, (ax * ca - ay * sa) / 600));
+    X.obs[6 * arms + 1] = (float)fmax(-1.0, fmin(1.0, (ax * sa + ay * ca) / 600));
+    m.prev_vx = cvx;
+    m.prev_vy = cvy;
+    X.obs[6 * arms + 2] = (float)((double)__popc(att) / arms);
+    X.obs[6 * arms + 3] = (float)(ext_sum / arms);
+    X.obs[6 * arms + 4] = (float)fmin(1.0, hypot(cvx, cvy) / 300);
+    X.obs[6 * arms + 5] = (float)fmax(-1.0, fmin(1.0, cav / 18));
+  }
+  __syncwarp();
+  return att;
+}
+
+// fused policy (one warp): proprio (n_in = 6A + 6) -> 64 tanh -> A*S motor
+// targets (tanh) + A adhesion values ((tanh + 1) / 2).  Weights of the
+// slot's individual, row-major with the bias last: W1 64 x (n_in + 1), then
+// W2 n_out x 65.
+__device__ void policy(const BatchArgs &A, const TplDev &td, WarpSmem &X, int slot, int lane) {
+  const int n_in = 6 * td.arms + 6, n_out = td.arms * td.segs + td.arms;
+  const float *w = A.pw + (size_t)A.pw_idx[slot] * A.n_params;
+  float hid[2];
+  for (int u = 0; u < 2; u++) {
+    const float *row = w + (size_t)(lane + 32 * u) * (n_in + 1);
+    float acc = __ldg(row + n_in);
+    for (int i = 0; i < n_in; i++) acc = fmaf(__ldg(row + i), X.obs[i], acc);
+    hid[u] = tanhf(acc);
+  }
+  const float *w2 = w + (size_t)KR_POLICY_HIDDEN * (n_in + 1);
+  for (int base = 0; base < n_out; base += 32) {
+    const int o = base + lane;
+    const float *row = w2 + (size_t)(o < n_out ? o : 0) * (KR_POLICY_HIDDEN + 1);
+    float acc = o < n_out ? __ldg(row + KR_POLICY_HIDDEN) : 0.f;
+    for (int j = 0; j < KR_POLICY_HIDDEN; j++) {
+      const float hj = __shfl_sync(0xffffffffu, hid[j >> 5], j & 31);
+      if (o < n_out) acc = fmaf(__ldg(row + j), hj, acc);
+    }
+    if (o < n_out) {
+      const float y = tanhf(acc);
+      X.ctrl[o] = o < td.arms * td.segs ? y : 0.5f * (y + 1.f);
+    }
+  }
+  __syncwarp();
+}
+
+__global__ void __launch_bounds__(32 * kMaxW) batch_kernel(BatchArgs A) {
+  extern __shared__ float smem[];
+  __shared__ int s_group;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  TplSmem P;
+  carve_tpl(P, smem, A.mb, A.mc, A.mp);
+  float *wbase = smem + tpl_smem_words(A.mb, A.mc, A.mp) + warp * warp_smem_words(A.mb, A.mc, A.mp);
+  for (;;) {
+    __syncthreads();
+    if (threadIdx.x == 0) s_group = atomicAdd(A.queue, 1);
+    __syncthreads();
+    const int g = s_group;
+    if (g >= A.n_groups) return;
+    const int first = A.groups[g * A.W];
+    const TplDev td = A.tpl[A.meta[first].tpl];
+    // stage the template statics (whole CTA)
+    for (int i = threadIdx.x; i < td.nb; i += blockDim.x) {
+      P.im[i] = A.T.im[td.o_b + i]; P.ii[i] = A.T.ii[td.o_b + i]; P.zero[i] = 0.f;
+      P.boff[i] = A.T.boff[td.o_b + i]; P.bcnt[i] = A.T.bcnt[td.o_b + i];
+    }
+    for (int k = threadIdx.x; k < td.nc; k += blockDim.x) {
+      const int o = td.o_c + k;
+      P.ab[k] = A.T.ab[o]; P.type[k] = A.T.type[o]; P.motor[k] = A.T.motor[o];
+      P.lax[k] = A.T.lax[o]; P.lay[k] = A.T.lay[o]; P.lbx[k] = A.T.lbx[o]; P.lby[k] = A.T.lby[o];
+      P.rest[k] = A.T.rest[o]; P.minA[k] = A.T.minA[o]; P.maxA[k] = A.T.maxA[o];
+    }
+    for (int l = threadIdx.x; l <= td.nlv; l += blockDim.x) P.lvl[l] = A.T.lvl[td.o_l + l];
+    for (int p = threadIdx.x; p < td.np; p += blockDim.x) {
+      P.plx[p] = A.T.plx[td.o_p + p]; P.ply[p] = A.T.ply[td.o_p + p]; P.pr[p] = A.T.pr[td.o_p + p];
+      P.pbody[p] = A.T.pbody[td.o_p + p];
+    }
+    for (int a = threadIdx.x; a < td.arms; a += blockDim.x) {
+      P.arm_tip[a] = A.T.arm_tip[td.o_a + a]; P.arm_grip[a] = A.T.arm_grip[td.o_a + a];
+      P.arm_seg0[a] = A.T.arm_seg0[td.o_a + a];
+    }
+    for (int q = threadIdx.x; q < td.arms * td.segs; q += blockDim.x) P.arm_segs[q] = A.T.arm_segs[td.o_s + q];
+    __syncthreads();
+
+    const int slot = warp < A.W ? A.groups[g * A.W + warp] : -1;
+    if (slot >= 0) {
+      kr::Island S;
+      WarpSmem X;
+      carve_warp(S, X, P, wbase, A.mb, A.mc, A.mp);
+      S.nb = td.nb; S.nc = td.nc; S.np = td.np; S.nlv = td.nlv;
+      SlotMeta m = A.meta[slot];
+      const int steps = min(A.max_steps, m.horizon - m.step);
+      const float *st = A.state + (size_t)slot * kStateStride;
+      float4 *gst = A.grip + (size_t)slot * KR_BATCH_MAX_ARMS;
+      float2 *glam = A.glam + (size_t)slot * KR_BATCH_MAX_ARMS;
+      double *cd = A.cd + (size_t)slot * KR_BATCH_MAX_ARMS;
+      if (steps > 0) {
+        for (int i = lane; i < td.nb; i += 32) {
+          S.px[i] = st[i]; S.py[i] = st[kBodyPad + i]; S.vx[i] = st[2 * kBodyPad + i];
+          S.vy[i] = st[3 * kBodyPad + i]; S.ang[i] = st[4 * kBodyPad + i]; S.av[i] = st[5 * kBodyPad + i];
+        }
+        for (int k = lane; k < td.nc; k += 32) {
+          const int ty = P.type[k];
+          S.tb[k] = ty;
+          S.lbx[k] = P.lbx[k]; S.lby[k] = P.lby[k];
+          S.comp[k] = ty == 1 ? m.comp : 0.f;
+          S.tgt[k] = 0.f;
+          S.brk[k] = 1e30f;
+          S.lamX[k] = 0.f; S.lamY[k] = 0.f;
+        }
+        __syncwarp();
+        if (lane < td.arms) {
+          const float4 gg = gst[lane];
+          const int k = P.arm_grip[lane];
+          S.lbx[k] = gg.x; S.lby[k] = gg.y; S.brk[k] = gg.z;
+          S.tb[k] = 2 | (gg.w != 0.f ? (1 << 8) : 0);
+          const float2 gl = glam[lane];
+          S.lamX[k] = gl.x; S.lamY[k] = gl.y;
+        }
+        if (A.ctrl_mode == KR_CTRL_BUFFER)
+          for (int q = lane; q < kCtrlStride; q += 32) X.ctrl[q] = A.ctrl_cur[(size_t)slot * kCtrlStride + q];
+        else if (A.ctrl_mode == KR_CTRL_STREAM)
+          for (int q = lane; q < kCtrlStride; q += 32) X.ctrl[q] = A.ctrl_cur[(size_t)slot * kCtrlStride + q];
+        __syncwarp();
+        const float4 *rects = A.rects + A.map_off[m.map];
+        const int nR = A.map_off[m.map + 1] - A.map_off[m.map];
+        const float cull_d = fmaxf(A.map_cull[m.map], td.r_max + 2.f + kr::kCullSlack + 1.f);
+        const int AS = td.arms * td.segs;
+        for (int s = 0; s < steps; s++) {
+          const int t = m.step;
+          // 1. proprioception of the current state
+          float4 gl = lane < td.arms ? make_float4(S.lbx[P.arm_grip[lane]], S.lby[P.arm_grip[lane]],
+                                                   S.brk[P.arm_grip[lane]],
+                                                   (S.tb[P.arm_grip[lane]] >> 8) ? 1.f : 0.f)
+                                     : make_float4(0.f, 0.f, 0.f, 0.f);
+          __shared__ float4 s_gl[kMaxW][KR_BATCH_MAX_ARMS];
+          if (lane < td.arms) s_gl[warp][lane] = gl;
+          __syncwarp();
+          if (A.obs_ring > 0 || A.ctrl_mode == KR_CTRL_POLICY) {
+            const unsigned att = proprio(A, td, P, S, X, m, s_gl[warp], lane);
+            if (A.obs_ring > 0) {
+              float *o = A.obs + ((size_t)slot * A.obs_ring + (t % A.obs_ring)) * KR_OBS_STRIDE;
+              for (int q = lane; q < 6 * td.arms + 6; q += 32) o[q] = X.obs[q];
+              if (lane == 0) o[KR_OBS_STRIDE - 1] = __uint_as_float(att);
+            }
+          }
+          // 2. controls
+          if (A.ctrl_mode == KR_CTRL_STREAM) {
+            if (t % A.ctrl_period == 0 && lane == 0) {
+              uint32_t r = m.rng;
+              for (int a = 0; a < td.arms; a++) {
+                for (int j = 0; j < td.segs; j++) X.ctrl[a * td.segs + j] = (float)(mulberry_next(r) * 2 - 1);
+                X.ctrl[AS + a] = (float)mulberry_next(r);
+              }
+              m.rng = r;
+            }
+          } else if (A.ctrl_mode == KR_CTRL_POLICY) {
+            policy(A, td, X, slot, lane);
+          }
+          __syncwarp();
+          // 3. applyControl: targets (clamped) and the reflex, core.js:183-220
+          for (int k = lane; k < td.nc; k += 32) {
+            const int mo = P.motor[k];
+            if (mo >= 0) {
+              const double lim = (mo % td.segs) == 0 ? kPiD * 0.62 : kPiD * 0.42;
+              S.tgt[k] = (float)fmax(-lim, fmin(lim, (double)X.ctrl[mo]));
+            }
+          }
+          bool attached_now = false;
+          if (lane < td.arms) {
+            const int a = lane, k = P.arm_grip[a], tip = P.arm_tip[a];
+            const double adh = fmax(0.0, fmin(1.0, (double)X.ctrl[AS + a]));
+            double c = cd[a];
+            if (c > 0) c -= A.dt;
+            if ((S.tb[k] >> 8) != 0) {
+              if (adh > 0.08 && c <= 0) {
+                const double slip = hypot((double)S.vx[tip], (double)S.vy[tip]);
+                if (slip < A.slip_max) {
+                  const double ta = (double)S.ang[tip];
+                  S.lbx[k] = (float)((double)S.px[tip] + kSegHalf * cos(ta));
+                  S.lby[k] = (float)((double)S.py[tip] + kSegHalf * sin(ta));
+                  S.tb[k] = 2;
+                  S.brk[k] = (float)(40.0 + 860.0 * adh);
+                  S.lamX[k] = 0.f; S.lamY[k] = 0.f;
+                  attached_now = true;
+                } else {
+                  c = A.cooldown;
+                }
+              }
+            } else {
+              S.brk[k] = (float)(40.0 + 860.0 * adh);
+              if (adh < 0.04) S.tb[k] = 2 | (1 << 8);
+            }
+            cd[a] = c;
+          }
+          m.attach_events += __popc(__ballot_sync(0xffffffffu, attached_now));
+          __syncwarp();
+          // 4. the XPBD step
+          kr::island_step(A.K, S, rects, nR, cull_d, lane);
+          // 5. bookkeeping
+          if (lane == 0) {
+            const double x = S.px[0], y = S.py[0];
+            m.path_len += hypot(x - m.last_x, y - m.last_y);
+            m.last_x = x; m.last_y = y;
+            m.step = t + 1;
+          }
+          m.step = t + 1;
+        }
+        // write back
+        float *sw = A.state + (size_t)slot * kStateStride;
+        for (int i = lane; i < td.nb; i += 32) {
+          sw[i] = S.px[i]; sw[kBodyPad + i] = S.py[i]; sw[2 * kBodyPad + i] = S.vx[i];
+          sw[3 * kBodyPad + i] = S.vy[i]; sw[4 * kBodyPad + i] = S.ang[i]; sw[5 * kBodyPad + i] = S.av[i];
+        }
+        if (lane < td.arms) {
+          const int k = P.arm_grip[lane];
+          gst[lane] = make_float4(S.lbx[k], S.lby[k], S.brk[k], (S.tb[k] >> 8) ? 1.f : 0.f);
+          glam[lane] = make_float2(S.lamX[k], S.lamY[k]);
+        }
+        for (int q = lane; q < kCtrlStride; q += 32) A.ctrl_cur[(size_t)slot * kCtrlStride + q] = X.ctrl[q];
+        if (lane == 0) A.meta[slot] = m;
+      }
+    }
+  }
+}
+
+__global__ void spawn_kernel(float *state, float4 *grip, float2 *glam, double *cd, SlotMeta *meta,
+                             float *ctrl, const float *pose, const SlotMeta *init, int first, int n) {
+  const int i = blockIdx.x;
+  if (i >= n) return;
+  const int slot = first + i;
+  const float *src = pose + (size_t)i * kStateStride;
+  float *dst = state + (size_t)slot * kStateStride;
+  for (int q = threadIdx.x; q < kStateStride; q += blockDim.x) dst[q] = src[q];
+  if (threadIdx.x < KR_BATCH_MAX_ARMS) {
+    grip[(size_t)slot * KR_BATCH_MAX_ARMS + threadIdx.x] = make_float4(0.f, 0.f, 0.f, 1.f);
+    glam[(size_t)slot * KR_BATCH_MAX_ARMS + threadIdx.x] = make_float2(0.f, 0.f);
+    cd[(size_t)slot * KR_BATCH_MAX_ARMS + threadIdx.x] = 0.0;
+  }
+  for (int q = threadIdx.x; q < kCtrlStride; q += blockDim.x) ctrl[(size_t)slot * kCtrlStride + q] = 0.f;
+  if (threadIdx.x == 0) meta[slot] = init[i];
+}
+
+}  // namespace
+
+struct kr_batch {
+  kr_batch_desc d{};
+  kr::SolverConsts K{};
+  std::string err;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  int capacity = 0, n_maps = 0;
+  // templates
+  std::vector<kr::Template> tpls;
+  std::map<std::pair<int, int>, int> tpl_index;
+  std::vector<TplDev> h_tpl;
+  TplDev *d_tpl = nullptr;
+  void *d_tpl_arrays[22] = {nullptr};
+  TplArrays T{};
+  int mb = 4, mc = 4, mp = 4;
+  // maps
+  float4 *d_rects = nullptr;
+  int *d_map_off = nullptr;
+  float *d_map_cull = nullptr;
+  std::vector<float> h_map_cull;
+  // slots
+  float *d_state = nullptr;
+  float4 *d_grip = nullptr;
+  float2 *d_glam = nullptr;
+  double *d_cd = nullptr;
+  float *d_ctrl = nullptr;
+  SlotMeta *d_meta = nullptr;
+  float *d_obs = nullptr;
+  std::vector<SlotMeta> h_meta;   // host mirror of tpl / map / horizon (step on device)
+  std::vector<int> h_remaining;   // remaining steps as of the last schedule
+  // groups
+  int *d_groups = nullptr;
+  size_t c_groups = 0;
+  int n_groups = 0;
+  bool groups_dirty = true;
+  int *d_queue = nullptr;
+  // launch shape
+  int W = 8, ctas_per_sm = 0, n_sm = 0;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  // policy
+  float *d_pw = nullptr;
+  int *d_pw_idx = nullptr;
+  int n_params = 0, n_individuals = 0;
+
+  int fail(int code, const std::string &m) { err = m; return code; }
+  int cuda_fail(cudaError_t e, const char *what) {
+    err = std::string("CUDA error in ") + what + ": " + cudaGetErrorString(e);
+    return KR_ERR_CUDA;
+  }
+};
+
+namespace {
+thread_local std::string g_batch_error;
+
+template <typename T>
+cudaError_t upload_vec(T **d, const std::vector<T> &v) {
+  if (*d) cudaFree(*d);
+  *d = nullptr;
+  cudaError_t e = cudaMalloc(reinterpret_cast<void **>(d), std::max<size_t>(v.size(), 1) * sizeof(T));
+  if (e != cudaSuccess || v.empty()) return e;
+  return cudaMemcpy(*d, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice);
+}
+
+int ensure_template(kr_batch *b, int arms, int segs) {
+  auto key = std::make_pair(arms, segs);
+  auto it = b->tpl_index.find(key);
+  if (it != b->tpl_index.end()) return it->second;
+  kr::Template t;
+  std::string err;
+  if (!kr::build_template(arms, segs, &t, &err)) return -1;
+  const int id = (int)b->tpls.size();
+  b->tpls.push_back(std::move(t));
+  b->tpl_index[key] = id;
+  return id;
+}
+
+int upload_templates(kr_batch *b) {
+  std::vector<float> im, ii, lax, lay, lbx, lby, rest, minA, maxA, plx, ply, pr;
+  std::vector<int> boff, bcnt, ab, type, motor, lvl, pbody, tip, grip, seg0, segs;
+  b->h_tpl.clear();
+  int mb = 4, mc = 4, mp = 4;
+  for (const auto &t : b->tpls) {
+    TplDev d{};
+    d.nb = t.nb; d.nc = t.nc; d.np = t.np; d.nlv = t.nlv; d.arms = t.arms; d.segs = t.segs;
+    d.r_max = t.r_max; d.reach = t.reach;
+    d.o_b = (int)im.size(); d.o_c = (int)ab.size(); d.o_l = (int)lvl.size(); d.o_p = (int)plx.size();
+    d.o_a = (int)tip.size(); d.o_s = (int)segs.size();
+    im.insert(im.end(), t.im.begin(), t.im.end()); ii.insert(ii.end(), t.ii.begin(), t.ii.end());
+    boff.insert(boff.end(), t.boff.begin(), t.boff.end()); bcnt.insert(bcnt.end(), t.bcnt.begin(), t.bcnt.end());
+    ab.insert(ab.end(), t.ab.begin(), t.ab.end()); type.insert(type.end(), t.type.begin(), t.type.end());
+    motor.insert(motor.end(), t.motor.begin(), t.motor.end());
+    lax.insert(lax.end(), t.lax.begin(), t.lax.end()); lay.insert(lay.end(), t.lay.begin(), t.lay.end());
+    lbx.insert(lbx.end(), t.lbx.begin(), t.lbx.end()); lby.insert(lby.end(), t.lby.begin(), t.lby.end());
+    rest.insert(rest.end(), t.rest.begin(), t.rest.end());
+    minA.insert(minA.end(), t.minA.begin(), t.minA.end()); maxA.insert(maxA.end(), t.maxA.begin(), t.maxA.end());
+    lvl.insert(lvl.end(), t.lvl.begin(), t.lvl.end());
+    plx.insert(plx.end(), t.plx.begin(), t.plx.end()); ply.insert(ply.end(), t.ply.begin(), t.ply.end());
+    pr.insert(pr.end(), t.pr.begin(), t.pr.end()); pbody.insert(pbody.end(), t.pbody.begin(), t.pbody.end());
+    tip.insert(tip.end(), t.arm_tip.begin(), t.arm_tip.end());
+    grip.insert(grip.end(), t.arm_grip.begin(), t.arm_grip.end());
+    seg0.insert(seg0.end(), t.arm_seg0.begin(), t.arm_seg0.end());
+    segs.insert(segs.end(), t.arm_segs.begin(), t.arm_segs.end());
+    b->h_tpl.push_back(d);
+    mb = std::max(mb, (t.nb + 3) & ~3); mc = std::max(mc, (t.nc + 3) & ~3); mp = std::max(mp, (t.np + 3) & ~3);
+  }
+  cudaError_t e = cudaSuccess;
+  void **A = b->d_tpl_arrays;
+#define UP(i, vec) if (e == cudaSuccess) e = upload_vec(reinterpret_cast<decltype(vec.data()) *>(&A[i]), vec)
+  UP(0, im); UP(1, ii); UP(2, boff); UP(3, bcnt); UP(4, ab); UP(5, type); UP(6, motor); UP(7, lax);
+  UP(8, lay); UP(9, lbx); UP(10, lby); UP(11, rest); UP(12, minA); UP(13, maxA); UP(14, lvl);
+  UP(15, plx); UP(16, ply); UP(17, pr); UP(18, pbody); UP(19, tip); UP(20, grip); UP(21, seg0);
+#undef UP
+  if (e != cudaSuccess) return b->cuda_fail(e, "upload(templates)");
+  int *d_segs = nullptr;
+  e = upload_vec(&d_segs, segs);
+  if (e != cudaSuccess) return b->cuda_fail(e, "upload(template segments)");
+  TplArrays &T = b->T;
+  T.im = (const float *)A[0]; T.ii = (const float *)A[1]; T.boff = (const int *)A[2]; T.bcnt = (const int *)A[3];
+  T.ab = (const int *)A[4]; T.type = (const int *)A[5]; T.motor = (const int *)A[6];
+  T.lax = (const float *)A[7]; T.lay = (const float *)A[8]; T.lbx = (const float *)A[9]; T.lby = (const float *)A[10];
+  T.rest = (const float *)A[11]; T.minA = (const float *)A[12]; T.maxA = (const float *)A[13];
+  T.lvl = (const int *)A[14]; T.plx = (const float *)A[15]; T.ply = (const float *)A[16]; T.pr = (const float *)A[17];
+  T.pbody = (const int *)A[18]; T.arm_tip = (const int *)A[19]; T.arm_grip = (const int *)A[20];
+  T.arm_seg0 = (const int *)A[21];
+  if (T.arm_segs) cudaFree(const_cast<int *>(T.arm_segs));
+  T.arm_segs = d_segs;
+  if ((e = upload_vec(&b->d_tpl, b->h_tpl)) != cudaSuccess) return b->cuda_fail(e, "upload(template table)");
+  b->mb = mb; b->mc = mc; b->mp = mp;
+  return KR_OK;
+}
+
+size_t smem_bytes(const kr_batch *b) {
+  return sizeof(float) * ((size_t)tpl_smem_words(b->mb, b->mc, b->mp) +
+                          (size_t)b->W * warp_smem_words(b->mb, b->mc, b->mp)) + 16;
+}
+
+// groups of up to W slots of one template, longest remaining horizon first
+int build_groups(kr_batch *b, const std::vector<int> &remaining) {
+  std::vector<int> live;
+  for (int s = 0; s < b->capacity; s++)
+    if (b->h_meta[s].horizon > 0 && remaining[s] > 0) live.push_back(s);
+  std::stable_sort(live.begin(), live.end(), [&](int x, int y) {
+    if (b->h_meta[x].tpl != b->h_meta[y].tpl) return b->h_meta[x].tpl < b->h_meta[y].tpl;
+    return remaining[x] > remaining[y];
+  });
+  std::vector<std::vector<int>> groups;
+  for (size_t i = 0; i < live.size();) {
+    std::vector<int> g;
+    const int t = b->h_meta[live[i]].tpl;
+    while (i < live.size() && (int)g.size() < b->W && b->h_meta[live[i]].tpl == t) g.push_back(live[i++]);
+    groups.push_back(g);
+  }
+  std::stable_sort(groups.begin(), groups.end(), [&](const std::vector<int> &x, const std::vector<int> &y) {
+    return remaining[x[0]] > remaining[y[0]];
+  });
+  std::vector<int> flat((size_t)groups.size() * b->W, -1);
+  for (size_t g = 0; g < groups.size(); g++)
+    for (size_t k = 0; k < groups[g].size(); k++) flat[g * b->W + k] = groups[g][k];
+  if (b->d_groups == nullptr || b->c_groups < std::max<size_t>(flat.size(), 1)) {
+    if (b->d_groups) cudaFree(b->d_groups);
+    b->d_groups = nullptr;
+    b->c_groups = std::max<size_t>(flat.size(), 1);
+    cudaError_t e = cudaMalloc(&b->d_groups, b->c_groups * sizeof(int));
+    if (e != cudaSuccess) return b->cuda_fail(e, "cudaMalloc(groups)");
+  }
+  if (!flat.empty()) {
+    cudaError_t e = cudaMemcpyAsync(b->d_groups, flat.data(), flat.size() * sizeof(int),
+                                    cudaMemcpyHostToDevice, b->stream);
+    if (e != cudaSuccess) return b->cuda_fail(e, "upload(groups)");
+    e = cudaStreamSynchronize(b->stream);
+    if (e != cudaSuccess) return b->cuda_fail(e, "upload(groups) sync");
+  }
+  b->n_groups = (int)groups.size();
+  b->groups_dirty = false;
+  return KR_OK;
+}
+
+}  // namespace
+
+extern "C" const char *kr_batch_last_error(const kr_batch *b) {
+  return b ? b->err.c_str() : g_batch_error.c_str();
+}
+
+extern "C" int kr_batch_create(const kr_batch_desc *desc, kr_batch **out) {
+  if (!desc || !out) { g_batch_error = "kr_batch_create: null argument"; return KR_ERR_INVALID; }
+  *out = nullptr;
+  const kr_batch_desc &d = *desc;
+  const kr_solver_params &p = d.solver;
+  const float hf = (float)p.h;
+  if (!(p.iterations >= 1 && p.iterations <= 64) || !(p.substeps >= 1 && p.substeps <= 64) ||
+      !(hf > 0.f && hf < 1.f)) {
+    g_batch_error = "implausible solver parameters (iterations 1..64, substeps 1..64, 0 < h < 1)";
+    return KR_ERR_INVALID;
+  }
+  if (d.n_maps < 1 || !d.rects || !d.map_rect_off) { g_batch_error = "need at least one map"; return KR_ERR_INVALID; }
+  if (d.capacity < 1 || d.capacity > (1 << 24)) { g_batch_error = "capacity out of range"; return KR_ERR_INVALID; }
+  if (d.obs_ring < 0 || d.obs_ring > 4096) { g_batch_error = "obs_ring out of range 0..4096"; return KR_ERR_INVALID; }
+  if (d.control_mode < 0 || d.control_mode > 2) { g_batch_error = "unknown control mode"; return KR_ERR_INVALID; }
+  if (d.control_mode == KR_CTRL_STREAM && d.control_period < 1) { g_batch_error = "control_period < 1"; return KR_ERR_INVALID; }
+  for (int m = 0; m < d.n_maps; m++) {
+    const int n = d.map_rect_off[m + 1] - d.map_rect_off[m];
+    if (d.map_rect_off[m] < 0 || !(n >= 1 && n <= 100000)) {
+      g_batch_error = "map " + std::to_string(m) + ": nRects implausible: " + std::to_string(n);
+      return KR_ERR_INVALID;
+    }
+  }
+  int dev = 0, n_dev = 0;
+  if (cudaGetDeviceCount(&n_dev) != cudaSuccess || n_dev == 0) {
+    cudaGetLastError();
+    g_batch_error = "no CUDA device available";
+    return KR_ERR_NODEVICE;
+  }
+  kr_batch *b = new kr_batch();
+  b->d = d;
+  b->d.rects = nullptr;
+  b->d.map_rect_off = nullptr;
+  b->capacity = d.capacity;
+  b->n_maps = d.n_maps;
+  kr::SolverConsts &K = b->K;
+  K.h = hf;
+  K.invH = (float)(1.0 / p.h);
+  K.invH2 = (float)(1.0 / (p.h * p.h));
+  const float nl = -(float)p.lin_drag, na = -(float)p.ang_drag;
+  K.linDamp = (float)std::exp((double)(nl * hf));
+  K.angDamp = (float)std::exp((double)(na * hf));
+  K.maxSpeed = (float)p.max_speed;
+  K.maxAngSpeed = (float)p.max_ang_speed;
+  K.substeps = p.substeps;
+  K.iterations = p.iterations;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&b->n_sm, cudaDevAttrMultiProcessorCount, dev);
+  auto bail = [&](cudaError_t e, const char *what) {
+    g_batch_error = std::string("CUDA error in ") + what + ": " + cudaGetErrorString(e);
+    kr_batch_destroy(b);
+    return KR_ERR_CUDA;
+  };
+  cudaError_t e;
+  if ((e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking)) != cudaSuccess) return bail(e, "cudaStreamCreate");
+  b->own_stream = true;
+  // maps: rects as x y x+w y+h, per-map culling distance (see kr_solver.cuh)
+  const int n_rects = d.map_rect_off[d.n_maps];
+  std::vector<float4> r4(n_rects);
+  std::vector<int> off(d.map_rect_off, d.map_rect_off + d.n_maps + 1);
+  b->h_map_cull.assign(d.n_maps, 0.f);
+  for (int m = 0; m < d.n_maps; m++) {
+    double ht = 0.0;
+    for (int i = off[m]; i < off[m + 1]; i++) {
+      const float x = d.rects[4 * i], y = d.rects[4 * i + 1], w = d.rects[4 * i + 2], h = d.rects[4 * i + 3];
+      r4[i] = make_float4(x, y, x + w, y + h);
+      const double t = 0.5 * std::min(std::fabs((double)w), std::fabs((double)h));
+      ht = std::isfinite(t) ? std::max(ht, t) : HUGE_VAL;
+    }
+    const double c = ht + 2.0 + kr::kCullSlack + 1.0;
+    b->h_map_cull[m] = std::isfinite(c) && c < 1e30 ? (float)c : 1e30f;
+  }
+  std::vector<float4> r4v(r4);
+  if ((e = upload_vec(&b->d_rects, r4v)) != cudaSuccess) return bail(e, "upload(rects)");
+  if ((e = upload_vec(&b->d_map_off, off)) != cudaSuccess) return bail(e, "upload(map offsets)");
+  if ((e = upload_vec(&b->d_map_cull, b->h_map_cull)) != cudaSuccess) return bail(e, "upload(map cull)");
+  const size_t C = (size_t)d.capacity;
+  if ((e = cudaMalloc(&b->d_state, C * kStateStride * sizeof(float))) != cudaSuccess) return bail(e, "cudaMalloc(state)");
+  if ((e = cudaMalloc(&b->d_grip, C * KR_BATCH_MAX_ARMS * sizeof(float4))) != cudaSuccess) return bail(e, "cudaMalloc(grips)");
+  if ((e = cudaMalloc(&b->d_glam, C * KR_BATCH_MAX_ARMS * sizeof(float2))) != cudaSuccess) return bail(e, "cudaMalloc(grip lambda)");
+  if ((e = cudaMalloc(&b->d_cd, C * KR_BATCH_MAX_ARMS * sizeof(double))) != cudaSuccess) return bail(e, "cudaMalloc(cooldown)");
+  if ((e = cudaMalloc(&b->d_ctrl, C * kCtrlStride * sizeof(float))) != cudaSuccess) return bail(e, "cudaMalloc(controls)");
+  if ((e = cudaMemset(b->d_ctrl, 0, C * kCtrlStride * sizeof(float))) != cudaSuccess) return bail(e, "cudaMemset(controls)");
+  if ((e = cudaMalloc(&b->d_meta, C * sizeof(SlotMeta))) != cudaSuccess) return bail(e, "cudaMalloc(meta)");
+  if ((e = cudaMemset(b->d_meta, 0, C * sizeof(SlotMeta))) != cudaSuccess) return bail(e, "cudaMemset(meta)");
+  if (d.obs_ring > 0) {
+    if ((e = cudaMalloc(&b->d_obs, C * d.obs_ring * KR_OBS_STRIDE * sizeof(float))) != cudaSuccess) return bail(e, "cudaMalloc(obs)");
+    if ((e = cudaMemset(b->d_obs, 0, C * d.obs_ring * KR_OBS_STRIDE * sizeof(float))) != cudaSuccess) return bail(e, "cudaMemset(obs)");
+  }
+  if ((e = cudaMalloc(&b->d_queue, sizeof(int))) != cudaSuccess) return bail(e, "cudaMalloc(queue)");
+  if ((e = cudaEventCreate(&b->ev0)) != cudaSuccess || (e = cudaEventCreate(&b->ev1)) != cudaSuccess) return bail(e, "cudaEventCreate");
+  b->h_meta.assign(C, SlotMeta{});
+  b->h_remaining.assign(C, 0);
+  // every slot starts empty (horizon 0)
+  *out = b;
+  return KR_OK;
+}
+
+extern "C" int kr_batch_spawn(kr_batch *b, int32_t first, int32_t n, const int32_t *arms,
+                              const int32_t *segs, const int32_t *map_id, const double *x,
+                              const double *y, const double *angle, const int32_t *horizon,
+                              const uint32_t *control_seed, const float *tone) {
+  if (!b) return KR_ERR_INVALID;
+  if (n <= 0) return KR_OK;
+  if (first < 0 || first + n > b->capacity) return b->fail(KR_ERR_INVALID, "spawn range outside the slots");
+  if (!arms || !segs || !map_id || !x || !y || !angle || !horizon)
+    return b->fail(KR_ERR_INVALID, "kr_batch_spawn: null argument");
+  const size_t tpl_before = b->tpls.size();
+  std::vector<float> pose((size_t)n * kStateStride, 0.f);
+  std::vector<SlotMeta> init(n);
+  std::vector<double> px(kr::kMaxTplBodies), py(kr::kMaxTplBodies), pa(kr::kMaxTplBodies);
+  for (int i = 0; i < n; i++) {
+    const int t = ensure_template(b, arms[i], segs[i]);
+    if (t < 0)
+      return b->fail(KR_ERR_INVALID, "creature " + std::to_string(first + i) + ": body shape " +
+                                         std::to_string(arms[i]) + "x" + std::to_string(segs[i]) +
+                                         " outside 1..8 arms x 1..9 segments");
+    if (map_id[i] < 0 || map_id[i] >= b->n_maps)
+      return b->fail(KR_ERR_INDEX, "creature " + std::to_string(first + i) + ": map " +
+                                       std::to_string(map_id[i]) + " of " + std::to_string(b->n_maps));
+    if (horizon[i] < 0) return b->fail(KR_ERR_INVALID, "negative horizon");
+    const kr::Template &T = b->tpls[t];
+    kr::spawn_pose(T, x[i], y[i], angle[i], 0.28, px.data(), py.data(), pa.data());
+    float *dst = pose.data() + (size_t)i * kStateStride;
+    for (int j = 0; j < T.nb; j++) {
+      dst[j] = (float)px[j];
+      dst[kBodyPad + j] = (float)py[j];
+      dst[4 * kBodyPad + j] = (float)pa[j];
+    }
+    SlotMeta &m = init[i];
+    m = SlotMeta{};
+    m.tpl = t;
+    m.map = map_id[i];
+    m.horizon = horizon[i];
+    m.step = 0;
+    m.rng = control_seed ? control_seed[i] : (uint32_t)(first + i);
+    const double tn = std::max(0.0, std::min(1.0, tone ? (double)tone[i] : 0.5));
+    m.tone = (float)tn;
+    m.comp = (float)(1.0 / (2000.0 + tn * (400000.0 - 2000.0)));
+    m.last_x = (double)(float)x[i];
+    m.last_y = (double)(float)y[i];
+    b->h_meta[first + i] = m;
+    b->h_remaining[first + i] = m.horizon;
+  }
+  if (b->tpls.size() != tpl_before) {
+    int rc = upload_templates(b);
+    if (rc != KR_OK) return rc;
+  }
+  float *d_pose = nullptr;
+  SlotMeta *d_init = nullptr;
+  cudaError_t e = cudaMallocAsync(&d_pose, pose.size() * sizeof(float), b->stream);
+  if (e == cudaSuccess) e = cudaMallocAsync(&d_init, init.size() * sizeof(SlotMeta), b->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(d_pose, pose.data(), pose.size() * sizeof(float), cudaMemcpyHostToDevice, b->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(d_init, init.data(), init.size() * sizeof(SlotMeta), cudaMemcpyHostToDevice, b->stream);
+  if (e == cudaSuccess) {
+    spawn_kernel<<<n, 128, 0, b->stream>>>(b->d_state, b->d_grip, b->d_glam, b->d_cd, b->d_meta, b->d_ctrl, d_pose, d_init, first, n);
+    e = cudaGetLastError();
+  }
+  if (d_pose) cudaFreeAsync(d_pose, b->stream);
+  if (d_init) cudaFreeAsync(d_init, b->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
+  if (e != cudaSuccess) return b->cuda_fail(e, "kr_batch_spawn");
+  b->groups_dirty = true;
+  return KR_OK;
+}
+
+extern "C" int kr_batch_set_controls(kr_batch *b, const float *controls) {
+  if (!b) return KR_ERR_INVALID;
+  if (!controls) return b->fail(KR_ERR_INVALID, "kr_batch_set_controls: null buffer");
+  cudaError_t e = cudaMemcpyAsync(b->d_ctrl, controls, (size_t)b->capacity * kCtrlStride * sizeof(float),
+                                  cudaMemcpyHostToDevice, b->stream);
+  if (e != cudaSuccess) return b->cuda_fail(e, "kr_batch_set_controls");
+  return KR_OK;
+}
+
+extern "C" int kr_batch_set_policy(kr_batch *b, const float *weights, int32_t n_individuals,
+                                   int32_t n_params, const int32_t *slot_individual) {
+  if (!b) return KR_ERR_INVALID;
+  if (!weights || !slot_individual || n_individuals <= 0 || n_params <= 0)
+    return b->fail(KR_ERR_INVALID, "kr_batch_set_policy: null argument or empty policy");
+  for (int s = 0; s < b->capacity; s++)
+    if (slot_individual[s] < 0 || slot_individual[s] >= n_individuals)
+      return b->fail(KR_ERR_INDEX, "slot " + std::to_string(s) + " refers to individual " +
+                                       std::to_string(slot_individual[s]) + " of " +
+                                       std::to_string(n_individuals));
+  const size_t need = (size_t)n_individuals * n_params;
+  if (!b->d_pw || (size_t)b->n_individuals * b->n_params < need) {
+    if (b->d_pw) cudaFree(b->d_pw);
+    b->d_pw = nullptr;
+    cudaError_t e = cudaMalloc(&b->d_pw, need * sizeof(float));
+    if (e != cudaSuccess) return b->cuda_fail(e, "cudaMalloc(policy weights)");
+  }
+  if (!b->d_pw_idx) {
+    cudaError_t e = cudaMalloc(&b->d_pw_idx, (size_t)b->capacity * sizeof(int));
+    if (e != cudaSuccess) return b->cuda_fail(e, "cudaMalloc(policy index)");
+  }
+  cudaError_t e = cudaMemcpyAsync(b->d_pw, weights, need * sizeof(float), cudaMemcpyHostToDevice, b->stream);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(b->d_pw_idx, slot_individual, (size_t)b->capacity * sizeof(int),
+                        cudaMemcpyHostToDevice, b->stream);
+  if (e != cudaSuccess) return b->cuda_fail(e, "kr_batch_set_policy");
+  b->n_individuals = n_individuals;
+  b->n_params = n_params;
+  return KR_OK;
+}
+
+extern "C" int kr_batch_set_launch(kr_batch *b, int32_t warps_per_cta, int32_t ctas_per_sm) {
+  if (!b) return KR_ERR_INVALID;
+  if (warps_per_cta < 1 || warps_per_cta > kMaxW) return b->fail(KR_ERR_INVALID, "warps_per_cta outside 1..16");
+  if (ctas_per_sm < 0 || ctas_per_sm > 64) return b->fail(KR_ERR_INVALID, "ctas_per_sm outside 0..64");
+  if (b->W != warps_per_cta) b->groups_dirty = true;
+  b->W = warps_per_cta;
+  b->ctas_per_sm = ctas_per_sm;
+  return KR_OK;
+}
+
+namespace {
+int launch(kr_batch *b, int max_steps, bool timed) {
+  if (b->tpls.empty()) return KR_OK;
+  if (b->d.control_mode == KR_CTRL_POLICY && !b->d_pw)
+    return b->fail(KR_ERR_STATE, "policy control without kr_batch_set_policy");
+  if (b->groups_dirty) {
+    int rc = build_groups(b, b->h_remaining);
+    if (rc != KR_OK) return rc;
+  }
+  if (b->n_groups == 0) return KR_OK;
+  BatchArgs A{};
+  A.K = b->K;
+  A.tpl = b->d_tpl;
+  A.T = b->T;
+  A.state = b->d_state; A.grip = b->d_grip; A.glam = b->d_glam; A.cd = b->d_cd; A.ctrl_cur = b->d_ctrl; A.meta = b->d_meta;
+  A.rects = b->d_rects; A.map_off = b->d_map_off; A.map_cull = b->d_map_cull;
+  A.groups = b->d_groups; A.n_groups = b->n_groups; A.W = b->W; A.queue = b->d_queue;
+  A.max_steps = max_steps;
+  A.ctrl_mode = b->d.control_mode; A.ctrl_period = std::max(1, b->d.control_period);
+  A.obs = b->d_obs; A.obs_ring = b->d.obs_ring;
+  A.slip_max = b->d.grip_slip_max; A.cooldown = b->d.grip_cooldown;
+  A.inv_h64 = 1.0 / b->d.solver.h;
+  A.dt = b->d.solver.h * b->d.solver.substeps;
+  A.pw = b->d_pw; A.pw_idx = b->d_pw_idx; A.n_params = b->n_params;
+  A.mb = b->mb; A.mc = b->mc; A.mp = b->mp;
+  const size_t smem = smem_bytes(b);
+  cudaError_t e = cudaFuncSetAttribute(batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return b->cuda_fail(e, "cudaFuncSetAttribute(batch_kernel)");
+  int per_sm = 0;
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_kernel, 32 * b->W, smem);
+  if (e != cudaSuccess) return b->cuda_fail(e, "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
+  if (per_sm < 1) return b->fail(KR_ERR_CAPACITY, "batch kernel does not fit on an SM with this launch shape");
+  if (b->ctas_per_sm > 0) per_sm = std::min(per_sm, b->ctas_per_sm);
+  const int grid = std::max(1, std::min(b->n_groups, per_sm * b->n_sm));
+  if ((e = cudaMemsetAsync(b->d_queue, 0, sizeof(int), b->stream)) != cudaSuccess) return b->cuda_fail(e, "queue reset");
+  if (timed) cudaEventRecord(b->ev0, b->stream);
+  batch_kernel<<<grid, 32 * b->W, smem, b->stream>>>(A);
+  if ((e = cudaGetLastError()) != cudaSuccess) return b->cuda_fail(e, "batch_kernel launch");
+  if (timed) cudaEventRecord(b->ev1, b->stream);
+  // remaining horizons as the next schedule sees them
+  for (int s = 0; s < b->capacity; s++)
+    if (b->h_remaining[s] > 0) b->h_remaining[s] = std::max(0, b->h_remaining[s] - max_steps);
+  return KR_OK;
+}
+}  // namespace
+
+extern "C" int kr_batch_run(kr_batch *b, int32_t max_steps) {
+  if (!b) return KR_ERR_INVALID;
+  if (max_steps < 0) return b->fail(KR_ERR_INVALID, "max_steps < 0");
+  if (max_steps == 0) return KR_OK;
+  const bool redo = b->groups_dirty;
+  int rc = launch(b, max_steps, true);
+  (void)redo;
+  b->groups_dirty = true;  // finished slots leave the queue at the next launch
+  return rc;
+}
+
+extern "C" int kr_batch_run_graph(kr_batch *b, int32_t max_steps, int32_t launches, int32_t replays) {
+  if (!b) return KR_ERR_INVALID;
+  if (max_steps <= 0 || launches <= 0 || replays < 0) return b->fail(KR_ERR_INVALID, "kr_batch_run_graph: bad counts");
+  if (b->groups_dirty) {
+    int rc = build_groups(b, b->h_remaining);
+    if (rc != KR_OK) return rc;
+  }
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  cudaError_t e = cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal);
+  if (e != cudaSuccess) return b->cuda_fail(e, "cudaStreamBeginCapture");
+  int rc = KR_OK;
+  for (int l = 0; l < launches && rc == KR_OK; l++) rc = launch(b, max_steps, false);
+  e = cudaStreamEndCapture(b->stream, &graph);
+  if (rc != KR_OK) { if (graph) cudaGraphDestroy(graph); return rc; }
+  if (e != cudaSuccess) return b->cuda_fail(e, "cudaStreamEndCapture");
+  e = cudaGraphInstantiate(&exec, graph, 0);
+  if (e != cudaSuccess) { cudaGraphDestroy(graph); return b->cuda_fail(e, "cudaGraphInstantiate"); }
+  cudaEventRecord(b->ev0, b->stream);
+  for (int r = 0; r < replays && e == cudaSuccess; r++) e = cudaGraphLaunch(exec, b->stream);
+  cudaEventRecord(b->ev1, b->stream);
+  cudaStreamSynchronize(b->stream);
+  cudaGraphExecDestroy(exec);
+  cudaGraphDestroy(graph);
+  if (e != cudaSuccess) return b->cuda_fail(e, "cudaGraphLaunch");
+  b->groups_dirty = true;
+  return KR_OK;
+}
+
+extern "C" int kr_batch_live(kr_batch *b, int32_t *live) {
+  if (!b || !live) return KR_ERR_INVALID;
+  std::vector<SlotMeta> m(b->capacity);
+  cudaError_t e = cudaMemcpyAsync(m.data(), b->d_meta, m.size() * sizeof(SlotMeta), cudaMemcpyDeviceToHost, b->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
+  if (e != cudaSuccess) return b->cuda_fail(e, "kr_batch_live");
+  int n = 0;
+  for (int s = 0; s < b->capacity; s++) {
+    b->h_remaining[s] = std::max(0, m[s].horizon - m[s].step);
+    if (b->h_remaining[s] > 0) n++;
+  }
+  *live = n;
+  b->groups_dirty = true;
+  return KR_OK;
+}
+
+extern "C" int kr_batch_read_state(kr_batch *b, int32_t first, int32_t n, float *bodies, float *grips,
+                                   int32_t *steps) {
+  if (!b) return KR_ERR_INVALID;
+  if (first < 0 || n < 0 || first + n > b->capacity) return b->fail(KR_ERR_INVALID, "read range outside the slots");
+  cudaError_t e = cudaSuccess;
+  std::vector<float> st((size_t)n * kStateStride);
+  std::vector<float4> gr((size_t)n * KR_BATCH_MAX_ARMS);
+  std::vector<SlotMeta> m(n);
+  if (n == 0) return KR_OK;
+  e = cudaMemcpyAsync(st.data(), b->d_state + (size_t)first * kStateStride, st.size() * sizeof(float), cudaMemcpyDeviceToHost, b->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(gr.data(), b->d_grip + (size_t)first * KR_BATCH_MAX_ARMS, gr.size() * sizeof(float4), cudaMemcpyDeviceToHost, b->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(m.data(), b->d_meta + first, m.size() * sizeof(SlotMeta), cudaMemcpyDeviceToHost, b->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
+  if (e != cudaSuccess) return b->cuda_fail(e, "kr_batch_read_state");
+  constexpr int NB = kr::kMaxTplBodies;
+  for (int i = 0; i < n; i++) {
+    if (bodies)
+      for (int j = 0; j < NB; j++)
+        for (int f = 0; f < 6; f++) bodies[((size_t)i * NB + j) * 6 + f] = st[(size_t)i * kStateStride + f * kBodyPad + j];
+    if (grips)
+      for (int a = 0; a < KR_BATCH_MAX_ARMS; a++) {
+        const float4 g = gr[(size_t)i * KR_BATCH_MAX_ARMS + a];
+        float *o = grips + ((size_t)i * KR_BATCH_MAX_ARMS + a) * 4;
+        o[0] = g.x; o[1] = g.y; o[2] = g.z; o[3] = g.w;
+      }
+    if (steps) steps[i] = m[i].step;
+  }
+  return KR_OK;
+}
+
+extern "C" int kr_batch_read_obs(kr_batch *b, int32_t first, int32_t n, float *obs) {
+  if (!b || !obs) return KR_ERR_INVALID;
+  if (b->d.obs_ring <= 0) return b->fail(KR_ERR_STATE, "no observation ring (obs_ring == 0)");
+  if (first < 0 || n < 0 || first + n > b->capacity) return b->fail(KR_ERR_INVALID, "read range outside the slots");
+  const size_t per = (size_t)b->d.obs_ring * KR_OBS_STRIDE;
+  cudaError_t e = cudaMemcpyAsync(obs, b->d_obs + (size_t)first * per, (size_t)n * per * sizeof(float),
+                                  cudaMemcpyDeviceToHost, b->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
+  if (e != cudaSuccess) return b->cuda_fail(e, "kr_batch_read_obs");
+  return KR_OK;
+}
+
+extern "C" int kr_batch_read_fitness(kr_batch *b, int32_t first, int32_t n, double *out) {
+  if (!b || !out) return KR_ERR_INVALID;
+  if (first < 0 || n < 0 || first + n > b->capacity) return b->fail(KR_ERR_INVALID, "read range outside the slots");
+  std::vector<SlotMeta> m(n);
+  cudaError_t e = cudaMemcpyAsync(m.data(), b->d_meta + first, m.size() * sizeof(SlotMeta), cudaMemcpyDeviceToHost, b->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
+  if (e != cudaSuccess) return b->cuda_fail(e, "kr_batch_read_fitness");
+  for (int i = 0; i < n; i++) {
+    out[4 * i] = m[i].path_len; out[4 * i + 1] = m[i].last_x; out[4 * i + 2] = m[i].last_y;
+    out[4 * i + 3] = m[i].attach_events;
+  }
+  return KR_OK;
+}
+
+extern "C" int kr_batch_last_ms(kr_batch *b, float *ms) {
+  if (!b || !ms) return KR_ERR_INVALID;
+  cudaError_t e = cudaEventSynchronize(b->ev1);
+  if (e == cudaSuccess) e = cudaEventElapsedTime(ms, b->ev0, b->ev1);
+  if (e != cudaSuccess) return b->cuda_fail(e, "kr_batch_last_ms");
+  return KR_OK;
+}
+
+extern "C" int kr_batch_sync(kr_batch *b) {
+  if (!b) return KR_ERR_INVALID;
+  cudaError_t e = cudaStreamSynchronize(b->stream);
+  if (e != cudaSuccess) return b->cuda_fail(e, "cudaStreamSynchronize");
+  return KR_OK;
+}
+
+extern "C" int kr_batch_set_stream(kr_batch *b, void *stream) {
+  if (!b) return KR_ERR_INVALID;
+  cudaError_t e = cudaStreamSynchronize(b->stream);
+  if (e != cudaSuccess) return b->cuda_fail(e, "cudaStreamSynchronize");
+  if (stream) {
+    if (b->own_stream) cudaStreamDestroy(b->stream);
+    b->own_stream = false;
+    b->stream = static_cast<cudaStream_t>(stream);
+  } else if (!b->own_stream) {
+    if ((e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking)) != cudaSuccess)
+      return b->cuda_fail(e, "cudaStreamCreate");
+    b->own_stream = true;
+  }
+  return KR_OK;
+}
+
+extern "C" void kr_batch_destroy(kr_batch *b) {
+  if (!b) return;
+  if (b->stream) cudaStreamSynchronize(b->stream);
+  for (void *p : b->d_tpl_arrays)
+    if (p) cudaFree(p);
+  void *ptrs[] = {b->d_tpl, const_cast<int *>(b->T.arm_segs), b->d_rects, b->d_map_off, b->d_map_cull,
+                  b->d_state, b->d_grip, b->d_glam, b->d_cd, b->d_ctrl, b->d_meta, b->d_obs, b->d_groups,
+                  b->d_queue, b->d_pw, b->d_pw_idx};
+  for (void *p : ptrs)
+    if (p) cudaFree(p);
+  if (b->ev0) cudaEventDestroy(b->ev0);
+  if (b->ev1) cudaEventDestroy(b->ev1);
+  if (b->own_stream && b->stream) cudaStreamDestroy(b->stream);
+  delete b;
+}

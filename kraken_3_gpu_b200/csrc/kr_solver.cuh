@@ -37,21 +37,65 @@ __device__ __forceinline__ float fmul(float a, float b) { return __fmul_rn(a, b)
 __device__ __forceinline__ float fdiv(float a, float b) { return __fdiv_rn(a, b); }
 __device__ __forceinline__ float fsqrt(float a) { return __fsqrt_rn(a); }
 
-// Math.fround(Math.cos(x)), Math.fround(Math.sin(x)) for an f32 argument.
+// Math.fround(Math.sin(x)) and Math.fround(Math.cos(x)) for an f32 argument:
+// both evaluated in f64 and rounded once to f32.  For |x| <= 2^20 the f64
+// value comes from a three-part Cody-Waite reduction by pi/2 (the first two
+// products are exact: 20-bit quotient times 33-bit constants) and the Taylor
+// series of sin and cos on |r| <= pi/4 (truncation below 3e-18 relative);
+// larger or non-finite arguments use CUDA's f64 sincos.  Either way the f64
+// result is within a few f64 ulp of the exact value, so its rounding to f32
+// is the correctly rounded f32 except within a few 2^-29 of a rounding
+// midpoint -- the same class as glibc's and V8's f64 sin/cos.
 __device__ __forceinline__ void sincos_r(float a, float *s, float *c) {
-  double sd, cd;
-  sincos(static_cast<double>(a), &sd, &cd);
-  *s = static_cast<float>(sd);
-  *c = static_cast<float>(cd);
+  const double x = static_cast<double>(a);
+  if (!(fabs(x) <= 1048576.0)) {
+    double sd, cd;
+    sincos(x, &sd, &cd);
+    *s = static_cast<float>(sd);
+    *c = static_cast<float>(cd);
+    return;
+  }
+  const double k = rint(x * 0.6366197723675814);  // 2/pi
+  double r = fma(-k, 1.5707963267341256, x);      // pi/2 high part, 33 bits
+  r = fma(-k, 6.077100506303966e-11, r);          // middle part, 33 bits
+  r = fma(-k, 2.0222662487959506e-21, r);         // low part
+  const double r2 = r * r;
+  // sin(r) = r + r^3 (-1/3! + r^2 (1/5! - ...)), terms through r^17
+  double ps = 2.8114572543455206e-15;
+  ps = fma(ps, r2, -7.647163731819816e-13);
+  ps = fma(ps, r2, 1.6059043836821613e-10);
+  ps = fma(ps, r2, -2.505210838544172e-08);
+  ps = fma(ps, r2, 2.7557319223985893e-06);
+  ps = fma(ps, r2, -0.0001984126984126984);
+  ps = fma(ps, r2, 0.008333333333333333);
+  ps = fma(ps, r2, -0.16666666666666666);
+  const double sr = fma(r * r2, ps, r);
+  // cos(r) = 1 + r^2 (-1/2! + r^2 (1/4! - ...)), terms through r^16
+  double pc = 4.779477332387385e-14;
+  pc = fma(pc, r2, -1.1470745597729725e-11);
+  pc = fma(pc, r2, 2.08767569878681e-09);
+  pc = fma(pc, r2, -2.755731922398589e-07);
+  pc = fma(pc, r2, 2.48015873015873e-05);
+  pc = fma(pc, r2, -0.001388888888888889);
+  pc = fma(pc, r2, 0.041666666666666664);
+  pc = fma(pc, r2, -0.5);
+  const double cr = fma(r2, pc, 1.0);
+  const int n = static_cast<int>(static_cast<long long>(k) & 3);
+  const double sv = (n == 0) ? sr : (n == 1) ? cr : (n == 2) ? -sr : -cr;
+  const double cv = (n == 0) ? cr : (n == 1) ? -sr : (n == 2) ? -cr : sr;
+  *s = static_cast<float>(sv);
+  *c = static_cast<float>(cv);
 }
 
 // trunc(x / TAU) exactly, as the f64 quotient of f32solver.mjs:38 gives it.
-// For |x| >= TAU both x and q*TAU are multiples of 2^-21, so the remainder
-// x - q*TAU is exact in one fma and decides whether the rounded f32 quotient
-// crossed an integer; for |x| < TAU the truncated quotient is 0 either way.
+// The f32 estimate q = trunc(x * (1/TAU)) is off by at most one near an
+// integer; the remainder x - q*TAU is then exact in one fma (both terms are
+// multiples of 2^-21 for |x| >= 4 and it stays below 8 in magnitude) and
+// decides the correction.  |x| < 4 has quotient 0.
 __device__ __forceinline__ float trunc_quot_tau(float x) {
-  float q = truncf(__fdiv_rn(x, kTau));
-  float r = fmaf(-q, kTau, x);
+  if (fabsf(x) < 4.f) return 0.f;
+  float q = truncf(__fmul_rn(x, 0.15915494f));
+  const float r = fmaf(-q, kTau, x);
   if (x >= 0.f) {
     if (r < 0.f) q -= 1.f;
     else if (r >= kTau) q += 1.f;
@@ -88,16 +132,17 @@ __device__ __forceinline__ float length2(float x, float y) {
 
 // Rect as stored on the device: x, y, x + w, y + h (all f32, the sums
 // rounded once as solver.wgsl:120-121 computes r.x + r.w).
-// sdfF, f32solver.mjs:139-166 (solver.wgsl:114-147).  The division of the
-// outward normal is deferred to the final winner: bnx/bny are overwritten by
-// every later winner, so only the last winner's dx/best and dy/best survive.
-__device__ __forceinline__ bool sdf(const float4 *__restrict__ rects, int nR, float x, float y,
-                                    float *od, float *onx, float *ony) {
-  float best = kSdfInf, thr = __int_as_float(0x7f800000);  // best*best of 1e30 is +inf in f32
+// sdfF, f32solver.mjs:139-166 (solver.wgsl:114-147), over the rects
+// idx[0..n) in ascending order (or 0..n when idx is null).  The division of
+// the outward normal is deferred to the final winner: bnx/bny are overwritten
+// by every later winner, so only the last winner's dx/best, dy/best survive.
+__device__ __forceinline__ bool sdf(const float4 *__restrict__ rects, const short *idx, int n,
+                                    float x, float y, float *od, float *onx, float *ony) {
+  float best = kSdfInf, thr = __int_as_float(0x7f800000);  // f32 1e30*1e30 = +inf
   float wdx = 0.f, wdy = 0.f, inx = 0.f, iny = 0.f;
   bool inside = false;
-  for (int i = 0; i < nR; i++) {
-    const float4 r = __ldg(rects + i);
+  for (int q = 0; q < n; q++) {
+    const float4 r = __ldg(rects + (idx ? idx[q] : q));
     float cx = x < r.x ? r.x : (x > r.z ? r.z : x);
     float cy = y < r.y ? r.y : (y > r.w ? r.w : y);
     float dx = fsub(x, cx), dy = fsub(y, cy);
@@ -131,21 +176,44 @@ __device__ __forceinline__ bool sdf(const float4 *__restrict__ rects, int nR, fl
   return true;
 }
 
+// Exact rect culling for one collision pass of one creature.
+//
+// Let D = max(largest collision radius, largest half-thickness min(w,h)/2 of
+// a rect) + 2.  Drop every rect farther than D from every point the pass
+// evaluates.  The sequential SDF fold then returns the same winner, or in
+// both cases a winner farther than D - 1 (> radius + 1: no correction):
+//  * a state's threshold f(best^2) never falls below the squared distance
+//    of any rect processed so far, except that an inside winner sets it to
+//    at most half-thickness^2 < (D - 1)^2; a dropped rect (d^2 > D^2) can
+//    therefore only beat states with threshold >= (D - 1)^2 ("far" states);
+//  * by monotone rounding, a rect that fails to beat a far state is itself
+//    far, and an inside rect beats every far state; so the folds with and
+//    without the dropped rects hold equal states or two far states.
+// The pass keeps a point's evaluation on the culled list only while the
+// point lies in the box the list was built for (kCullSlack inside the cull
+// margin); otherwise it uses the full list.
+constexpr int kMaxCulled = 64;
+constexpr float kCullSlack = 6.f;
+
 // Shared-memory view of one island (one warp).  Constraint slots are in
 // schedule order: level by level, each level body-disjoint.
 struct Island {
   // bodies (local index)
   float *px, *py, *ppx, *ppy, *vx, *vy, *ang, *angP, *av, *im, *ii, *fx, *fy, *tq;
+  float *bs, *bc;  // sin / cos of angP during a collision pass
   // constraint slots
   int *ab;     // a | (b << 16), b == 0xffff for a world anchor
   int *tb;     // type | (broken << 8)
   float *lax, *lay, *lbx, *lby, *comp, *rest, *tgt, *minA, *maxA, *lamX, *lamY, *lam, *brk;
   // collision points, grouped per local body in groupCollPoints order
   float *plx, *ply, *pr;
+  int *pbody;             // local body of each point
+  float *pdx, *pdy;       // speculative correction of each point
+  int *pflag;             // 1 if the speculative evaluation corrects
   int *boff, *bcnt;
-  int nb, nc, np, nlv, nrounds;
-  const int *lvl;        // level offsets, nlv + 1 (global, read-only)
-  const short *clane;    // collision lane table, nrounds x 32 (global, read-only)
+  short *cull;            // culled rect list (kMaxCulled)
+  int nb, nc, np, nlv;
+  const int *lvl;         // level offsets, nlv + 1 (global, read-only)
 };
 
 // integrateF, f32solver.mjs:177-200 (solver.wgsl:166-205)
@@ -280,31 +348,121 @@ __device__ __forceinline__ void solve_angle(const SolverConsts &K, Island &S, in
   }
 }
 
-// solveCollisionsF 'seq' for one body, f32solver.mjs:317-344
-// (solver.wgsl:373-402): its points in order, each correction cumulative.
-// angP does not change inside the loop, so sin/cos are taken once.
-__device__ __forceinline__ void collide_body(Island &S, int j, const float4 *__restrict__ rects,
-                                             int nR) {
-  if (S.im[j] == 0.f) return;
-  int cnt = S.bcnt[j];
-  if (cnt == 0) return;
-  int o = S.boff[j];
-  float sa, ca;
-  sincos_r(S.angP[j], &sa, &ca);
-  float px = S.ppx[j], py = S.ppy[j];
-  for (int q = 0; q < cnt; q++) {
-    float lx = S.plx[o + q], ly = S.ply[o + q];
-    float wx = fadd(px, fsub(fmul(lx, ca), fmul(ly, sa)));
-    float wy = fadd(py, fadd(fmul(lx, sa), fmul(ly, ca)));
-    float d, nx, ny;
-    if (!sdf(rects, nR, wx, wy, &d, &nx, &ny)) continue;
-    float pen = fsub(S.pr[o + q], d);
-    if (pen <= kSlackPos) continue;
-    px = fadd(px, fmul(nx, pen));
-    py = fadd(py, fmul(ny, pen));
+__device__ __forceinline__ float warp_min(float v) {
+  for (int o = 16; o > 0; o >>= 1) v = fminf(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+__device__ __forceinline__ float warp_max(float v) {
+  for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+
+// One collision pass of the island: solveCollisionsF 'seq',
+// f32solver.mjs:317-344 (solver.wgsl:373-402) -- per body, its points in
+// order, each correction cumulative.  Evaluated as
+//   1. sin/cos of angP per body (angP does not change in the pass),
+//   2. every point at its body's pose at the start of the pass, plus the
+//      bounding box of those positions, and the culled rect list,
+//   3. per body, the points in order: a point's evaluation from step 2 is
+//      the sequential one as long as no earlier point of that body moved
+//      it; after the first correction the remaining points of that body are
+//      re-evaluated at the moved pose, exactly as the sequential loop does.
+// cull_d = D + kCullSlack with D as in the comment above kMaxCulled.
+__device__ __forceinline__ void collide_island(Island &S, const float4 *__restrict__ rects, int nR,
+                                               float cull_d, int lane) {
+  for (int j = lane; j < S.nb; j += 32) {
+    float s, c;
+    sincos_r(S.angP[j], &s, &c);
+    S.bs[j] = s;
+    S.bc[j] = c;
   }
-  S.ppx[j] = px;
-  S.ppy[j] = py;
+  __syncwarp();
+  float mnx = __int_as_float(0x7f800000), mny = mnx, mxx = -mnx, mxy = -mnx;
+  for (int p = lane; p < S.np; p += 32) {
+    const int j = S.pbody[p];
+    const float ca = S.bc[j], sa = S.bs[j], lx = S.plx[p], ly = S.ply[p];
+    const float wx = fadd(S.ppx[j], fsub(fmul(lx, ca), fmul(ly, sa)));
+    const float wy = fadd(S.ppy[j], fadd(fmul(lx, sa), fmul(ly, ca)));
+    S.pdx[p] = wx;  // position for now, correction below
+    S.pdy[p] = wy;
+    mnx = fminf(mnx, wx); mxx = fmaxf(mxx, wx);
+    mny = fminf(mny, wy); mxy = fmaxf(mxy, wy);
+  }
+  mnx = warp_min(mnx); mny = warp_min(mny);
+  mxx = warp_max(mxx); mxy = warp_max(mxy);
+  // culled list, ascending rect order
+  const float bx0 = mnx - cull_d, bx1 = mxx + cull_d, by0 = mny - cull_d, by1 = mxy + cull_d;
+  int ncull = 0;
+  bool full = !(bx0 <= bx1 && by0 <= by1);  // no finite point: use the full list
+  for (int base = 0; base < nR && !full; base += 32) {
+    const int i = base + lane;
+    bool keep = false;
+    if (i < nR) {
+      const float4 r = __ldg(rects + i);
+      keep = !(r.z < bx0 || r.x > bx1 || r.w < by0 || r.y > by1);
+    }
+    const unsigned m = __ballot_sync(0xffffffffu, keep);
+    const int at = ncull + __popc(m & ((1u << lane) - 1u));
+    if (keep && at < kMaxCulled) S.cull[at] = static_cast<short>(i);
+    ncull += __popc(m);
+    if (ncull > kMaxCulled) full = true;
+  }
+  __syncwarp();
+  const short *list = full ? nullptr : S.cull;
+  const int nlist = full ? nR : ncull;
+  const float sx0 = mnx - kCullSlack, sx1 = mxx + kCullSlack;
+  const float sy0 = mny - kCullSlack, sy1 = mxy + kCullSlack;
+  for (int p = lane; p < S.np; p += 32) {
+    const int j = S.pbody[p];
+    int flag = 0;
+    float cx = 0.f, cy = 0.f;
+    if (S.im[j] != 0.f) {
+      float d, nx, ny;
+      if (sdf(rects, list, nlist, S.pdx[p], S.pdy[p], &d, &nx, &ny)) {
+        const float pen = fsub(S.pr[p], d);
+        if (pen > kSlackPos) {
+          flag = 1;
+          cx = fmul(nx, pen);
+          cy = fmul(ny, pen);
+        }
+      }
+    }
+    S.pflag[p] = flag;
+    S.pdx[p] = cx;
+    S.pdy[p] = cy;
+  }
+  __syncwarp();
+  for (int j = lane; j < S.nb; j += 32) {
+    if (S.im[j] == 0.f) continue;
+    const int o = S.boff[j], cnt = S.bcnt[j];
+    float px = S.ppx[j], py = S.ppy[j];
+    const float ca = S.bc[j], sa = S.bs[j];
+    bool moved = false;
+    for (int q = 0; q < cnt; q++) {
+      const int p = o + q;
+      if (!moved) {
+        if (S.pflag[p]) {
+          px = fadd(px, S.pdx[p]);
+          py = fadd(py, S.pdy[p]);
+          moved = true;
+        }
+        continue;
+      }
+      const float lx = S.plx[p], ly = S.ply[p];
+      const float wx = fadd(px, fsub(fmul(lx, ca), fmul(ly, sa)));
+      const float wy = fadd(py, fadd(fmul(lx, sa), fmul(ly, ca)));
+      const bool in_box = wx >= sx0 && wx <= sx1 && wy >= sy0 && wy <= sy1;
+      float d, nx, ny;
+      if (!sdf(rects, in_box ? list : nullptr, in_box ? nlist : nR, wx, wy, &d, &nx, &ny)) continue;
+      const float pen = fsub(S.pr[p], d);
+      if (pen <= kSlackPos) continue;
+      px = fadd(px, fmul(nx, pen));
+      py = fadd(py, fmul(ny, pen));
+    }
+    S.ppx[j] = px;
+    S.ppy[j] = py;
+  }
+  __syncwarp();
 }
 
 // finalizeF, f32solver.mjs:376-399 (solver.wgsl:405-430)
@@ -349,7 +507,8 @@ __device__ __forceinline__ void grip_break(const SolverConsts &K, Island &S, int
 // of f32solver.mjs:419-428): substeps x (reset lambda, integrate,
 // iterations x (constraint levels, collisions), finalize), then grip break.
 __device__ __forceinline__ void island_step(const SolverConsts &K, Island &S,
-                                            const float4 *__restrict__ rects, int nR, int lane) {
+                                            const float4 *__restrict__ rects, int nR, float cull_d,
+                                            int lane) {
   for (int s = 0; s < K.substeps; s++) {
     for (int k = lane; k < S.nc; k += 32) { S.lamX[k] = 0.f; S.lamY[k] = 0.f; S.lam[k] = 0.f; }
     for (int i = lane; i < S.nb; i += 32) integrate_body(K, S, i);
@@ -365,11 +524,7 @@ __device__ __forceinline__ void island_step(const SolverConsts &K, Island &S,
         }
         __syncwarp();
       }
-      for (int r = 0; r < S.nrounds; r++) {
-        const int j = S.clane[r * 32 + lane];
-        if (j >= 0) collide_body(S, j, rects, nR);
-      }
-      __syncwarp();
+      collide_island(S, rects, nR, cull_d, lane);
     }
     for (int i = lane; i < S.nb; i += 32) finalize_body(K, S, i);
     __syncwarp();

@@ -36,10 +36,7 @@ thread_local std::string g_last_error;
 constexpr int kWarpsPerBlock = 4;
 
 // Per-island record, one int array of kIslandInts per island.
-enum {
-  I_BODY_OFF = 0, I_NB, I_CON_OFF, I_NC, I_PT_OFF, I_NP, I_LVL_OFF, I_NLV, I_ROUND_OFF,
-  I_NROUNDS, kIslandInts
-};
+enum { I_BODY_OFF = 0, I_NB, I_CON_OFF, I_NC, I_PT_OFF, I_NP, I_LVL_OFF, I_NLV, kIslandInts };
 
 struct DeviceTables {
   const int *isl;          // nI x kIslandInts
@@ -49,7 +46,6 @@ struct DeviceTables {
   const int *pts;          // global collision point index, local-body grouped
   const int2 *bpt;         // per island body: (offset within island points, count)
   const int *lvl;          // level offsets per island (nlv + 1 each)
-  const short *clane;      // collision lane table per island (nrounds x 32)
 };
 
 struct StepArgs {
@@ -60,13 +56,14 @@ struct StepArgs {
   const uint4 *coll;       // nP x 4 words
   const float4 *rects;     // nR x (x, y, x+w, y+h)
   int nR;
+  float cull_d;            // rect culling distance of a collision pass
   int nI;
   int maxB, maxC, maxP;    // smem carve sizes (per warp)
   DeviceTables T;
 };
 
 __host__ __device__ inline int warp_smem_words(int mb, int mc, int mp) {
-  return 16 * mb + 15 * mc + 3 * mp;
+  return 18 * mb + 15 * mc + 7 * mp + kr::kMaxCulled / 2;
 }
 
 __device__ inline void carve(kr::Island &S, float *base, int mb, int mc, int mp) {
@@ -75,6 +72,7 @@ __device__ inline void carve(kr::Island &S, float *base, int mb, int mc, int mp)
   S.vx = p; p += mb; S.vy = p; p += mb; S.ang = p; p += mb; S.angP = p; p += mb;
   S.av = p; p += mb; S.im = p; p += mb; S.ii = p; p += mb;
   S.fx = p; p += mb; S.fy = p; p += mb; S.tq = p; p += mb;
+  S.bs = p; p += mb; S.bc = p; p += mb;
   S.boff = reinterpret_cast<int *>(p); p += mb;
   S.bcnt = reinterpret_cast<int *>(p); p += mb;
   S.ab = reinterpret_cast<int *>(p); p += mc;
@@ -84,6 +82,10 @@ __device__ inline void carve(kr::Island &S, float *base, int mb, int mc, int mp)
   S.maxA = p; p += mc; S.lamX = p; p += mc; S.lamY = p; p += mc; S.lam = p; p += mc;
   S.brk = p; p += mc;
   S.plx = p; p += mp; S.ply = p; p += mp; S.pr = p; p += mp;
+  S.pdx = p; p += mp; S.pdy = p; p += mp;
+  S.pbody = reinterpret_cast<int *>(p); p += mp;
+  S.pflag = reinterpret_cast<int *>(p); p += mp;
+  S.cull = reinterpret_cast<short *>(p);
 }
 
 __global__ void __launch_bounds__(32 * kWarpsPerBlock)
@@ -97,9 +99,8 @@ plain_step_kernel(StepArgs A) {
   const int *rec = A.T.isl + island * kIslandInts;
   const int bo = rec[I_BODY_OFF], co = rec[I_CON_OFF], po = rec[I_PT_OFF];
   S.nb = rec[I_NB]; S.nc = rec[I_NC]; S.np = rec[I_NP];
-  S.nlv = rec[I_NLV]; S.nrounds = rec[I_NROUNDS];
+  S.nlv = rec[I_NLV];
   S.lvl = A.T.lvl + rec[I_LVL_OFF];
-  S.clane = A.T.clane + rec[I_ROUND_OFF];
 
   // stage bodies (48 B AoS -> SoA) and forces
   for (int i = lane; i < S.nb; i += 32) {
@@ -113,6 +114,7 @@ plain_step_kernel(StepArgs A) {
     S.fx[i] = f.x; S.fy[i] = f.y; S.tq[i] = f.z;
     const int2 bp = A.T.bpt[bo + i];
     S.boff[i] = bp.x; S.bcnt[i] = bp.y;
+    for (int q = 0; q < bp.y; q++) S.pbody[bp.x + q] = i;
   }
   // stage constraints (80 B AoS -> SoA, schedule order)
   for (int k = lane; k < S.nc; k += 32) {
@@ -137,7 +139,7 @@ plain_step_kernel(StepArgs A) {
   }
   __syncwarp();
 
-  kr::island_step(A.K, S, A.rects, A.nR, lane);
+  kr::island_step(A.K, S, A.rects, A.nR, A.cull_d, lane);
 
   // write back bodies, consumed forces and constraint multipliers / flags
   for (int i = lane; i < S.nb; i += 32) {
@@ -194,9 +196,9 @@ struct kr_world {
   int *d_isl = nullptr, *d_ibodies = nullptr, *d_icons = nullptr, *d_iab = nullptr,
       *d_ipts = nullptr, *d_lvl = nullptr;
   int2 *d_bpt = nullptr;
-  short *d_clane = nullptr;
-  size_t c_isl = 0, c_ibodies = 0, c_icons = 0, c_iab = 0, c_ipts = 0, c_lvl = 0, c_bpt = 0,
-         c_clane = 0;
+  size_t c_isl = 0, c_ibodies = 0, c_icons = 0, c_iab = 0, c_ipts = 0, c_lvl = 0, c_bpt = 0;
+  float max_half_thick = 0.f;  // largest min(w, h) / 2 of the map's rects
+  float cull_d = 0.f;
   int nI = 0, maxB = 1, maxC = 1, maxP = 1, maxLv = 0;
   bool uploaded = false;
   cudaStream_t stream = nullptr;
@@ -332,10 +334,25 @@ extern "C" int kr_create(const kr_solver_params *params, uint32_t n_bodies, uint
   if ((e = cudaMemset(w->d_forces, 0, sizeof(float) * 4 * n_bodies)) != cudaSuccess)
     return cleanup_fail(e, "cudaMemset(forces)");
   std::vector<float4> r4(n_rects);
+  double half_thick = 0.0, r_max = 0.0;
   for (uint32_t i = 0; i < n_rects; i++) {
     const float x = rects[4 * i], y = rects[4 * i + 1], rw = rects[4 * i + 2], rh = rects[4 * i + 3];
     r4[i] = make_float4(x, y, x + rw, y + rh);  // f32 sums, as solver.wgsl:120-121
+    const double ht = 0.5 * std::min(std::fabs((double)rw), std::fabs((double)rh));
+    if (std::isfinite(ht)) half_thick = std::max(half_thick, ht);
+    else half_thick = HUGE_VAL;
   }
+  for (uint32_t i = 0; i < n_coll_pts; i++) {
+    float r;
+    std::memcpy(&r, &coll_pts[4 * i + 3], sizeof(float));
+    if (std::isfinite(r)) r_max = std::max(r_max, std::fabs((double)r));
+    else r_max = HUGE_VAL;
+  }
+  // D = max(radius, half thickness) + 2, plus the slack of the culling box;
+  // the f32 rounding of the box test is covered by the +1
+  const double cull = std::max(r_max, half_thick) + 2.0 + kr::kCullSlack + 1.0;
+  w->cull_d = std::isfinite(cull) && cull < 1e30 ? (float)cull : 1e30f;
+  w->max_half_thick = (float)std::min(half_thick, 1e30);
   if ((e = cudaMalloc(&w->d_rects, sizeof(float4) * n_rects)) != cudaSuccess)
     return cleanup_fail(e, "cudaMalloc(rects)");
   if ((e = cudaMemcpy(w->d_rects, r4.data(), sizeof(float4) * n_rects, cudaMemcpyHostToDevice)) !=
@@ -397,7 +414,6 @@ int build_schedule(kr_world *w, const float *bodies, const uint32_t *cons) {
 
   std::vector<int> isl(nI * (size_t)kIslandInts), h_bodies, h_cons, h_ab, h_pts, h_lvl;
   std::vector<int2> h_bpt;
-  std::vector<short> h_clane;
   h_bodies.reserve(nB); h_cons.reserve(nC); h_ab.reserve(nC);
   int maxB = 1, maxC = 1, maxP = 1, maxLv = 0;
   std::vector<int> last_level, level, order, cnt_per_level;
@@ -458,42 +474,18 @@ int build_schedule(kr_world *w, const float *bodies, const uint32_t *cons) {
     // collision points in local body order
     rec[I_PT_OFF] = (int)h_pts.size();
     int np = 0;
-    std::vector<std::pair<int, int>> load_bodies;  // (count, local body)
     for (int j = 0; j < nb; j++) {
       const int g = bl[j];
       const uint32_t off = w->h_coll_range[g], cnt = w->h_coll_range[nB + g];
       h_bpt.push_back(make_int2(np, (int)cnt));
       for (uint32_t q = 0; q < cnt; q++) h_pts.push_back((int)(off + q));
       np += (int)cnt;
-      const float im = bodies[12 * (size_t)g + 9];
-      if (cnt > 0 && im != 0.f) load_bodies.emplace_back((int)cnt, j);
     }
     if (np > KR_MAX_ISLAND_COLLPTS)
       return w->fail(KR_ERR_CAPACITY, "connected component " + std::to_string(I) + " has " +
                                           std::to_string(np) + " collision points; the kernel holds " +
                                           std::to_string(KR_MAX_ISLAND_COLLPTS));
     rec[I_NP] = np;
-    // longest-first onto the least loaded lane
-    std::stable_sort(load_bodies.begin(), load_bodies.end(),
-                     [](const std::pair<int, int> &x, const std::pair<int, int> &y) {
-                       return x.first > y.first;
-                     });
-    std::vector<int> lane_load(32, 0);
-    std::vector<std::vector<int>> lane_q(32);
-    for (const auto &lb : load_bodies) {
-      int best = 0;
-      for (int l = 1; l < 32; l++)
-        if (lane_load[l] < lane_load[best]) best = l;
-      lane_load[best] += lb.first;
-      lane_q[best].push_back(lb.second);
-    }
-    int rounds = 0;
-    for (int l = 0; l < 32; l++) rounds = std::max(rounds, (int)lane_q[l].size());
-    rec[I_ROUND_OFF] = (int)h_clane.size();
-    rec[I_NROUNDS] = rounds;
-    for (int r = 0; r < rounds; r++)
-      for (int l = 0; l < 32; l++)
-        h_clane.push_back(r < (int)lane_q[l].size() ? (short)lane_q[l][r] : (short)-1);
     maxB = std::max(maxB, nb);
     maxC = std::max(maxC, nc);
     maxP = std::max(maxP, np);
@@ -507,7 +499,6 @@ int build_schedule(kr_world *w, const float *bodies, const uint32_t *cons) {
   if ((e = dev_upload(&w->d_ipts, &w->c_ipts, h_pts)) != cudaSuccess) return w->cuda_fail(e, "upload(island points)");
   if ((e = dev_upload(&w->d_bpt, &w->c_bpt, h_bpt)) != cudaSuccess) return w->cuda_fail(e, "upload(body point ranges)");
   if ((e = dev_upload(&w->d_lvl, &w->c_lvl, h_lvl)) != cudaSuccess) return w->cuda_fail(e, "upload(levels)");
-  if ((e = dev_upload(&w->d_clane, &w->c_clane, h_clane)) != cudaSuccess) return w->cuda_fail(e, "upload(lane table)");
   w->nI = nI;
   // round up so every per-warp region keeps 16-byte alignment of its arrays
   w->maxB = (maxB + 3) & ~3;
@@ -603,8 +594,8 @@ extern "C" int kr_step(kr_world *w, int32_t n_steps) {
   A.nR = (int)w->nR;
   A.nI = w->nI;
   A.maxB = w->maxB; A.maxC = w->maxC; A.maxP = w->maxP;
-  A.T = DeviceTables{w->d_isl, w->d_ibodies, w->d_icons, w->d_iab, w->d_ipts, w->d_bpt, w->d_lvl,
-                     w->d_clane};
+  A.T = DeviceTables{w->d_isl, w->d_ibodies, w->d_icons, w->d_iab, w->d_ipts, w->d_bpt, w->d_lvl};
+  A.cull_d = w->cull_d;
   const size_t smem = w->smem_bytes;
   cudaError_t e;
   const int grid = (w->nI + kWarpsPerBlock - 1) / kWarpsPerBlock;
@@ -664,7 +655,7 @@ extern "C" void kr_destroy(kr_world *w) {
   if (!w) return;
   if (w->stream) cudaStreamSynchronize(w->stream);
   void *ptrs[] = {w->d_bodies, w->d_cons, w->d_stage, w->d_forces, w->d_rects, w->d_coll, w->d_isl,
-                  w->d_ibodies, w->d_icons, w->d_iab, w->d_ipts, w->d_lvl, w->d_bpt, w->d_clane};
+                  w->d_ibodies, w->d_icons, w->d_iab, w->d_ipts, w->d_lvl, w->d_bpt};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   if (w->own_stream && w->stream) cudaStreamDestroy(w->stream);

@@ -102,6 +102,8 @@ def lib(opcount: bool = False) -> C.CDLL:
         "or_arm_reach": (d, [i]),
         "or_sim_create": (vp, [u32, i, d, d, i, i, d, i, i]),
         "or_sim_free": (None, [vp]),
+        "or_sim_new": (vp, [d, d, dp, i, i, i, d]),
+        "or_sim_add_creature": (i, [vp, d, d, d, i, i]),
         "or_sim_world": (vp, [vp]),
         "or_sim_rects": (i, [vp, dp, i]),
         "or_sim_ncreatures": (i, [vp]),
@@ -363,13 +365,20 @@ class Kraken:
 
 
 class Sim:
-    """createSim (core.js:37-74) with prey 0; physics, colouring and reflex only."""
+    """createSim (core.js:37-74) with prey 0; physics, colouring and reflex only.
+
+    With ``rects`` given, an empty sim on that map instead; creatures are then
+    added at explicit poses with :meth:`add_creature`."""
 
     def __init__(self, seed=1, creatures=1, width=1440.0, height=810.0, substeps=2,
-                 iterations=4, h=1 / 120, arms=6, segs=7, opcount=False):
+                 iterations=4, h=1 / 120, arms=6, segs=7, opcount=False, rects=None):
         self.L = lib(opcount)
-        self.ptr = self.L.or_sim_create(seed & 0xFFFFFFFF, creatures, width, height,
-                                        substeps, iterations, h, arms, segs)
+        if rects is None:
+            self.ptr = self.L.or_sim_create(seed & 0xFFFFFFFF, creatures, width, height,
+                                            substeps, iterations, h, arms, segs)
+        else:
+            r = np.ascontiguousarray(rects, dtype=np.float64).reshape(-1, 4)
+            self.ptr = self.L.or_sim_new(width, height, _dp(r), len(r), substeps, iterations, h)
         self.world = World(substeps, iterations, h, _ptr=self.L.or_sim_world(self.ptr),
                            _owner=self, opcount=opcount)
         buf = np.zeros((512, 4))
@@ -386,6 +395,16 @@ class Sim:
         if getattr(self, "ptr", None):
             self.L.or_sim_free(self.ptr)
             self.ptr = None
+
+    def add_creature(self, x, y, angle, arms=6, segs=7) -> "Kraken":
+        i = self.L.or_sim_add_creature(self.ptr, x, y, angle, arms, segs)
+        if i < 0:
+            raise ValueError("bad body shape")
+        k = KrakenStruct()
+        self.L.or_sim_kraken(self.ptr, i, C.byref(k))
+        kr = Kraken(self.world, k)
+        self.creatures.append(kr)
+        return kr
 
     def set_reflex(self, slip_max=150.0, cooldown=0.05):
         self.L.or_sim_set_reflex(self.ptr, slip_max, cooldown)

@@ -1229,22 +1229,53 @@ struct or_sim {
   double gripSlipMax, gripCooldown;
 };
 
-/* createSim, core.js:37-74 (prey 0; senses, lights and fitness are not on
- * the physics path). Colouring follows core.js:45-58: one body mask for the
- * whole world, constraints coloured in creation order, then grouped. */
-or_sim *or_sim_create(uint32_t seed, int creatures, double width, double height,
-                      int substeps, int iterations, double h, int arms, int segs) {
+/* An empty sim on the given map (rects x y w h), solver constants of
+ * XpbdWorld's defaults with the given substeps / iterations / h. */
+or_sim *or_sim_new(double width, double height, const double *rects, int nR, int substeps,
+                   int iterations, double h) {
   or_sim *s = (or_sim *)calloc(1, sizeof(or_sim));
   s->w = or_world_new(substeps, iterations, h, 3.0, 3.0, 360, 18);
   s->width = width; s->height = height;
   s->gripSlipMax = 150;
   s->gripCooldown = 0.05;
-  double tmp[4 * 256];
-  s->nR = or_make_map(width, height, 14, 4, 3, 0.48, seed, tmp, 256);
-  if (s->nR > 256) s->nR = 256;
-  s->rects = (double *)malloc(sizeof(double) * 4 * (size_t)(s->nR > 0 ? s->nR : 1));
-  memcpy(s->rects, tmp, sizeof(double) * 4 * (size_t)s->nR);
+  s->nR = nR;
+  s->rects = (double *)malloc(sizeof(double) * 4 * (size_t)(nR > 0 ? nR : 1));
+  if (nR > 0) memcpy(s->rects, rects, sizeof(double) * 4 * (size_t)nR);
   or_world_set_rects(s->w, s->rects, s->nR);
+  return s;
+}
+
+/* Adds one creature at a given pose (spawnKraken, kraken.js:64-148) with its
+ * constraints coloured in creation order on a fresh per-creature mask (the
+ * colours createSim gives a creature whose bodies are all below 65536) and
+ * the whole list regrouped by colour; returns the creature index. */
+int or_sim_add_creature(or_sim *s, double x, double y, double angle, int arms, int segs) {
+  int c0 = s->w->nC;
+  s->cr = (or_creature *)realloc(s->cr, sizeof(or_creature) * (size_t)(s->nCr + 1));
+  or_creature *c = &s->cr[s->nCr];
+  memset(c, 0, sizeof(*c));
+  if (or_spawn_kraken(s->w, x, y, angle, arms, segs, B_SPAWN_CURL, &c->k) < 0) return -1;
+  c->tone = 0.5;
+  uint32_t *mask = (uint32_t *)calloc((size_t)s->w->n, sizeof(uint32_t));
+  for (int id = c0; id < s->w->nC; id++) {
+    orc_t *cc = &s->w->cons[id];
+    if (cc->color < 0) cc->color = or_assign_color(mask, cc->a, cc->b >= 0 ? cc->b : -1);
+  }
+  free(mask);
+  s->w->colored = 0;
+  or_group_by_color(s->w);
+  return s->nCr++;
+}
+
+/* createSim, core.js:37-74 (prey 0; senses, lights and fitness are not on
+ * the physics path). Colouring follows core.js:45-58: one body mask for the
+ * whole world, constraints coloured in creation order, then grouped. */
+or_sim *or_sim_create(uint32_t seed, int creatures, double width, double height,
+                      int substeps, int iterations, double h, int arms, int segs) {
+  double tmp[4 * 256];
+  int nR = or_make_map(width, height, 14, 4, 3, 0.48, seed, tmp, 256);
+  if (nR > 256) nR = 256;
+  or_sim *s = or_sim_new(width, height, tmp, nR, substeps, iterations, h);
   uint32_t rnd = seed ^ 0x9e3779b9u;
   s->nCr = creatures;
   s->cr = (or_creature *)calloc((size_t)(creatures > 0 ? creatures : 1), sizeof(or_creature));

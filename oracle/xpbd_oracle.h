@@ -119,6 +119,9 @@ double or_arm_reach(int segs);
 /* createSim (core.js:37-74): world + map + creatures, coloured and grouped */
 or_sim *or_sim_create(uint32_t seed, int creatures, double width, double height,
                       int substeps, int iterations, double h, int arms, int segs);
+or_sim *or_sim_new(double width, double height, const double *rects, int nR, int substeps,
+                   int iterations, double h);
+int or_sim_add_creature(or_sim *s, double x, double y, double angle, int arms, int segs);
 void or_sim_free(or_sim *s);
 or_world *or_sim_world(or_sim *s);
 int or_sim_rects(const or_sim *s, double *out, int max);
