@@ -1,0 +1,405 @@
+#!/usr/bin/env python
+"""Creature-steps/s of Kraken 3's XPBD creature step on B200.
+
+Workload (default): 16,384 creatures on 64 maps, bodies of 4-8 arms x 5-9
+segments, horizons U{200..2000} env steps, controls from per-creature
+mulberry32 streams redrawn every 6 steps (tone 0.5), S=2 substeps x I=4
+iterations at h = 1/120 -- seeded synthetic data in the shapes of the
+uneven-batching configuration.  One bench step = one full rollout of every
+creature to its horizon, restored from a device snapshot, run by the
+persistent kernel (one launch).  value = creature-steps / device time.
+
+Also measured on the same workload and GPU: the plain form (one launch per
+env step), the CUDA-graph form (the per-step launches replayed as a graph),
+the end-to-end rate through the public API with host buffers (spawn from
+host arrays, run, read results back), the FP32-issue roofline of the kernel
+and the CPU oracle (FP64 restatement of the reference's xpbd.js) on the host
+cores as a reported baseline.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "creature-steps/s at 16k mixed envs (persistent served form; plain per-step launch beside it)"
+UNIT = "creature-steps/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--n", type=int, default=16384)
+    ap.add_argument("--maps", type=int, default=64)
+    ap.add_argument("--hmin", type=int, default=200)
+    ap.add_argument("--hmax", type=int, default=2000)
+    ap.add_argument("--seed", type=int, default=2)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-plain", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--warps", type=int, default=0, help="warps per CTA (0: autotune)")
+    return ap.parse_args()
+
+
+# ---------------------------------------------------------------------------
+# clocks during the timed region
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.f = tempfile.NamedTemporaryFile(mode="w+", suffix=".csv", delete=False)
+        self.p = None
+
+    def start(self):
+        try:
+            self.p = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=self.f, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.p = None
+
+    def stop(self):
+        if self.p is not None:
+            self.p.terminate()
+            try:
+                self.p.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.p.kill()
+        self.f.flush()
+        self.f.seek(0)
+        rows = [r.strip().split(",") for r in self.f.read().splitlines() if r.strip()]
+        os.unlink(self.f.name)
+        sm, mx, reasons = [], [], set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for r in rows:
+            try:
+                sm.append(float(r[1]))
+                mx.append(float(r[2]))
+            except (ValueError, IndexError):
+                continue
+            for n, v in zip(names, r[5:9]):
+                if v.strip().lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+# CPU oracle (the reported baseline and the reference arm)
+# ---------------------------------------------------------------------------
+def cpu_oracle_rate(w, seconds: float, threads: int, f32: bool = False, opcount: bool = False):
+    """FP64 oracle (the restated xpbd.js) on a sample of the workload: each
+    thread owns independent one-creature sims and steps them round robin
+    for `seconds`; ctypes releases the GIL, so threads run in parallel."""
+    from kraken_3_gpu_b200.workloads import TONE, ControlStream
+    from oracle import binding as ob
+
+    def make(i):
+        sim = ob.Sim(rects=w.maps[w.map_id[i]], opcount=opcount)
+        sim.add_creature(w.x[i], w.y[i], w.angle[i], int(w.arms[i]), int(w.segs[i]))
+        if f32:
+            sim.world.f32ify()
+            sim.world.round_state()
+        return [sim, ControlStream(int(w.arms[i]), int(w.segs[i]), seed=int(w.seed[i])), 0]
+
+    per_thread = 8
+    counts = [0] * threads
+    stop = time.perf_counter() + seconds
+
+    def work(t):
+        sims = [make((t * per_thread + k) % w.n) for k in range(per_thread)]
+        n = 0
+        while time.perf_counter() < stop:
+            for s in sims:
+                tg, ad = s[1].at(s[2])
+                s[0].apply_control_motors(0, TONE, tg, ad)
+                (s[0].step32 if f32 else s[0].step)()
+                s[2] += 1
+                n += 1
+        counts[t] = n
+
+    t0 = time.perf_counter()
+    ths = [threading.Thread(target=work, args=(t,)) for t in range(threads)]
+    for th in ths:
+        th.start()
+    for th in ths:
+        th.join()
+    el = time.perf_counter() - t0
+    return sum(counts) / el, sum(counts), el
+
+
+def ops_per_creature_step(w, sample: int = 48, steps: int = 60) -> float:
+    """f32 rounding ops per creature-step of the restated f32 algorithm
+    (tools/f32solver.mjs, collMode seq) on a sample of the workload's bodies
+    and maps: the algorithmic work the roofline divides by."""
+    from kraken_3_gpu_b200.workloads import TONE, ControlStream
+    from oracle import binding as ob
+
+    L = ob.lib(opcount=True)
+    total_ops, total_steps = 0, 0
+    idx = np.linspace(0, w.n - 1, sample).astype(int)
+    for i in idx:
+        sim = ob.Sim(rects=w.maps[w.map_id[i]], opcount=True)
+        sim.add_creature(w.x[i], w.y[i], w.angle[i], int(w.arms[i]), int(w.segs[i]))
+        sim.world.f32ify()
+        sim.world.round_state()
+        cs = ControlStream(int(w.arms[i]), int(w.segs[i]), seed=int(w.seed[i]))
+        L.or_f32_op_count_reset()
+        for s in range(steps):
+            tg, ad = cs.at(s)
+            sim.apply_control_motors(0, TONE, tg, ad)
+            sim.step32()
+        total_ops += L.or_f32_op_count()
+        total_steps += steps
+    # weight by each creature's horizon share is unnecessary: the sample is
+    # spread evenly over the workload
+    return total_ops / total_steps
+
+
+# ---------------------------------------------------------------------------
+# distributed plumbing
+# ---------------------------------------------------------------------------
+def dist_env():
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", 1))
+    local = int(os.environ.get("LOCAL_RANK", 0))
+    return rank, world, local
+
+
+def reference_arm(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return
+    from kraken_3_gpu_b200 import workloads
+    w = workloads.uneven(n=min(args.n, 4096), n_maps=args.maps, seed=args.seed,
+                         h_min=args.hmin, h_max=args.hmax)
+    threads = os.cpu_count() or 1
+    per = max(2.0, min(20.0, 60.0 / max(1, args.steps + args.warmup)))
+    for _ in range(args.warmup):
+        cpu_oracle_rate(w, per / 4, threads)
+    vals, total, el = [], 0, 0.0
+    for _ in range(args.steps):
+        v, n, e = cpu_oracle_rate(w, per, threads)
+        vals.append(v)
+        total += n
+        el += e
+    value = total / el
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT,
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": per * 1000, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "uneven-16k", "creatures": args.n, "maps": args.maps,
+                   "bodies": "4-8 arms x 5-9 segs", "horizons": f"{args.hmin}-{args.hmax}",
+                   "substeps": 2, "iterations": 4, "parallelism": "host threads"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                         "sample": f"{threads} threads x 8 one-creature worlds of the workload, "
+                                   f"{per:.1f} s per step (FP64 restatement of src/physics/xpbd.js; "
+                                   "the reference is browser JavaScript, no JS runtime on the box)"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        reference_arm(args)
+        return
+    import torch
+
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    # one explicit stream for the engine, the events and the copies
+    torch.cuda.set_stream(torch.cuda.Stream())
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+
+    def barrier():
+        if world > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
+
+    def all_max(x: float) -> float:
+        if world == 1:
+            return x
+        t = torch.tensor([x], device="cuda", dtype=torch.float64)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        return float(t.item())
+
+    from kraken_3_gpu_b200 import batch, workloads
+
+    w = workloads.uneven(n=args.n, n_maps=args.maps, seed=args.seed + 1000 * rank,
+                         h_min=args.hmin, h_max=args.hmax)
+    units = w.creature_steps()
+    max_h = int(w.horizon.max())
+    stream = torch.cuda.current_stream()
+    eng = batch.BatchEngine(w.maps, w.n)
+    eng.set_stream(stream.cuda_stream)
+    workloads.spawn_all(eng, w)
+    eng.snapshot()
+
+    # autotune the launch shape (creatures per CTA) on a short slice
+    launches = 0
+    if args.warps:
+        best_w = args.warps
+    else:
+        best_w, best_t = 8, float("inf")
+        for wp in (4, 8, 16):
+            eng.set_launch(wp, 0)
+            eng.restore()
+            eng.run(40)
+            launches += 1
+            eng.sync()
+            t = eng.last_ms()
+            if t < best_t:
+                best_w, best_t = wp, t
+    eng.set_launch(best_w, 0)
+
+    # warm-up: full rollouts
+    for _ in range(args.warmup):
+        eng.restore()
+        eng.run(max_h)
+    barrier()
+
+    sampler = ClockSampler(local)
+    sampler.start()
+    time.sleep(0.3)
+    kernel_ms = []
+    barrier()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        eng.restore()
+        eng.run(max_h)
+        kernel_ms.append(None)
+    e1.record(stream)
+    e1.synchronize()
+    barrier()
+    elapsed_ms = e0.elapsed_time(e1)
+    # the kernel's own duration (last launch of each step, timed by events
+    # around the launch on the same stream)
+    eng.restore()
+    eng.run(max_h)
+    kms = eng.last_ms()
+    clocks = sampler.stop()
+    gpu_launches = args.steps * 1
+    t_max = all_max(elapsed_ms)
+    value = world * units * args.steps / (t_max / 1000.0)
+    ms_per_step = t_max / args.steps
+
+    # plain form (one launch per env step) and the CUDA-graph step loop
+    extra = {}
+    if not args.no_plain:
+        eng.restore()
+        torch.cuda.synchronize()
+        p0 = torch.cuda.Event(enable_timing=True)
+        p1 = torch.cuda.Event(enable_timing=True)
+        p0.record(stream)
+        eng.run_launches(1, max_h)
+        p1.record(stream)
+        p1.synchronize()
+        plain_ms = all_max(p0.elapsed_time(p1))
+        extra["plain_per_step_launch"] = {"value": world * units / (plain_ms / 1000.0),
+                                          "ms_per_rollout": plain_ms, "launches": max_h}
+        eng.restore()
+        torch.cuda.synchronize()
+        g0 = time.perf_counter()
+        eng.run_graph(1, max_h, 1)
+        g_ms = all_max((time.perf_counter() - g0) * 1000.0)
+        extra["graph_step_loop"] = {"value": world * units / (g_ms / 1000.0),
+                                    "ms_per_rollout_incl_capture": g_ms}
+
+    # end to end through the public API with host buffers: spawn from host
+    # arrays, run the rollout, read every creature's result back
+    e2e_iters = max(1, min(args.steps, 2))
+    eng2 = batch.BatchEngine(w.maps, w.n)
+    eng2.set_stream(stream.cuda_stream)
+    eng2.set_launch(best_w, 0)
+    workloads.spawn_all(eng2, w)
+    eng2.run(1)
+    torch.cuda.synchronize()
+    h0 = time.perf_counter()
+    for _ in range(e2e_iters):
+        workloads.spawn_all(eng2, w)
+        eng2.run(max_h)
+        fit = eng2.read_fitness()
+        st = eng2.read_state()
+    e2e_s = all_max(time.perf_counter() - h0)
+    h2d = w.n * (4 * 4 + 8 * 3 + 4 + 4) + w.n * 6 * 76 * 4  # spawn args + staged poses
+    d2h = fit.nbytes + sum(v.nbytes for v in st.values())
+    eng2.close()
+
+    # roofline: f32 rounding ops per creature-step of the restated f32
+    # algorithm (op-counting oracle build) x creature-steps per launch /
+    # launch duration, against the measured dependent-free FMA issue rate
+    roof = None
+    cpu = None
+    if rank == 0:
+        fma_rate = batch.probe_fp32_rate()
+        if not args.no_cpu_baseline and world == 1:
+            ops = ops_per_creature_step(w)
+            achieved = ops * units / (kms / 1000.0)
+            roof = {"bound": "fp32", "achieved": achieved / 1e12, "peak": fma_rate / 1e12,
+                    "unit": "TFLOP/s", "frac": achieved / fma_rate, "traffic": None,
+                    "ops_per_creature_step": ops, "kernel_ms": kms,
+                    "peak_note": "measured dependent-free f32 FMA issue rate (lane-ops/s) on this GPU"}
+            threads = os.cpu_count() or 1
+            cv, cn, ce = cpu_oracle_rate(w, args.cpu_seconds, threads)
+            cpu = {"value": cv, "unit": UNIT, "cores": threads, "kind": "port",
+                   "sample": f"{cn} creature-steps in {ce:.1f} s: {threads} threads x 8 one-creature "
+                             "worlds of the workload, FP64 restatement of src/physics/xpbd.js"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "uneven-16k", "creatures": w.n, "maps": args.maps,
+                       "bodies": "4-8 arms x 5-9 segs", "horizons": f"{args.hmin}-{args.hmax}",
+                       "creature_steps_per_rollout": units, "substeps": 2, "iterations": 4,
+                       "controls": "device mulberry32 streams, redraw every 6 steps",
+                       "warps_per_cta": best_w, "parallelism": f"replicas x{world}",
+                       "l2": "state per rollout restored from a device snapshot; working set "
+                             f"{w.n * 2.4 / 1024:.0f} MB of state, compute-bound"},
+            "roofline": roof, "cpu_baseline": cpu, "clocks": clocks,
+            "e2e": {"value": world * units * e2e_iters / e2e_s, "unit": UNIT,
+                    "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+            "gpu_launches": gpu_launches, **extra,
+        }
+        print(json.dumps(line), flush=True)
+    eng.close()
+    if world > 1:
+        torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -88,6 +88,11 @@ int kr_batch_set_policy(kr_batch *b, const float *weights, int32_t n_individuals
  * one persistent launch.  Asynchronous; returns once enqueued. */
 int kr_batch_run(kr_batch *b, int32_t max_steps);
 
+/* `launches` back-to-back launches of steps_per_launch env steps each over
+ * the same creature groups, no host work between them (with
+ * steps_per_launch = 1: the plain one-launch-per-env-step form). */
+int kr_batch_run_launches(kr_batch *b, int32_t steps_per_launch, int32_t launches);
+
 /* Capture `launches` consecutive kr_batch_run(max_steps) calls into one CUDA
  * graph and replay it `replays` times. */
 int kr_batch_run_graph(kr_batch *b, int32_t max_steps, int32_t launches, int32_t replays);
@@ -110,6 +115,17 @@ int kr_batch_read_obs(kr_batch *b, int32_t first, int32_t n, float *obs);
 /* Per-slot accumulators (synchronous): n x 4 f64 -- path length of the
  * mantle, x and y of the mantle, attach events. */
 int kr_batch_read_fitness(kr_batch *b, int32_t first, int32_t n, double *out);
+
+/* Keep a device copy of every slot's state (bodies, grips, reflex
+ * cooldowns, current controls, step counters) and put it back later -- the
+ * snapshot/restore of a rollout; both asynchronous device-to-device copies
+ * (the snapshot synchronizes once when it first allocates). */
+int kr_batch_snapshot(kr_batch *b);
+int kr_batch_restore(kr_batch *b);
+
+/* Dependent-free f32 FMA throughput of the device (FMA instructions per
+ * second over every SM), the issue-rate ceiling of the f32 path. */
+int kr_probe_fp32_rate(double *fma_per_s);
 
 /* Launch shape: warps (creatures) per CTA (1..16) and CTAs per SM
  * (0 = as many as fit). */

@@ -58,6 +58,7 @@ def _lib():
         "kr_batch_set_policy": (C.c_int, [vp, _F32P, i32, i32, _I32P]),
         "kr_batch_run": (C.c_int, [vp, i32]),
         "kr_batch_run_graph": (C.c_int, [vp, i32, i32, i32]),
+        "kr_batch_run_launches": (C.c_int, [vp, i32, i32]),
         "kr_batch_live": (C.c_int, [vp, _I32P]),
         "kr_batch_read_state": (C.c_int, [vp, i32, i32, _F32P, _F32P, _I32P]),
         "kr_batch_read_obs": (C.c_int, [vp, i32, i32, _F32P]),
@@ -68,6 +69,9 @@ def _lib():
         "kr_batch_set_stream": (C.c_int, [vp, vp]),
         "kr_batch_destroy": (None, [vp]),
         "kr_batch_last_error": (C.c_char_p, [vp]),
+        "kr_batch_snapshot": (C.c_int, [vp]),
+        "kr_batch_restore": (C.c_int, [vp]),
+        "kr_probe_fp32_rate": (C.c_int, [_F64P]),
     }
     for name, (res, args) in sigs.items():
         fn = getattr(L, name)
@@ -152,11 +156,23 @@ class BatchEngine:
         _check(_lib().kr_batch_set_policy(self.h, w.ctypes.data_as(_F32P), w.shape[0], w.shape[1],
                                           idx.ctypes.data_as(_I32P)), self.h)
 
+    def snapshot(self):
+        _check(_lib().kr_batch_snapshot(self.h), self.h)
+
+    def restore(self):
+        _check(_lib().kr_batch_restore(self.h), self.h)
+
     def set_launch(self, warps_per_cta, ctas_per_sm=0):
         _check(_lib().kr_batch_set_launch(self.h, warps_per_cta, ctas_per_sm), self.h)
 
     def run(self, max_steps):
         _check(_lib().kr_batch_run(self.h, max_steps), self.h)
+
+    def run_launches(self, steps_per_launch, launches):
+        _check(_lib().kr_batch_run_launches(self.h, steps_per_launch, launches), self.h)
+
+    def set_stream(self, stream_ptr):
+        _check(_lib().kr_batch_set_stream(self.h, C.c_void_p(stream_ptr)), self.h)
 
     def run_graph(self, max_steps, launches, replays=1):
         _check(_lib().kr_batch_run_graph(self.h, max_steps, launches, replays), self.h)
@@ -203,3 +219,10 @@ def policy_params(arms=6, segs=7) -> int:
     """Parameter count of the fused controller for an arms x segs body."""
     n_in, n_out = 6 * arms + 6, arms * segs + arms
     return POLICY_HIDDEN * (n_in + 1) + n_out * (POLICY_HIDDEN + 1)
+
+
+def probe_fp32_rate() -> float:
+    """Measured dependent-free f32 FMA instructions per second of the device."""
+    r = C.c_double()
+    _check(_lib().kr_probe_fp32_rate(C.byref(r)), None)
+    return r.value

@@ -502,6 +502,16 @@ struct kr_batch {
   int n_groups = 0;
   bool groups_dirty = true;
   int *d_queue = nullptr;
+  // snapshot of every slot (kr_batch_snapshot / kr_batch_restore)
+  float *s_state = nullptr;
+  float4 *s_grip = nullptr;
+  float2 *s_glam = nullptr;
+  double *s_cd = nullptr;
+  float *s_ctrl = nullptr;
+  SlotMeta *s_meta = nullptr;
+  std::vector<int> s_remaining;
+  int *s_groups = nullptr;        // groups built for the snapshot state
+  int s_n_groups = -1, s_W = 0;
   // launch shape
   int W = 8, ctas_per_sm = 0, n_sm = 0;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
@@ -1061,11 +1071,130 @@ extern "C" void kr_batch_destroy(kr_batch *b) {
     if (p) cudaFree(p);
   void *ptrs[] = {b->d_tpl, const_cast<int *>(b->T.arm_segs), b->d_rects, b->d_map_off, b->d_map_cull,
                   b->d_state, b->d_grip, b->d_glam, b->d_cd, b->d_ctrl, b->d_meta, b->d_obs, b->d_groups,
-                  b->d_queue, b->d_pw, b->d_pw_idx};
+                  b->d_queue, b->d_pw, b->d_pw_idx, b->s_state, b->s_grip, b->s_glam, b->s_cd,
+                  b->s_ctrl, b->s_meta, b->s_groups};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   if (b->ev0) cudaEventDestroy(b->ev0);
   if (b->ev1) cudaEventDestroy(b->ev1);
   if (b->own_stream && b->stream) cudaStreamDestroy(b->stream);
   delete b;
+}
+
+namespace {
+template <typename T>
+cudaError_t copy_all(T **dst, const T *src, size_t n, cudaStream_t st) {
+  if (!*dst) {
+    cudaError_t e = cudaMalloc(reinterpret_cast<void **>(dst), n * sizeof(T));
+    if (e != cudaSuccess) return e;
+  }
+  return cudaMemcpyAsync(*dst, src, n * sizeof(T), cudaMemcpyDeviceToDevice, st);
+}
+}  // namespace
+
+extern "C" int kr_batch_snapshot(kr_batch *b) {
+  if (!b) return KR_ERR_INVALID;
+  const size_t C = (size_t)b->capacity;
+  cudaError_t e = copy_all(&b->s_state, b->d_state, C * kStateStride, b->stream);
+  if (e == cudaSuccess) e = copy_all(&b->s_grip, b->d_grip, C * KR_BATCH_MAX_ARMS, b->stream);
+  if (e == cudaSuccess) e = copy_all(&b->s_glam, b->d_glam, C * KR_BATCH_MAX_ARMS, b->stream);
+  if (e == cudaSuccess) e = copy_all(&b->s_cd, b->d_cd, C * KR_BATCH_MAX_ARMS, b->stream);
+  if (e == cudaSuccess) e = copy_all(&b->s_ctrl, b->d_ctrl, C * kCtrlStride, b->stream);
+  if (e == cudaSuccess) e = copy_all(&b->s_meta, b->d_meta, C, b->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
+  if (e != cudaSuccess) return b->cuda_fail(e, "kr_batch_snapshot");
+  b->s_remaining = b->h_remaining;
+  b->s_n_groups = -1;  // groups for this state are cached at the first restore
+  return KR_OK;
+}
+
+extern "C" int kr_batch_restore(kr_batch *b) {
+  if (!b) return KR_ERR_INVALID;
+  if (!b->s_state) return b->fail(KR_ERR_STATE, "restore before snapshot");
+  const size_t C = (size_t)b->capacity;
+  cudaError_t e = cudaMemcpyAsync(b->d_state, b->s_state, C * kStateStride * sizeof(float), cudaMemcpyDeviceToDevice, b->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(b->d_grip, b->s_grip, C * KR_BATCH_MAX_ARMS * sizeof(float4), cudaMemcpyDeviceToDevice, b->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(b->d_glam, b->s_glam, C * KR_BATCH_MAX_ARMS * sizeof(float2), cudaMemcpyDeviceToDevice, b->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(b->d_cd, b->s_cd, C * KR_BATCH_MAX_ARMS * sizeof(double), cudaMemcpyDeviceToDevice, b->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(b->d_ctrl, b->s_ctrl, C * kCtrlStride * sizeof(float), cudaMemcpyDeviceToDevice, b->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(b->d_meta, b->s_meta, C * sizeof(SlotMeta), cudaMemcpyDeviceToDevice, b->stream);
+  if (e != cudaSuccess) return b->cuda_fail(e, "kr_batch_restore");
+  b->h_remaining = b->s_remaining;
+  // the work groups of the snapshot state: built once, then copied back
+  if (b->s_n_groups < 0 || b->s_W != b->W) {
+    int rc = build_groups(b, b->h_remaining);
+    if (rc != KR_OK) return rc;
+    if (b->s_groups) cudaFree(b->s_groups);
+    b->s_groups = nullptr;
+    e = cudaMalloc(&b->s_groups, std::max<size_t>(b->c_groups, 1) * sizeof(int));
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(b->s_groups, b->d_groups, (size_t)b->n_groups * b->W * sizeof(int),
+                          cudaMemcpyDeviceToDevice, b->stream);
+    if (e != cudaSuccess) return b->cuda_fail(e, "kr_batch_restore(groups)");
+    b->s_n_groups = b->n_groups;
+    b->s_W = b->W;
+  } else {
+    e = cudaMemcpyAsync(b->d_groups, b->s_groups, (size_t)b->s_n_groups * b->W * sizeof(int),
+                        cudaMemcpyDeviceToDevice, b->stream);
+    if (e != cudaSuccess) return b->cuda_fail(e, "kr_batch_restore(groups)");
+    b->n_groups = b->s_n_groups;
+  }
+  b->groups_dirty = false;
+  return KR_OK;
+}
+
+namespace {
+// n independent f32 FMA chains per thread (no dependence between chains)
+__global__ void fma_probe_kernel(float *out, int iters) {
+  float a0 = threadIdx.x * 1e-3f, a1 = a0 + 1.f, a2 = a0 + 2.f, a3 = a0 + 3.f;
+  float a4 = a0 + 4.f, a5 = a0 + 5.f, a6 = a0 + 6.f, a7 = a0 + 7.f;
+  const float m = 0.9999999f, c = 1e-7f;
+  for (int i = 0; i < iters; i++) {
+    a0 = fmaf(a0, m, c); a1 = fmaf(a1, m, c); a2 = fmaf(a2, m, c); a3 = fmaf(a3, m, c);
+    a4 = fmaf(a4, m, c); a5 = fmaf(a5, m, c); a6 = fmaf(a6, m, c); a7 = fmaf(a7, m, c);
+  }
+  if (a0 + a1 + a2 + a3 + a4 + a5 + a6 + a7 == 12345.f) out[threadIdx.x] = a0;
+}
+}  // namespace
+
+extern "C" int kr_probe_fp32_rate(double *fma_per_s) {
+  if (!fma_per_s) return KR_ERR_INVALID;
+  int dev = 0, n_sm = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev);
+  float *out = nullptr;
+  cudaEvent_t e0, e1;
+  cudaError_t e = cudaMalloc(&out, 1024 * sizeof(float));
+  if (e != cudaSuccess) { g_batch_error = cudaGetErrorString(e); return KR_ERR_CUDA; }
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  const int iters = 1 << 16, blocks = n_sm * 8, threads = 256;
+  fma_probe_kernel<<<blocks, threads>>>(out, 256);
+  cudaEventRecord(e0);
+  fma_probe_kernel<<<blocks, threads>>>(out, iters);
+  cudaEventRecord(e1);
+  e = cudaEventSynchronize(e1);
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFree(out);
+  if (e != cudaSuccess) { g_batch_error = cudaGetErrorString(e); return KR_ERR_CUDA; }
+  *fma_per_s = (double)blocks * threads * iters * 8.0 / (ms * 1e-3);
+  return KR_OK;
+}
+
+extern "C" int kr_batch_run_launches(kr_batch *b, int32_t steps_per_launch, int32_t launches) {
+  if (!b) return KR_ERR_INVALID;
+  if (steps_per_launch <= 0 || launches < 0) return b->fail(KR_ERR_INVALID, "kr_batch_run_launches: bad counts");
+  if (b->groups_dirty) {
+    int rc = build_groups(b, b->h_remaining);
+    if (rc != KR_OK) return rc;
+  }
+  for (int l = 0; l < launches; l++) {
+    int rc = launch(b, steps_per_launch, l == launches - 1);
+    if (rc != KR_OK) return rc;
+  }
+  b->groups_dirty = true;
+  return KR_OK;
 }

@@ -20,6 +20,28 @@ from .kraken import arm_reach
 from .world_map import find_spawn, make_map, mulberry32
 
 WIDTH, HEIGHT = 1440, 810
+TONE = 0.5  # creature default tone, core.js:81 (compliance 1 / 201000)
+
+
+class ControlStream:
+    """Host mirror of the engine's device control stream: per arm-segment
+    muscle targets ~ U[-1, 1] rad and per-arm adhesion ~ U[0, 1], redrawn
+    every `every` env steps from mulberry32(seed); draw order per arm: its
+    motors (shoulder first), then its adhesion."""
+
+    def __init__(self, n_arms=6, n_segs=7, seed=0, every=6):
+        self.rnd = mulberry32(seed)
+        self.A, self.S, self.every = n_arms, n_segs, every
+        self.targets = np.zeros(n_arms * n_segs)
+        self.adhesion = np.zeros(n_arms)
+
+    def at(self, step):
+        if step % self.every == 0:
+            for a in range(self.A):
+                for j in range(self.S):
+                    self.targets[a * self.S + j] = self.rnd() * 2 - 1
+                self.adhesion[a] = self.rnd()
+        return self.targets, self.adhesion
 
 
 @dataclass

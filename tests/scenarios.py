@@ -1,31 +1,14 @@
-"""Seeded scenarios shared by the GPU tests and the smoke/bench code paths.
+"""Seeded scenarios shared by the GPU tests.
 
-config0_controls: per arm-segment muscle targets ~ U[-1, 1] rad and per-arm
-adhesion ~ U[0, 1], redrawn every 6 env steps from mulberry32(seed), draw
-order per arm: its motors (shoulder first), then its adhesion.  Tone is fixed
-at 0.5 (compliance 1/201000, the creature default of core.js:81).
+ControlStream (from the package): per arm-segment muscle targets ~ U[-1, 1]
+rad and per-arm adhesion ~ U[0, 1], redrawn every 6 env steps from
+mulberry32(seed), draw order per arm: its motors (shoulder first), then its
+adhesion.  Tone is fixed at 0.5 (compliance 1/201000, the creature default of
+core.js:81).
 """
 import numpy as np
 
-from kraken_3_gpu_b200 import world_map
-
-TONE = 0.5
-
-
-class ControlStream:
-    def __init__(self, n_arms=6, n_segs=7, seed=0, every=6):
-        self.rnd = world_map.mulberry32(seed)
-        self.A, self.S, self.every = n_arms, n_segs, every
-        self.targets = np.zeros(n_arms * n_segs)
-        self.adhesion = np.zeros(n_arms)
-
-    def at(self, step):
-        if step % self.every == 0:
-            for a in range(self.A):
-                for j in range(self.S):
-                    self.targets[a * self.S + j] = self.rnd() * 2 - 1
-                self.adhesion[a] = self.rnd()
-        return self.targets, self.adhesion
+from kraken_3_gpu_b200.workloads import TONE, ControlStream  # noqa: F401
 
 
 def ulp_distance(a32: np.ndarray, b32: np.ndarray) -> np.ndarray:
