@@ -112,6 +112,44 @@ int kr_set_stream(kr_world *w, void *stream);
  * number of constraint levels of the largest one. */
 int kr_world_islands(const kr_world *w, int32_t *n_islands, int32_t *max_levels);
 
+/* Allocation-free step.  No counterpart in the reference: gpuworld.js always
+ * owns its device buffers.  This entry point is for callers that cannot
+ * allocate GPU memory themselves or through this library -- code inside a
+ * host application's own device-memory pool, an embedding that must own
+ * every allocation, or a latency-critical loop where a cudaMalloc (and the
+ * synchronization it implies) is not allowed.  It advances the world n_steps
+ * env steps exactly like kr_step (same kernel, same results), with every
+ * buffer in device memory owned by the caller:
+ *   bodies   n_bodies x 12 f32 (in/out)     cons   n_constraints x 20 words (in/out)
+ *   forces   n_bodies x 4 f32 (in/out)      rects  n_rects x 4 f32 (x y w h)
+ *   coll_pts n_coll_pts x 4 words and coll_range 2 x n_bodies u32, as for kr_create.
+ * The per-creature schedule is rebuilt on the device at every call into one
+ * file-scope device array of fixed size (about 270 KB; every GPU that loads
+ * the library holds it until the process exits), so the call allocates
+ * nothing, neither on the device nor on the host.  Limits: at most
+ * KR_NOALLOC_MAX_BODIES bodies, KR_NOALLOC_MAX_CONSTRAINTS constraints,
+ * KR_NOALLOC_MAX_COLLPTS collision points and KR_NOALLOC_MAX_RECTS rects;
+ * larger worlds are rejected with KR_ERR_CAPACITY before any GPU work, and a
+ * creature above the KR_MAX_ISLAND_* capacities is found by the schedule
+ * builder and rejected with the same code before any step runs.  Other codes: KR_ERR_INVALID
+ * (null pointer, implausible parameter, inconsistent coll_range),
+ * KR_ERR_INDEX (a constraint's body index out of range), KR_ERR_CUDA.  No
+ * message is recorded (recording one would allocate).
+ * The first call on a device looks up the device address of the scratch
+ * array; make that first call before any stream capture.  The call waits for
+ * the schedule builder on `stream` (cudaStream_t as void*, NULL = the legacy
+ * default stream), then enqueues the steps asynchronously.  Every call on a
+ * device shares the one scratch array: calls that overlap on the GPU (other
+ * host threads, other streams) race and must not be issued. */
+#define KR_NOALLOC_MAX_BODIES 2048
+#define KR_NOALLOC_MAX_CONSTRAINTS 4096
+#define KR_NOALLOC_MAX_COLLPTS 4096
+#define KR_NOALLOC_MAX_RECTS 1024
+int kr_step_noalloc(const kr_solver_params *params, uint32_t n_bodies, uint32_t n_constraints,
+                    float *bodies, uint32_t *cons, float *forces, const float *rects,
+                    uint32_t n_rects, const uint32_t *coll_pts, uint32_t n_coll_pts,
+                    const uint32_t *coll_range, int32_t n_steps, void *stream);
+
 /* destroy (gpuworld.js:466-472): frees device memory; NULL is a no-op. */
 void kr_destroy(kr_world *w);
 

@@ -88,8 +88,9 @@ __device__ inline void carve(kr::Island &S, float *base, int mb, int mc, int mp)
   S.cull = reinterpret_cast<short *>(p);
 }
 
-__global__ void __launch_bounds__(32 * kWarpsPerBlock)
-plain_step_kernel(StepArgs A) {
+// One launch of the plain step for the island of this warp (shared by the
+// plain kernel and its allocation-free variant).
+__device__ __forceinline__ void plain_step_body(const StepArgs &A) {
   extern __shared__ float smem[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int island = blockIdx.x * kWarpsPerBlock + warp;
@@ -162,6 +163,10 @@ plain_step_kernel(StepArgs A) {
     c[15] = __float_as_uint(S.lam[k]);
     c[17] = (S.tb[k] >> 8) != 0 ? 1u : 0u;
   }
+}
+
+__global__ void __launch_bounds__(32 * kWarpsPerBlock) plain_step_kernel(StepArgs A) {
+  plain_step_body(A);
 }
 
 template <typename T>
@@ -660,4 +665,276 @@ extern "C" void kr_destroy(kr_world *w) {
     if (p) cudaFree(p);
   if (w->own_stream && w->stream) cudaStreamDestroy(w->stream);
   delete w;
+}
+
+// ---------------------------------------------------------------------------
+// Allocation-free step (kr_step_noalloc).
+//
+// For callers that cannot allocate GPU memory -- code running inside a
+// host-side memory pool, an embedding that owns every device allocation, a
+// real-time loop where cudaMalloc's implicit synchronization is not
+// allowed.  Everything the step needs beyond the caller's own buffers (the
+// per-creature schedule, the converted rect list, the culling distance)
+// lives in one file-scope device array of fixed size, so the call allocates
+// nothing on the device or the host.
+//
+// Scratch layout (words): island records, island bodies, schedule slots,
+// slot body pairs, island points, body point ranges, level offsets, rects,
+// and the builder's temporaries.  The array is shared by every call on a
+// device and keeps the last call's contents; the builder initializes every
+// word it reads before reading it.
+// ---------------------------------------------------------------------------
+namespace {
+
+constexpr int kNaB = KR_NOALLOC_MAX_BODIES;
+constexpr int kNaC = KR_NOALLOC_MAX_CONSTRAINTS;
+constexpr int kNaP = KR_NOALLOC_MAX_COLLPTS;
+constexpr int kNaR = KR_NOALLOC_MAX_RECTS;
+// region offsets in words
+constexpr int kOffHdr = 0;                                  // n_islands, cull_d, status, pad
+constexpr int kOffIsl = 4;
+constexpr int kOffBodies = kOffIsl + kNaB * kIslandInts;
+constexpr int kOffCons = kOffBodies + kNaB;
+constexpr int kOffAb = kOffCons + kNaC;
+constexpr int kOffPts = kOffAb + kNaC;
+constexpr int kOffBpt = ((kOffPts + kNaP) + 1) & ~1;       // int2, 8-byte aligned
+constexpr int kOffLvl = kOffBpt + 2 * kNaB;
+constexpr int kOffRects = ((kOffLvl + kNaC + kNaB) + 3) & ~3;  // float4, 16-byte aligned
+constexpr int kOffParent = kOffRects + 4 * kNaR;
+constexpr int kOffIslandOf = kOffParent + kNaB;
+constexpr int kOffLocal = kOffIslandOf + kNaB;
+constexpr int kOffRootIsl = kOffLocal + kNaB;
+constexpr int kOffCnt = kOffRootIsl + kNaB;                 // kNaB + 1
+constexpr int kOffLast = kOffCnt + kNaB + 1;
+constexpr int kOffLevel = kOffLast + kNaB;
+constexpr int kOffCur = kOffLevel + kNaC;                   // kNaC + 1
+constexpr int kScratchWords = kOffCur + kNaC + 1;
+
+static __device__ __align__(256) int g_noalloc_scratch[kScratchWords];
+
+// Single-thread schedule builder: the same islands, bodies, levels, slot
+// order and point ranges as build_schedule(), written into the scratch.
+__global__ void noalloc_schedule_kernel(int *W, const float *bodies, const uint32_t *cons,
+                                        const float *rects, const uint32_t *coll_pts,
+                                        const uint32_t *coll_range, int nB, int nC, int nP, int nR) {
+  if (blockIdx.x != 0 || threadIdx.x != 0) return;
+  int *isl = W + kOffIsl, *ib = W + kOffBodies, *icons = W + kOffCons, *iab = W + kOffAb;
+  int *ipts = W + kOffPts, *lvl = W + kOffLvl;
+  int2 *bpt = reinterpret_cast<int2 *>(W + kOffBpt);
+  float4 *r4 = reinterpret_cast<float4 *>(W + kOffRects);
+  int *parent = W + kOffParent, *island_of = W + kOffIslandOf, *local = W + kOffLocal;
+  int *root_isl = W + kOffRootIsl, *cnt = W + kOffCnt, *last = W + kOffLast;
+  int *level = W + kOffLevel, *cur = W + kOffCur;
+  W[kOffHdr + 0] = 0;
+  W[kOffHdr + 2] = KR_OK;
+  // collRange must tile the points in body order (gpuworld.js:193-199)
+  uint32_t acc = 0;
+  for (int g = 0; g < nB; g++) {
+    if (coll_range[g] != acc) { W[kOffHdr + 2] = KR_ERR_INVALID; return; }
+    acc += coll_range[nB + g];
+  }
+  if (acc != (uint32_t)nP) { W[kOffHdr + 2] = KR_ERR_INVALID; return; }
+  for (int g = 0; g < nB; g++) { parent[g] = g; root_isl[g] = -1; }
+  for (int k = 0; k < nC; k++) {
+    const uint32_t a = cons[20 * (size_t)k], b = cons[20 * (size_t)k + 1];
+    if (a >= (uint32_t)nB || (b != 0xffffffffu && b >= (uint32_t)nB)) { W[kOffHdr + 2] = KR_ERR_INDEX; return; }
+    if (b != 0xffffffffu) {
+      int ra = (int)a, rb = (int)b;
+      while (parent[ra] != ra) { parent[ra] = parent[parent[ra]]; ra = parent[ra]; }
+      while (parent[rb] != rb) { parent[rb] = parent[parent[rb]]; rb = parent[rb]; }
+      if (ra != rb) parent[max(ra, rb)] = min(ra, rb);
+    }
+  }
+  int nI = 0;
+  for (int g = 0; g < nB; g++) {
+    int r = g;
+    while (parent[r] != r) r = parent[r];
+    if (root_isl[r] < 0) root_isl[r] = nI++;
+    island_of[g] = root_isl[r];
+  }
+  // bodies per island, ascending
+  for (int I = 0; I <= nI; I++) cnt[I] = 0;
+  for (int g = 0; g < nB; g++) cnt[island_of[g] + 1]++;
+  for (int I = 0; I < nI; I++) cnt[I + 1] += cnt[I];
+  for (int I = 0; I < nI; I++) {
+    int *rec = isl + I * kIslandInts;
+    rec[I_BODY_OFF] = cnt[I];
+    rec[I_NB] = cnt[I + 1] - cnt[I];
+    if (rec[I_NB] > KR_MAX_ISLAND_BODIES) { W[kOffHdr + 2] = KR_ERR_CAPACITY; return; }
+  }
+  for (int I = 0; I < nI; I++) cur[I] = cnt[I];
+  for (int g = 0; g < nB; g++) {
+    const int I = island_of[g];
+    local[g] = cur[I] - cnt[I];
+    ib[cur[I]++] = g;
+  }
+  // constraints per island, list order
+  for (int I = 0; I <= nI; I++) cnt[I] = 0;
+  for (int k = 0; k < nC; k++) cnt[island_of[cons[20 * (size_t)k]] + 1]++;
+  for (int I = 0; I < nI; I++) cnt[I + 1] += cnt[I];
+  for (int I = 0; I < nI; I++) cur[I] = cnt[I];
+  for (int k = 0; k < nC; k++) icons[cur[island_of[cons[20 * (size_t)k]]]++] = k;
+  // levels per island, then a stable counting sort of its slots by level
+  int lvl_off = 0, pt_off = 0;
+  for (int I = 0; I < nI; I++) {
+    int *rec = isl + I * kIslandInts;
+    const int co = cnt[I], nc = cnt[I + 1] - cnt[I], bo = rec[I_BODY_OFF], nb = rec[I_NB];
+    if (nc > KR_MAX_ISLAND_CONSTRAINTS) { W[kOffHdr + 2] = KR_ERR_CAPACITY; return; }
+    for (int j = 0; j < nb; j++) last[j] = -1;
+    int nlv = 0;
+    for (int q = 0; q < nc; q++) {
+      const uint32_t *c = cons + 20 * (size_t)icons[co + q];
+      const int a = local[c[0]];
+      const int b = c[1] == 0xffffffffu ? -1 : local[c[1]];
+      int L = last[a] + 1;
+      if (b >= 0) L = max(L, last[b] + 1);
+      level[q] = L;
+      last[a] = L;
+      if (b >= 0) last[b] = L;
+      nlv = max(nlv, L + 1);
+    }
+    if (nlv > KR_MAX_LEVELS) { W[kOffHdr + 2] = KR_ERR_CAPACITY; return; }
+    int *lv = lvl + lvl_off;
+    for (int L = 0; L <= nlv; L++) lv[L] = 0;
+    for (int q = 0; q < nc; q++) lv[level[q] + 1]++;
+    for (int L = 0; L < nlv; L++) lv[L + 1] += lv[L];
+    // stable sort of the island's slots by level; `last` is reused as the
+    // per-level cursor (nlv <= KR_MAX_LEVELS < bodies region) and `level`
+    // then holds each list position's destination slot
+    for (int L = 0; L < nlv; L++) last[L] = lv[L];
+    for (int q = 0; q < nc; q++) {
+      const int k = icons[co + q];
+      const int s = last[level[q]]++;
+      // iab holds the final slot's body pair; icons is rewritten after
+      const uint32_t *c = cons + 20 * (size_t)k;
+      const uint32_t a = (uint32_t)local[c[0]];
+      const uint32_t b = c[1] == 0xffffffffu ? 0xffffu : (uint32_t)local[c[1]];
+      iab[co + s] = (int)(a | (b << 16));
+      level[q] = s;  // destination slot of list position q
+    }
+    // permute constraint ids into slot order via the `cur` tail as temp
+    for (int q = 0; q < nc; q++) cur[q] = icons[co + q];
+    for (int q = 0; q < nc; q++) icons[co + level[q]] = cur[q];
+    rec[I_CON_OFF] = co;
+    rec[I_NC] = nc;
+    rec[I_LVL_OFF] = lvl_off;
+    rec[I_NLV] = nlv;
+    lvl_off += nlv + 1;
+    // collision points in local body order
+    rec[I_PT_OFF] = pt_off;
+    int np = 0;
+    for (int j = 0; j < nb; j++) {
+      const int g = ib[bo + j];
+      const uint32_t off = coll_range[g], cn = coll_range[nB + g];
+      bpt[bo + j] = make_int2(np, (int)cn);
+      for (uint32_t q = 0; q < cn; q++) ipts[pt_off + np + (int)q] = (int)(off + q);
+      np += (int)cn;
+    }
+    if (np > KR_MAX_ISLAND_COLLPTS) { W[kOffHdr + 2] = KR_ERR_CAPACITY; return; }
+    rec[I_NP] = np;
+    pt_off += np;
+  }
+  // rects and the culling distance, as kr_create derives them
+  double half_thick = 0.0, r_max = 0.0;
+  for (int i = 0; i < nR; i++) {
+    const float x = rects[4 * i], y = rects[4 * i + 1], rw = rects[4 * i + 2], rh = rects[4 * i + 3];
+    r4[i] = make_float4(x, y, x + rw, y + rh);
+    const double ht = 0.5 * fmin(fabs((double)rw), fabs((double)rh));
+    half_thick = isfinite(ht) ? fmax(half_thick, ht) : HUGE_VAL;
+  }
+  for (int i = 0; i < nP; i++) {
+    const float r = __uint_as_float(coll_pts[4 * i + 3]);
+    r_max = isfinite(r) ? fmax(r_max, fabs((double)r)) : HUGE_VAL;
+  }
+  const double cull = fmax(r_max, half_thick) + 2.0 + kr::kCullSlack + 1.0;
+  reinterpret_cast<float *>(W)[kOffHdr + 1] = (isfinite(cull) && cull < 1e30) ? (float)cull : 1e30f;
+  W[kOffHdr + 0] = nI;
+}
+
+__global__ void __launch_bounds__(32 * kWarpsPerBlock) noalloc_step_kernel(StepArgs A, const int *W) {
+  StepArgs B = A;
+  B.nI = W[kOffHdr + 0];
+  B.cull_d = reinterpret_cast<const float *>(W)[kOffHdr + 1];
+  if (W[kOffHdr + 2] != KR_OK) return;
+  plain_step_body(B);
+}
+
+int g_noalloc_status_host = 0;
+void *g_noalloc_ptr[64] = {nullptr};
+
+}  // namespace
+
+extern "C" int kr_step_noalloc(const kr_solver_params *params, uint32_t n_bodies, uint32_t n_constraints,
+                               float *bodies, uint32_t *cons, float *forces, const float *rects,
+                               uint32_t n_rects, const uint32_t *coll_pts, uint32_t n_coll_pts,
+                               const uint32_t *coll_range, int32_t n_steps, void *stream) {
+  if (!params || !bodies || !forces || !rects || !coll_range || (n_constraints && !cons) ||
+      (n_coll_pts && !coll_pts) || n_steps < 0)
+    return KR_ERR_INVALID;
+  const kr_solver_params &p = *params;
+  const float hf = static_cast<float>(p.h);
+  if (!(p.iterations >= 1 && p.iterations <= 64) || !(p.substeps >= 1 && p.substeps <= 64) ||
+      !(hf > 0.f && hf < 1.f) || n_bodies < 1 || n_rects < 1)
+    return KR_ERR_INVALID;
+  if (n_bodies > (uint32_t)kNaB || n_constraints > (uint32_t)kNaC || n_coll_pts > (uint32_t)kNaP ||
+      n_rects > (uint32_t)kNaR)
+    return KR_ERR_CAPACITY;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return KR_ERR_CUDA;
+  // set-up once per device, with that device current: the device address of
+  // the scratch array (its host-side name is only a stand-in)
+  if (!g_noalloc_ptr[dev]) {
+    void *ptr = nullptr;
+    if (cudaGetSymbolAddress(&ptr, g_noalloc_scratch) != cudaSuccess || !ptr) return KR_ERR_CUDA;
+    g_noalloc_ptr[dev] = ptr;
+  }
+  int *W = static_cast<int *>(g_noalloc_ptr[dev]);
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  if (n_steps == 0) return KR_OK;
+  noalloc_schedule_kernel<<<1, 32, 0, st>>>(W, bodies, cons, rects, coll_pts, coll_range,
+                                           (int)n_bodies, (int)n_constraints, (int)n_coll_pts,
+                                           (int)n_rects);
+  if (cudaGetLastError() != cudaSuccess) return KR_ERR_CUDA;
+  // the builder's verdict decides the return code (a 4-byte copy into static
+  // host memory, which also orders this call after the builder)
+  if (cudaMemcpyAsync(&g_noalloc_status_host, W + kOffHdr + 2, sizeof(int), cudaMemcpyDeviceToHost,
+                      st) != cudaSuccess ||
+      cudaStreamSynchronize(st) != cudaSuccess)
+    return KR_ERR_CUDA;
+  if (g_noalloc_status_host != KR_OK) return g_noalloc_status_host;
+  StepArgs A;
+  A.K.h = hf;
+  A.K.invH = static_cast<float>(1.0 / p.h);
+  A.K.invH2 = static_cast<float>(1.0 / (p.h * p.h));
+  const float nl = -static_cast<float>(p.lin_drag), na = -static_cast<float>(p.ang_drag);
+  A.K.linDamp = static_cast<float>(std::exp(static_cast<double>(nl * hf)));
+  A.K.angDamp = static_cast<float>(std::exp(static_cast<double>(na * hf)));
+  A.K.maxSpeed = static_cast<float>(p.max_speed);
+  A.K.maxAngSpeed = static_cast<float>(p.max_ang_speed);
+  A.K.substeps = p.substeps;
+  A.K.iterations = p.iterations;
+  A.bodies = bodies;
+  A.cons = cons;
+  A.forces = forces;
+  A.coll = reinterpret_cast<const uint4 *>(coll_pts);
+  A.rects = reinterpret_cast<const float4 *>(W + kOffRects);
+  A.nR = (int)n_rects;
+  A.cull_d = 0.f;
+  A.nI = 0;
+  // shared memory for the largest island the world can hold
+  A.maxB = ((int)std::min<uint32_t>(n_bodies, KR_MAX_ISLAND_BODIES) + 3) & ~3;
+  A.maxC = ((int)std::min<uint32_t>(std::max<uint32_t>(n_constraints, 1), KR_MAX_ISLAND_CONSTRAINTS) + 3) & ~3;
+  A.maxP = ((int)std::min<uint32_t>(std::max<uint32_t>(n_coll_pts, 1), KR_MAX_ISLAND_COLLPTS) + 3) & ~3;
+  A.T = DeviceTables{W + kOffIsl, W + kOffBodies, W + kOffCons, W + kOffAb, W + kOffPts,
+                     reinterpret_cast<const int2 *>(W + kOffBpt), W + kOffLvl};
+  const size_t smem = sizeof(float) * kWarpsPerBlock * (size_t)warp_smem_words(A.maxB, A.maxC, A.maxP);
+  if (cudaFuncSetAttribute(noalloc_step_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)smem) != cudaSuccess)
+    return KR_ERR_CUDA;
+  const int grid = ((int)n_bodies + kWarpsPerBlock - 1) / kWarpsPerBlock;  // islands <= bodies
+  for (int s = 0; s < n_steps; s++) {
+    noalloc_step_kernel<<<grid, 32 * kWarpsPerBlock, smem, st>>>(A, W);
+    if (cudaGetLastError() != cudaSuccess) return KR_ERR_CUDA;
+  }
+  return KR_OK;
 }
