@@ -112,6 +112,11 @@ int kr_batch_read_state(kr_batch *b, int32_t first, int32_t n, float *bodies, fl
  * the proprioception read at the start of env step t. */
 int kr_batch_read_obs(kr_batch *b, int32_t first, int32_t n, float *obs);
 
+/* The controls each slot used in its last env step (synchronous): n x
+ * KR_BATCH_MAX_ARMS * (KR_BATCH_MAX_SEGS + 1) f32 in the kr_batch_set_controls
+ * record layout (motor controls before clamping, adhesion values). */
+int kr_batch_read_controls(kr_batch *b, int32_t first, int32_t n, float *controls);
+
 /* Per-slot accumulators (synchronous): n x 4 f64 -- path length of the
  * mantle, x and y of the mantle, attach events. */
 int kr_batch_read_fitness(kr_batch *b, int32_t first, int32_t n, double *out);
@@ -127,9 +132,18 @@ int kr_batch_restore(kr_batch *b);
  * second over every SM), the issue-rate ceiling of the f32 path. */
 int kr_probe_fp32_rate(double *fma_per_s);
 
-/* Launch shape: warps (creatures) per CTA (1..16) and CTAs per SM
- * (0 = as many as fit). */
-int kr_batch_set_launch(kr_batch *b, int32_t warps_per_cta, int32_t ctas_per_sm);
+/* Launch shape: lanes per creature (32, 16 or 8: a warp carries 32 / lanes
+ * creatures), warps per CTA (1..16, at most 64 creatures per CTA) and CTAs
+ * per SM (0 = 16 / warps).  A CTA gets an equal share of the SM's shared
+ * memory; a group of one body template holds as many creatures as fit in it.
+ * Results do not depend on the launch shape. */
+int kr_batch_set_launch(kr_batch *b, int32_t lanes_per_creature, int32_t warps_per_cta,
+                        int32_t ctas_per_sm);
+
+/* The current launch shape and the dynamic shared memory of a CTA (bytes;
+ * 0 before the first spawn).  Any pointer may be NULL. */
+int kr_batch_get_launch(kr_batch *b, int32_t *lanes_per_creature, int32_t *warps_per_cta,
+                        int32_t *ctas_per_sm, int32_t *smem_bytes);
 
 /* Device time of the last kr_batch_run launch in ms (synchronous). */
 int kr_batch_last_ms(kr_batch *b, float *ms);

@@ -63,7 +63,9 @@ def _lib():
         "kr_batch_read_state": (C.c_int, [vp, i32, i32, _F32P, _F32P, _I32P]),
         "kr_batch_read_obs": (C.c_int, [vp, i32, i32, _F32P]),
         "kr_batch_read_fitness": (C.c_int, [vp, i32, i32, _F64P]),
-        "kr_batch_set_launch": (C.c_int, [vp, i32, i32]),
+        "kr_batch_read_controls": (C.c_int, [vp, i32, i32, _F32P]),
+        "kr_batch_set_launch": (C.c_int, [vp, i32, i32, i32]),
+        "kr_batch_get_launch": (C.c_int, [vp, _I32P, _I32P, _I32P, _I32P]),
         "kr_batch_last_ms": (C.c_int, [vp, _F32P]),
         "kr_batch_sync": (C.c_int, [vp]),
         "kr_batch_set_stream": (C.c_int, [vp, vp]),
@@ -162,8 +164,17 @@ class BatchEngine:
     def restore(self):
         _check(_lib().kr_batch_restore(self.h), self.h)
 
-    def set_launch(self, warps_per_cta, ctas_per_sm=0):
-        _check(_lib().kr_batch_set_launch(self.h, warps_per_cta, ctas_per_sm), self.h)
+    def set_launch(self, warps_per_cta, ctas_per_sm=0, lanes_per_creature=32):
+        """Launch shape: G lanes per creature (32, 16 or 8), warps per CTA,
+        CTAs per SM (0: 16 / warps).  Results do not depend on it."""
+        _check(_lib().kr_batch_set_launch(self.h, lanes_per_creature, warps_per_cta, ctas_per_sm),
+               self.h)
+
+    def get_launch(self):
+        v = [C.c_int32() for _ in range(4)]
+        _check(_lib().kr_batch_get_launch(self.h, *[C.byref(x) for x in v]), self.h)
+        return {"lanes_per_creature": v[0].value, "warps_per_cta": v[1].value,
+                "ctas_per_sm": v[2].value, "smem_bytes": v[3].value}
 
     def run(self, max_steps):
         _check(_lib().kr_batch_run(self.h, max_steps), self.h)
@@ -206,6 +217,14 @@ class BatchEngine:
         n = self.capacity - first if n is None else n
         out = np.zeros((n, self.obs_ring, OBS_STRIDE), dtype=np.float32)
         _check(_lib().kr_batch_read_obs(self.h, first, n, out.ctypes.data_as(_F32P)), self.h)
+        return out
+
+    def read_controls(self, first=0, n=None):
+        """Controls of each slot's last env step: (n, CTRL_STRIDE) f32, motor
+        controls (arm-major, shoulder first) then adhesion values."""
+        n = self.capacity - first if n is None else n
+        out = np.zeros((n, CTRL_STRIDE), dtype=np.float32)
+        _check(_lib().kr_batch_read_controls(self.h, first, n, out.ctypes.data_as(_F32P)), self.h)
         return out
 
     def read_fitness(self, first=0, n=None):

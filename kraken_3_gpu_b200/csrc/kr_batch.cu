@@ -1,14 +1,18 @@
 // kr_batch.cu -- the batched creature engine (include/kraken_batch.h).
 //
-// Work unit: a group of up to W creatures of one body template.  A CTA of W
-// warps takes a group from a device queue, stages the template's static
-// arrays once in shared memory, and each warp advances one creature for the
-// whole run (up to max_steps env steps) with its state in shared memory and
-// registers.  Groups are queued longest-remaining-horizon first so the tail
-// of a run is short.  Per env step the warp computes the proprioception of
-// the current state (f64, lanes over arms), draws or reads the controls,
-// runs the suction-cup reflex (f64, lane per arm), then the XPBD step of
-// kr_solver.cuh (f32 in f32solver.mjs op order) and the grip break.
+// Work unit: a group of creatures of one body template.  A CTA of W warps
+// takes a group from a device queue and stages the template's static arrays
+// once in shared memory; every creature is advanced by G lanes of one warp
+// (G = 32, 16 or 8, so a warp carries 32 / G creatures) for the whole run (up
+// to max_steps env steps) with its state in shared memory and registers.
+// Shared memory is carved per template: a CTA has a fixed budget, and a group
+// holds as many creatures of its template as fit (at most W * 32 / G), so
+// small bodies pack more creatures per CTA than large ones.  Groups are
+// queued longest-remaining-horizon first so the tail of a run is short.  Per
+// env step a creature's lanes compute the proprioception of the current state
+// (f64, lanes over arms), draw or read the controls, run the suction-cup
+// reflex (f64, lane per arm), then the XPBD step of kr_solver.cuh (f32 in
+// f32solver.mjs op order) and the grip break.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -24,7 +28,8 @@
 
 namespace {
 
-constexpr int kMaxW = 16;
+constexpr int kMaxW = 16;                                      // warps per CTA
+constexpr int kMaxCPC = 64;                                    // creatures per CTA (W * 32 / G)
 constexpr int kBodyPad = 76;                                   // >= kMaxTplBodies, /4
 constexpr int kStateStride = 6 * kBodyPad;                     // px py vx vy ang av
 constexpr int kCtrlStride = KR_BATCH_MAX_ARMS * (KR_BATCH_MAX_SEGS + 1);  // 80
@@ -42,7 +47,7 @@ struct TplDev {
 struct TplArrays {
   const float *im, *ii;
   const int *boff, *bcnt;
-  const int *ab, *type, *motor;
+  const int *ab, *type, *motor, *garm;
   const float *lax, *lay, *lbx, *lby, *rest, *minA, *maxA;
   const int *lvl;
   const float *plx, *ply, *pr;
@@ -74,9 +79,9 @@ struct BatchArgs {
   const float4 *rects;   // x y x+w y+h
   const int *map_off;    // n_maps + 1
   const float *map_cull; // per map cull distance
-  const int *groups;     // n_groups x W slot ids, -1 = empty
+  const int *groups;     // n_groups x cpc slot ids, -1 = empty
   int n_groups;
-  int W;
+  int cpc;               // creature entries per group (W * 32 / G)
   int *queue;            // group counter
   int max_steps;
   int ctrl_mode;
@@ -88,26 +93,28 @@ struct BatchArgs {
   const float *pw;       // n_individuals x n_params
   const int *pw_idx;     // individual of each slot
   int n_params;
-  // smem carve sizes
-  int mb, mc, mp;
 };
 
-// --- shared-memory layout -------------------------------------------------
+// --- shared-memory layout, carved per template ------------------------------
+// Every region is a multiple of 4 words, so each region and each creature's
+// base stay 16-byte aligned (the f64 and float4 views included).
 constexpr int kLvlWords = (kr::kMaxTplLevels + 1 + 3) & ~3;                 // 68
 constexpr int kArmWords = (3 * KR_BATCH_MAX_ARMS + KR_BATCH_MAX_ARMS * KR_BATCH_MAX_SEGS + 3) & ~3;
-constexpr int kPairDoubles = KR_BATCH_MAX_ARMS * (KR_BATCH_MAX_SEGS - 1);      // 64
-// every region a multiple of 4 words, so each region and each warp's base
-// stay 16-byte aligned (the f64 region included)
-__host__ __device__ inline int tpl_smem_words(int mb, int mc, int mp) {
-  return 5 * mb + 10 * mc + kLvlWords + 4 * mp + kArmWords;
+__host__ __device__ constexpr int r4(int n) { return (n + 3) & ~3; }
+
+// statics of the template, once per CTA
+__host__ __device__ inline int tpl_smem_words(int nb, int nc, int np) {
+  return 5 * r4(nb) + 11 * r4(nc) + 4 * r4(np) + kLvlWords + kArmWords;
 }
-__host__ __device__ inline int warp_smem_words(int mb, int mc, int mp) {
-  return 11 * mb + 8 * mc + 3 * mp + kr::kMaxCulled / 2 + kCtrlStride + 64 + 2 * kPairDoubles;
+// one creature: bodies, grip and motor state, lambda, collision scratch
+__host__ __device__ inline int creature_smem_words(int nb, int nc, int np, int arms, int segs) {
+  return 11 * r4(nb) + 2 * r4(nc) + r4(arms * segs) + r4(arms * segs + arms) + 4 * arms + 3 * r4(np) +
+         kr::kMaxCulled / 2;
 }
 
 struct TplSmem {
   float *im, *ii, *zero;
-  int *boff, *bcnt, *ab, *type, *motor;
+  int *boff, *bcnt, *ab, *type, *motor, *garm;
   float *lax, *lay, *lbx, *lby, *rest, *minA, *maxA;
   int *lvl;
   float *plx, *ply, *pr;
@@ -115,13 +122,15 @@ struct TplSmem {
   int *arm_tip, *arm_grip, *arm_seg0, *arm_segs;
 };
 
-__device__ inline void carve_tpl(TplSmem &P, float *p, int mb, int mc, int mp) {
+__device__ inline void carve_tpl(TplSmem &P, float *p, const TplDev &td) {
+  const int mb = r4(td.nb), mc = r4(td.nc), mp = r4(td.np);
   P.im = p; p += mb; P.ii = p; p += mb; P.zero = p; p += mb;
   P.boff = reinterpret_cast<int *>(p); p += mb;
   P.bcnt = reinterpret_cast<int *>(p); p += mb;
   P.ab = reinterpret_cast<int *>(p); p += mc;
   P.type = reinterpret_cast<int *>(p); p += mc;
   P.motor = reinterpret_cast<int *>(p); p += mc;
+  P.garm = reinterpret_cast<int *>(p); p += mc;
   P.lax = p; p += mc; P.lay = p; p += mc; P.lbx = p; p += mc; P.lby = p; p += mc;
   P.rest = p; p += mc; P.minA = p; p += mc; P.maxA = p; p += mc;
   P.lvl = reinterpret_cast<int *>(p); p += kLvlWords;
@@ -133,32 +142,40 @@ __device__ inline void carve_tpl(TplSmem &P, float *p, int mb, int mc, int mp) {
   P.arm_segs = reinterpret_cast<int *>(p);
 }
 
-struct WarpSmem {
-  float *ctrl;     // kCtrlStride
-  float *obs;      // 64
-  double *pair;    // kPairDoubles: atan2 terms of armCurl
+struct CreatureSmem {
+  float *ctrl;     // arms * segs motor controls, then arms adhesion values
+  float *obs;      // proprioception (aliases the collision scratch pdy)
+  double *pair;    // atan2 terms of armCurl (aliases the collision scratch pdx)
 };
 
-__device__ inline void carve_warp(kr::Island &S, WarpSmem &X, const TplSmem &P, float *p, int mb,
-                                  int mc, int mp) {
+__device__ inline void carve_creature(kr::Island &S, CreatureSmem &X, const TplSmem &P, float *p,
+                                      const TplDev &td) {
+  const int mb = r4(td.nb), mc = r4(td.nc), mp = r4(td.np), AS = td.arms * td.segs;
   S.px = p; p += mb; S.py = p; p += mb; S.ppx = p; p += mb; S.ppy = p; p += mb;
   S.vx = p; p += mb; S.vy = p; p += mb; S.ang = p; p += mb; S.angP = p; p += mb;
   S.av = p; p += mb; S.bs = p; p += mb; S.bc = p; p += mb;
-  S.tb = reinterpret_cast<int *>(p); p += mc;
-  S.lbx = p; p += mc; S.lby = p; p += mc; S.comp = p; p += mc; S.tgt = p; p += mc;
-  S.lamX = p; p += mc; S.lamY = p; p += mc; S.brk = p; p += mc;
+  S.lamX = p; p += mc; S.lamY = p; p += mc;
   S.lam = S.lamX;  // pins use lamX/lamY, angles lam: never both on one slot
+  S.tgt_m = p; p += r4(AS);
+  X.ctrl = p; p += r4(AS + td.arms);
+  S.anc = p; p += 4 * td.arms;
   S.pdx = p; p += mp; S.pdy = p; p += mp;
   S.pflag = reinterpret_cast<int *>(p); p += mp;
-  S.cull = reinterpret_cast<short *>(p); p += kr::kMaxCulled / 2;
-  X.ctrl = p; p += kCtrlStride;
-  X.obs = p; p += 64;
-  X.pair = reinterpret_cast<double *>(p);
+  S.cull = reinterpret_cast<short *>(p);
+  // proprioception scratch: live only before the XPBD step of an env step,
+  // when the collision scratch is dead (2 * arms * (segs - 1) <= np and
+  // 6 * arms + 6 <= np for every template shape)
+  X.pair = reinterpret_cast<double *>(S.pdx);
+  X.obs = S.pdy;
   // statics shared by the CTA
   S.im = P.im; S.ii = P.ii; S.fx = P.zero; S.fy = P.zero; S.tq = P.zero;
-  S.ab = P.ab; S.lax = P.lax; S.lay = P.lay; S.rest = P.rest; S.minA = P.minA; S.maxA = P.maxA;
+  S.ab = P.ab; S.type = P.type; S.garm = P.garm; S.motor = P.motor;
+  S.lax = P.lax; S.lay = P.lay; S.lbx = P.lbx; S.lby = P.lby;
+  S.rest = P.rest; S.minA = P.minA; S.maxA = P.maxA;
   S.plx = P.plx; S.ply = P.ply; S.pr = P.pr; S.pbody = P.pbody; S.boff = P.boff; S.bcnt = P.bcnt;
   S.lvl = P.lvl;
+  S.tb = nullptr; S.comp = nullptr; S.tgt = nullptr; S.brk = nullptr;
+  S.nb = td.nb; S.nc = td.nc; S.np = td.np; S.nlv = td.nlv;
 }
 
 __device__ inline double mulberry_next(uint32_t &s) {
@@ -173,19 +190,21 @@ __device__ inline double clamp_sym(double v, double m) { return v > m ? m : (v <
 
 // proprioception of the current state, readProprio (core.js:129-175), f64;
 // writes 6A+6 values into X.obs and returns the attached-arm bitmask
+template <int G>
 __device__ unsigned proprio(const BatchArgs &A, const TplDev &td, const TplSmem &P, kr::Island &S,
-                            WarpSmem &X, SlotMeta &m, const float4 *grip_st, int lane) {
-  const int arms = td.arms, segs = td.segs;
+                            CreatureSmem &X, SlotMeta &m, const kr::Lanes<G> &L) {
+  const int arms = td.arms, segs = td.segs, lane = L.lane;
+  const float4 *grip_st = reinterpret_cast<const float4 *>(S.anc);
   const double cx = S.px[0], cy = S.py[0], cvx = S.vx[0], cvy = S.vy[0];
   const double angle = S.ang[0], cav = S.av[0];
   // armCurl terms: atan2(sin d, cos d) per adjacent segment pair
   const int npair = arms * (segs - 1);
-  for (int q = lane; q < npair; q += 32) {
+  for (int q = lane; q < npair; q += G) {
     const int a = q / (segs - 1), i = q % (segs - 1) + 1;
     const double d = (double)S.ang[P.arm_segs[a * segs + i]] - (double)S.ang[P.arm_segs[a * segs + i - 1]];
     X.pair[q] = atan2(sin(d), cos(d));
   }
-  __syncwarp();
+  L.sync();
   double ext = 0.0, curl = 0.0, sh = 0.0, tx = 0.0, ty = 0.0;
   bool attached = false;
   if (lane < arms) {
@@ -202,10 +221,10 @@ __device__ unsigned proprio(const BatchArgs &A, const TplDev &td, const TplSmem 
     ext = fmin(1.0, hypot(tx - (double)S.px[s0], ty - (double)S.py[s0]) / fmax(1.0, td.reach));
     attached = grip_st[a].w == 0.f;
   }
-  const unsigned att = __ballot_sync(0xffffffffu, attached) & ((1u << arms) - 1u);
+  const unsigned att = L.ballot(attached) & ((1u << arms) - 1u);
   // sums in arm order, like the sequential loop
   double ext_sum = 0.0;
-  for (int a = 0; a < arms; a++) ext_sum += __shfl_sync(0xffffffffu, ext, a);
+  for (int a = 0; a < arms; a++) ext_sum += __shfl_sync(L.mask, ext, a, G);
   const double ca = cos(-angle), sa = sin(-angle);
   const double SL = kPiD * 0.62, JL = kPiD * 0.42;
   if (lane < arms) {
@@ -232,56 +251,190 @@ __device__ unsigned proprio(const BatchArgs &A, const TplDev &td, const TplSmem 
     X.obs[6 * arms + 4] = (float)fmin(1.0, hypot(cvx, cvy) / 300);
     X.obs[6 * arms + 5] = (float)fmax(-1.0, fmin(1.0, cav / 18));
   }
-  __syncwarp();
+  L.sync();
   return att;
 }
 
-// fused policy (one warp): proprio (n_in = 6A + 6) -> 64 tanh -> A*S motor
+// fused policy (G lanes): proprio (n_in = 6A + 6) -> 64 tanh -> A*S motor
 // targets (tanh) + A adhesion values ((tanh + 1) / 2).  Weights of the
 // slot's individual, row-major with the bias last: W1 64 x (n_in + 1), then
-// W2 n_out x 65.
-__device__ void policy(const BatchArgs &A, const TplDev &td, WarpSmem &X, int slot, int lane) {
-  const int n_in = 6 * td.arms + 6, n_out = td.arms * td.segs + td.arms;
+// W2 n_out x 65.  Every dot product accumulates in index order.
+template <int G>
+__device__ void policy(const BatchArgs &A, const TplDev &td, CreatureSmem &X, int slot,
+                       const kr::Lanes<G> &L) {
+  constexpr int HPL = KR_POLICY_HIDDEN / G;  // hidden units per lane
+  const int n_in = 6 * td.arms + 6, n_out = td.arms * td.segs + td.arms, lane = L.lane;
   const float *w = A.pw + (size_t)A.pw_idx[slot] * A.n_params;
-  float hid[2];
-  for (int u = 0; u < 2; u++) {
-    const float *row = w + (size_t)(lane + 32 * u) * (n_in + 1);
+  float hid[HPL];
+#pragma unroll
+  for (int u = 0; u < HPL; u++) {
+    const float *row = w + (size_t)(lane + G * u) * (n_in + 1);
     float acc = __ldg(row + n_in);
     for (int i = 0; i < n_in; i++) acc = fmaf(__ldg(row + i), X.obs[i], acc);
     hid[u] = tanhf(acc);
   }
   const float *w2 = w + (size_t)KR_POLICY_HIDDEN * (n_in + 1);
-  for (int base = 0; base < n_out; base += 32) {
+  for (int base = 0; base < n_out; base += G) {
     const int o = base + lane;
     const float *row = w2 + (size_t)(o < n_out ? o : 0) * (KR_POLICY_HIDDEN + 1);
     float acc = o < n_out ? __ldg(row + KR_POLICY_HIDDEN) : 0.f;
-    for (int j = 0; j < KR_POLICY_HIDDEN; j++) {
-      const float hj = __shfl_sync(0xffffffffu, hid[j >> 5], j & 31);
-      if (o < n_out) acc = fmaf(__ldg(row + j), hj, acc);
+#pragma unroll
+    for (int u = 0; u < HPL; u++) {
+      for (int j = 0; j < G; j++) {
+        const float hj = __shfl_sync(L.mask, hid[u], j, G);
+        if (o < n_out) acc = fmaf(__ldg(row + u * G + j), hj, acc);
+      }
     }
     if (o < n_out) {
       const float y = tanhf(acc);
       X.ctrl[o] = o < td.arms * td.segs ? y : 0.5f * (y + 1.f);
     }
   }
-  __syncwarp();
+  L.sync();
 }
 
-__global__ void __launch_bounds__(32 * kMaxW) batch_kernel(BatchArgs A) {
-  extern __shared__ float smem[];
+// One creature (slot) advanced by its G lanes for up to A.max_steps env steps.
+template <int G>
+__device__ void run_creature(const BatchArgs &A, const TplDev &td, const TplSmem &P, float *base,
+                             int slot, const kr::Lanes<G> &L) {
+  const int lane = L.lane;
+  kr::Island S;
+  CreatureSmem X;
+  carve_creature(S, X, P, base, td);
+  SlotMeta m = A.meta[slot];
+  const int steps = min(A.max_steps, m.horizon - m.step);
+  if (steps <= 0) return;
+  const int arms = td.arms, AS = td.arms * td.segs;
+  const float *st = A.state + (size_t)slot * kStateStride;
+  float4 *gst = A.grip + (size_t)slot * KR_BATCH_MAX_ARMS;
+  float2 *glam = A.glam + (size_t)slot * KR_BATCH_MAX_ARMS;
+  double *cdp = A.cd + (size_t)slot * KR_BATCH_MAX_ARMS;
+  for (int i = lane; i < td.nb; i += G) {
+    S.px[i] = st[i]; S.py[i] = st[kBodyPad + i]; S.vx[i] = st[2 * kBodyPad + i];
+    S.vy[i] = st[3 * kBodyPad + i]; S.ang[i] = st[4 * kBodyPad + i]; S.av[i] = st[5 * kBodyPad + i];
+  }
+  for (int k = lane; k < td.nc; k += G) { S.lamX[k] = 0.f; S.lamY[k] = 0.f; }
+  S.comp_m = m.comp;
+  double cd = 0.0;  // reflex cooldown of arm `lane`
+  L.sync();
+  if (lane < arms) {
+    reinterpret_cast<float4 *>(S.anc)[lane] = gst[lane];
+    const float2 gl = glam[lane];
+    const int k = P.arm_grip[lane];
+    S.lamX[k] = gl.x; S.lamY[k] = gl.y;
+    cd = cdp[lane];
+  }
+  const float *cin = A.ctrl_cur + (size_t)slot * kCtrlStride;
+  for (int q = lane; q < AS + arms; q += G) X.ctrl[q] = cin[q];
+  L.sync();
+  const float4 *rects = A.rects + A.map_off[m.map];
+  const int nR = A.map_off[m.map + 1] - A.map_off[m.map];
+  const float cull_d = fmaxf(A.map_cull[m.map], td.r_max + 2.f + kr::kCullSlack + 1.f);
+  for (int s = 0; s < steps; s++) {
+    const int t = m.step;
+    // 1. proprioception of the current state
+    if (A.obs_ring > 0 || A.ctrl_mode == KR_CTRL_POLICY) {
+      const unsigned att = proprio<G>(A, td, P, S, X, m, L);
+      if (A.obs_ring > 0) {
+        float *o = A.obs + ((size_t)slot * A.obs_ring + (t % A.obs_ring)) * KR_OBS_STRIDE;
+        for (int q = lane; q < 6 * arms + 6; q += G) o[q] = X.obs[q];
+        if (lane == 0) o[KR_OBS_STRIDE - 1] = __uint_as_float(att);
+      }
+    }
+    // 2. controls
+    if (A.ctrl_mode == KR_CTRL_STREAM) {
+      if (t % A.ctrl_period == 0 && lane == 0) {
+        uint32_t r = m.rng;
+        for (int a = 0; a < arms; a++) {
+          for (int j = 0; j < td.segs; j++) X.ctrl[a * td.segs + j] = (float)(mulberry_next(r) * 2 - 1);
+          X.ctrl[AS + a] = (float)mulberry_next(r);
+        }
+        m.rng = r;
+      }
+    } else if (A.ctrl_mode == KR_CTRL_POLICY) {
+      policy<G>(A, td, X, slot, L);
+    }
+    L.sync();
+    // 3. applyControl: targets (clamped) and the reflex, core.js:183-220
+    for (int mo = lane; mo < AS; mo += G) {
+      const double lim = (mo % td.segs) == 0 ? kPiD * 0.62 : kPiD * 0.42;
+      S.tgt_m[mo] = (float)fmax(-lim, fmin(lim, (double)X.ctrl[mo]));
+    }
+    bool attached_now = false;
+    if (lane < arms) {
+      const int a = lane, k = P.arm_grip[a], tip = P.arm_tip[a];
+      float *an = S.anc + 4 * a;
+      const double adh = fmax(0.0, fmin(1.0, (double)X.ctrl[AS + a]));
+      double c = cd;
+      if (c > 0) c -= A.dt;
+      if (an[3] != 0.f) {
+        if (adh > 0.08 && c <= 0) {
+          const double slip = hypot((double)S.vx[tip], (double)S.vy[tip]);
+          if (slip < A.slip_max) {
+            const double ta = (double)S.ang[tip];
+            an[0] = (float)((double)S.px[tip] + kSegHalf * cos(ta));
+            an[1] = (float)((double)S.py[tip] + kSegHalf * sin(ta));
+            an[2] = (float)(40.0 + 860.0 * adh);
+            an[3] = 0.f;
+            S.lamX[k] = 0.f; S.lamY[k] = 0.f;
+            attached_now = true;
+          } else {
+            c = A.cooldown;
+          }
+        }
+      } else {
+        an[2] = (float)(40.0 + 860.0 * adh);
+        if (adh < 0.04) an[3] = 1.f;
+      }
+      cd = c;
+    }
+    m.attach_events += __popc(L.ballot(attached_now));
+    L.sync();
+    // 4. the XPBD step
+    kr::island_step<kr::CompactAccess, G>(A.K, S, rects, nR, cull_d, L);
+    // 5. bookkeeping
+    if (lane == 0) {
+      const double x = S.px[0], y = S.py[0];
+      m.path_len += hypot(x - m.last_x, y - m.last_y);
+      m.last_x = x; m.last_y = y;
+    }
+    m.step = t + 1;
+  }
+  // write back
+  float *sw = A.state + (size_t)slot * kStateStride;
+  for (int i = lane; i < td.nb; i += G) {
+    sw[i] = S.px[i]; sw[kBodyPad + i] = S.py[i]; sw[2 * kBodyPad + i] = S.vx[i];
+    sw[3 * kBodyPad + i] = S.vy[i]; sw[4 * kBodyPad + i] = S.ang[i]; sw[5 * kBodyPad + i] = S.av[i];
+  }
+  if (lane < arms) {
+    const int k = P.arm_grip[lane];
+    gst[lane] = reinterpret_cast<const float4 *>(S.anc)[lane];
+    glam[lane] = make_float2(S.lamX[k], S.lamY[k]);
+    cdp[lane] = cd;
+  }
+  float *cout = A.ctrl_cur + (size_t)slot * kCtrlStride;
+  for (int q = lane; q < AS + arms; q += G) cout[q] = X.ctrl[q];
+  if (lane == 0) A.meta[slot] = m;
+}
+
+template <int G>
+__global__ void __launch_bounds__(32 * kMaxW, 1) batch_kernel(BatchArgs A) {
+  constexpr int CPW = 32 / G;  // creatures per warp
+  extern __shared__ __align__(16) float smem[];
   __shared__ int s_group;
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  TplSmem P;
-  carve_tpl(P, smem, A.mb, A.mc, A.mp);
-  float *wbase = smem + tpl_smem_words(A.mb, A.mc, A.mp) + warp * warp_smem_words(A.mb, A.mc, A.mp);
+  const int warp = threadIdx.x >> 5, wl = threadIdx.x & 31;
+  const kr::Lanes<G> L(wl);
+  const int c = warp * CPW + wl / G;  // creature entry of this lane group
   for (;;) {
     __syncthreads();
     if (threadIdx.x == 0) s_group = atomicAdd(A.queue, 1);
     __syncthreads();
     const int g = s_group;
     if (g >= A.n_groups) return;
-    const int first = A.groups[g * A.W];
+    const int first = A.groups[g * A.cpc];
     const TplDev td = A.tpl[A.meta[first].tpl];
+    TplSmem P;
+    carve_tpl(P, smem, td);
     // stage the template statics (whole CTA)
     for (int i = threadIdx.x; i < td.nb; i += blockDim.x) {
       P.im[i] = A.T.im[td.o_b + i]; P.ii[i] = A.T.ii[td.o_b + i]; P.zero[i] = 0.f;
@@ -289,7 +442,7 @@ __global__ void __launch_bounds__(32 * kMaxW) batch_kernel(BatchArgs A) {
     }
     for (int k = threadIdx.x; k < td.nc; k += blockDim.x) {
       const int o = td.o_c + k;
-      P.ab[k] = A.T.ab[o]; P.type[k] = A.T.type[o]; P.motor[k] = A.T.motor[o];
+      P.ab[k] = A.T.ab[o]; P.type[k] = A.T.type[o]; P.motor[k] = A.T.motor[o]; P.garm[k] = A.T.garm[o];
       P.lax[k] = A.T.lax[o]; P.lay[k] = A.T.lay[o]; P.lbx[k] = A.T.lbx[o]; P.lby[k] = A.T.lby[o];
       P.rest[k] = A.T.rest[o]; P.minA[k] = A.T.minA[o]; P.maxA[k] = A.T.maxA[o];
     }
@@ -304,145 +457,11 @@ __global__ void __launch_bounds__(32 * kMaxW) batch_kernel(BatchArgs A) {
     }
     for (int q = threadIdx.x; q < td.arms * td.segs; q += blockDim.x) P.arm_segs[q] = A.T.arm_segs[td.o_s + q];
     __syncthreads();
-
-    const int slot = warp < A.W ? A.groups[g * A.W + warp] : -1;
+    const int slot = c < A.cpc ? A.groups[g * A.cpc + c] : -1;
     if (slot >= 0) {
-      kr::Island S;
-      WarpSmem X;
-      carve_warp(S, X, P, wbase, A.mb, A.mc, A.mp);
-      S.nb = td.nb; S.nc = td.nc; S.np = td.np; S.nlv = td.nlv;
-      SlotMeta m = A.meta[slot];
-      const int steps = min(A.max_steps, m.horizon - m.step);
-      const float *st = A.state + (size_t)slot * kStateStride;
-      float4 *gst = A.grip + (size_t)slot * KR_BATCH_MAX_ARMS;
-      float2 *glam = A.glam + (size_t)slot * KR_BATCH_MAX_ARMS;
-      double *cd = A.cd + (size_t)slot * KR_BATCH_MAX_ARMS;
-      if (steps > 0) {
-        for (int i = lane; i < td.nb; i += 32) {
-          S.px[i] = st[i]; S.py[i] = st[kBodyPad + i]; S.vx[i] = st[2 * kBodyPad + i];
-          S.vy[i] = st[3 * kBodyPad + i]; S.ang[i] = st[4 * kBodyPad + i]; S.av[i] = st[5 * kBodyPad + i];
-        }
-        for (int k = lane; k < td.nc; k += 32) {
-          const int ty = P.type[k];
-          S.tb[k] = ty;
-          S.lbx[k] = P.lbx[k]; S.lby[k] = P.lby[k];
-          S.comp[k] = ty == 1 ? m.comp : 0.f;
-          S.tgt[k] = 0.f;
-          S.brk[k] = 1e30f;
-          S.lamX[k] = 0.f; S.lamY[k] = 0.f;
-        }
-        __syncwarp();
-        if (lane < td.arms) {
-          const float4 gg = gst[lane];
-          const int k = P.arm_grip[lane];
-          S.lbx[k] = gg.x; S.lby[k] = gg.y; S.brk[k] = gg.z;
-          S.tb[k] = 2 | (gg.w != 0.f ? (1 << 8) : 0);
-          const float2 gl = glam[lane];
-          S.lamX[k] = gl.x; S.lamY[k] = gl.y;
-        }
-        if (A.ctrl_mode == KR_CTRL_BUFFER)
-          for (int q = lane; q < kCtrlStride; q += 32) X.ctrl[q] = A.ctrl_cur[(size_t)slot * kCtrlStride + q];
-        else if (A.ctrl_mode == KR_CTRL_STREAM)
-          for (int q = lane; q < kCtrlStride; q += 32) X.ctrl[q] = A.ctrl_cur[(size_t)slot * kCtrlStride + q];
-        __syncwarp();
-        const float4 *rects = A.rects + A.map_off[m.map];
-        const int nR = A.map_off[m.map + 1] - A.map_off[m.map];
-        const float cull_d = fmaxf(A.map_cull[m.map], td.r_max + 2.f + kr::kCullSlack + 1.f);
-        const int AS = td.arms * td.segs;
-        for (int s = 0; s < steps; s++) {
-          const int t = m.step;
-          // 1. proprioception of the current state
-          float4 gl = lane < td.arms ? make_float4(S.lbx[P.arm_grip[lane]], S.lby[P.arm_grip[lane]],
-                                                   S.brk[P.arm_grip[lane]],
-                                                   (S.tb[P.arm_grip[lane]] >> 8) ? 1.f : 0.f)
-                                     : make_float4(0.f, 0.f, 0.f, 0.f);
-          __shared__ float4 s_gl[kMaxW][KR_BATCH_MAX_ARMS];
-          if (lane < td.arms) s_gl[warp][lane] = gl;
-          __syncwarp();
-          if (A.obs_ring > 0 || A.ctrl_mode == KR_CTRL_POLICY) {
-            const unsigned att = proprio(A, td, P, S, X, m, s_gl[warp], lane);
-            if (A.obs_ring > 0) {
-              float *o = A.obs + ((size_t)slot * A.obs_ring + (t % A.obs_ring)) * KR_OBS_STRIDE;
-              for (int q = lane; q < 6 * td.arms + 6; q += 32) o[q] = X.obs[q];
-              if (lane == 0) o[KR_OBS_STRIDE - 1] = __uint_as_float(att);
-            }
-          }
-          // 2. controls
-          if (A.ctrl_mode == KR_CTRL_STREAM) {
-            if (t % A.ctrl_period == 0 && lane == 0) {
-              uint32_t r = m.rng;
-              for (int a = 0; a < td.arms; a++) {
-                for (int j = 0; j < td.segs; j++) X.ctrl[a * td.segs + j] = (float)(mulberry_next(r) * 2 - 1);
-                X.ctrl[AS + a] = (float)mulberry_next(r);
-              }
-              m.rng = r;
-            }
-          } else if (A.ctrl_mode == KR_CTRL_POLICY) {
-            policy(A, td, X, slot, lane);
-          }
-          __syncwarp();
-          // 3. applyControl: targets (clamped) and the reflex, core.js:183-220
-          for (int k = lane; k < td.nc; k += 32) {
-            const int mo = P.motor[k];
-            if (mo >= 0) {
-              const double lim = (mo % td.segs) == 0 ? kPiD * 0.62 : kPiD * 0.42;
-              S.tgt[k] = (float)fmax(-lim, fmin(lim, (double)X.ctrl[mo]));
-            }
-          }
-          bool attached_now = false;
-          if (lane < td.arms) {
-            const int a = lane, k = P.arm_grip[a], tip = P.arm_tip[a];
-            const double adh = fmax(0.0, fmin(1.0, (double)X.ctrl[AS + a]));
-            double c = cd[a];
-            if (c > 0) c -= A.dt;
-            if ((S.tb[k] >> 8) != 0) {
-              if (adh > 0.08 && c <= 0) {
-                const double slip = hypot((double)S.vx[tip], (double)S.vy[tip]);
-                if (slip < A.slip_max) {
-                  const double ta = (double)S.ang[tip];
-                  S.lbx[k] = (float)((double)S.px[tip] + kSegHalf * cos(ta));
-                  S.lby[k] = (float)((double)S.py[tip] + kSegHalf * sin(ta));
-                  S.tb[k] = 2;
-                  S.brk[k] = (float)(40.0 + 860.0 * adh);
-                  S.lamX[k] = 0.f; S.lamY[k] = 0.f;
-                  attached_now = true;
-                } else {
-                  c = A.cooldown;
-                }
-              }
-            } else {
-              S.brk[k] = (float)(40.0 + 860.0 * adh);
-              if (adh < 0.04) S.tb[k] = 2 | (1 << 8);
-            }
-            cd[a] = c;
-          }
-          m.attach_events += __popc(__ballot_sync(0xffffffffu, attached_now));
-          __syncwarp();
-          // 4. the XPBD step
-          kr::island_step(A.K, S, rects, nR, cull_d, lane);
-          // 5. bookkeeping
-          if (lane == 0) {
-            const double x = S.px[0], y = S.py[0];
-            m.path_len += hypot(x - m.last_x, y - m.last_y);
-            m.last_x = x; m.last_y = y;
-            m.step = t + 1;
-          }
-          m.step = t + 1;
-        }
-        // write back
-        float *sw = A.state + (size_t)slot * kStateStride;
-        for (int i = lane; i < td.nb; i += 32) {
-          sw[i] = S.px[i]; sw[kBodyPad + i] = S.py[i]; sw[2 * kBodyPad + i] = S.vx[i];
-          sw[3 * kBodyPad + i] = S.vy[i]; sw[4 * kBodyPad + i] = S.ang[i]; sw[5 * kBodyPad + i] = S.av[i];
-        }
-        if (lane < td.arms) {
-          const int k = P.arm_grip[lane];
-          gst[lane] = make_float4(S.lbx[k], S.lby[k], S.brk[k], (S.tb[k] >> 8) ? 1.f : 0.f);
-          glam[lane] = make_float2(S.lamX[k], S.lamY[k]);
-        }
-        for (int q = lane; q < kCtrlStride; q += 32) A.ctrl_cur[(size_t)slot * kCtrlStride + q] = X.ctrl[q];
-        if (lane == 0) A.meta[slot] = m;
-      }
+      float *base = smem + tpl_smem_words(td.nb, td.nc, td.np) +
+                    c * creature_smem_words(td.nb, td.nc, td.np, td.arms, td.segs);
+      run_creature<G>(A, td, P, base, slot, L);
     }
   }
 }
@@ -478,9 +497,8 @@ struct kr_batch {
   std::map<std::pair<int, int>, int> tpl_index;
   std::vector<TplDev> h_tpl;
   TplDev *d_tpl = nullptr;
-  void *d_tpl_arrays[22] = {nullptr};
+  void *d_tpl_arrays[23] = {nullptr};
   TplArrays T{};
-  int mb = 4, mc = 4, mp = 4;
   // maps
   float4 *d_rects = nullptr;
   int *d_map_off = nullptr;
@@ -511,9 +529,14 @@ struct kr_batch {
   SlotMeta *s_meta = nullptr;
   std::vector<int> s_remaining;
   int *s_groups = nullptr;        // groups built for the snapshot state
-  int s_n_groups = -1, s_W = 0;
+  int s_n_groups = -1, s_cpc = 0, s_G = 0;
   // launch shape
-  int W = 8, ctas_per_sm = 0, n_sm = 0;
+  int G = 16, W = 8, ctas_per_sm = 0, n_sm = 0;
+  int smem_per_sm = 0, smem_reserved = 0, smem_optin = 0;
+  int cpc = 8;                  // creature entries per group: W * 32 / G
+  std::vector<int> tpl_cpg;     // creatures per group of each template
+  size_t smem_dyn = 0;          // dynamic shared memory per CTA
+  bool shape_dirty = true;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   // policy
   float *d_pw = nullptr;
@@ -554,9 +577,8 @@ int ensure_template(kr_batch *b, int arms, int segs) {
 
 int upload_templates(kr_batch *b) {
   std::vector<float> im, ii, lax, lay, lbx, lby, rest, minA, maxA, plx, ply, pr;
-  std::vector<int> boff, bcnt, ab, type, motor, lvl, pbody, tip, grip, seg0, segs;
+  std::vector<int> boff, bcnt, ab, type, motor, garm, lvl, pbody, tip, grip, seg0, segs;
   b->h_tpl.clear();
-  int mb = 4, mc = 4, mp = 4;
   for (const auto &t : b->tpls) {
     TplDev d{};
     d.nb = t.nb; d.nc = t.nc; d.np = t.np; d.nlv = t.nlv; d.arms = t.arms; d.segs = t.segs;
@@ -567,6 +589,11 @@ int upload_templates(kr_batch *b) {
     boff.insert(boff.end(), t.boff.begin(), t.boff.end()); bcnt.insert(bcnt.end(), t.bcnt.begin(), t.bcnt.end());
     ab.insert(ab.end(), t.ab.begin(), t.ab.end()); type.insert(type.end(), t.type.begin(), t.type.end());
     motor.insert(motor.end(), t.motor.begin(), t.motor.end());
+    {
+      std::vector<int> ga(t.nc, -1);
+      for (int a = 0; a < t.arms; a++) ga[t.arm_grip[a]] = a;
+      garm.insert(garm.end(), ga.begin(), ga.end());
+    }
     lax.insert(lax.end(), t.lax.begin(), t.lax.end()); lay.insert(lay.end(), t.lay.begin(), t.lay.end());
     lbx.insert(lbx.end(), t.lbx.begin(), t.lbx.end()); lby.insert(lby.end(), t.lby.begin(), t.lby.end());
     rest.insert(rest.end(), t.rest.begin(), t.rest.end());
@@ -579,7 +606,6 @@ int upload_templates(kr_batch *b) {
     seg0.insert(seg0.end(), t.arm_seg0.begin(), t.arm_seg0.end());
     segs.insert(segs.end(), t.arm_segs.begin(), t.arm_segs.end());
     b->h_tpl.push_back(d);
-    mb = std::max(mb, (t.nb + 3) & ~3); mc = std::max(mc, (t.nc + 3) & ~3); mp = std::max(mp, (t.np + 3) & ~3);
   }
   cudaError_t e = cudaSuccess;
   void **A = b->d_tpl_arrays;
@@ -587,6 +613,7 @@ int upload_templates(kr_batch *b) {
   UP(0, im); UP(1, ii); UP(2, boff); UP(3, bcnt); UP(4, ab); UP(5, type); UP(6, motor); UP(7, lax);
   UP(8, lay); UP(9, lbx); UP(10, lby); UP(11, rest); UP(12, minA); UP(13, maxA); UP(14, lvl);
   UP(15, plx); UP(16, ply); UP(17, pr); UP(18, pbody); UP(19, tip); UP(20, grip); UP(21, seg0);
+  UP(22, garm);
 #undef UP
   if (e != cudaSuccess) return b->cuda_fail(e, "upload(templates)");
   int *d_segs = nullptr;
@@ -599,21 +626,51 @@ int upload_templates(kr_batch *b) {
   T.rest = (const float *)A[11]; T.minA = (const float *)A[12]; T.maxA = (const float *)A[13];
   T.lvl = (const int *)A[14]; T.plx = (const float *)A[15]; T.ply = (const float *)A[16]; T.pr = (const float *)A[17];
   T.pbody = (const int *)A[18]; T.arm_tip = (const int *)A[19]; T.arm_grip = (const int *)A[20];
-  T.arm_seg0 = (const int *)A[21];
+  T.arm_seg0 = (const int *)A[21]; T.garm = (const int *)A[22];
   if (T.arm_segs) cudaFree(const_cast<int *>(T.arm_segs));
   T.arm_segs = d_segs;
   if ((e = upload_vec(&b->d_tpl, b->h_tpl)) != cudaSuccess) return b->cuda_fail(e, "upload(template table)");
-  b->mb = mb; b->mc = mc; b->mp = mp;
+  b->shape_dirty = true;
   return KR_OK;
 }
 
-size_t smem_bytes(const kr_batch *b) {
-  return sizeof(float) * ((size_t)tpl_smem_words(b->mb, b->mc, b->mp) +
-                          (size_t)b->W * warp_smem_words(b->mb, b->mc, b->mp)) + 16;
+// Launch shape: creatures per group of every template and the dynamic shared
+// memory of a CTA.  A CTA gets an equal share of the SM's shared memory for
+// ctas_per_sm CTAs (default: 16 warps per SM); a template's group holds as
+// many creatures as fit in that share, at most W * 32 / G.
+int plan_shape(kr_batch *b) {
+  b->cpc = b->W * (32 / b->G);
+  const int ctas = b->ctas_per_sm > 0 ? b->ctas_per_sm : std::max(1, 16 / b->W);
+  long budget = std::min<long>(b->smem_optin, (long)b->smem_per_sm / ctas - b->smem_reserved) - 64;
+  budget = (budget / 16) * 16;
+  const long words = budget / 4;
+  b->tpl_cpg.assign(b->h_tpl.size(), 0);
+  size_t need_max = 16;
+  for (size_t t = 0; t < b->h_tpl.size(); t++) {
+    const TplDev &d = b->h_tpl[t];
+    const long tw = tpl_smem_words(d.nb, d.nc, d.np);
+    const long cw = creature_smem_words(d.nb, d.nc, d.np, d.arms, d.segs);
+    const long fit = (words - tw) / cw;
+    if (fit < 1)
+      return b->fail(KR_ERR_CAPACITY, "body " + std::to_string(d.arms) + "x" + std::to_string(d.segs) +
+                                          " does not fit the shared memory of " + std::to_string(ctas) +
+                                          " CTAs per SM");
+    const int cpg = (int)std::min<long>(b->cpc, fit);
+    b->tpl_cpg[t] = cpg;
+    need_max = std::max(need_max, (size_t)(tw + (long)cpg * cw) * sizeof(float));
+  }
+  b->smem_dyn = need_max;
+  b->shape_dirty = false;
+  return KR_OK;
 }
 
-// groups of up to W slots of one template, longest remaining horizon first
+// groups of up to tpl_cpg slots of one template, longest remaining horizon
+// first; creatures that share a warp are adjacent in remaining horizon
 int build_groups(kr_batch *b, const std::vector<int> &remaining) {
+  if (b->shape_dirty) {
+    int rc = plan_shape(b);
+    if (rc != KR_OK) return rc;
+  }
   std::vector<int> live;
   for (int s = 0; s < b->capacity; s++)
     if (b->h_meta[s].horizon > 0 && remaining[s] > 0) live.push_back(s);
@@ -625,15 +682,15 @@ int build_groups(kr_batch *b, const std::vector<int> &remaining) {
   for (size_t i = 0; i < live.size();) {
     std::vector<int> g;
     const int t = b->h_meta[live[i]].tpl;
-    while (i < live.size() && (int)g.size() < b->W && b->h_meta[live[i]].tpl == t) g.push_back(live[i++]);
+    while (i < live.size() && (int)g.size() < b->tpl_cpg[t] && b->h_meta[live[i]].tpl == t) g.push_back(live[i++]);
     groups.push_back(g);
   }
   std::stable_sort(groups.begin(), groups.end(), [&](const std::vector<int> &x, const std::vector<int> &y) {
     return remaining[x[0]] > remaining[y[0]];
   });
-  std::vector<int> flat((size_t)groups.size() * b->W, -1);
+  std::vector<int> flat((size_t)groups.size() * b->cpc, -1);
   for (size_t g = 0; g < groups.size(); g++)
-    for (size_t k = 0; k < groups[g].size(); k++) flat[g * b->W + k] = groups[g][k];
+    for (size_t k = 0; k < groups[g].size(); k++) flat[g * b->cpc + k] = groups[g][k];
   if (b->d_groups == nullptr || b->c_groups < std::max<size_t>(flat.size(), 1)) {
     if (b->d_groups) cudaFree(b->d_groups);
     b->d_groups = nullptr;
@@ -707,6 +764,9 @@ extern "C" int kr_batch_create(const kr_batch_desc *desc, kr_batch **out) {
   K.iterations = p.iterations;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&b->n_sm, cudaDevAttrMultiProcessorCount, dev);
+  cudaDeviceGetAttribute(&b->smem_per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
+  cudaDeviceGetAttribute(&b->smem_reserved, cudaDevAttrReservedSharedMemoryPerBlock, dev);
+  cudaDeviceGetAttribute(&b->smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
   auto bail = [&](cudaError_t e, const char *what) {
     g_batch_error = std::string("CUDA error in ") + what + ": " + cudaGetErrorString(e);
     kr_batch_destroy(b);
@@ -865,22 +925,61 @@ extern "C" int kr_batch_set_policy(kr_batch *b, const float *weights, int32_t n_
   return KR_OK;
 }
 
-extern "C" int kr_batch_set_launch(kr_batch *b, int32_t warps_per_cta, int32_t ctas_per_sm) {
+extern "C" int kr_batch_set_launch(kr_batch *b, int32_t lanes_per_creature, int32_t warps_per_cta,
+                                   int32_t ctas_per_sm) {
   if (!b) return KR_ERR_INVALID;
+  if (lanes_per_creature != 32 && lanes_per_creature != 16 && lanes_per_creature != 8)
+    return b->fail(KR_ERR_INVALID, "lanes_per_creature must be 32, 16 or 8");
   if (warps_per_cta < 1 || warps_per_cta > kMaxW) return b->fail(KR_ERR_INVALID, "warps_per_cta outside 1..16");
-  if (ctas_per_sm < 0 || ctas_per_sm > 64) return b->fail(KR_ERR_INVALID, "ctas_per_sm outside 0..64");
-  if (b->W != warps_per_cta) b->groups_dirty = true;
+  if (warps_per_cta * (32 / lanes_per_creature) > kMaxCPC)
+    return b->fail(KR_ERR_INVALID, "more than 64 creatures per CTA");
+  if (ctas_per_sm < 0 || ctas_per_sm > 32) return b->fail(KR_ERR_INVALID, "ctas_per_sm outside 0..32");
+  if (b->W != warps_per_cta || b->G != lanes_per_creature || b->ctas_per_sm != ctas_per_sm) {
+    b->groups_dirty = true;
+    b->shape_dirty = true;
+  }
+  b->G = lanes_per_creature;
   b->W = warps_per_cta;
   b->ctas_per_sm = ctas_per_sm;
   return KR_OK;
 }
 
+extern "C" int kr_batch_get_launch(kr_batch *b, int32_t *lanes_per_creature, int32_t *warps_per_cta,
+                                   int32_t *ctas_per_sm, int32_t *smem_bytes) {
+  if (!b) return KR_ERR_INVALID;
+  if (b->shape_dirty && !b->h_tpl.empty()) {
+    int rc = plan_shape(b);
+    if (rc != KR_OK) return rc;
+  }
+  if (lanes_per_creature) *lanes_per_creature = b->G;
+  if (warps_per_cta) *warps_per_cta = b->W;
+  if (ctas_per_sm) *ctas_per_sm = b->ctas_per_sm;
+  if (smem_bytes) *smem_bytes = (int32_t)b->smem_dyn;
+  return KR_OK;
+}
+
 namespace {
+template <int G>
+cudaError_t launch_g(const BatchArgs &A, kr_batch *b, int *grid_out) {
+  auto *fn = batch_kernel<G>;
+  cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b->smem_dyn);
+  if (e != cudaSuccess) return e;
+  int per_sm = 0;
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, 32 * b->W, b->smem_dyn);
+  if (e != cudaSuccess) return e;
+  if (per_sm < 1) { *grid_out = 0; return cudaSuccess; }
+  if (b->ctas_per_sm > 0) per_sm = std::min(per_sm, b->ctas_per_sm);
+  const int grid = std::max(1, std::min(b->n_groups, per_sm * b->n_sm));
+  *grid_out = grid;
+  fn<<<grid, 32 * b->W, b->smem_dyn, b->stream>>>(A);
+  return cudaGetLastError();
+}
+
 int launch(kr_batch *b, int max_steps, bool timed) {
   if (b->tpls.empty()) return KR_OK;
   if (b->d.control_mode == KR_CTRL_POLICY && !b->d_pw)
     return b->fail(KR_ERR_STATE, "policy control without kr_batch_set_policy");
-  if (b->groups_dirty) {
+  if (b->groups_dirty || b->shape_dirty) {
     int rc = build_groups(b, b->h_remaining);
     if (rc != KR_OK) return rc;
   }
@@ -891,7 +990,7 @@ int launch(kr_batch *b, int max_steps, bool timed) {
   A.T = b->T;
   A.state = b->d_state; A.grip = b->d_grip; A.glam = b->d_glam; A.cd = b->d_cd; A.ctrl_cur = b->d_ctrl; A.meta = b->d_meta;
   A.rects = b->d_rects; A.map_off = b->d_map_off; A.map_cull = b->d_map_cull;
-  A.groups = b->d_groups; A.n_groups = b->n_groups; A.W = b->W; A.queue = b->d_queue;
+  A.groups = b->d_groups; A.n_groups = b->n_groups; A.cpc = b->cpc; A.queue = b->d_queue;
   A.max_steps = max_steps;
   A.ctrl_mode = b->d.control_mode; A.ctrl_period = std::max(1, b->d.control_period);
   A.obs = b->d_obs; A.obs_ring = b->d.obs_ring;
@@ -899,20 +998,13 @@ int launch(kr_batch *b, int max_steps, bool timed) {
   A.inv_h64 = 1.0 / b->d.solver.h;
   A.dt = b->d.solver.h * b->d.solver.substeps;
   A.pw = b->d_pw; A.pw_idx = b->d_pw_idx; A.n_params = b->n_params;
-  A.mb = b->mb; A.mc = b->mc; A.mp = b->mp;
-  const size_t smem = smem_bytes(b);
-  cudaError_t e = cudaFuncSetAttribute(batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  if (e != cudaSuccess) return b->cuda_fail(e, "cudaFuncSetAttribute(batch_kernel)");
-  int per_sm = 0;
-  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_kernel, 32 * b->W, smem);
-  if (e != cudaSuccess) return b->cuda_fail(e, "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
-  if (per_sm < 1) return b->fail(KR_ERR_CAPACITY, "batch kernel does not fit on an SM with this launch shape");
-  if (b->ctas_per_sm > 0) per_sm = std::min(per_sm, b->ctas_per_sm);
-  const int grid = std::max(1, std::min(b->n_groups, per_sm * b->n_sm));
+  cudaError_t e;
   if ((e = cudaMemsetAsync(b->d_queue, 0, sizeof(int), b->stream)) != cudaSuccess) return b->cuda_fail(e, "queue reset");
   if (timed) cudaEventRecord(b->ev0, b->stream);
-  batch_kernel<<<grid, 32 * b->W, smem, b->stream>>>(A);
-  if ((e = cudaGetLastError()) != cudaSuccess) return b->cuda_fail(e, "batch_kernel launch");
+  int grid = 0;
+  e = b->G == 32 ? launch_g<32>(A, b, &grid) : b->G == 16 ? launch_g<16>(A, b, &grid) : launch_g<8>(A, b, &grid);
+  if (e != cudaSuccess) return b->cuda_fail(e, "batch_kernel launch");
+  if (grid == 0) return b->fail(KR_ERR_CAPACITY, "batch kernel does not fit on an SM with this launch shape");
   if (timed) cudaEventRecord(b->ev1, b->stream);
   // remaining horizons as the next schedule sees them
   for (int s = 0; s < b->capacity; s++)
@@ -935,7 +1027,7 @@ extern "C" int kr_batch_run(kr_batch *b, int32_t max_steps) {
 extern "C" int kr_batch_run_graph(kr_batch *b, int32_t max_steps, int32_t launches, int32_t replays) {
   if (!b) return KR_ERR_INVALID;
   if (max_steps <= 0 || launches <= 0 || replays < 0) return b->fail(KR_ERR_INVALID, "kr_batch_run_graph: bad counts");
-  if (b->groups_dirty) {
+  if (b->groups_dirty || b->shape_dirty) {
     int rc = build_groups(b, b->h_remaining);
     if (rc != KR_OK) return rc;
   }
@@ -1016,6 +1108,16 @@ extern "C" int kr_batch_read_obs(kr_batch *b, int32_t first, int32_t n, float *o
                                   cudaMemcpyDeviceToHost, b->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
   if (e != cudaSuccess) return b->cuda_fail(e, "kr_batch_read_obs");
+  return KR_OK;
+}
+
+extern "C" int kr_batch_read_controls(kr_batch *b, int32_t first, int32_t n, float *controls) {
+  if (!b || !controls) return KR_ERR_INVALID;
+  if (first < 0 || n < 0 || first + n > b->capacity) return b->fail(KR_ERR_INVALID, "read range outside the slots");
+  cudaError_t e = cudaMemcpyAsync(controls, b->d_ctrl + (size_t)first * kCtrlStride,
+                                  (size_t)n * kCtrlStride * sizeof(float), cudaMemcpyDeviceToHost, b->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
+  if (e != cudaSuccess) return b->cuda_fail(e, "kr_batch_read_controls");
   return KR_OK;
 }
 
@@ -1121,20 +1223,21 @@ extern "C" int kr_batch_restore(kr_batch *b) {
   if (e != cudaSuccess) return b->cuda_fail(e, "kr_batch_restore");
   b->h_remaining = b->s_remaining;
   // the work groups of the snapshot state: built once, then copied back
-  if (b->s_n_groups < 0 || b->s_W != b->W) {
+  if (b->s_n_groups < 0 || b->s_cpc != b->cpc || b->s_G != b->G || b->shape_dirty) {
     int rc = build_groups(b, b->h_remaining);
     if (rc != KR_OK) return rc;
     if (b->s_groups) cudaFree(b->s_groups);
     b->s_groups = nullptr;
     e = cudaMalloc(&b->s_groups, std::max<size_t>(b->c_groups, 1) * sizeof(int));
     if (e == cudaSuccess)
-      e = cudaMemcpyAsync(b->s_groups, b->d_groups, (size_t)b->n_groups * b->W * sizeof(int),
+      e = cudaMemcpyAsync(b->s_groups, b->d_groups, (size_t)b->n_groups * b->cpc * sizeof(int),
                           cudaMemcpyDeviceToDevice, b->stream);
     if (e != cudaSuccess) return b->cuda_fail(e, "kr_batch_restore(groups)");
     b->s_n_groups = b->n_groups;
-    b->s_W = b->W;
+    b->s_cpc = b->cpc;
+    b->s_G = b->G;
   } else {
-    e = cudaMemcpyAsync(b->d_groups, b->s_groups, (size_t)b->s_n_groups * b->W * sizeof(int),
+    e = cudaMemcpyAsync(b->d_groups, b->s_groups, (size_t)b->s_n_groups * b->cpc * sizeof(int),
                         cudaMemcpyDeviceToDevice, b->stream);
     if (e != cudaSuccess) return b->cuda_fail(e, "kr_batch_restore(groups)");
     b->n_groups = b->s_n_groups;
@@ -1187,7 +1290,7 @@ extern "C" int kr_probe_fp32_rate(double *fma_per_s) {
 extern "C" int kr_batch_run_launches(kr_batch *b, int32_t steps_per_launch, int32_t launches) {
   if (!b) return KR_ERR_INVALID;
   if (steps_per_launch <= 0 || launches < 0) return b->fail(KR_ERR_INVALID, "kr_batch_run_launches: bad counts");
-  if (b->groups_dirty) {
+  if (b->groups_dirty || b->shape_dirty) {
     int rc = build_groups(b, b->h_remaining);
     if (rc != KR_OK) return rc;
   }

@@ -195,25 +195,99 @@ __device__ __forceinline__ bool sdf(const float4 *__restrict__ rects, const shor
 constexpr int kMaxCulled = 64;
 constexpr float kCullSlack = 6.f;
 
-// Shared-memory view of one island (one warp).  Constraint slots are in
-// schedule order: level by level, each level body-disjoint.
+// A group of G lanes of one warp advancing one creature (G = 32, 16, 8):
+// lanes of a group loop with stride G and synchronize, reduce and vote only
+// among themselves, so a warp can carry 32 / G creatures of one template.
+template <int G>
+struct Lanes {
+  int lane;        // 0 .. G-1
+  int base;        // first warp lane of the group
+  unsigned mask;   // the group's lanes in the warp
+  __device__ __forceinline__ explicit Lanes(int warp_lane)
+      : lane(warp_lane & (G - 1)), base(warp_lane & ~(G - 1)),
+        mask(G == 32 ? 0xffffffffu : (((1u << G) - 1u) << (warp_lane & ~(G - 1)))) {}
+  __device__ __forceinline__ void sync() const { __syncwarp(mask); }
+  __device__ __forceinline__ unsigned ballot(bool p) const {
+    const unsigned b = __ballot_sync(mask, p);
+    return G == 32 ? b : (b >> base) & ((1u << G) - 1u);
+  }
+  __device__ __forceinline__ float min(float v) const {
+    for (int o = G / 2; o > 0; o >>= 1) v = fminf(v, __shfl_xor_sync(mask, v, o, G));
+    return v;
+  }
+  __device__ __forceinline__ float max(float v) const {
+    for (int o = G / 2; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(mask, v, o, G));
+    return v;
+  }
+};
+
+// Shared-memory view of one island (one creature).  Constraint slots are in
+// schedule order: level by level, each level body-disjoint.  Two layouts:
+//  * per slot (gpuworld drop-in): every field an array over the slots;
+//  * compact (batched engine): the template's statics, plus per creature
+//    only lambda, the motor targets and the grip state (grips are the only
+//    constraints with a moving anchor, a break force and a broken flag;
+//    motors the only ones with a target and a nonzero compliance).
 struct Island {
   // bodies (local index)
   float *px, *py, *ppx, *ppy, *vx, *vy, *ang, *angP, *av, *im, *ii, *fx, *fy, *tq;
   float *bs, *bc;  // sin / cos of angP during a collision pass
   // constraint slots
-  int *ab;     // a | (b << 16), b == 0xffff for a world anchor
-  int *tb;     // type | (broken << 8)
-  float *lax, *lay, *lbx, *lby, *comp, *rest, *tgt, *minA, *maxA, *lamX, *lamY, *lam, *brk;
+  const int *ab;   // a | (b << 16), b == 0xffff for a world anchor
+  int *tb;         // per slot: type | (broken << 8)
+  const float *lax, *lay, *rest, *minA, *maxA;
+  float *lbx, *lby;         // per slot (drop-in); template statics (batched)
+  float *comp, *tgt, *brk;  // per slot (drop-in)
+  float *lamX, *lamY, *lam;
+  // compact layout (batched engine)
+  const int *type;   // per slot static type
+  const int *garm;   // per slot: arm of a grip, else -1
+  const int *motor;  // per slot: motor index of an angle constraint, else -1
+  float *tgt_m;      // per motor target
+  float *anc;        // per arm: anchor x, y, break force, broken (1.f / 0.f)
+  float comp_m;      // motor compliance of the creature
   // collision points, grouped per local body in groupCollPoints order
-  float *plx, *ply, *pr;
-  int *pbody;             // local body of each point
+  const float *plx, *ply, *pr;
+  const int *pbody;       // local body of each point
   float *pdx, *pdy;       // speculative correction of each point
   int *pflag;             // 1 if the speculative evaluation corrects
-  int *boff, *bcnt;
+  const int *boff, *bcnt;
   short *cull;            // culled rect list (kMaxCulled)
   int nb, nc, np, nlv;
-  const int *lvl;         // level offsets, nlv + 1 (global, read-only)
+  const int *lvl;         // level offsets, nlv + 1
+};
+
+// Field access of the two layouts (same values, different storage).
+struct SlotAccess {
+  __device__ static __forceinline__ int type(const Island &S, int k) { return S.tb[k] & 0xff; }
+  __device__ static __forceinline__ bool broken(const Island &S, int k) { return (S.tb[k] >> 8) != 0; }
+  __device__ static __forceinline__ void set_broken(Island &S, int k) { S.tb[k] |= 1 << 8; }
+  __device__ static __forceinline__ float lbx(const Island &S, int k) { return S.lbx[k]; }
+  __device__ static __forceinline__ float lby(const Island &S, int k) { return S.lby[k]; }
+  __device__ static __forceinline__ float comp(const Island &S, int k) { return S.comp[k]; }
+  __device__ static __forceinline__ float tgt(const Island &S, int k) { return S.tgt[k]; }
+  __device__ static __forceinline__ float brk(const Island &S, int k) { return S.brk[k]; }
+};
+struct CompactAccess {
+  __device__ static __forceinline__ int type(const Island &S, int k) { return S.type[k]; }
+  __device__ static __forceinline__ bool broken(const Island &S, int k) {
+    const int a = S.garm[k];
+    return a >= 0 && S.anc[4 * a + 3] != 0.f;
+  }
+  __device__ static __forceinline__ void set_broken(Island &S, int k) { S.anc[4 * S.garm[k] + 3] = 1.f; }
+  __device__ static __forceinline__ float lbx(const Island &S, int k) {
+    const int a = S.garm[k];
+    return a >= 0 ? S.anc[4 * a] : S.lbx[k];
+  }
+  __device__ static __forceinline__ float lby(const Island &S, int k) {
+    const int a = S.garm[k];
+    return a >= 0 ? S.anc[4 * a + 1] : S.lby[k];
+  }
+  __device__ static __forceinline__ float comp(const Island &S, int k) {
+    return S.type[k] == 1 ? S.comp_m : 0.f;
+  }
+  __device__ static __forceinline__ float tgt(const Island &S, int k) { return S.tgt_m[S.motor[k]]; }
+  __device__ static __forceinline__ float brk(const Island &S, int k) { return S.anc[4 * S.garm[k] + 2]; }
 };
 
 // integrateF, f32solver.mjs:177-200 (solver.wgsl:166-205)
@@ -245,6 +319,7 @@ __device__ __forceinline__ void integrate_body(const SolverConsts &K, Island &S,
 
 // solvePinF, f32solver.mjs:203-256 (solver.wgsl:225-290); grips are pins
 // against the world anchor (lbx, lby).
+template <class Acc>
 __device__ __forceinline__ void solve_pin(const SolverConsts &K, Island &S, int k) {
   int ab = S.ab[k];
   int A = ab & 0xffff, B = (ab >> 16) & 0xffff;
@@ -254,7 +329,7 @@ __device__ __forceinline__ void solve_pin(const SolverConsts &K, Island &S, int 
   float rax = fsub(fmul(lax, ca), fmul(lay, sa));
   float ray = fadd(fmul(lax, sa), fmul(lay, ca));
   float gax = fadd(S.ppx[A], rax), gay = fadd(S.ppy[A], ray);
-  float gbx = S.lbx[k], gby = S.lby[k];
+  float gbx = Acc::lbx(S, k), gby = Acc::lby(S, k);
   float rbx = 0.f, rby = 0.f, wB = 0.f, wIB = 0.f;
   const bool hasB = B != 0xffff;
   if (hasB) {
@@ -278,7 +353,7 @@ __device__ __forceinline__ void solve_pin(const SolverConsts &K, Island &S, int 
   float k11 = fadd(fadd(wSum, fmul(fmul(wIA, pay), pay)), fmul(fmul(wIB, pby), pby));
   float det = fsub(fmul(k00, k11), fmul(k01, k01));
   if (fabsf(det) < kEpsDet) return;
-  float alphaTilde = fmul(S.comp[k], K.invH2);
+  float alphaTilde = fmul(Acc::comp(S, k), K.invH2);
   float lx0 = S.lamX[k], ly0 = S.lamY[k];
   float bx = fadd(Cx, fmul(alphaTilde, lx0));
   float by = fadd(Cy, fmul(alphaTilde, ly0));
@@ -300,6 +375,7 @@ __device__ __forceinline__ void solve_pin(const SolverConsts &K, Island &S, int 
 
 // solveAngleF, f32solver.mjs:258-301 (solver.wgsl:292-350): muscle
 // (compliant) part, then the one-sided joint limit.
+template <class Acc>
 __device__ __forceinline__ void solve_angle(const SolverConsts &K, Island &S, int k) {
   int ab = S.ab[k];
   int A = ab & 0xffff, B = (ab >> 16) & 0xffff;
@@ -315,10 +391,10 @@ __device__ __forceinline__ void solve_angle(const SolverConsts &K, Island &S, in
   if (wSum <= 0.f) return;
   float rest = S.rest[k];
   float dev = angle_delta(rel, rest);
-  float C = angle_delta(dev, S.tgt[k]);
+  float C = angle_delta(dev, Acc::tgt(S, k));
   if (!(C == C)) return;
   if (fabsf(C) >= kSlackAng) {
-    float alphaTilde = fmul(S.comp[k], K.invH2);
+    float alphaTilde = fmul(Acc::comp(S, k), K.invH2);
     float l0 = S.lam[k];
     float dl = -fdiv(fadd(C, fmul(alphaTilde, l0)), fadd(wSum, alphaTilde));
     if (!(dl == dl)) return;
@@ -348,15 +424,6 @@ __device__ __forceinline__ void solve_angle(const SolverConsts &K, Island &S, in
   }
 }
 
-__device__ __forceinline__ float warp_min(float v) {
-  for (int o = 16; o > 0; o >>= 1) v = fminf(v, __shfl_xor_sync(0xffffffffu, v, o));
-  return v;
-}
-__device__ __forceinline__ float warp_max(float v) {
-  for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
-  return v;
-}
-
 // One collision pass of the island: solveCollisionsF 'seq',
 // f32solver.mjs:317-344 (solver.wgsl:373-402) -- per body, its points in
 // order, each correction cumulative.  Evaluated as
@@ -368,17 +435,18 @@ __device__ __forceinline__ float warp_max(float v) {
 //      it; after the first correction the remaining points of that body are
 //      re-evaluated at the moved pose, exactly as the sequential loop does.
 // cull_d = D + kCullSlack with D as in the comment above kMaxCulled.
+template <int G>
 __device__ __forceinline__ void collide_island(Island &S, const float4 *__restrict__ rects, int nR,
-                                               float cull_d, int lane) {
-  for (int j = lane; j < S.nb; j += 32) {
+                                               float cull_d, const Lanes<G> &L) {
+  for (int j = L.lane; j < S.nb; j += G) {
     float s, c;
     sincos_r(S.angP[j], &s, &c);
     S.bs[j] = s;
     S.bc[j] = c;
   }
-  __syncwarp();
+  L.sync();
   float mnx = __int_as_float(0x7f800000), mny = mnx, mxx = -mnx, mxy = -mnx;
-  for (int p = lane; p < S.np; p += 32) {
+  for (int p = L.lane; p < S.np; p += G) {
     const int j = S.pbody[p];
     const float ca = S.bc[j], sa = S.bs[j], lx = S.plx[p], ly = S.ply[p];
     const float wx = fadd(S.ppx[j], fsub(fmul(lx, ca), fmul(ly, sa)));
@@ -388,31 +456,31 @@ __device__ __forceinline__ void collide_island(Island &S, const float4 *__restri
     mnx = fminf(mnx, wx); mxx = fmaxf(mxx, wx);
     mny = fminf(mny, wy); mxy = fmaxf(mxy, wy);
   }
-  mnx = warp_min(mnx); mny = warp_min(mny);
-  mxx = warp_max(mxx); mxy = warp_max(mxy);
+  mnx = L.min(mnx); mny = L.min(mny);
+  mxx = L.max(mxx); mxy = L.max(mxy);
   // culled list, ascending rect order
   const float bx0 = mnx - cull_d, bx1 = mxx + cull_d, by0 = mny - cull_d, by1 = mxy + cull_d;
   int ncull = 0;
   bool full = !(bx0 <= bx1 && by0 <= by1);  // no finite point: use the full list
-  for (int base = 0; base < nR && !full; base += 32) {
-    const int i = base + lane;
+  for (int base = 0; base < nR && !full; base += G) {
+    const int i = base + L.lane;
     bool keep = false;
     if (i < nR) {
       const float4 r = __ldg(rects + i);
       keep = !(r.z < bx0 || r.x > bx1 || r.w < by0 || r.y > by1);
     }
-    const unsigned m = __ballot_sync(0xffffffffu, keep);
-    const int at = ncull + __popc(m & ((1u << lane) - 1u));
+    const unsigned m = L.ballot(keep);
+    const int at = ncull + __popc(m & ((1u << L.lane) - 1u));
     if (keep && at < kMaxCulled) S.cull[at] = static_cast<short>(i);
     ncull += __popc(m);
     if (ncull > kMaxCulled) full = true;
   }
-  __syncwarp();
+  L.sync();
   const short *list = full ? nullptr : S.cull;
   const int nlist = full ? nR : ncull;
   const float sx0 = mnx - kCullSlack, sx1 = mxx + kCullSlack;
   const float sy0 = mny - kCullSlack, sy1 = mxy + kCullSlack;
-  for (int p = lane; p < S.np; p += 32) {
+  for (int p = L.lane; p < S.np; p += G) {
     const int j = S.pbody[p];
     int flag = 0;
     float cx = 0.f, cy = 0.f;
@@ -431,8 +499,8 @@ __device__ __forceinline__ void collide_island(Island &S, const float4 *__restri
     S.pdx[p] = cx;
     S.pdy[p] = cy;
   }
-  __syncwarp();
-  for (int j = lane; j < S.nb; j += 32) {
+  L.sync();
+  for (int j = L.lane; j < S.nb; j += G) {
     if (S.im[j] == 0.f) continue;
     const int o = S.boff[j], cnt = S.bcnt[j];
     float px = S.ppx[j], py = S.ppy[j];
@@ -462,7 +530,7 @@ __device__ __forceinline__ void collide_island(Island &S, const float4 *__restri
     S.ppx[j] = px;
     S.ppy[j] = py;
   }
-  __syncwarp();
+  L.sync();
 }
 
 // finalizeF, f32solver.mjs:376-399 (solver.wgsl:405-430)
@@ -492,45 +560,45 @@ __device__ __forceinline__ void finalize_body(const SolverConsts &K, Island &S, 
 }
 
 // gripBreakF, f32solver.mjs:402-416 (solver.wgsl:433-442)
+template <class Acc>
 __device__ __forceinline__ void grip_break(const SolverConsts &K, Island &S, int k) {
-  int tb = S.tb[k];
-  if ((tb & 0xff) != 2 || (tb >> 8) != 0) return;
+  if (Acc::type(S, k) != 2 || Acc::broken(S, k)) return;
   float f = fmul(length2(S.lamX[k], S.lamY[k]), K.invH);
-  if (f > S.brk[k]) {
-    S.tb[k] = tb | (1 << 8);
+  if (f > Acc::brk(S, k)) {
+    Acc::set_broken(S, k);
     S.lamX[k] = 0.f;
     S.lamY[k] = 0.f;
   }
 }
 
-// One env step of one island by one warp (xpbd.js:487-490 with the substep
-// of f32solver.mjs:419-428): substeps x (reset lambda, integrate,
+// One env step of one island by a group of G lanes (xpbd.js:487-490 with the
+// substep of f32solver.mjs:419-428): substeps x (reset lambda, integrate,
 // iterations x (constraint levels, collisions), finalize), then grip break.
+template <class Acc, int G>
 __device__ __forceinline__ void island_step(const SolverConsts &K, Island &S,
                                             const float4 *__restrict__ rects, int nR, float cull_d,
-                                            int lane) {
+                                            const Lanes<G> &L) {
   for (int s = 0; s < K.substeps; s++) {
-    for (int k = lane; k < S.nc; k += 32) { S.lamX[k] = 0.f; S.lamY[k] = 0.f; S.lam[k] = 0.f; }
-    for (int i = lane; i < S.nb; i += 32) integrate_body(K, S, i);
-    __syncwarp();
+    for (int k = L.lane; k < S.nc; k += G) { S.lamX[k] = 0.f; S.lamY[k] = 0.f; S.lam[k] = 0.f; }
+    for (int i = L.lane; i < S.nb; i += G) integrate_body(K, S, i);
+    L.sync();
     for (int it = 0; it < K.iterations; it++) {
       for (int l = 0; l < S.nlv; l++) {
         const int beg = S.lvl[l], end = S.lvl[l + 1];
-        for (int k = beg + lane; k < end; k += 32) {
-          const int tb = S.tb[k];
-          if ((tb >> 8) != 0) continue;  // broken
-          if ((tb & 0xff) == 1) solve_angle(K, S, k);
-          else solve_pin(K, S, k);
+        for (int k = beg + L.lane; k < end; k += G) {
+          if (Acc::broken(S, k)) continue;
+          if (Acc::type(S, k) == 1) solve_angle<Acc>(K, S, k);
+          else solve_pin<Acc>(K, S, k);
         }
-        __syncwarp();
+        L.sync();
       }
-      collide_island(S, rects, nR, cull_d, lane);
+      collide_island<G>(S, rects, nR, cull_d, L);
     }
-    for (int i = lane; i < S.nb; i += 32) finalize_body(K, S, i);
-    __syncwarp();
+    for (int i = L.lane; i < S.nb; i += G) finalize_body(K, S, i);
+    L.sync();
   }
-  for (int k = lane; k < S.nc; k += 32) grip_break(K, S, k);
-  __syncwarp();
+  for (int k = L.lane; k < S.nc; k += G) grip_break<Acc>(K, S, k);
+  L.sync();
 }
 
 }  // namespace kr

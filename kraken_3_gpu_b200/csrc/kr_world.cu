@@ -66,26 +66,36 @@ __host__ __device__ inline int warp_smem_words(int mb, int mc, int mp) {
   return 18 * mb + 15 * mc + 7 * mp + kr::kMaxCulled / 2;
 }
 
-__device__ inline void carve(kr::Island &S, float *base, int mb, int mc, int mp) {
+// Writable views of the per-slot statics while they are staged; the solver
+// reads them through the const pointers of kr::Island.
+struct StageView {
+  int *ab, *boff, *bcnt, *pbody;
+  float *lax, *lay, *rest, *minA, *maxA, *plx, *ply, *pr;
+};
+
+__device__ inline void carve(kr::Island &S, StageView &V, float *base, int mb, int mc, int mp) {
   float *p = base;
   S.px = p; p += mb; S.py = p; p += mb; S.ppx = p; p += mb; S.ppy = p; p += mb;
   S.vx = p; p += mb; S.vy = p; p += mb; S.ang = p; p += mb; S.angP = p; p += mb;
   S.av = p; p += mb; S.im = p; p += mb; S.ii = p; p += mb;
   S.fx = p; p += mb; S.fy = p; p += mb; S.tq = p; p += mb;
   S.bs = p; p += mb; S.bc = p; p += mb;
-  S.boff = reinterpret_cast<int *>(p); p += mb;
-  S.bcnt = reinterpret_cast<int *>(p); p += mb;
-  S.ab = reinterpret_cast<int *>(p); p += mc;
+  V.boff = reinterpret_cast<int *>(p); p += mb;
+  V.bcnt = reinterpret_cast<int *>(p); p += mb;
+  V.ab = reinterpret_cast<int *>(p); p += mc;
   S.tb = reinterpret_cast<int *>(p); p += mc;
-  S.lax = p; p += mc; S.lay = p; p += mc; S.lbx = p; p += mc; S.lby = p; p += mc;
-  S.comp = p; p += mc; S.rest = p; p += mc; S.tgt = p; p += mc; S.minA = p; p += mc;
-  S.maxA = p; p += mc; S.lamX = p; p += mc; S.lamY = p; p += mc; S.lam = p; p += mc;
+  V.lax = p; p += mc; V.lay = p; p += mc; S.lbx = p; p += mc; S.lby = p; p += mc;
+  S.comp = p; p += mc; V.rest = p; p += mc; S.tgt = p; p += mc; V.minA = p; p += mc;
+  V.maxA = p; p += mc; S.lamX = p; p += mc; S.lamY = p; p += mc; S.lam = p; p += mc;
   S.brk = p; p += mc;
-  S.plx = p; p += mp; S.ply = p; p += mp; S.pr = p; p += mp;
+  V.plx = p; p += mp; V.ply = p; p += mp; V.pr = p; p += mp;
   S.pdx = p; p += mp; S.pdy = p; p += mp;
-  S.pbody = reinterpret_cast<int *>(p); p += mp;
+  V.pbody = reinterpret_cast<int *>(p); p += mp;
   S.pflag = reinterpret_cast<int *>(p); p += mp;
   S.cull = reinterpret_cast<short *>(p);
+  S.ab = V.ab; S.boff = V.boff; S.bcnt = V.bcnt; S.pbody = V.pbody;
+  S.lax = V.lax; S.lay = V.lay; S.rest = V.rest; S.minA = V.minA; S.maxA = V.maxA;
+  S.plx = V.plx; S.ply = V.ply; S.pr = V.pr;
 }
 
 // One launch of the plain step for the island of this warp (shared by the
@@ -96,7 +106,8 @@ __device__ __forceinline__ void plain_step_body(const StepArgs &A) {
   const int island = blockIdx.x * kWarpsPerBlock + warp;
   if (island >= A.nI) return;
   kr::Island S;
-  carve(S, smem + warp * warp_smem_words(A.maxB, A.maxC, A.maxP), A.maxB, A.maxC, A.maxP);
+  StageView V;
+  carve(S, V, smem + warp * warp_smem_words(A.maxB, A.maxC, A.maxP), A.maxB, A.maxC, A.maxP);
   const int *rec = A.T.isl + island * kIslandInts;
   const int bo = rec[I_BODY_OFF], co = rec[I_CON_OFF], po = rec[I_PT_OFF];
   S.nb = rec[I_NB]; S.nc = rec[I_NC]; S.np = rec[I_NP];
@@ -114,33 +125,33 @@ __device__ __forceinline__ void plain_step_body(const StepArgs &A) {
     const float4 f = reinterpret_cast<const float4 *>(A.forces)[g];
     S.fx[i] = f.x; S.fy[i] = f.y; S.tq[i] = f.z;
     const int2 bp = A.T.bpt[bo + i];
-    S.boff[i] = bp.x; S.bcnt[i] = bp.y;
-    for (int q = 0; q < bp.y; q++) S.pbody[bp.x + q] = i;
+    V.boff[i] = bp.x; V.bcnt[i] = bp.y;
+    for (int q = 0; q < bp.y; q++) V.pbody[bp.x + q] = i;
   }
   // stage constraints (80 B AoS -> SoA, schedule order)
   for (int k = lane; k < S.nc; k += 32) {
     const int g = A.T.cons[co + k];
     const uint4 *c4 = reinterpret_cast<const uint4 *>(A.cons + 20 * (size_t)g);
     const uint4 w0 = c4[0], w1 = c4[1], w2 = c4[2], w3 = c4[3], w4 = c4[4];
-    S.ab[k] = A.T.ab[co + k];
+    V.ab[k] = A.T.ab[co + k];
     S.tb[k] = static_cast<int>(w0.z & 0xffu) | ((w4.y != 0u ? 1 : 0) << 8);
-    S.lax[k] = __uint_as_float(w1.x); S.lay[k] = __uint_as_float(w1.y);
+    V.lax[k] = __uint_as_float(w1.x); V.lay[k] = __uint_as_float(w1.y);
     S.lbx[k] = __uint_as_float(w1.z); S.lby[k] = __uint_as_float(w1.w);
-    S.comp[k] = __uint_as_float(w2.x); S.rest[k] = __uint_as_float(w2.y);
-    S.tgt[k] = __uint_as_float(w2.z); S.minA[k] = __uint_as_float(w2.w);
-    S.maxA[k] = __uint_as_float(w3.x); S.lamX[k] = __uint_as_float(w3.y);
+    S.comp[k] = __uint_as_float(w2.x); V.rest[k] = __uint_as_float(w2.y);
+    S.tgt[k] = __uint_as_float(w2.z); V.minA[k] = __uint_as_float(w2.w);
+    V.maxA[k] = __uint_as_float(w3.x); S.lamX[k] = __uint_as_float(w3.y);
     S.lamY[k] = __uint_as_float(w3.z); S.lam[k] = __uint_as_float(w3.w);
     S.brk[k] = __uint_as_float(w4.x);
   }
   // stage collision points
   for (int p = lane; p < S.np; p += 32) {
     const uint4 cp = A.coll[A.T.pts[po + p]];
-    S.plx[p] = __uint_as_float(cp.y); S.ply[p] = __uint_as_float(cp.z);
-    S.pr[p] = __uint_as_float(cp.w);
+    V.plx[p] = __uint_as_float(cp.y); V.ply[p] = __uint_as_float(cp.z);
+    V.pr[p] = __uint_as_float(cp.w);
   }
   __syncwarp();
 
-  kr::island_step(A.K, S, A.rects, A.nR, A.cull_d, lane);
+  kr::island_step<kr::SlotAccess, 32>(A.K, S, A.rects, A.nR, A.cull_d, kr::Lanes<32>(lane));
 
   // write back bodies, consumed forces and constraint multipliers / flags
   for (int i = lane; i < S.nb; i += 32) {

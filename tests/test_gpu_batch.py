@@ -86,19 +86,25 @@ def test_chunked_runs_and_graph_equal_one_run():
         e.close()
 
 
-@pytest.mark.parametrize("warps", [1, 4, 16])
-def test_launch_shape_does_not_change_results(warps):
-    w = _small_uneven(n=20, h=30)
-    base = batch.BatchEngine(w.maps, w.n)
+@pytest.mark.parametrize("lanes,warps,ctas", [(32, 1, 1), (32, 16, 1), (16, 4, 2), (16, 8, 0),
+                                               (8, 2, 4), (8, 16, 1)])
+def test_launch_shape_does_not_change_results(lanes, warps, ctas):
+    """One to four creatures per warp, any CTA size: the same bits."""
+    w = _small_uneven(n=40, h=30)
+    base = batch.BatchEngine(w.maps, w.n, obs_ring=32)
     workloads.spawn_all(base, w)
     base.run(30)
-    other = batch.BatchEngine(w.maps, w.n)
-    other.set_launch(warps, 1)
+    other = batch.BatchEngine(w.maps, w.n, obs_ring=32)
+    other.set_launch(warps, ctas, lanes_per_creature=lanes)
     workloads.spawn_all(other, w)
-    other.run(30)
+    other.run(17)
+    other.run(13)
+    assert other.get_launch()["lanes_per_creature"] == lanes
     s0, s1 = base.read_state(), other.read_state()
-    for f in ("px", "py", "ang"):
-        assert np.array_equal(s0[f], s1[f])
+    for f in ("px", "py", "ang", "vx", "vy", "av", "grips", "steps"):
+        assert np.array_equal(s0[f], s1[f]), f
+    assert np.array_equal(base.read_obs(), other.read_obs())
+    assert np.array_equal(base.read_fitness(), other.read_fitness())
     base.close()
     other.close()
 
@@ -112,3 +118,58 @@ def test_horizons_stop_each_creature():
     assert np.array_equal(st["steps"], w.horizon)
     assert eng.live() == 0
     eng.close()
+
+
+def _mlp_reference(w, obs, arms, segs):
+    """The fused controller in f64: proprio -> 64 tanh -> A*S tanh targets
+    and A (tanh + 1) / 2 adhesion values (kraken_batch.h layout)."""
+    n_in, n_out, H = 6 * arms + 6, arms * segs + arms, batch.POLICY_HIDDEN
+    W1 = w[: H * (n_in + 1)].reshape(H, n_in + 1).astype(np.float64)
+    W2 = w[H * (n_in + 1): H * (n_in + 1) + n_out * (H + 1)].reshape(n_out, H + 1).astype(np.float64)
+    h = np.tanh(W1[:, :n_in] @ obs[:n_in].astype(np.float64) + W1[:, n_in])
+    y = np.tanh(W2[:, :H] @ h + W2[:, H])
+    y[arms * segs:] = 0.5 * (y[arms * segs:] + 1.0)
+    return y
+
+
+@pytest.mark.parametrize("lanes", [32, 16, 8])
+def test_fused_policy_matches_mlp_on_recorded_proprio(lanes):
+    w = _small_uneven(n=12, h=6)
+    rng = np.random.default_rng(3)
+    n_params = batch.policy_params(8, 9)
+    n_ind = 4
+    weights = rng.normal(0.0, 0.3, size=(n_ind, n_params)).astype(np.float32)
+    slot_ind = rng.integers(0, n_ind, size=w.n).astype(np.int32)
+    eng = batch.BatchEngine(w.maps, w.n, obs_ring=8, control="policy")
+    eng.set_launch(4, 0, lanes_per_creature=lanes)
+    workloads.spawn_all(eng, w)
+    eng.set_policy(weights, slot_ind)
+    for step in range(3):
+        eng.run(1)
+        obs = eng.read_obs()
+        ctrl = eng.read_controls()
+        for i in range(w.n):
+            A, S = int(w.arms[i]), int(w.segs[i])
+            want = _mlp_reference(weights[slot_ind[i]], obs[i, step], A, S)
+            got = ctrl[i, : A * S + A]
+            assert np.allclose(got, want, atol=2e-5, rtol=0), (i, step)
+    eng.close()
+
+
+def test_fused_policy_same_bits_for_every_launch_shape():
+    w = _small_uneven(n=20, h=25)
+    rng = np.random.default_rng(4)
+    weights = rng.normal(0.0, 0.2, size=(3, batch.policy_params(8, 9))).astype(np.float32)
+    slot_ind = rng.integers(0, 3, size=w.n).astype(np.int32)
+    out = []
+    for lanes, warps in ((32, 8), (16, 4), (8, 16)):
+        eng = batch.BatchEngine(w.maps, w.n, control="policy")
+        eng.set_launch(warps, 0, lanes_per_creature=lanes)
+        workloads.spawn_all(eng, w)
+        eng.set_policy(weights, slot_ind)
+        eng.run(25)
+        out.append(eng.read_state())
+        eng.close()
+    for s in out[1:]:
+        for f in ("px", "py", "ang", "grips"):
+            assert np.array_equal(out[0][f], s[f]), f
