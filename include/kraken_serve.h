@@ -1,0 +1,138 @@
+/*
+ * kraken_serve.h -- device-resident rollout server on B200 (sm_100a).
+ *
+ * Serves ES evaluation requests: a request is a mirrored population of
+ * creatures of one body shape on one map, spawned at a common pose, run for
+ * `horizon` env steps, each individual controlled by the fused policy MLP of
+ * kraken_batch.h with its own parameters theta + sigma * eps_k (even
+ * individual 2k) or theta - sigma * eps_k (odd 2k + 1), eps_k ~ N(0, 1) drawn
+ * on the device from the request's seed -- the mirrored sampling of the
+ * reference's ES (src/brain/es.js:67-81) -- or, without theta, by control
+ * streams from the seed.  The reference evaluates a population in lockstep
+ * through its hybrid loop (src/sim/gputrain.js:72-150); here requests arrive
+ * at any time and share the GPU:
+ *
+ *  - continuous batching: the slots are split into two partitions that run
+ *    alternately on two streams, chunk_steps env steps per round; a request
+ *    that arrives while others run is admitted at the next round of a
+ *    partition as soon as slots are free, and its creatures run in the same
+ *    launches as everyone else's (one partition's launch fills the tail of
+ *    the other's);
+ *  - admission against an HBM budget: every slot's device memory (state,
+ *    grips, controls, observation ring, policy weights) is accounted for at
+ *    creation; the budget fixes the slot count, requests wait in FIFO order
+ *    until enough slots are free;
+ *  - per-request completion: a request's results are gathered on the device
+ *    and copied back when its last round ends; its slots return to the pool.
+ *
+ * Every creature's trajectory depends only on its own request (body, map,
+ * pose, parameters, seed), so a request's results are bit-identical whether
+ * it runs alone or in any mix, in any slots, in either partition.
+ *
+ * Plain pointers and sizes; every call returns KR_OK (0) or a KR_ERR_* code
+ * of kraken_b200.h; the handle is not thread-safe (one host thread drives
+ * it).  Times are seconds on the server's clock (kr_server_now).
+ */
+#ifndef KRAKEN_SERVE_H
+#define KRAKEN_SERVE_H
+#include <stdint.h>
+
+#include "kraken_b200.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct kr_server kr_server;
+
+typedef struct kr_server_desc {
+  kr_solver_params solver;      /* shared by all creatures */
+  int32_t n_maps;               /* >= 1 */
+  const float *rects;           /* every map's rects, x y w h (f32) */
+  const int32_t *map_rect_off;  /* n_maps + 1 offsets into rects (in rects) */
+  uint64_t hbm_budget_bytes;    /* device memory the server may hold */
+  int32_t max_slots;            /* cap on concurrent creatures (0: what the budget allows) */
+  int32_t obs_ring;             /* steps of each creature's observation ring (0: none) */
+  int32_t chunk_steps;          /* env steps of a partition per round (>= 1) */
+  int32_t policy;               /* 1: keep fused-policy weights per slot (requests with theta) */
+  int32_t lanes_per_creature;   /* launch shape, kr_batch_set_launch (0: defaults) */
+  int32_t warps_per_cta;
+  int32_t ctas_per_sm;
+  double grip_slip_max;         /* px/s, core.js:30 */
+  double grip_cooldown;         /* s, core.js:31 */
+} kr_server_desc;
+
+typedef struct kr_request {
+  int32_t population;           /* individuals, >= 1 (mirrored pairs: even) */
+  int32_t horizon;              /* env steps, >= 1 */
+  int32_t arms, segs;           /* body shape (1..8 x 1..9) */
+  int32_t map_id;
+  double x, y, angle;           /* common spawn pose (spawnKraken, src/body/kraken.js:64-101) */
+  float tone;                   /* muscle tone 0..1 */
+  const float *theta;           /* NULL: control streams; else n_params floats (kraken_batch.h layout) */
+  int32_t n_params;
+  float sigma;
+  uint64_t seed;                /* eps (policy) or control streams (no theta) */
+  double arrival;               /* server time the request arrives (< 0: now) */
+} kr_request;
+
+/* results per individual: path length of the mantle, final mantle x, y,
+ * attach events */
+#define KR_RESULT_WORDS 4
+
+typedef struct kr_server_stats {
+  int32_t capacity;             /* slots */
+  int32_t partition_capacity;   /* slots one partition may hold */
+  int32_t live;                 /* creatures on the device */
+  int32_t queued;               /* requests waiting for admission */
+  int64_t submitted, admitted, completed, rounds;
+  double creature_steps;        /* env steps run by every admitted creature so far */
+  double device_ms;             /* summed kernel time of the rounds */
+  uint64_t bytes_per_slot;      /* device bytes of one slot */
+  uint64_t device_bytes;        /* device bytes the server holds */
+} kr_server_stats;
+
+/* The slot count and per-slot bytes a descriptor yields (no device needed). */
+int kr_server_plan(const kr_server_desc *d, int32_t *capacity, uint64_t *bytes_per_slot);
+
+int kr_server_create(const kr_server_desc *d, kr_server **out);
+double kr_server_now(const kr_server *s);
+
+/* Queue a request (theta is copied); *id identifies it.  Rejects a
+ * population larger than a partition, an unknown map or body shape, and a
+ * theta shorter than the body's policy needs. */
+int kr_server_submit(kr_server *s, const kr_request *r, int64_t *id);
+
+/* One scheduling round of the next partition: wait for its previous round,
+ * complete the requests that ended there, admit arrived requests into free
+ * slots, launch chunk_steps env steps of its creatures.  *busy = 1 while any
+ * request is queued or running. */
+int kr_server_pump(kr_server *s, int32_t *busy);
+
+/* Pump until every submitted request has completed (sleeps while the next
+ * request has not arrived yet). */
+int kr_server_drain(kr_server *s);
+
+/* Ids of requests completed since the last poll (up to cap). */
+int kr_server_poll(kr_server *s, int64_t *ids, int32_t cap, int32_t *n);
+
+/* Results of a completed request: population x KR_RESULT_WORDS f64, and
+ * times[3] = arrival, admission and completion (server clock).  Either
+ * pointer may be NULL. */
+int kr_server_result(kr_server *s, int64_t id, double *results, double *times);
+
+/* Forget a completed request. */
+int kr_server_release(kr_server *s, int64_t id);
+
+int kr_server_get_stats(kr_server *s, kr_server_stats *out);
+
+/* The first n normal numbers eps(seed, pair, 0..n) the device draws for
+ * mirrored pair `pair` of a request (synchronous; for checking). */
+int kr_policy_eps(uint64_t seed, int32_t pair, int32_t n, float *out);
+void kr_server_destroy(kr_server *s);
+const char *kr_server_last_error(const kr_server *s);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

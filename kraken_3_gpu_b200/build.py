@@ -16,7 +16,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "libkraken_b200.so")
-SOURCES = ["kr_world.cu", "kr_batch.cu", "kr_template.cpp"]
+SOURCES = ["kr_world.cu", "kr_batch.cu", "kr_serve.cu", "kr_template.cpp"]
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
     "-lineinfo", "-O3", "-std=c++17", "-fmad=false",

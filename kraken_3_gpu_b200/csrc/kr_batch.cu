@@ -22,49 +22,13 @@
 #include <string>
 #include <vector>
 
-#include "../../include/kraken_batch.h"
-#include "kr_solver.cuh"
-#include "kr_template.h"
+#include "kr_batch_impl.h"
 
 namespace {
+using namespace krb;
 
-constexpr int kMaxW = 16;                                      // warps per CTA
-constexpr int kMaxCPC = 64;                                    // creatures per CTA (W * 32 / G)
-constexpr int kBodyPad = 76;                                   // >= kMaxTplBodies, /4
-constexpr int kStateStride = 6 * kBodyPad;                     // px py vx vy ang av
-constexpr int kCtrlStride = KR_BATCH_MAX_ARMS * (KR_BATCH_MAX_SEGS + 1);  // 80
 constexpr double kPiD = 3.141592653589793;
 constexpr double kSegHalf = 13.5 * 0.5;                        // tipPosition L
-
-struct TplDev {
-  int nb, nc, np, nlv, arms, segs;
-  float r_max;
-  float pad0;
-  double reach;
-  int o_b, o_c, o_l, o_p, o_a, o_s;
-};
-
-struct TplArrays {
-  const float *im, *ii;
-  const int *boff, *bcnt;
-  const int *ab, *type, *motor, *garm;
-  const float *lax, *lay, *lbx, *lby, *rest, *minA, *maxA;
-  const int *lvl;
-  const float *plx, *ply, *pr;
-  const int *pbody;
-  const int *arm_tip, *arm_grip, *arm_seg0, *arm_segs;
-};
-
-struct SlotMeta {
-  int tpl, map, horizon, step;
-  uint32_t rng;
-  float comp;       // muscle compliance (f32 as packControls writes it)
-  float tone;
-  int attach_events;
-  double prev_vx, prev_vy;
-  double path_len;
-  double last_x, last_y;
-};
 
 struct BatchArgs {
   kr::SolverConsts K;
@@ -84,7 +48,6 @@ struct BatchArgs {
   int cpc;               // creature entries per group (W * 32 / G)
   int *queue;            // group counter
   int max_steps;
-  int ctrl_mode;
   int ctrl_period;
   float *obs;            // capacity x ring x KR_OBS_STRIDE
   int obs_ring;
@@ -333,7 +296,7 @@ __device__ void run_creature(const BatchArgs &A, const TplDev &td, const TplSmem
   for (int s = 0; s < steps; s++) {
     const int t = m.step;
     // 1. proprioception of the current state
-    if (A.obs_ring > 0 || A.ctrl_mode == KR_CTRL_POLICY) {
+    if (A.obs_ring > 0 || m.ctrl == KR_CTRL_POLICY) {
       const unsigned att = proprio<G>(A, td, P, S, X, m, L);
       if (A.obs_ring > 0) {
         float *o = A.obs + ((size_t)slot * A.obs_ring + (t % A.obs_ring)) * KR_OBS_STRIDE;
@@ -342,7 +305,7 @@ __device__ void run_creature(const BatchArgs &A, const TplDev &td, const TplSmem
       }
     }
     // 2. controls
-    if (A.ctrl_mode == KR_CTRL_STREAM) {
+    if (m.ctrl == KR_CTRL_STREAM) {
       if (t % A.ctrl_period == 0 && lane == 0) {
         uint32_t r = m.rng;
         for (int a = 0; a < arms; a++) {
@@ -351,7 +314,7 @@ __device__ void run_creature(const BatchArgs &A, const TplDev &td, const TplSmem
         }
         m.rng = r;
       }
-    } else if (A.ctrl_mode == KR_CTRL_POLICY) {
+    } else if (m.ctrl == KR_CTRL_POLICY) {
       policy<G>(A, td, X, slot, L);
     }
     L.sync();
@@ -466,11 +429,13 @@ __global__ void __launch_bounds__(32 * kMaxW, 1) batch_kernel(BatchArgs A) {
   }
 }
 
+// writes n prepared creatures into slots[0..n): pose, released grips, zero
+// lambda / cooldown / controls, meta
 __global__ void spawn_kernel(float *state, float4 *grip, float2 *glam, double *cd, SlotMeta *meta,
-                             float *ctrl, const float *pose, const SlotMeta *init, int first, int n) {
+                             float *ctrl, const int *slots, const float *pose, const SlotMeta *init, int n) {
   const int i = blockIdx.x;
   if (i >= n) return;
-  const int slot = first + i;
+  const int slot = slots[i];
   const float *src = pose + (size_t)i * kStateStride;
   float *dst = state + (size_t)slot * kStateStride;
   for (int q = threadIdx.x; q < kStateStride; q += blockDim.x) dst[q] = src[q];
@@ -485,70 +450,6 @@ __global__ void spawn_kernel(float *state, float4 *grip, float2 *glam, double *c
 
 }  // namespace
 
-struct kr_batch {
-  kr_batch_desc d{};
-  kr::SolverConsts K{};
-  std::string err;
-  cudaStream_t stream = nullptr;
-  bool own_stream = false;
-  int capacity = 0, n_maps = 0;
-  // templates
-  std::vector<kr::Template> tpls;
-  std::map<std::pair<int, int>, int> tpl_index;
-  std::vector<TplDev> h_tpl;
-  TplDev *d_tpl = nullptr;
-  void *d_tpl_arrays[23] = {nullptr};
-  TplArrays T{};
-  // maps
-  float4 *d_rects = nullptr;
-  int *d_map_off = nullptr;
-  float *d_map_cull = nullptr;
-  std::vector<float> h_map_cull;
-  // slots
-  float *d_state = nullptr;
-  float4 *d_grip = nullptr;
-  float2 *d_glam = nullptr;
-  double *d_cd = nullptr;
-  float *d_ctrl = nullptr;
-  SlotMeta *d_meta = nullptr;
-  float *d_obs = nullptr;
-  std::vector<SlotMeta> h_meta;   // host mirror of tpl / map / horizon (step on device)
-  std::vector<int> h_remaining;   // remaining steps as of the last schedule
-  // groups
-  int *d_groups = nullptr;
-  size_t c_groups = 0;
-  int n_groups = 0;
-  bool groups_dirty = true;
-  int *d_queue = nullptr;
-  // snapshot of every slot (kr_batch_snapshot / kr_batch_restore)
-  float *s_state = nullptr;
-  float4 *s_grip = nullptr;
-  float2 *s_glam = nullptr;
-  double *s_cd = nullptr;
-  float *s_ctrl = nullptr;
-  SlotMeta *s_meta = nullptr;
-  std::vector<int> s_remaining;
-  int *s_groups = nullptr;        // groups built for the snapshot state
-  int s_n_groups = -1, s_cpc = 0, s_G = 0;
-  // launch shape
-  int G = 16, W = 8, ctas_per_sm = 0, n_sm = 0;
-  int smem_per_sm = 0, smem_reserved = 0, smem_optin = 0;
-  int cpc = 8;                  // creature entries per group: W * 32 / G
-  std::vector<int> tpl_cpg;     // creatures per group of each template
-  size_t smem_dyn = 0;          // dynamic shared memory per CTA
-  bool shape_dirty = true;
-  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
-  // policy
-  float *d_pw = nullptr;
-  int *d_pw_idx = nullptr;
-  int n_params = 0, n_individuals = 0;
-
-  int fail(int code, const std::string &m) { err = m; return code; }
-  int cuda_fail(cudaError_t e, const char *what) {
-    err = std::string("CUDA error in ") + what + ": " + cudaGetErrorString(e);
-    return KR_ERR_CUDA;
-  }
-};
 
 namespace {
 thread_local std::string g_batch_error;
@@ -560,6 +461,24 @@ cudaError_t upload_vec(T **d, const std::vector<T> &v) {
   cudaError_t e = cudaMalloc(reinterpret_cast<void **>(d), std::max<size_t>(v.size(), 1) * sizeof(T));
   if (e != cudaSuccess || v.empty()) return e;
   return cudaMemcpy(*d, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice);
+}
+
+// relative cost of one env step of a template (constraint and collision work)
+double tpl_cost(const TplDev &d) { return (double)d.nc + 0.5 * (double)d.np; }
+}  // namespace
+
+namespace krb {
+
+cudaStream_t part_stream(const kr_batch *b, const Part &p) { return p.stream ? p.stream : b->stream; }
+
+void free_part(Part &p) {
+  if (p.d_groups) cudaFree(p.d_groups);
+  if (p.h_groups) cudaFreeHost(p.h_groups);
+  if (p.d_queue) cudaFree(p.d_queue);
+  if (p.staged) cudaEventDestroy(p.staged);
+  if (p.ev0) cudaEventDestroy(p.ev0);
+  if (p.ev1) cudaEventDestroy(p.ev1);
+  p = Part{};
 }
 
 int ensure_template(kr_batch *b, int arms, int segs) {
@@ -607,7 +526,9 @@ int upload_templates(kr_batch *b) {
     segs.insert(segs.end(), t.arm_segs.begin(), t.arm_segs.end());
     b->h_tpl.push_back(d);
   }
-  cudaError_t e = cudaSuccess;
+  // the device may still read the old tables in a queued launch
+  cudaError_t e = cudaDeviceSynchronize();
+  if (e != cudaSuccess) return b->cuda_fail(e, "upload(templates) sync");
   void **A = b->d_tpl_arrays;
 #define UP(i, vec) if (e == cudaSuccess) e = upload_vec(reinterpret_cast<decltype(vec.data()) *>(&A[i]), vec)
   UP(0, im); UP(1, ii); UP(2, boff); UP(3, bcnt); UP(4, ab); UP(5, type); UP(6, motor); UP(7, lax);
@@ -661,56 +582,224 @@ int plan_shape(kr_batch *b) {
   }
   b->smem_dyn = need_max;
   b->shape_dirty = false;
+  b->main.dirty = true;
   return KR_OK;
 }
 
-// groups of up to tpl_cpg slots of one template, longest remaining horizon
-// first; creatures that share a warp are adjacent in remaining horizon
-int build_groups(kr_batch *b, const std::vector<int> &remaining) {
+// Groups of up to tpl_cpg slots of one template.  Creatures of one template
+// are sorted by remaining steps, so the creatures that share a warp finish
+// together; groups are queued by their work (steps this launch x template
+// cost), largest first, so the launch ends on short groups.
+int build_groups(kr_batch *b, Part &p, int max_steps) {
   if (b->shape_dirty) {
     int rc = plan_shape(b);
     if (rc != KR_OK) return rc;
   }
+  const std::vector<int> &rem = b->h_remaining;
   std::vector<int> live;
-  for (int s = 0; s < b->capacity; s++)
-    if (b->h_meta[s].horizon > 0 && remaining[s] > 0) live.push_back(s);
+  if (p.all) {
+    for (int s = 0; s < b->capacity; s++)
+      if (b->h_meta[s].horizon > 0 && rem[s] > 0) live.push_back(s);
+  } else {
+    for (int s : p.slots)
+      if (rem[s] > 0) live.push_back(s);
+  }
+  for (int s : live) {
+    const SlotMeta &m = b->h_meta[s];
+    if (m.ctrl != KR_CTRL_POLICY) continue;
+    const TplDev &t = b->h_tpl[m.tpl];
+    const int need = KR_POLICY_HIDDEN * (6 * t.arms + 7) + (t.arms * t.segs + t.arms) * (KR_POLICY_HIDDEN + 1);
+    if (!b->d_pw || b->n_params < need)
+      return b->fail(KR_ERR_STATE, "slot " + std::to_string(s) + ": policy control needs " + std::to_string(need) +
+                                       " parameters per individual (kr_batch_set_policy)");
+  }
   std::stable_sort(live.begin(), live.end(), [&](int x, int y) {
     if (b->h_meta[x].tpl != b->h_meta[y].tpl) return b->h_meta[x].tpl < b->h_meta[y].tpl;
-    return remaining[x] > remaining[y];
+    return rem[x] > rem[y];
   });
-  std::vector<std::vector<int>> groups;
+  std::vector<std::pair<double, int>> order;  // (work, first index into live)
+  std::vector<int> starts, sizes;
   for (size_t i = 0; i < live.size();) {
-    std::vector<int> g;
     const int t = b->h_meta[live[i]].tpl;
-    while (i < live.size() && (int)g.size() < b->tpl_cpg[t] && b->h_meta[live[i]].tpl == t) g.push_back(live[i++]);
-    groups.push_back(g);
+    const size_t st = i;
+    int n = 0;
+    while (i < live.size() && n < b->tpl_cpg[t] && b->h_meta[live[i]].tpl == t) { i++; n++; }
+    const double work = (double)std::min(max_steps, rem[live[st]]) * tpl_cost(b->h_tpl[t]);
+    order.push_back({work, (int)starts.size()});
+    starts.push_back((int)st);
+    sizes.push_back(n);
   }
-  std::stable_sort(groups.begin(), groups.end(), [&](const std::vector<int> &x, const std::vector<int> &y) {
-    return remaining[x[0]] > remaining[y[0]];
-  });
-  std::vector<int> flat((size_t)groups.size() * b->cpc, -1);
-  for (size_t g = 0; g < groups.size(); g++)
-    for (size_t k = 0; k < groups[g].size(); k++) flat[g * b->cpc + k] = groups[g][k];
-  if (b->d_groups == nullptr || b->c_groups < std::max<size_t>(flat.size(), 1)) {
-    if (b->d_groups) cudaFree(b->d_groups);
-    b->d_groups = nullptr;
-    b->c_groups = std::max<size_t>(flat.size(), 1);
-    cudaError_t e = cudaMalloc(&b->d_groups, b->c_groups * sizeof(int));
+  std::stable_sort(order.begin(), order.end(),
+                   [](const std::pair<double, int> &x, const std::pair<double, int> &y) { return x.first > y.first; });
+  const size_t need = std::max<size_t>(order.size() * b->cpc, 1);
+  cudaStream_t st = part_stream(b, p);
+  if (p.staged_pending) {
+    cudaError_t e = cudaEventSynchronize(p.staged);
+    if (e != cudaSuccess) return b->cuda_fail(e, "groups staging sync");
+    p.staged_pending = false;
+  }
+  if (!p.h_groups || p.ch_groups < need) {
+    if (p.h_groups) cudaFreeHost(p.h_groups);
+    p.h_groups = nullptr;
+    cudaError_t e = cudaMallocHost(&p.h_groups, need * sizeof(int));
+    if (e != cudaSuccess) return b->cuda_fail(e, "cudaMallocHost(groups)");
+    p.ch_groups = need;
+  }
+  if (!p.d_groups || p.c_groups < need) {
+    if (p.d_groups) {
+      cudaStreamSynchronize(st);
+      cudaFree(p.d_groups);
+    }
+    p.d_groups = nullptr;
+    cudaError_t e = cudaMalloc(&p.d_groups, need * sizeof(int));
     if (e != cudaSuccess) return b->cuda_fail(e, "cudaMalloc(groups)");
+    p.c_groups = need;
   }
-  if (!flat.empty()) {
-    cudaError_t e = cudaMemcpyAsync(b->d_groups, flat.data(), flat.size() * sizeof(int),
-                                    cudaMemcpyHostToDevice, b->stream);
+  if (!p.d_queue) {
+    cudaError_t e = cudaMalloc(&p.d_queue, sizeof(int));
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&p.staged, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreate(&p.ev0);
+    if (e == cudaSuccess) e = cudaEventCreate(&p.ev1);
+    if (e != cudaSuccess) return b->cuda_fail(e, "part setup");
+  }
+  std::fill(p.h_groups, p.h_groups + order.size() * b->cpc, -1);
+  for (size_t g = 0; g < order.size(); g++) {
+    const int k = order[g].second;
+    for (int q = 0; q < sizes[k]; q++) p.h_groups[g * b->cpc + q] = live[starts[k] + q];
+  }
+  if (!order.empty()) {
+    cudaError_t e = cudaMemcpyAsync(p.d_groups, p.h_groups, order.size() * b->cpc * sizeof(int),
+                                    cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaEventRecord(p.staged, st);
     if (e != cudaSuccess) return b->cuda_fail(e, "upload(groups)");
-    e = cudaStreamSynchronize(b->stream);
-    if (e != cudaSuccess) return b->cuda_fail(e, "upload(groups) sync");
+    p.staged_pending = true;
   }
-  b->n_groups = (int)groups.size();
-  b->groups_dirty = false;
+  p.n_groups = (int)order.size();
+  p.dirty = false;
   return KR_OK;
 }
 
+}  // namespace krb
+
+namespace {
+template <int G>
+cudaError_t launch_g(const BatchArgs &A, kr_batch *b, cudaStream_t st, int n_groups, int *grid_out) {
+  auto *fn = batch_kernel<G>;
+  cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b->smem_dyn);
+  if (e != cudaSuccess) return e;
+  int per_sm = 0;
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, 32 * b->W, b->smem_dyn);
+  if (e != cudaSuccess) return e;
+  if (per_sm < 1) { *grid_out = 0; return cudaSuccess; }
+  if (b->ctas_per_sm > 0) per_sm = std::min(per_sm, b->ctas_per_sm);
+  const int grid = std::max(1, std::min(n_groups, per_sm * b->n_sm));
+  *grid_out = grid;
+  fn<<<grid, 32 * b->W, b->smem_dyn, st>>>(A);
+  return cudaGetLastError();
+}
 }  // namespace
+
+namespace krb {
+
+int launch_part(kr_batch *b, Part &p, int max_steps, bool timed) {
+  if (b->tpls.empty()) return KR_OK;
+  if (b->d.control_mode == KR_CTRL_POLICY && !b->d_pw)
+    return b->fail(KR_ERR_STATE, "policy control without kr_batch_set_policy");
+  if (p.dirty || b->shape_dirty) {
+    int rc = build_groups(b, p, max_steps);
+    if (rc != KR_OK) return rc;
+  }
+  if (p.n_groups == 0) return KR_OK;
+  cudaStream_t st = part_stream(b, p);
+  BatchArgs A{};
+  A.K = b->K;
+  A.tpl = b->d_tpl;
+  A.T = b->T;
+  A.state = b->d_state; A.grip = b->d_grip; A.glam = b->d_glam; A.cd = b->d_cd; A.ctrl_cur = b->d_ctrl; A.meta = b->d_meta;
+  A.rects = b->d_rects; A.map_off = b->d_map_off; A.map_cull = b->d_map_cull;
+  A.groups = p.d_groups; A.n_groups = p.n_groups; A.cpc = b->cpc; A.queue = p.d_queue;
+  A.max_steps = max_steps;
+  A.ctrl_period = std::max(1, b->d.control_period);
+  A.obs = b->d_obs; A.obs_ring = b->d.obs_ring;
+  A.slip_max = b->d.grip_slip_max; A.cooldown = b->d.grip_cooldown;
+  A.inv_h64 = 1.0 / b->d.solver.h;
+  A.dt = b->d.solver.h * b->d.solver.substeps;
+  A.pw = b->d_pw; A.pw_idx = b->d_pw_idx; A.n_params = b->n_params;
+  cudaError_t e;
+  if ((e = cudaMemsetAsync(p.d_queue, 0, sizeof(int), st)) != cudaSuccess) return b->cuda_fail(e, "queue reset");
+  if (timed) cudaEventRecord(p.ev0, st);
+  int grid = 0;
+  e = b->G == 32 ? launch_g<32>(A, b, st, p.n_groups, &grid)
+                 : b->G == 16 ? launch_g<16>(A, b, st, p.n_groups, &grid) : launch_g<8>(A, b, st, p.n_groups, &grid);
+  if (e != cudaSuccess) return b->cuda_fail(e, "batch_kernel launch");
+  if (grid == 0) return b->fail(KR_ERR_CAPACITY, "batch kernel does not fit on an SM with this launch shape");
+  if (timed) cudaEventRecord(p.ev1, st);
+  // remaining horizons as the next schedule sees them
+  if (p.all) {
+    for (int s = 0; s < b->capacity; s++)
+      if (b->h_remaining[s] > 0) b->h_remaining[s] = std::max(0, b->h_remaining[s] - max_steps);
+  } else {
+    for (int s : p.slots)
+      if (b->h_remaining[s] > 0) b->h_remaining[s] = std::max(0, b->h_remaining[s] - max_steps);
+  }
+  return KR_OK;
+}
+
+int prepare_spawn(kr_batch *b, int n, const int32_t *arms, const int32_t *segs, const int32_t *map_id,
+                  const double *x, const double *y, const double *angle, const int32_t *horizon,
+                  const uint32_t *control_seed, const float *tone, int ctrl_mode, SpawnInit *out,
+                  int *first_bad) {
+  const size_t tpl_before = b->tpls.size();
+  out->pose.assign((size_t)n * kStateStride, 0.f);
+  out->meta.assign(n, SlotMeta{});
+  std::vector<double> px(kr::kMaxTplBodies), py(kr::kMaxTplBodies), pa(kr::kMaxTplBodies);
+  for (int i = 0; i < n; i++) {
+    *first_bad = i;
+    const int t = ensure_template(b, arms[i], segs[i]);
+    if (t < 0)
+      return b->fail(KR_ERR_INVALID, "body shape " + std::to_string(arms[i]) + "x" + std::to_string(segs[i]) +
+                                         " outside 1..8 arms x 1..9 segments");
+    if (map_id[i] < 0 || map_id[i] >= b->n_maps)
+      return b->fail(KR_ERR_INDEX, "map " + std::to_string(map_id[i]) + " of " + std::to_string(b->n_maps));
+    if (horizon[i] < 0) return b->fail(KR_ERR_INVALID, "negative horizon");
+    const kr::Template &T = b->tpls[t];
+    kr::spawn_pose(T, x[i], y[i], angle[i], 0.28, px.data(), py.data(), pa.data());
+    float *dst = out->pose.data() + (size_t)i * kStateStride;
+    for (int j = 0; j < T.nb; j++) {
+      dst[j] = (float)px[j];
+      dst[kBodyPad + j] = (float)py[j];
+      dst[4 * kBodyPad + j] = (float)pa[j];
+    }
+    SlotMeta &m = out->meta[i];
+    m = SlotMeta{};
+    m.tpl = t;
+    m.map = map_id[i];
+    m.horizon = horizon[i];
+    m.step = 0;
+    m.ctrl = ctrl_mode;
+    m.rng = control_seed ? control_seed[i] : 0u;
+    const double tn = std::max(0.0, std::min(1.0, tone ? (double)tone[i] : 0.5));
+    m.tone = (float)tn;
+    m.comp = (float)(1.0 / (2000.0 + tn * (400000.0 - 2000.0)));
+    m.last_x = (double)(float)x[i];
+    m.last_y = (double)(float)y[i];
+  }
+  *first_bad = -1;
+  if (b->tpls.size() != tpl_before) return upload_templates(b);
+  return KR_OK;
+}
+
+cudaError_t launch_spawn(kr_batch *b, const int *d_slots, const float *d_pose, const SlotMeta *d_meta,
+                         int n, cudaStream_t stream) {
+  if (n <= 0) return cudaSuccess;
+  spawn_kernel<<<n, 128, 0, stream>>>(b->d_state, b->d_grip, b->d_glam, b->d_cd, b->d_meta, b->d_ctrl,
+                                      d_slots, d_pose, d_meta, n);
+  return cudaGetLastError();
+}
+
+}  // namespace krb
+
+using namespace krb;
 
 extern "C" const char *kr_batch_last_error(const kr_batch *b) {
   return b ? b->err.c_str() : g_batch_error.c_str();
@@ -791,8 +880,7 @@ extern "C" int kr_batch_create(const kr_batch_desc *desc, kr_batch **out) {
     const double c = ht + 2.0 + kr::kCullSlack + 1.0;
     b->h_map_cull[m] = std::isfinite(c) && c < 1e30 ? (float)c : 1e30f;
   }
-  std::vector<float4> r4v(r4);
-  if ((e = upload_vec(&b->d_rects, r4v)) != cudaSuccess) return bail(e, "upload(rects)");
+  if ((e = upload_vec(&b->d_rects, r4)) != cudaSuccess) return bail(e, "upload(rects)");
   if ((e = upload_vec(&b->d_map_off, off)) != cudaSuccess) return bail(e, "upload(map offsets)");
   if ((e = upload_vec(&b->d_map_cull, b->h_map_cull)) != cudaSuccess) return bail(e, "upload(map cull)");
   const size_t C = (size_t)d.capacity;
@@ -808,8 +896,6 @@ extern "C" int kr_batch_create(const kr_batch_desc *desc, kr_batch **out) {
     if ((e = cudaMalloc(&b->d_obs, C * d.obs_ring * KR_OBS_STRIDE * sizeof(float))) != cudaSuccess) return bail(e, "cudaMalloc(obs)");
     if ((e = cudaMemset(b->d_obs, 0, C * d.obs_ring * KR_OBS_STRIDE * sizeof(float))) != cudaSuccess) return bail(e, "cudaMemset(obs)");
   }
-  if ((e = cudaMalloc(&b->d_queue, sizeof(int))) != cudaSuccess) return bail(e, "cudaMalloc(queue)");
-  if ((e = cudaEventCreate(&b->ev0)) != cudaSuccess || (e = cudaEventCreate(&b->ev1)) != cudaSuccess) return bail(e, "cudaEventCreate");
   b->h_meta.assign(C, SlotMeta{});
   b->h_remaining.assign(C, 0);
   // every slot starts empty (horizon 0)
@@ -826,62 +912,38 @@ extern "C" int kr_batch_spawn(kr_batch *b, int32_t first, int32_t n, const int32
   if (first < 0 || first + n > b->capacity) return b->fail(KR_ERR_INVALID, "spawn range outside the slots");
   if (!arms || !segs || !map_id || !x || !y || !angle || !horizon)
     return b->fail(KR_ERR_INVALID, "kr_batch_spawn: null argument");
-  const size_t tpl_before = b->tpls.size();
-  std::vector<float> pose((size_t)n * kStateStride, 0.f);
-  std::vector<SlotMeta> init(n);
-  std::vector<double> px(kr::kMaxTplBodies), py(kr::kMaxTplBodies), pa(kr::kMaxTplBodies);
-  for (int i = 0; i < n; i++) {
-    const int t = ensure_template(b, arms[i], segs[i]);
-    if (t < 0)
-      return b->fail(KR_ERR_INVALID, "creature " + std::to_string(first + i) + ": body shape " +
-                                         std::to_string(arms[i]) + "x" + std::to_string(segs[i]) +
-                                         " outside 1..8 arms x 1..9 segments");
-    if (map_id[i] < 0 || map_id[i] >= b->n_maps)
-      return b->fail(KR_ERR_INDEX, "creature " + std::to_string(first + i) + ": map " +
-                                       std::to_string(map_id[i]) + " of " + std::to_string(b->n_maps));
-    if (horizon[i] < 0) return b->fail(KR_ERR_INVALID, "negative horizon");
-    const kr::Template &T = b->tpls[t];
-    kr::spawn_pose(T, x[i], y[i], angle[i], 0.28, px.data(), py.data(), pa.data());
-    float *dst = pose.data() + (size_t)i * kStateStride;
-    for (int j = 0; j < T.nb; j++) {
-      dst[j] = (float)px[j];
-      dst[kBodyPad + j] = (float)py[j];
-      dst[4 * kBodyPad + j] = (float)pa[j];
-    }
-    SlotMeta &m = init[i];
-    m = SlotMeta{};
-    m.tpl = t;
-    m.map = map_id[i];
-    m.horizon = horizon[i];
-    m.step = 0;
-    m.rng = control_seed ? control_seed[i] : (uint32_t)(first + i);
-    const double tn = std::max(0.0, std::min(1.0, tone ? (double)tone[i] : 0.5));
-    m.tone = (float)tn;
-    m.comp = (float)(1.0 / (2000.0 + tn * (400000.0 - 2000.0)));
-    m.last_x = (double)(float)x[i];
-    m.last_y = (double)(float)y[i];
-    b->h_meta[first + i] = m;
-    b->h_remaining[first + i] = m.horizon;
+  std::vector<uint32_t> seeds(n);
+  for (int i = 0; i < n; i++) seeds[i] = control_seed ? control_seed[i] : (uint32_t)(first + i);
+  SpawnInit init;
+  int bad = -1;
+  int rc = prepare_spawn(b, n, arms, segs, map_id, x, y, angle, horizon, seeds.data(), tone,
+                         b->d.control_mode, &init, &bad);
+  if (rc != KR_OK) {
+    b->err = "creature " + std::to_string(first + bad) + ": " + b->err;
+    return rc;
   }
-  if (b->tpls.size() != tpl_before) {
-    int rc = upload_templates(b);
-    if (rc != KR_OK) return rc;
+  std::vector<int> slots(n);
+  for (int i = 0; i < n; i++) {
+    slots[i] = first + i;
+    b->h_meta[first + i] = init.meta[i];
+    b->h_remaining[first + i] = init.meta[i].horizon;
   }
   float *d_pose = nullptr;
   SlotMeta *d_init = nullptr;
-  cudaError_t e = cudaMallocAsync(&d_pose, pose.size() * sizeof(float), b->stream);
-  if (e == cudaSuccess) e = cudaMallocAsync(&d_init, init.size() * sizeof(SlotMeta), b->stream);
-  if (e == cudaSuccess) e = cudaMemcpyAsync(d_pose, pose.data(), pose.size() * sizeof(float), cudaMemcpyHostToDevice, b->stream);
-  if (e == cudaSuccess) e = cudaMemcpyAsync(d_init, init.data(), init.size() * sizeof(SlotMeta), cudaMemcpyHostToDevice, b->stream);
-  if (e == cudaSuccess) {
-    spawn_kernel<<<n, 128, 0, b->stream>>>(b->d_state, b->d_grip, b->d_glam, b->d_cd, b->d_meta, b->d_ctrl, d_pose, d_init, first, n);
-    e = cudaGetLastError();
-  }
+  int *d_slots = nullptr;
+  cudaError_t e = cudaMallocAsync(&d_pose, init.pose.size() * sizeof(float), b->stream);
+  if (e == cudaSuccess) e = cudaMallocAsync(&d_init, init.meta.size() * sizeof(SlotMeta), b->stream);
+  if (e == cudaSuccess) e = cudaMallocAsync(&d_slots, slots.size() * sizeof(int), b->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(d_pose, init.pose.data(), init.pose.size() * sizeof(float), cudaMemcpyHostToDevice, b->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(d_init, init.meta.data(), init.meta.size() * sizeof(SlotMeta), cudaMemcpyHostToDevice, b->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(d_slots, slots.data(), slots.size() * sizeof(int), cudaMemcpyHostToDevice, b->stream);
+  if (e == cudaSuccess) e = launch_spawn(b, d_slots, d_pose, d_init, n, b->stream);
   if (d_pose) cudaFreeAsync(d_pose, b->stream);
   if (d_init) cudaFreeAsync(d_init, b->stream);
+  if (d_slots) cudaFreeAsync(d_slots, b->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
   if (e != cudaSuccess) return b->cuda_fail(e, "kr_batch_spawn");
-  b->groups_dirty = true;
+  b->main.dirty = true;
   return KR_OK;
 }
 
@@ -899,26 +961,39 @@ extern "C" int kr_batch_set_policy(kr_batch *b, const float *weights, int32_t n_
   if (!b) return KR_ERR_INVALID;
   if (!weights || !slot_individual || n_individuals <= 0 || n_params <= 0)
     return b->fail(KR_ERR_INVALID, "kr_batch_set_policy: null argument or empty policy");
-  for (int s = 0; s < b->capacity; s++)
+  for (int s = 0; s < b->capacity; s++) {
     if (slot_individual[s] < 0 || slot_individual[s] >= n_individuals)
       return b->fail(KR_ERR_INDEX, "slot " + std::to_string(s) + " refers to individual " +
                                        std::to_string(slot_individual[s]) + " of " +
                                        std::to_string(n_individuals));
+    const SlotMeta &m = b->h_meta[s];
+    if (m.horizon > 0) {
+      const kr::Template &t = b->tpls[m.tpl];
+      const int need = KR_POLICY_HIDDEN * (6 * t.arms + 7) + (t.arms * t.segs + t.arms) * (KR_POLICY_HIDDEN + 1);
+      if (n_params < need)
+        return b->fail(KR_ERR_INVALID, "slot " + std::to_string(s) + ": a " + std::to_string(t.arms) + "x" +
+                                           std::to_string(t.segs) + " body needs " + std::to_string(need) +
+                                           " policy parameters, got " + std::to_string(n_params));
+    }
+  }
   const size_t need = (size_t)n_individuals * n_params;
+  cudaError_t e = cudaStreamSynchronize(b->stream);
+  if (e != cudaSuccess) return b->cuda_fail(e, "kr_batch_set_policy sync");
   if (!b->d_pw || (size_t)b->n_individuals * b->n_params < need) {
     if (b->d_pw) cudaFree(b->d_pw);
     b->d_pw = nullptr;
-    cudaError_t e = cudaMalloc(&b->d_pw, need * sizeof(float));
+    e = cudaMalloc(&b->d_pw, need * sizeof(float));
     if (e != cudaSuccess) return b->cuda_fail(e, "cudaMalloc(policy weights)");
   }
   if (!b->d_pw_idx) {
-    cudaError_t e = cudaMalloc(&b->d_pw_idx, (size_t)b->capacity * sizeof(int));
+    e = cudaMalloc(&b->d_pw_idx, (size_t)b->capacity * sizeof(int));
     if (e != cudaSuccess) return b->cuda_fail(e, "cudaMalloc(policy index)");
   }
-  cudaError_t e = cudaMemcpyAsync(b->d_pw, weights, need * sizeof(float), cudaMemcpyHostToDevice, b->stream);
+  e = cudaMemcpyAsync(b->d_pw, weights, need * sizeof(float), cudaMemcpyHostToDevice, b->stream);
   if (e == cudaSuccess)
     e = cudaMemcpyAsync(b->d_pw_idx, slot_individual, (size_t)b->capacity * sizeof(int),
                         cudaMemcpyHostToDevice, b->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
   if (e != cudaSuccess) return b->cuda_fail(e, "kr_batch_set_policy");
   b->n_individuals = n_individuals;
   b->n_params = n_params;
@@ -935,7 +1010,7 @@ extern "C" int kr_batch_set_launch(kr_batch *b, int32_t lanes_per_creature, int3
     return b->fail(KR_ERR_INVALID, "more than 64 creatures per CTA");
   if (ctas_per_sm < 0 || ctas_per_sm > 32) return b->fail(KR_ERR_INVALID, "ctas_per_sm outside 0..32");
   if (b->W != warps_per_cta || b->G != lanes_per_creature || b->ctas_per_sm != ctas_per_sm) {
-    b->groups_dirty = true;
+    b->main.dirty = true;
     b->shape_dirty = true;
   }
   b->G = lanes_per_creature;
@@ -958,98 +1033,59 @@ extern "C" int kr_batch_get_launch(kr_batch *b, int32_t *lanes_per_creature, int
   return KR_OK;
 }
 
-namespace {
-template <int G>
-cudaError_t launch_g(const BatchArgs &A, kr_batch *b, int *grid_out) {
-  auto *fn = batch_kernel<G>;
-  cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b->smem_dyn);
-  if (e != cudaSuccess) return e;
-  int per_sm = 0;
-  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, 32 * b->W, b->smem_dyn);
-  if (e != cudaSuccess) return e;
-  if (per_sm < 1) { *grid_out = 0; return cudaSuccess; }
-  if (b->ctas_per_sm > 0) per_sm = std::min(per_sm, b->ctas_per_sm);
-  const int grid = std::max(1, std::min(b->n_groups, per_sm * b->n_sm));
-  *grid_out = grid;
-  fn<<<grid, 32 * b->W, b->smem_dyn, b->stream>>>(A);
-  return cudaGetLastError();
-}
-
-int launch(kr_batch *b, int max_steps, bool timed) {
-  if (b->tpls.empty()) return KR_OK;
-  if (b->d.control_mode == KR_CTRL_POLICY && !b->d_pw)
-    return b->fail(KR_ERR_STATE, "policy control without kr_batch_set_policy");
-  if (b->groups_dirty || b->shape_dirty) {
-    int rc = build_groups(b, b->h_remaining);
-    if (rc != KR_OK) return rc;
-  }
-  if (b->n_groups == 0) return KR_OK;
-  BatchArgs A{};
-  A.K = b->K;
-  A.tpl = b->d_tpl;
-  A.T = b->T;
-  A.state = b->d_state; A.grip = b->d_grip; A.glam = b->d_glam; A.cd = b->d_cd; A.ctrl_cur = b->d_ctrl; A.meta = b->d_meta;
-  A.rects = b->d_rects; A.map_off = b->d_map_off; A.map_cull = b->d_map_cull;
-  A.groups = b->d_groups; A.n_groups = b->n_groups; A.cpc = b->cpc; A.queue = b->d_queue;
-  A.max_steps = max_steps;
-  A.ctrl_mode = b->d.control_mode; A.ctrl_period = std::max(1, b->d.control_period);
-  A.obs = b->d_obs; A.obs_ring = b->d.obs_ring;
-  A.slip_max = b->d.grip_slip_max; A.cooldown = b->d.grip_cooldown;
-  A.inv_h64 = 1.0 / b->d.solver.h;
-  A.dt = b->d.solver.h * b->d.solver.substeps;
-  A.pw = b->d_pw; A.pw_idx = b->d_pw_idx; A.n_params = b->n_params;
-  cudaError_t e;
-  if ((e = cudaMemsetAsync(b->d_queue, 0, sizeof(int), b->stream)) != cudaSuccess) return b->cuda_fail(e, "queue reset");
-  if (timed) cudaEventRecord(b->ev0, b->stream);
-  int grid = 0;
-  e = b->G == 32 ? launch_g<32>(A, b, &grid) : b->G == 16 ? launch_g<16>(A, b, &grid) : launch_g<8>(A, b, &grid);
-  if (e != cudaSuccess) return b->cuda_fail(e, "batch_kernel launch");
-  if (grid == 0) return b->fail(KR_ERR_CAPACITY, "batch kernel does not fit on an SM with this launch shape");
-  if (timed) cudaEventRecord(b->ev1, b->stream);
-  // remaining horizons as the next schedule sees them
-  for (int s = 0; s < b->capacity; s++)
-    if (b->h_remaining[s] > 0) b->h_remaining[s] = std::max(0, b->h_remaining[s] - max_steps);
-  return KR_OK;
-}
-}  // namespace
-
 extern "C" int kr_batch_run(kr_batch *b, int32_t max_steps) {
   if (!b) return KR_ERR_INVALID;
   if (max_steps < 0) return b->fail(KR_ERR_INVALID, "max_steps < 0");
   if (max_steps == 0) return KR_OK;
-  const bool redo = b->groups_dirty;
-  int rc = launch(b, max_steps, true);
-  (void)redo;
-  b->groups_dirty = true;  // finished slots leave the queue at the next launch
-  return rc;
+  b->main.dirty = true;  // finished slots leave the queue, work estimates change
+  return launch_part(b, b->main, max_steps, true);
+}
+
+extern "C" int kr_batch_run_launches(kr_batch *b, int32_t steps_per_launch, int32_t launches) {
+  if (!b) return KR_ERR_INVALID;
+  if (steps_per_launch <= 0 || launches < 0) return b->fail(KR_ERR_INVALID, "kr_batch_run_launches: bad counts");
+  b->main.dirty = true;
+  for (int l = 0; l < launches; l++) {
+    // the groups of the first launch serve every launch (finished slots are skipped by the kernel)
+    int rc = launch_part(b, b->main, steps_per_launch, l == launches - 1);
+    if (rc != KR_OK) return rc;
+  }
+  b->main.dirty = true;
+  return KR_OK;
 }
 
 extern "C" int kr_batch_run_graph(kr_batch *b, int32_t max_steps, int32_t launches, int32_t replays) {
   if (!b) return KR_ERR_INVALID;
   if (max_steps <= 0 || launches <= 0 || replays < 0) return b->fail(KR_ERR_INVALID, "kr_batch_run_graph: bad counts");
-  if (b->groups_dirty || b->shape_dirty) {
-    int rc = build_groups(b, b->h_remaining);
-    if (rc != KR_OK) return rc;
+  b->main.dirty = true;
+  int rc = build_groups(b, b->main, max_steps);
+  if (rc != KR_OK) return rc;
+  if (b->main.staged_pending) {
+    cudaEventSynchronize(b->main.staged);
+    b->main.staged_pending = false;
   }
+  const std::vector<int> before = b->h_remaining;
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
   cudaError_t e = cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal);
   if (e != cudaSuccess) return b->cuda_fail(e, "cudaStreamBeginCapture");
-  int rc = KR_OK;
-  for (int l = 0; l < launches && rc == KR_OK; l++) rc = launch(b, max_steps, false);
+  for (int l = 0; l < launches && rc == KR_OK; l++) rc = launch_part(b, b->main, max_steps, false);
   e = cudaStreamEndCapture(b->stream, &graph);
   if (rc != KR_OK) { if (graph) cudaGraphDestroy(graph); return rc; }
   if (e != cudaSuccess) return b->cuda_fail(e, "cudaStreamEndCapture");
   e = cudaGraphInstantiate(&exec, graph, 0);
   if (e != cudaSuccess) { cudaGraphDestroy(graph); return b->cuda_fail(e, "cudaGraphInstantiate"); }
-  cudaEventRecord(b->ev0, b->stream);
+  cudaEventRecord(b->main.ev0, b->stream);
   for (int r = 0; r < replays && e == cudaSuccess; r++) e = cudaGraphLaunch(exec, b->stream);
-  cudaEventRecord(b->ev1, b->stream);
+  cudaEventRecord(b->main.ev1, b->stream);
   cudaStreamSynchronize(b->stream);
   cudaGraphExecDestroy(exec);
   cudaGraphDestroy(graph);
   if (e != cudaSuccess) return b->cuda_fail(e, "cudaGraphLaunch");
-  b->groups_dirty = true;
+  // every replay advanced every slot by launches x max_steps
+  const long adv = (long)max_steps * launches * replays;
+  for (int s = 0; s < b->capacity; s++) b->h_remaining[s] = (int)std::max<long>(0, before[s] - adv);
+  b->main.dirty = true;
   return KR_OK;
 }
 
@@ -1065,7 +1101,7 @@ extern "C" int kr_batch_live(kr_batch *b, int32_t *live) {
     if (b->h_remaining[s] > 0) n++;
   }
   *live = n;
-  b->groups_dirty = true;
+  b->main.dirty = true;
   return KR_OK;
 }
 
@@ -1073,12 +1109,11 @@ extern "C" int kr_batch_read_state(kr_batch *b, int32_t first, int32_t n, float 
                                    int32_t *steps) {
   if (!b) return KR_ERR_INVALID;
   if (first < 0 || n < 0 || first + n > b->capacity) return b->fail(KR_ERR_INVALID, "read range outside the slots");
-  cudaError_t e = cudaSuccess;
+  if (n == 0) return KR_OK;
   std::vector<float> st((size_t)n * kStateStride);
   std::vector<float4> gr((size_t)n * KR_BATCH_MAX_ARMS);
   std::vector<SlotMeta> m(n);
-  if (n == 0) return KR_OK;
-  e = cudaMemcpyAsync(st.data(), b->d_state + (size_t)first * kStateStride, st.size() * sizeof(float), cudaMemcpyDeviceToHost, b->stream);
+  cudaError_t e = cudaMemcpyAsync(st.data(), b->d_state + (size_t)first * kStateStride, st.size() * sizeof(float), cudaMemcpyDeviceToHost, b->stream);
   if (e == cudaSuccess) e = cudaMemcpyAsync(gr.data(), b->d_grip + (size_t)first * KR_BATCH_MAX_ARMS, gr.size() * sizeof(float4), cudaMemcpyDeviceToHost, b->stream);
   if (e == cudaSuccess) e = cudaMemcpyAsync(m.data(), b->d_meta + first, m.size() * sizeof(SlotMeta), cudaMemcpyDeviceToHost, b->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
@@ -1137,8 +1172,9 @@ extern "C" int kr_batch_read_fitness(kr_batch *b, int32_t first, int32_t n, doub
 
 extern "C" int kr_batch_last_ms(kr_batch *b, float *ms) {
   if (!b || !ms) return KR_ERR_INVALID;
-  cudaError_t e = cudaEventSynchronize(b->ev1);
-  if (e == cudaSuccess) e = cudaEventElapsedTime(ms, b->ev0, b->ev1);
+  if (!b->main.ev1) return b->fail(KR_ERR_STATE, "no launch yet");
+  cudaError_t e = cudaEventSynchronize(b->main.ev1);
+  if (e == cudaSuccess) e = cudaEventElapsedTime(ms, b->main.ev0, b->main.ev1);
   if (e != cudaSuccess) return b->cuda_fail(e, "kr_batch_last_ms");
   return KR_OK;
 }
@@ -1168,17 +1204,16 @@ extern "C" int kr_batch_set_stream(kr_batch *b, void *stream) {
 
 extern "C" void kr_batch_destroy(kr_batch *b) {
   if (!b) return;
-  if (b->stream) cudaStreamSynchronize(b->stream);
+  cudaDeviceSynchronize();
   for (void *p : b->d_tpl_arrays)
     if (p) cudaFree(p);
+  free_part(b->main);
   void *ptrs[] = {b->d_tpl, const_cast<int *>(b->T.arm_segs), b->d_rects, b->d_map_off, b->d_map_cull,
-                  b->d_state, b->d_grip, b->d_glam, b->d_cd, b->d_ctrl, b->d_meta, b->d_obs, b->d_groups,
-                  b->d_queue, b->d_pw, b->d_pw_idx, b->s_state, b->s_grip, b->s_glam, b->s_cd,
+                  b->d_state, b->d_grip, b->d_glam, b->d_cd, b->d_ctrl, b->d_meta, b->d_obs,
+                  b->d_pw, b->d_pw_idx, b->s_state, b->s_grip, b->s_glam, b->s_cd,
                   b->s_ctrl, b->s_meta, b->s_groups};
   for (void *p : ptrs)
     if (p) cudaFree(p);
-  if (b->ev0) cudaEventDestroy(b->ev0);
-  if (b->ev1) cudaEventDestroy(b->ev1);
   if (b->own_stream && b->stream) cudaStreamDestroy(b->stream);
   delete b;
 }
@@ -1223,26 +1258,27 @@ extern "C" int kr_batch_restore(kr_batch *b) {
   if (e != cudaSuccess) return b->cuda_fail(e, "kr_batch_restore");
   b->h_remaining = b->s_remaining;
   // the work groups of the snapshot state: built once, then copied back
+  Part &p = b->main;
   if (b->s_n_groups < 0 || b->s_cpc != b->cpc || b->s_G != b->G || b->shape_dirty) {
-    int rc = build_groups(b, b->h_remaining);
+    int rc = build_groups(b, p, 1 << 30);
     if (rc != KR_OK) return rc;
     if (b->s_groups) cudaFree(b->s_groups);
     b->s_groups = nullptr;
-    e = cudaMalloc(&b->s_groups, std::max<size_t>(b->c_groups, 1) * sizeof(int));
-    if (e == cudaSuccess)
-      e = cudaMemcpyAsync(b->s_groups, b->d_groups, (size_t)b->n_groups * b->cpc * sizeof(int),
+    e = cudaMalloc(&b->s_groups, std::max<size_t>(p.c_groups, 1) * sizeof(int));
+    if (e == cudaSuccess && p.n_groups > 0)
+      e = cudaMemcpyAsync(b->s_groups, p.d_groups, (size_t)p.n_groups * b->cpc * sizeof(int),
                           cudaMemcpyDeviceToDevice, b->stream);
     if (e != cudaSuccess) return b->cuda_fail(e, "kr_batch_restore(groups)");
-    b->s_n_groups = b->n_groups;
+    b->s_n_groups = p.n_groups;
     b->s_cpc = b->cpc;
     b->s_G = b->G;
-  } else {
-    e = cudaMemcpyAsync(b->d_groups, b->s_groups, (size_t)b->s_n_groups * b->cpc * sizeof(int),
+  } else if (b->s_n_groups > 0) {
+    e = cudaMemcpyAsync(p.d_groups, b->s_groups, (size_t)b->s_n_groups * b->cpc * sizeof(int),
                         cudaMemcpyDeviceToDevice, b->stream);
     if (e != cudaSuccess) return b->cuda_fail(e, "kr_batch_restore(groups)");
-    b->n_groups = b->s_n_groups;
+    p.n_groups = b->s_n_groups;
   }
-  b->groups_dirty = false;
+  p.dirty = false;
   return KR_OK;
 }
 
@@ -1284,20 +1320,5 @@ extern "C" int kr_probe_fp32_rate(double *fma_per_s) {
   cudaFree(out);
   if (e != cudaSuccess) { g_batch_error = cudaGetErrorString(e); return KR_ERR_CUDA; }
   *fma_per_s = (double)blocks * threads * iters * 8.0 / (ms * 1e-3);
-  return KR_OK;
-}
-
-extern "C" int kr_batch_run_launches(kr_batch *b, int32_t steps_per_launch, int32_t launches) {
-  if (!b) return KR_ERR_INVALID;
-  if (steps_per_launch <= 0 || launches < 0) return b->fail(KR_ERR_INVALID, "kr_batch_run_launches: bad counts");
-  if (b->groups_dirty || b->shape_dirty) {
-    int rc = build_groups(b, b->h_remaining);
-    if (rc != KR_OK) return rc;
-  }
-  for (int l = 0; l < launches; l++) {
-    int rc = launch(b, steps_per_launch, l == launches - 1);
-    if (rc != KR_OK) return rc;
-  }
-  b->groups_dirty = true;
   return KR_OK;
 }

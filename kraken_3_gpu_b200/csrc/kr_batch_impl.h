@@ -1,0 +1,172 @@
+// kr_batch_impl.h -- host-side internals of the batched engine, shared by
+// kr_batch.cu (the engine and its kernel) and kr_serve.cu (the rollout
+// server built on the engine's slots).  Not part of the C ABI.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <map>
+#include <string>
+#include <utility>
+#include <vector>
+
+#include "../../include/kraken_batch.h"
+#include "kr_solver.cuh"
+#include "kr_template.h"
+
+namespace krb {
+
+constexpr int kMaxW = 16;                                      // warps per CTA
+constexpr int kMaxCPC = 64;                                    // creatures per CTA (W * 32 / G)
+constexpr int kBodyPad = 76;                                   // >= kMaxTplBodies, /4
+constexpr int kStateStride = 6 * kBodyPad;                     // px py vx vy ang av
+constexpr int kCtrlStride = KR_BATCH_MAX_ARMS * (KR_BATCH_MAX_SEGS + 1);  // 80
+
+// Template record on the device: sizes and offsets into the flat arrays.
+struct TplDev {
+  int nb, nc, np, nlv, arms, segs;
+  float r_max;
+  float pad0;
+  double reach;
+  int o_b, o_c, o_l, o_p, o_a, o_s;
+};
+
+struct TplArrays {
+  const float *im, *ii;
+  const int *boff, *bcnt;
+  const int *ab, *type, *motor, *garm;
+  const float *lax, *lay, *lbx, *lby, *rest, *minA, *maxA;
+  const int *lvl;
+  const float *plx, *ply, *pr;
+  const int *pbody;
+  const int *arm_tip, *arm_grip, *arm_seg0, *arm_segs;
+};
+
+// Per-slot record (device resident; the host keeps a mirror of the static
+// fields).
+struct SlotMeta {
+  int tpl, map, horizon, step;
+  uint32_t rng;
+  float comp;       // muscle compliance (f32 as packControls writes it)
+  float tone;
+  int attach_events;
+  int ctrl;         // KR_CTRL_* of this slot
+  int pad;
+  double prev_vx, prev_vy;
+  double path_len;
+  double last_x, last_y;
+};
+
+// A set of slots launched together on one stream: every slot (the public
+// engine calls) or an explicit list (the rollout server's partitions).
+struct Part {
+  bool all = true;
+  std::vector<int> slots;
+  int *d_groups = nullptr;        // n_groups x cpc slot ids
+  size_t c_groups = 0;
+  int *h_groups = nullptr;        // pinned staging of the groups
+  size_t ch_groups = 0;
+  int n_groups = 0;
+  bool dirty = true;
+  int *d_queue = nullptr;         // work-queue counter
+  cudaStream_t stream = nullptr;  // the engine's stream when null
+  cudaEvent_t staged = nullptr;   // the groups' host-to-device copy has run
+  bool staged_pending = false;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;  // launch timing
+};
+
+// slot data a spawn writes, built on the host
+struct SpawnInit {
+  std::vector<float> pose;       // n x kStateStride
+  std::vector<SlotMeta> meta;    // n
+};
+
+}  // namespace krb
+
+struct kr_batch {
+  kr_batch_desc d{};
+  kr::SolverConsts K{};
+  std::string err;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  int capacity = 0, n_maps = 0;
+  // templates
+  std::vector<kr::Template> tpls;
+  std::map<std::pair<int, int>, int> tpl_index;
+  std::vector<krb::TplDev> h_tpl;
+  krb::TplDev *d_tpl = nullptr;
+  void *d_tpl_arrays[23] = {nullptr};
+  krb::TplArrays T{};
+  // maps
+  float4 *d_rects = nullptr;
+  int *d_map_off = nullptr;
+  float *d_map_cull = nullptr;
+  std::vector<float> h_map_cull;
+  // slots
+  float *d_state = nullptr;
+  float4 *d_grip = nullptr;
+  float2 *d_glam = nullptr;
+  double *d_cd = nullptr;
+  float *d_ctrl = nullptr;
+  krb::SlotMeta *d_meta = nullptr;
+  float *d_obs = nullptr;
+  std::vector<krb::SlotMeta> h_meta;   // host mirror of tpl / map / horizon (step on device)
+  std::vector<int> h_remaining;        // remaining steps as of the last schedule
+  // the partition of every slot (public engine calls)
+  krb::Part main;
+  // snapshot of every slot (kr_batch_snapshot / kr_batch_restore)
+  float *s_state = nullptr;
+  float4 *s_grip = nullptr;
+  float2 *s_glam = nullptr;
+  double *s_cd = nullptr;
+  float *s_ctrl = nullptr;
+  krb::SlotMeta *s_meta = nullptr;
+  std::vector<int> s_remaining;
+  int *s_groups = nullptr;        // groups built for the snapshot state
+  int s_n_groups = -1, s_cpc = 0, s_G = 0;
+  // launch shape
+  int G = 16, W = 8, ctas_per_sm = 0, n_sm = 0;
+  int smem_per_sm = 0, smem_reserved = 0, smem_optin = 0;
+  int cpc = 16;                 // creature entries per group: W * 32 / G
+  std::vector<int> tpl_cpg;     // creatures per group of each template
+  size_t smem_dyn = 0;          // dynamic shared memory per CTA
+  bool shape_dirty = true;
+  // policy: n_params floats per individual, individual of each slot
+  float *d_pw = nullptr;
+  int *d_pw_idx = nullptr;
+  int n_params = 0, n_individuals = 0;
+
+  int fail(int code, const std::string &m) { err = m; return code; }
+  int cuda_fail(cudaError_t e, const char *what) {
+    err = std::string("CUDA error in ") + what + ": " + cudaGetErrorString(e);
+    return KR_ERR_CUDA;
+  }
+};
+
+namespace krb {
+
+// template id of an arms x segs body (built on first use), -1 if out of range
+int ensure_template(kr_batch *b, int arms, int segs);
+// (re)uploads every template; call after ensure_template added one
+int upload_templates(kr_batch *b);
+// creatures per group of every template and the CTA's shared memory
+int plan_shape(kr_batch *b);
+// groups of the part's live slots, longest work first, staged to the device
+int build_groups(kr_batch *b, Part &p, int max_steps);
+// one persistent launch over the part's groups, min(max_steps, remaining)
+// env steps per slot; asynchronous on the part's stream
+int launch_part(kr_batch *b, Part &p, int max_steps, bool timed);
+// host-side initial data of n creatures (spawn pose, meta); fails on a bad
+// body shape or map
+int prepare_spawn(kr_batch *b, int n, const int32_t *arms, const int32_t *segs, const int32_t *map_id,
+                  const double *x, const double *y, const double *angle, const int32_t *horizon,
+                  const uint32_t *control_seed, const float *tone, int ctrl_mode, SpawnInit *out,
+                  int *first_bad);
+// writes prepared creatures into the given slots (device copies of the
+// pose / meta / slot arrays), asynchronous on `stream`
+cudaError_t launch_spawn(kr_batch *b, const int *d_slots, const float *d_pose, const SlotMeta *d_meta,
+                         int n, cudaStream_t stream);
+cudaStream_t part_stream(const kr_batch *b, const Part &p);
+void free_part(Part &p);
+
+}  // namespace krb

@@ -1,0 +1,621 @@
+// kr_serve.cu -- the rollout server (include/kraken_serve.h) on the batched
+// engine's slots.
+//
+// Scheduling.  The slots are split into two partitions, each with its own
+// stream.  A round of partition p: wait for p's previous round (partition
+// 1 - p keeps the GPU busy meanwhile), complete the requests that ended in
+// it, admit arrived requests (FIFO) into free slots of p, stage their spawn
+// and policy weights, and launch chunk_steps env steps of every creature of
+// p (the engine's persistent kernel over groups of one template, largest
+// work first).  Rounds alternate between the partitions, so one
+// partition's launch is queued behind the other's and fills its tail.
+//
+// A request's completion round is known when it is admitted (every creature
+// advances min(chunk, remaining) steps per round), so the results of the
+// requests ending in a round are gathered on the device and copied back in
+// that round, with no extra synchronization.
+//
+// Policy weights: theta + sigma * eps (even individuals) and theta - sigma *
+// eps (odd), eps from a counter-based generator -- splitmix64 (Steele, Lea,
+// Flood 2014) of (seed, pair, parameter) gives two 24-bit uniforms, Box-Muller
+// gives the normal -- so every individual's weights are a pure function of
+// the request and the device needs no generator state.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <deque>
+#include <string>
+#include <thread>
+#include <unordered_map>
+#include <vector>
+
+#include "../../include/kraken_serve.h"
+#include "kr_batch_impl.h"
+
+namespace {
+using namespace krb;
+
+constexpr int kMaxParams = KR_POLICY_HIDDEN * (6 * KR_BATCH_MAX_ARMS + 7) +
+                           (KR_BATCH_MAX_ARMS * KR_BATCH_MAX_SEGS + KR_BATCH_MAX_ARMS) * (KR_POLICY_HIDDEN + 1);
+constexpr int kMaxAdmitPerRound = 64;   // requests admitted into one partition per round
+constexpr uint64_t kFixedBytes = 8ull << 20;  // tables, maps, queues, events
+
+thread_local std::string g_serve_error;
+
+int policy_params(int arms, int segs) {
+  return KR_POLICY_HIDDEN * (6 * arms + 7) + (arms * segs + arms) * (KR_POLICY_HIDDEN + 1);
+}
+
+__host__ __device__ inline uint64_t splitmix64(uint64_t z) {
+  z += 0x9e3779b97f4a7c15ULL;
+  z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ULL;
+  z = (z ^ (z >> 27)) * 0x94d049bb133111ebULL;
+  return z ^ (z >> 31);
+}
+
+// standard normal number `p` of mirrored pair `pair` of a request
+__device__ inline float eps_normal(uint64_t seed, int pair, int p) {
+  const uint64_t x = splitmix64(seed ^ splitmix64(((uint64_t)(uint32_t)pair << 32) | (uint32_t)p));
+  const double u1 = ((double)(x >> 40) + 1.0) * (1.0 / 16777216.0);  // (0, 1]
+  const double u2 = (double)(x & 0xffffffULL) * (1.0 / 16777216.0);  // [0, 1)
+  return (float)(sqrt(-2.0 * log(u1)) * cospi(2.0 * u2));
+}
+
+__global__ void eps_kernel(uint64_t seed, int pair, int n, float *out) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p < n) out[p] = eps_normal(seed, pair, p);
+}
+
+struct PJob {
+  int slot, theta_off, n_params, pair;
+  float sign, sigma;
+  uint64_t seed;
+};
+
+// weights of newly admitted individuals: theta +- sigma * eps
+__global__ void perturb_kernel(float *w, int stride, const float *theta, const PJob *jobs, int n) {
+  if ((int)blockIdx.x >= n) return;
+  const PJob j = jobs[blockIdx.x];
+  float *dst = w + (size_t)j.slot * stride;
+  const float *th = theta + j.theta_off;
+  for (int p = threadIdx.x; p < j.n_params; p += blockDim.x) {
+    const float d = __fmul_rn(j.sigma, eps_normal(j.seed, j.pair, p));
+    dst[p] = __fadd_rn(th[p], j.sign < 0.f ? -d : d);
+  }
+}
+
+// results of the creatures in slots[0..n)
+__global__ void gather_kernel(const SlotMeta *meta, const int *slots, int n, double *out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const SlotMeta m = meta[slots[i]];
+  out[KR_RESULT_WORDS * i] = m.path_len;
+  out[KR_RESULT_WORDS * i + 1] = m.last_x;
+  out[KR_RESULT_WORDS * i + 2] = m.last_y;
+  out[KR_RESULT_WORDS * i + 3] = (double)m.attach_events;
+}
+
+struct Req {
+  int64_t id = 0;
+  kr_request r{};
+  std::vector<float> theta;
+  int part = -1;
+  std::vector<int> slots;
+  int rounds_left = 0;
+  double arrival = 0, admitted = -1, completed = -1;
+  std::vector<double> results;
+  bool done = false;
+};
+
+// staging of one partition (pinned host + device), reused every round
+struct Stage {
+  float *h_pose = nullptr, *d_pose = nullptr;      // part_cap x kStateStride
+  SlotMeta *h_meta = nullptr, *d_meta = nullptr;   // part_cap
+  int *h_slots = nullptr, *d_slots = nullptr;      // part_cap
+  PJob *h_jobs = nullptr, *d_jobs = nullptr;       // part_cap
+  float *h_theta = nullptr, *d_theta = nullptr;    // kMaxAdmitPerRound x kMaxParams
+  int *h_rslots = nullptr, *d_rslots = nullptr;    // part_cap
+  double *h_res = nullptr, *d_res = nullptr;       // part_cap x KR_RESULT_WORDS
+};
+
+struct Round {
+  bool inflight = false;
+  cudaEvent_t done = nullptr;
+  std::vector<int64_t> completing;
+  bool timed = false;
+};
+
+uint64_t slot_bytes(const kr_server_desc &d) {
+  uint64_t b = (uint64_t)kStateStride * 4 + KR_BATCH_MAX_ARMS * (16 + 8 + 8) + (uint64_t)kCtrlStride * 4 +
+               sizeof(SlotMeta);
+  b += (uint64_t)d.obs_ring * KR_OBS_STRIDE * 4;
+  if (d.policy) b += (uint64_t)kMaxParams * 4 + 4;
+  // partition staging and work groups (two partitions of half the slots)
+  b += (uint64_t)kStateStride * 4 + sizeof(SlotMeta) + 4 + sizeof(PJob) + 4 + KR_RESULT_WORDS * 8 + 2 * 4;
+  return b;
+}
+
+uint64_t fixed_bytes(const kr_server_desc &d) {
+  uint64_t b = kFixedBytes;
+  if (d.n_maps > 0 && d.map_rect_off) b += (uint64_t)d.map_rect_off[d.n_maps] * 16 + (uint64_t)d.n_maps * 8;
+  if (d.policy) b += 2ull * kMaxAdmitPerRound * kMaxParams * 4;
+  return b;
+}
+
+}  // namespace
+
+struct kr_server {
+  kr_server_desc d{};
+  kr_batch *b = nullptr;
+  Part parts[2];
+  Stage stage[2];
+  Round round[2];
+  cudaStream_t streams[2] = {nullptr, nullptr};
+  std::vector<int64_t> active[2];
+  int part_used[2] = {0, 0};
+  int next = 0;
+  int capacity = 0, part_cap = 0, chunk = 1;
+  uint64_t bytes_per_slot = 0, device_bytes = 0;
+  std::deque<int64_t> queue;
+  std::unordered_map<int64_t, Req> reqs;
+  std::vector<int> free_slots;
+  std::vector<int64_t> done_ids;
+  int64_t next_id = 1;
+  int64_t submitted = 0, admitted = 0, completed = 0, rounds = 0;
+  double creature_steps = 0, device_ms = 0;
+  std::chrono::steady_clock::time_point t0;
+  std::string err;
+
+  double now() const {
+    return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  }
+  int fail(int code, const std::string &m) { err = m; return code; }
+  int cuda_fail(cudaError_t e, const char *what) {
+    err = std::string("CUDA error in ") + what + ": " + cudaGetErrorString(e);
+    return KR_ERR_CUDA;
+  }
+  int batch_fail(int rc) {
+    err = std::string("engine: ") + kr_batch_last_error(b);
+    return rc;
+  }
+};
+
+namespace {
+
+int check_desc(const kr_server_desc *d, std::string *why) {
+  if (!d) { *why = "null descriptor"; return KR_ERR_INVALID; }
+  if (d->chunk_steps < 1 || d->chunk_steps > 1 << 20) { *why = "chunk_steps outside 1..2^20"; return KR_ERR_INVALID; }
+  if (d->obs_ring < 0 || d->obs_ring > 4096) { *why = "obs_ring outside 0..4096"; return KR_ERR_INVALID; }
+  if (d->max_slots < 0) { *why = "max_slots < 0"; return KR_ERR_INVALID; }
+  if (d->n_maps < 1 || !d->rects || !d->map_rect_off) { *why = "need at least one map"; return KR_ERR_INVALID; }
+  return KR_OK;
+}
+
+int plan(const kr_server_desc *d, int32_t *capacity, uint64_t *per_slot, std::string *why) {
+  int rc = check_desc(d, why);
+  if (rc != KR_OK) return rc;
+  const uint64_t ps = slot_bytes(*d), fx = fixed_bytes(*d);
+  if (d->hbm_budget_bytes <= fx + 2 * ps) {
+    *why = "HBM budget below the server's fixed " + std::to_string(fx) + " bytes plus two slots of " +
+           std::to_string(ps) + " bytes";
+    return KR_ERR_CAPACITY;
+  }
+  uint64_t cap = (d->hbm_budget_bytes - fx) / ps;
+  if (d->max_slots > 0) cap = std::min<uint64_t>(cap, (uint64_t)d->max_slots);
+  cap = std::min<uint64_t>(cap, 1u << 24);
+  cap &= ~1ull;  // two equal partitions
+  if (cap < 2) { *why = "fewer than two slots"; return KR_ERR_CAPACITY; }
+  *capacity = (int32_t)cap;
+  *per_slot = ps;
+  return KR_OK;
+}
+
+template <typename T>
+cudaError_t pinned_pair(T **h, T **d, size_t n) {
+  cudaError_t e = cudaMallocHost(reinterpret_cast<void **>(h), std::max<size_t>(n, 1) * sizeof(T));
+  if (e == cudaSuccess) e = cudaMalloc(reinterpret_cast<void **>(d), std::max<size_t>(n, 1) * sizeof(T));
+  return e;
+}
+
+void free_stage(Stage &s) {
+  cudaFreeHost(s.h_pose); cudaFree(s.d_pose); cudaFreeHost(s.h_meta); cudaFree(s.d_meta);
+  cudaFreeHost(s.h_slots); cudaFree(s.d_slots); cudaFreeHost(s.h_jobs); cudaFree(s.d_jobs);
+  cudaFreeHost(s.h_theta); cudaFree(s.d_theta); cudaFreeHost(s.h_rslots); cudaFree(s.d_rslots);
+  cudaFreeHost(s.h_res); cudaFree(s.d_res);
+  s = Stage{};
+}
+
+// completes the requests of partition p whose last round just ended
+void finish_round(kr_server *S, int p) {
+  Round &R = S->round[p];
+  const double t = S->now();
+  if (R.timed) {
+    float ms = 0.f;
+    if (cudaEventElapsedTime(&ms, S->parts[p].ev0, S->parts[p].ev1) == cudaSuccess) S->device_ms += ms;
+  }
+  size_t off = 0;
+  for (int64_t id : R.completing) {
+    Req &q = S->reqs[id];
+    const size_t n = q.slots.size();
+    q.results.assign(S->stage[p].h_res + off * KR_RESULT_WORDS, S->stage[p].h_res + (off + n) * KR_RESULT_WORDS);
+    off += n;
+    q.completed = t;
+    q.done = true;
+    for (int s : q.slots) {
+      S->b->h_meta[s].horizon = 0;
+      S->b->h_remaining[s] = 0;
+      S->free_slots.push_back(s);
+    }
+    S->part_used[p] -= (int)n;
+    S->completed++;
+    S->done_ids.push_back(id);
+    auto &act = S->active[p];
+    act.erase(std::remove(act.begin(), act.end(), id), act.end());
+  }
+  if (!R.completing.empty()) {
+    std::vector<int> keep;
+    keep.reserve(S->part_used[p]);
+    for (int64_t id : S->active[p])
+      for (int s : S->reqs[id].slots) keep.push_back(s);
+    S->parts[p].slots.swap(keep);
+  }
+  R.completing.clear();
+  R.inflight = false;
+}
+
+// admits arrived requests into free slots of partition p and stages them
+int admit(kr_server *S, int p) {
+  Stage &st = S->stage[p];
+  cudaStream_t stream = S->streams[p];
+  const double t = S->now();
+  int n_new = 0, n_req = 0, theta_off = 0;
+  while (!S->queue.empty() && n_req < kMaxAdmitPerRound) {
+    Req &q = S->reqs[S->queue.front()];
+    if (q.arrival > t) break;
+    const int pop = q.r.population;
+    if (pop > (int)S->free_slots.size() || S->part_used[p] + pop > S->part_cap) break;
+    // the creature data of one individual, replicated
+    SpawnInit init;
+    int bad = -1;
+    const uint32_t seed0 = 0;
+    int rc = prepare_spawn(S->b, 1, &q.r.arms, &q.r.segs, &q.r.map_id, &q.r.x, &q.r.y, &q.r.angle, &q.r.horizon,
+                           &seed0, &q.r.tone, q.theta.empty() ? KR_CTRL_STREAM : KR_CTRL_POLICY, &init, &bad);
+    if (rc != KR_OK) return S->batch_fail(rc);
+    q.slots.resize(pop);
+    for (int i = 0; i < pop; i++) {
+      const int s = S->free_slots.back();
+      S->free_slots.pop_back();
+      q.slots[i] = s;
+      SlotMeta m = init.meta[0];
+      m.rng = (uint32_t)splitmix64(q.r.seed + (uint64_t)i);
+      std::copy(init.pose.begin(), init.pose.end(), st.h_pose + (size_t)n_new * kStateStride);
+      st.h_meta[n_new] = m;
+      st.h_slots[n_new] = s;
+      if (!q.theta.empty()) {
+        PJob &j = st.h_jobs[n_new];
+        j.slot = s; j.theta_off = theta_off; j.n_params = (int)q.theta.size(); j.pair = i / 2;
+        j.sign = (i & 1) ? -1.f : 1.f; j.sigma = q.r.sigma; j.seed = q.r.seed;
+      } else {
+        st.h_jobs[n_new] = PJob{s, 0, 0, 0, 1.f, 0.f, 0};
+      }
+      S->b->h_meta[s] = m;
+      S->b->h_remaining[s] = m.horizon;
+      n_new++;
+    }
+    if (!q.theta.empty()) {
+      std::copy(q.theta.begin(), q.theta.end(), st.h_theta + theta_off);
+      theta_off += (int)q.theta.size();
+    }
+    q.part = p;
+    q.admitted = t;
+    q.rounds_left = (q.r.horizon + S->chunk - 1) / S->chunk;
+    S->part_used[p] += pop;
+    S->active[p].push_back(q.id);
+    for (int s : q.slots) S->parts[p].slots.push_back(s);
+    S->queue.pop_front();
+    S->admitted++;
+    n_req++;
+  }
+  if (n_new == 0) return KR_OK;
+  cudaError_t e = cudaMemcpyAsync(st.d_pose, st.h_pose, (size_t)n_new * kStateStride * sizeof(float),
+                                  cudaMemcpyHostToDevice, stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(st.d_meta, st.h_meta, (size_t)n_new * sizeof(SlotMeta), cudaMemcpyHostToDevice, stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(st.d_slots, st.h_slots, (size_t)n_new * sizeof(int), cudaMemcpyHostToDevice, stream);
+  if (e == cudaSuccess) e = launch_spawn(S->b, st.d_slots, st.d_pose, st.d_meta, n_new, stream);
+  if (e == cudaSuccess && S->d.policy && theta_off > 0) {
+    e = cudaMemcpyAsync(st.d_theta, st.h_theta, (size_t)theta_off * sizeof(float), cudaMemcpyHostToDevice, stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(st.d_jobs, st.h_jobs, (size_t)n_new * sizeof(PJob), cudaMemcpyHostToDevice, stream);
+    if (e == cudaSuccess) {
+      perturb_kernel<<<n_new, 256, 0, stream>>>(S->b->d_pw, kMaxParams, st.d_theta, st.d_jobs, n_new);
+      e = cudaGetLastError();
+    }
+  }
+  if (e != cudaSuccess) return S->cuda_fail(e, "admission staging");
+  return KR_OK;
+}
+
+int run_round(kr_server *S, int p) {
+  Round &R = S->round[p];
+  if (R.inflight) {
+    cudaError_t e = cudaEventSynchronize(R.done);
+    if (e != cudaSuccess) return S->cuda_fail(e, "round wait");
+    finish_round(S, p);
+  }
+  int rc = admit(S, p);
+  if (rc != KR_OK) return rc;
+  Part &P = S->parts[p];
+  if (P.slots.empty()) return KR_OK;
+  for (int s : P.slots) S->creature_steps += std::min(S->chunk, S->b->h_remaining[s]);
+  P.dirty = true;
+  rc = launch_part(S->b, P, S->chunk, true);
+  if (rc != KR_OK) return S->batch_fail(rc);
+  R.timed = true;
+  // requests ending in this round: gather their results
+  Stage &st = S->stage[p];
+  int n_res = 0;
+  for (int64_t id : S->active[p]) {
+    Req &q = S->reqs[id];
+    if (--q.rounds_left > 0) continue;
+    R.completing.push_back(id);
+    for (int s : q.slots) st.h_rslots[n_res++] = s;
+  }
+  cudaStream_t stream = S->streams[p];
+  cudaError_t e = cudaSuccess;
+  if (n_res > 0) {
+    e = cudaMemcpyAsync(st.d_rslots, st.h_rslots, (size_t)n_res * sizeof(int), cudaMemcpyHostToDevice, stream);
+    if (e == cudaSuccess) {
+      gather_kernel<<<(n_res + 127) / 128, 128, 0, stream>>>(S->b->d_meta, st.d_rslots, n_res, st.d_res);
+      e = cudaGetLastError();
+    }
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(st.h_res, st.d_res, (size_t)n_res * KR_RESULT_WORDS * sizeof(double),
+                          cudaMemcpyDeviceToHost, stream);
+  }
+  if (e == cudaSuccess) e = cudaEventRecord(R.done, stream);
+  if (e != cudaSuccess) return S->cuda_fail(e, "round results");
+  R.inflight = true;
+  S->rounds++;
+  return KR_OK;
+}
+
+bool busy(const kr_server *S) {
+  return !S->queue.empty() || !S->active[0].empty() || !S->active[1].empty() || S->round[0].inflight ||
+         S->round[1].inflight;
+}
+
+}  // namespace
+
+extern "C" int kr_server_plan(const kr_server_desc *d, int32_t *capacity, uint64_t *bytes_per_slot) {
+  int32_t cap = 0;
+  uint64_t ps = 0;
+  int rc = plan(d, &cap, &ps, &g_serve_error);
+  if (rc != KR_OK) return rc;
+  if (capacity) *capacity = cap;
+  if (bytes_per_slot) *bytes_per_slot = ps;
+  return KR_OK;
+}
+
+extern "C" int kr_server_create(const kr_server_desc *d, kr_server **out) {
+  if (!out) { g_serve_error = "null output"; return KR_ERR_INVALID; }
+  *out = nullptr;
+  int32_t cap = 0;
+  uint64_t ps = 0;
+  int rc = plan(d, &cap, &ps, &g_serve_error);
+  if (rc != KR_OK) return rc;
+  kr_batch_desc bd{};
+  bd.solver = d->solver;
+  bd.n_maps = d->n_maps;
+  bd.rects = d->rects;
+  bd.map_rect_off = d->map_rect_off;
+  bd.capacity = cap;
+  bd.obs_ring = d->obs_ring;
+  bd.grip_slip_max = d->grip_slip_max;
+  bd.grip_cooldown = d->grip_cooldown;
+  bd.control_mode = KR_CTRL_STREAM;  // per slot: policy for requests with theta
+  bd.control_period = 6;
+  kr_batch *b = nullptr;
+  rc = kr_batch_create(&bd, &b);
+  if (rc != KR_OK) { g_serve_error = std::string("engine: ") + kr_batch_last_error(nullptr); return rc; }
+  kr_server *S = new kr_server();
+  S->d = *d;
+  S->d.rects = nullptr;
+  S->d.map_rect_off = nullptr;
+  S->b = b;
+  S->capacity = cap;
+  S->part_cap = cap / 2;
+  S->chunk = d->chunk_steps;
+  S->bytes_per_slot = ps;
+  S->t0 = std::chrono::steady_clock::now();
+  auto bail = [&](int code) {
+    g_serve_error = S->err;
+    kr_server_destroy(S);
+    return code;
+  };
+  if (d->lanes_per_creature > 0 || d->warps_per_cta > 0 || d->ctas_per_sm > 0) {
+    rc = kr_batch_set_launch(b, d->lanes_per_creature > 0 ? d->lanes_per_creature : 16,
+                             d->warps_per_cta > 0 ? d->warps_per_cta : 8, std::max(0, d->ctas_per_sm));
+    if (rc != KR_OK) { S->batch_fail(rc); return bail(rc); }
+  }
+  // every body shape up front: no template upload while rounds are in flight
+  for (int a = 1; a <= KR_BATCH_MAX_ARMS; a++)
+    for (int sg = 1; sg <= KR_BATCH_MAX_SEGS; sg++)
+      if (ensure_template(b, a, sg) < 0) { S->err = "template build failed"; return bail(KR_ERR_INVALID); }
+  rc = upload_templates(b);
+  if (rc == KR_OK) rc = plan_shape(b);
+  if (rc != KR_OK) { S->batch_fail(rc); return bail(rc); }
+  cudaError_t e = cudaSuccess;
+  if (d->policy) {
+    e = cudaMalloc(&b->d_pw, (size_t)cap * kMaxParams * sizeof(float));
+    std::vector<int> idx(cap);
+    for (int s = 0; s < cap; s++) idx[s] = s;
+    if (e == cudaSuccess) e = cudaMalloc(&b->d_pw_idx, (size_t)cap * sizeof(int));
+    if (e == cudaSuccess) e = cudaMemcpy(b->d_pw_idx, idx.data(), idx.size() * sizeof(int), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemset(b->d_pw, 0, (size_t)cap * kMaxParams * sizeof(float));
+    b->n_params = kMaxParams;
+    b->n_individuals = cap;
+    if (e != cudaSuccess) { S->cuda_fail(e, "policy weights"); return bail(KR_ERR_CUDA); }
+  }
+  for (int p = 0; p < 2; p++) {
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&S->streams[p], cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&S->round[p].done, cudaEventDisableTiming);
+    S->parts[p].all = false;
+    S->parts[p].stream = S->streams[p];
+    Stage &st = S->stage[p];
+    const size_t pc = (size_t)S->part_cap;
+    if (e == cudaSuccess) e = pinned_pair(&st.h_pose, &st.d_pose, pc * kStateStride);
+    if (e == cudaSuccess) e = pinned_pair(&st.h_meta, &st.d_meta, pc);
+    if (e == cudaSuccess) e = pinned_pair(&st.h_slots, &st.d_slots, pc);
+    if (e == cudaSuccess) e = pinned_pair(&st.h_jobs, &st.d_jobs, pc);
+    if (e == cudaSuccess) e = pinned_pair(&st.h_theta, &st.d_theta, d->policy ? (size_t)kMaxAdmitPerRound * kMaxParams : 1);
+    if (e == cudaSuccess) e = pinned_pair(&st.h_rslots, &st.d_rslots, pc);
+    if (e == cudaSuccess) e = pinned_pair(&st.h_res, &st.d_res, pc * KR_RESULT_WORDS);
+  }
+  if (e == cudaSuccess) e = cudaDeviceSynchronize();
+  if (e != cudaSuccess) { S->cuda_fail(e, "server setup"); return bail(KR_ERR_CUDA); }
+  S->free_slots.resize(cap);
+  for (int s = 0; s < cap; s++) S->free_slots[s] = cap - 1 - s;  // lowest slots first
+  S->device_bytes = ps * (uint64_t)cap + fixed_bytes(*d);
+  *out = S;
+  return KR_OK;
+}
+
+extern "C" double kr_server_now(const kr_server *s) { return s ? s->now() : 0.0; }
+
+extern "C" int kr_server_submit(kr_server *S, const kr_request *r, int64_t *id) {
+  if (!S || !r) return KR_ERR_INVALID;
+  if (r->population < 1 || r->population > S->part_cap)
+    return S->fail(KR_ERR_CAPACITY, "population " + std::to_string(r->population) + " outside 1.." +
+                                        std::to_string(S->part_cap) + " (half the slots)");
+  if (r->horizon < 1) return S->fail(KR_ERR_INVALID, "horizon < 1");
+  if (r->arms < 1 || r->arms > KR_BATCH_MAX_ARMS || r->segs < 1 || r->segs > KR_BATCH_MAX_SEGS)
+    return S->fail(KR_ERR_INVALID, "body shape outside 1..8 arms x 1..9 segments");
+  if (r->map_id < 0 || r->map_id >= S->d.n_maps) return S->fail(KR_ERR_INDEX, "unknown map");
+  if (!(std::isfinite(r->x) && std::isfinite(r->y) && std::isfinite(r->angle)))
+    return S->fail(KR_ERR_INVALID, "spawn pose not finite");
+  Req q;
+  q.id = S->next_id++;
+  q.r = *r;
+  q.r.theta = nullptr;
+  if (r->theta) {
+    if (!S->d.policy) return S->fail(KR_ERR_STATE, "server created without policy weights");
+    const int need = policy_params(r->arms, r->segs);
+    if (r->n_params < need)
+      return S->fail(KR_ERR_INVALID, "theta has " + std::to_string(r->n_params) + " parameters, a " +
+                                         std::to_string(r->arms) + "x" + std::to_string(r->segs) + " body needs " +
+                                         std::to_string(need));
+    if (!(std::isfinite(r->sigma))) return S->fail(KR_ERR_INVALID, "sigma not finite");
+    q.theta.assign(r->theta, r->theta + need);
+  }
+  q.arrival = r->arrival < 0 ? S->now() : r->arrival;
+  // FIFO by arrival time (requests submitted ahead of their arrival keep their order)
+  auto it = S->queue.end();
+  while (it != S->queue.begin() && S->reqs[*(it - 1)].arrival > q.arrival) --it;
+  S->queue.insert(it, q.id);
+  S->reqs.emplace(q.id, std::move(q));
+  S->submitted++;
+  if (id) *id = S->next_id - 1;
+  return KR_OK;
+}
+
+extern "C" int kr_server_pump(kr_server *S, int32_t *busy_out) {
+  if (!S) return KR_ERR_INVALID;
+  const int p = S->next;
+  S->next ^= 1;
+  int rc = run_round(S, p);
+  if (busy_out) *busy_out = busy(S) ? 1 : 0;
+  return rc;
+}
+
+extern "C" int kr_server_drain(kr_server *S) {
+  if (!S) return KR_ERR_INVALID;
+  while (busy(S)) {
+    if (!S->round[0].inflight && !S->round[1].inflight && S->active[0].empty() && S->active[1].empty() &&
+        !S->queue.empty()) {
+      const double wait = S->reqs[S->queue.front()].arrival - S->now();
+      if (wait > 0) std::this_thread::sleep_for(std::chrono::duration<double>(std::min(wait, 1.0)));
+    }
+    int rc = kr_server_pump(S, nullptr);
+    if (rc != KR_OK) return rc;
+  }
+  return KR_OK;
+}
+
+extern "C" int kr_server_poll(kr_server *S, int64_t *ids, int32_t cap, int32_t *n) {
+  if (!S || !n || (cap > 0 && !ids)) return KR_ERR_INVALID;
+  const int k = std::min<int>(cap, (int)S->done_ids.size());
+  for (int i = 0; i < k; i++) ids[i] = S->done_ids[i];
+  S->done_ids.erase(S->done_ids.begin(), S->done_ids.begin() + k);
+  *n = k;
+  return KR_OK;
+}
+
+extern "C" int kr_server_result(kr_server *S, int64_t id, double *results, double *times) {
+  if (!S) return KR_ERR_INVALID;
+  auto it = S->reqs.find(id);
+  if (it == S->reqs.end()) return S->fail(KR_ERR_INDEX, "unknown request " + std::to_string(id));
+  const Req &q = it->second;
+  if (!q.done) return S->fail(KR_ERR_STATE, "request " + std::to_string(id) + " has not completed");
+  if (results) std::copy(q.results.begin(), q.results.end(), results);
+  if (times) { times[0] = q.arrival; times[1] = q.admitted; times[2] = q.completed; }
+  return KR_OK;
+}
+
+extern "C" int kr_server_release(kr_server *S, int64_t id) {
+  if (!S) return KR_ERR_INVALID;
+  auto it = S->reqs.find(id);
+  if (it == S->reqs.end()) return S->fail(KR_ERR_INDEX, "unknown request " + std::to_string(id));
+  if (!it->second.done) return S->fail(KR_ERR_STATE, "request " + std::to_string(id) + " has not completed");
+  S->reqs.erase(it);
+  return KR_OK;
+}
+
+extern "C" int kr_server_get_stats(kr_server *S, kr_server_stats *o) {
+  if (!S || !o) return KR_ERR_INVALID;
+  o->capacity = S->capacity;
+  o->partition_capacity = S->part_cap;
+  o->live = S->part_used[0] + S->part_used[1];
+  o->queued = (int32_t)S->queue.size();
+  o->submitted = S->submitted;
+  o->admitted = S->admitted;
+  o->completed = S->completed;
+  o->rounds = S->rounds;
+  o->creature_steps = S->creature_steps;
+  o->device_ms = S->device_ms;
+  o->bytes_per_slot = S->bytes_per_slot;
+  o->device_bytes = S->device_bytes;
+  return KR_OK;
+}
+
+extern "C" int kr_policy_eps(uint64_t seed, int32_t pair, int32_t n, float *out) {
+  if (!out || n < 0) { g_serve_error = "kr_policy_eps: bad arguments"; return KR_ERR_INVALID; }
+  if (n == 0) return KR_OK;
+  float *d = nullptr;
+  cudaError_t e = cudaMalloc(&d, (size_t)n * sizeof(float));
+  if (e == cudaSuccess) {
+    eps_kernel<<<(n + 255) / 256, 256>>>(seed, pair, n, d);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaMemcpy(out, d, (size_t)n * sizeof(float), cudaMemcpyDeviceToHost);
+  if (d) cudaFree(d);
+  if (e != cudaSuccess) { g_serve_error = cudaGetErrorString(e); return KR_ERR_CUDA; }
+  return KR_OK;
+}
+
+extern "C" void kr_server_destroy(kr_server *S) {
+  if (!S) return;
+  cudaDeviceSynchronize();
+  for (int p = 0; p < 2; p++) {
+    free_part(S->parts[p]);
+    free_stage(S->stage[p]);
+    if (S->round[p].done) cudaEventDestroy(S->round[p].done);
+    if (S->streams[p]) cudaStreamDestroy(S->streams[p]);
+  }
+  if (S->b) kr_batch_destroy(S->b);
+  delete S;
+}
+
+extern "C" const char *kr_server_last_error(const kr_server *S) {
+  return S ? S->err.c_str() : g_serve_error.c_str();
+}

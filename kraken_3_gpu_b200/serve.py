@@ -1,0 +1,195 @@
+"""Rollout server (include/kraken_serve.h) from Python.
+
+    srv = Server(maps, hbm_budget=8 << 30, max_slots=16384, chunk_steps=32)
+    rid = srv.submit(population=64, horizon=600, arms=6, segs=7, map_id=0,
+                     x=400, y=300, angle=0.0, theta=theta, sigma=0.02, seed=7)
+    srv.drain()
+    res = srv.result(rid)        # {"results": (64, 4) f64, "arrival", "admitted", "completed"}
+
+Requests are mirrored ES populations (individual 2k: theta + sigma*eps_k,
+2k+1: theta - sigma*eps_k, eps drawn on the device from the seed) of one body
+shape on one map; without theta the individuals follow control streams from
+the seed.  Requests arriving while others run are admitted into free slots
+between rounds and share the GPU's launches (continuous batching); the HBM
+budget fixes the slot count.  There is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _native
+from .batch import policy_params  # noqa: F401  (parameter count of a body's policy)
+
+RESULT_WORDS = 4
+RESULT_FIELDS = ("path_len", "x", "y", "attach_events")
+
+_F32P = C.POINTER(C.c_float)
+_F64P = C.POINTER(C.c_double)
+_I32P = C.POINTER(C.c_int32)
+_I64P = C.POINTER(C.c_int64)
+
+
+class ServerDesc(C.Structure):
+    _fields_ = [("solver", _native.SolverParams), ("n_maps", C.c_int32), ("rects", _F32P),
+                ("map_rect_off", _I32P), ("hbm_budget_bytes", C.c_uint64), ("max_slots", C.c_int32),
+                ("obs_ring", C.c_int32), ("chunk_steps", C.c_int32), ("policy", C.c_int32),
+                ("lanes_per_creature", C.c_int32), ("warps_per_cta", C.c_int32),
+                ("ctas_per_sm", C.c_int32), ("grip_slip_max", C.c_double),
+                ("grip_cooldown", C.c_double)]
+
+
+class Request(C.Structure):
+    _fields_ = [("population", C.c_int32), ("horizon", C.c_int32), ("arms", C.c_int32),
+                ("segs", C.c_int32), ("map_id", C.c_int32), ("x", C.c_double), ("y", C.c_double),
+                ("angle", C.c_double), ("tone", C.c_float), ("theta", _F32P), ("n_params", C.c_int32),
+                ("sigma", C.c_float), ("seed", C.c_uint64), ("arrival", C.c_double)]
+
+
+class Stats(C.Structure):
+    _fields_ = [("capacity", C.c_int32), ("partition_capacity", C.c_int32), ("live", C.c_int32),
+                ("queued", C.c_int32), ("submitted", C.c_int64), ("admitted", C.c_int64),
+                ("completed", C.c_int64), ("rounds", C.c_int64), ("creature_steps", C.c_double),
+                ("device_ms", C.c_double), ("bytes_per_slot", C.c_uint64), ("device_bytes", C.c_uint64)]
+
+
+_bound = False
+
+
+def _lib():
+    global _bound
+    L = _native.lib()
+    if _bound:
+        return L
+    vp, i32 = C.c_void_p, C.c_int32
+    sigs = {
+        "kr_server_plan": (C.c_int, [C.POINTER(ServerDesc), _I32P, C.POINTER(C.c_uint64)]),
+        "kr_server_create": (C.c_int, [C.POINTER(ServerDesc), C.POINTER(vp)]),
+        "kr_server_now": (C.c_double, [vp]),
+        "kr_server_submit": (C.c_int, [vp, C.POINTER(Request), _I64P]),
+        "kr_server_pump": (C.c_int, [vp, _I32P]),
+        "kr_server_drain": (C.c_int, [vp]),
+        "kr_server_poll": (C.c_int, [vp, _I64P, i32, _I32P]),
+        "kr_server_result": (C.c_int, [vp, C.c_int64, _F64P, _F64P]),
+        "kr_server_release": (C.c_int, [vp, C.c_int64]),
+        "kr_server_get_stats": (C.c_int, [vp, C.POINTER(Stats)]),
+        "kr_server_destroy": (None, [vp]),
+        "kr_server_last_error": (C.c_char_p, [vp]),
+        "kr_policy_eps": (C.c_int, [C.c_uint64, i32, i32, _F32P]),
+    }
+    for name, (res, args) in sigs.items():
+        fn = getattr(L, name)
+        fn.restype = res
+        fn.argtypes = args
+    _bound = True
+    return L
+
+
+def _check(rc, h):
+    if rc != 0:
+        msg = _lib().kr_server_last_error(h)
+        raise _native.KrError(rc, (msg or b"").decode() or f"kraken server error {rc}")
+
+
+def _desc(maps, hbm_budget, max_slots, obs_ring, chunk_steps, policy, lanes, warps, ctas,
+          substeps, iterations, h, lin_drag, ang_drag, max_speed, max_ang_speed, grip_slip_max,
+          grip_cooldown):
+    rect_list = [np.asarray(m, dtype=np.float32).reshape(-1, 4) for m in maps]
+    off = np.zeros(len(rect_list) + 1, dtype=np.int32)
+    for i, r in enumerate(rect_list):
+        off[i + 1] = off[i] + len(r)
+    rects = np.ascontiguousarray(np.concatenate(rect_list) if rect_list else
+                                 np.zeros((0, 4), np.float32), dtype=np.float32)
+    d = ServerDesc(_native.SolverParams(h, substeps, iterations, lin_drag, ang_drag, max_speed,
+                                        max_ang_speed),
+                   len(rect_list), rects.ctypes.data_as(_F32P), off.ctypes.data_as(_I32P),
+                   int(hbm_budget), int(max_slots), int(obs_ring), int(chunk_steps), int(policy),
+                   int(lanes), int(warps), int(ctas), grip_slip_max, grip_cooldown)
+    return d, (rects, off)
+
+
+_DEFAULTS = dict(max_slots=0, obs_ring=0, chunk_steps=32, policy=True, lanes=0, warps=0, ctas=0,
+                 substeps=2, iterations=4, h=1 / 120, lin_drag=3.0, ang_drag=3.0, max_speed=360.0,
+                 max_ang_speed=18.0, grip_slip_max=150.0, grip_cooldown=0.05)
+
+
+def plan(maps, hbm_budget, **kw):
+    """(slots, bytes per slot) the server would have: pure host arithmetic."""
+    o = dict(_DEFAULTS, **kw)
+    d, keep = _desc(maps, hbm_budget, **o)
+    cap, ps = C.c_int32(), C.c_uint64()
+    _check(_lib().kr_server_plan(C.byref(d), C.byref(cap), C.byref(ps)), None)
+    return cap.value, ps.value
+
+
+def policy_eps(seed, pair, n):
+    """The device's eps(seed, pair, 0..n) (standard normal numbers)."""
+    out = np.zeros(n, dtype=np.float32)
+    _check(_lib().kr_policy_eps(seed, pair, n, out.ctypes.data_as(_F32P)), None)
+    return out
+
+
+class Server:
+    """One rollout server handle (kr_server)."""
+
+    def __init__(self, maps, hbm_budget, **kw):
+        o = dict(_DEFAULTS, **kw)
+        d, keep = _desc(maps, hbm_budget, **o)
+        self.h = C.c_void_p()
+        _check(_lib().kr_server_create(C.byref(d), C.byref(self.h)), None)
+
+    def close(self):
+        if getattr(self, "h", None) and self.h.value:
+            _lib().kr_server_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def now(self) -> float:
+        return _lib().kr_server_now(self.h)
+
+    def submit(self, population, horizon, arms, segs, map_id, x, y, angle, theta=None, sigma=0.0,
+               seed=0, tone=0.5, arrival=-1.0) -> int:
+        th = None if theta is None else np.ascontiguousarray(theta, dtype=np.float32).ravel()
+        r = Request(int(population), int(horizon), int(arms), int(segs), int(map_id), float(x),
+                    float(y), float(angle), float(tone),
+                    th.ctypes.data_as(_F32P) if th is not None else None,
+                    0 if th is None else th.size, float(sigma), int(seed) & (2**64 - 1),
+                    float(arrival))
+        rid = C.c_int64()
+        _check(_lib().kr_server_submit(self.h, C.byref(r), C.byref(rid)), self.h)
+        return rid.value
+
+    def pump(self) -> bool:
+        busy = C.c_int32()
+        _check(_lib().kr_server_pump(self.h, C.byref(busy)), self.h)
+        return bool(busy.value)
+
+    def drain(self):
+        _check(_lib().kr_server_drain(self.h), self.h)
+
+    def poll(self, cap=4096):
+        ids = np.zeros(cap, dtype=np.int64)
+        n = C.c_int32()
+        _check(_lib().kr_server_poll(self.h, ids.ctypes.data_as(_I64P), cap, C.byref(n)), self.h)
+        return [int(i) for i in ids[: n.value]]
+
+    def result(self, rid, population):
+        out = np.zeros((population, RESULT_WORDS), dtype=np.float64)
+        t = np.zeros(3, dtype=np.float64)
+        _check(_lib().kr_server_result(self.h, rid, out.ctypes.data_as(_F64P),
+                                       t.ctypes.data_as(_F64P)), self.h)
+        return {"results": out, "arrival": t[0], "admitted": t[1], "completed": t[2]}
+
+    def release(self, rid):
+        _check(_lib().kr_server_release(self.h, rid), self.h)
+
+    def stats(self):
+        s = Stats()
+        _check(_lib().kr_server_get_stats(self.h, C.byref(s)), self.h)
+        return {f: getattr(s, f) for f, _ in Stats._fields_}

@@ -1,0 +1,126 @@
+"""GPU tests of the rollout server: device eps, weights, results alone vs in
+the mix, queued admission under an HBM budget, repeatability."""
+import numpy as np
+import pytest
+
+from kraken_3_gpu_b200 import batch, serve, workloads
+from tests import serve_ref
+
+pytestmark = pytest.mark.gpu
+
+
+def _maps():
+    return workloads.uneven(n=4, n_maps=6, seed=11, h_min=10, h_max=20).maps
+
+
+def _spawn_xy(maps, m):
+    """A free spot of map m (the workload builder's spawn rule)."""
+    w = workloads.uneven(n=64, n_maps=len(maps), seed=11, h_min=10, h_max=20)
+    i = int(np.flatnonzero(w.map_id == m)[0])
+    return float(w.x[i]), float(w.y[i])
+
+
+def _requests(maps, seed=0, n=12, pop_max=24, h_max=150):
+    rng = np.random.default_rng(seed)
+    reqs = []
+    for k in range(n):
+        arms, segs = int(rng.integers(4, 9)), int(rng.integers(5, 10))
+        m = int(rng.integers(0, len(maps)))
+        x, y = _spawn_xy(maps, m)
+        policy = k % 3 != 2
+        theta = rng.normal(0, 0.1, serve.policy_params(arms, segs)).astype(np.float32) if policy else None
+        reqs.append(dict(population=2 * int(rng.integers(1, pop_max // 2 + 1)),
+                         horizon=int(rng.integers(40, h_max)), arms=arms, segs=segs, map_id=m,
+                         x=x, y=y, angle=float(rng.uniform(0, 2 * np.pi)), theta=theta,
+                         sigma=0.02, seed=int(rng.integers(0, 2**63))))
+    return reqs
+
+
+def test_device_eps_matches_restatement():
+    for seed, pair in ((0, 0), (12345, 7), (2**63 + 5, 300)):
+        got = serve.policy_eps(seed, pair, 2000)
+        want = serve_ref.eps(seed, pair, 2000)
+        assert np.allclose(got, want, rtol=2e-7, atol=1e-7)
+
+
+def test_server_equals_engine_with_explicit_mirrored_weights():
+    maps = _maps()
+    arms, segs, pop, H = 6, 7, 6, 90
+    x, y = _spawn_xy(maps, 2)
+    rng = np.random.default_rng(5)
+    n_par = serve.policy_params(arms, segs)
+    theta = rng.normal(0, 0.1, n_par).astype(np.float32)
+    sigma, seed = 0.05, 99
+    srv = serve.Server(maps, 1 << 30, max_slots=64, chunk_steps=16)
+    rid = srv.submit(pop, H, arms, segs, 2, x, y, 0.7, theta=theta, sigma=sigma, seed=seed)
+    srv.drain()
+    got = srv.result(rid, pop)["results"]
+    srv.close()
+    W = np.stack([serve_ref.mirrored_weights(theta, sigma, serve.policy_eps(seed, i // 2, n_par),
+                                             1 if i % 2 == 0 else -1) for i in range(pop)])
+    eng = batch.BatchEngine(maps, pop, control="policy")
+    eng.spawn(0, [arms] * pop, [segs] * pop, [2] * pop, [x] * pop, [y] * pop, [0.7] * pop, [H] * pop)
+    eng.set_policy(W, np.arange(pop, dtype=np.int32))
+    eng.run(H)
+    want = eng.read_fitness()
+    eng.close()
+    assert np.array_equal(got, want)
+    assert not np.array_equal(got[0], got[1])  # the mirrored pair differs
+
+
+def _run(maps, reqs, max_slots, stagger=0.0, chunk=16, obs_ring=0):
+    srv = serve.Server(maps, 2 << 30, max_slots=max_slots, chunk_steps=chunk, obs_ring=obs_ring)
+    t0 = srv.now() + 0.01
+    ids = [srv.submit(**r, arrival=t0 + k * stagger) for k, r in enumerate(reqs)]
+    srv.drain()
+    out = [srv.result(i, r["population"]) for i, r in zip(ids, reqs)]
+    st = srv.stats()
+    srv.close()
+    return out, st
+
+
+def test_each_request_same_alone_and_in_the_mix():
+    maps = _maps()
+    reqs = _requests(maps)
+    alone = [_run(maps, [r], max_slots=64)[0][0] for r in reqs]
+    mixed, st = _run(maps, reqs, max_slots=96, stagger=0.004)
+    assert st["completed"] == len(reqs)
+    for a, m in zip(alone, mixed):
+        assert np.array_equal(a["results"], m["results"])
+    # continuous batching: a request admitted while an earlier one was running
+    overlap = any(mixed[j]["admitted"] > mixed[i]["admitted"] and mixed[j]["admitted"] < mixed[i]["completed"]
+                  for i in range(len(reqs)) for j in range(len(reqs)))
+    assert overlap
+    for m in mixed:
+        assert m["arrival"] <= m["admitted"] <= m["completed"]
+
+
+def test_queued_admission_under_budget_bit_identical_three_runs():
+    maps = _maps()
+    reqs = _requests(maps, seed=3, n=16, pop_max=16, h_max=120)
+    for r in reqs:
+        r["theta"] = None  # control streams, as the memory-bound configuration
+    budget_slots = 32
+    runs = [_run(maps, reqs, max_slots=budget_slots, obs_ring=128) for _ in range(3)]
+    total = sum(r["population"] for r in reqs)
+    assert total > budget_slots
+    for out, st in runs:
+        assert st["capacity"] == budget_slots and st["completed"] == len(reqs)
+        # some request waited for slots
+        assert max(o["admitted"] - o["arrival"] for o in out) > 0
+    for out, _ in runs[1:]:
+        for a, b in zip(runs[0][0], out):
+            assert np.array_equal(a["results"], b["results"])
+
+
+def test_server_rejects_bad_requests():
+    maps = _maps()
+    srv = serve.Server(maps, 1 << 30, max_slots=16)
+    from kraken_3_gpu_b200 import _native
+    with pytest.raises(_native.KrError):
+        srv.submit(10, 50, 6, 7, 0, 100, 100, 0)  # more than a partition (8)
+    with pytest.raises(_native.KrError):
+        srv.submit(2, 50, 6, 7, 99, 100, 100, 0)  # unknown map
+    with pytest.raises(_native.KrError):
+        srv.submit(2, 50, 6, 7, 0, 100, 100, 0, theta=np.zeros(10, np.float32))
+    srv.close()

@@ -1,0 +1,43 @@
+"""Rollout server host logic without a GPU: the HBM-budget plan."""
+import pytest
+
+from kraken_3_gpu_b200 import _native, serve, workloads
+from tests import serve_ref
+
+
+def _maps():
+    return workloads.uneven(n=4, n_maps=3, seed=1, h_min=10, h_max=20).maps
+
+
+def test_plan_fills_the_budget_with_slots():
+    maps = _maps()
+    cap, per = serve.plan(maps, 1 << 30)
+    cap2, per2 = serve.plan(maps, 2 << 30)
+    assert per == per2 and cap % 2 == 0 and cap2 % 2 == 0
+    assert cap * per <= 1 << 30 < (cap + 2) * per + (16 << 20)
+    assert 2 * cap - 2 <= cap2 <= 2 * cap + 2 + (16 << 20) // per
+    assert serve.plan(maps, 1 << 30, max_slots=100) == (100, per)
+
+
+def test_plan_counts_policy_weights_and_observation_ring():
+    maps = _maps()
+    _, with_policy = serve.plan(maps, 1 << 30, policy=True)
+    _, without = serve.plan(maps, 1 << 30, policy=False)
+    assert with_policy - without == 4 * serve.policy_params(8, 9) + 4
+    _, ring = serve.plan(maps, 1 << 30, policy=False, obs_ring=128)
+    assert ring - without == 128 * 56 * 4
+
+
+def test_plan_rejects_a_budget_below_two_slots():
+    with pytest.raises(_native.KrError) as e:
+        serve.plan(_maps(), 1 << 20)
+    assert e.value.code == _native.KR_ERR_CAPACITY and "budget" in str(e.value)
+    with pytest.raises(_native.KrError):
+        serve.plan(_maps(), 1 << 30, chunk_steps=0)
+
+
+def test_eps_restatement_is_standard_normal():
+    import numpy as np
+    e = serve_ref.eps(7, 3, 4000)
+    assert abs(e.mean()) < 0.06 and abs(e.std() - 1.0) < 0.05
+    assert not np.array_equal(e, serve_ref.eps(7, 4, 4000))
