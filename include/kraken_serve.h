@@ -68,6 +68,8 @@ typedef struct kr_request {
   int32_t arms, segs;           /* body shape (1..8 x 1..9) */
   int32_t map_id;
   double x, y, angle;           /* common spawn pose (spawnKraken, src/body/kraken.js:64-101) */
+  const double *xs, *ys, *angles;     /* or one pose per individual (all three, or NULL) */
+  const uint32_t *control_seeds;      /* no theta: stream seed per individual (NULL: from seed) */
   float tone;                   /* muscle tone 0..1 */
   const float *theta;           /* NULL: control streams; else n_params floats (kraken_batch.h layout) */
   int32_t n_params;
@@ -90,6 +92,8 @@ typedef struct kr_server_stats {
   double device_ms;             /* summed kernel time of the rounds */
   uint64_t bytes_per_slot;      /* device bytes of one slot */
   uint64_t device_bytes;        /* device bytes the server holds */
+  uint64_t h2d_bytes;           /* host-to-device bytes copied so far (spawns, weights, schedules) */
+  uint64_t d2h_bytes;           /* device-to-host bytes copied so far (results) */
 } kr_server_stats;
 
 /* The slot count and per-slot bytes a descriptor yields (no device needed). */
@@ -102,6 +106,11 @@ double kr_server_now(const kr_server *s);
  * population larger than a partition, an unknown map or body shape, and a
  * theta shorter than the body's policy needs. */
 int kr_server_submit(kr_server *s, const kr_request *r, int64_t *id);
+
+/* kr_server_submit for n requests in one call; stops at the first rejected
+ * request (its status is returned), *n_submitted = requests queued. */
+int kr_server_submit_batch(kr_server *s, const kr_request *reqs, int32_t n, int64_t *ids,
+                           int32_t *n_submitted);
 
 /* One scheduling round of the next partition: wait for its previous round,
  * complete the requests that ended there, admit arrived requests into free
@@ -121,6 +130,12 @@ int kr_server_poll(kr_server *s, int64_t *ids, int32_t cap, int32_t *n);
  * pointer may be NULL. */
 int kr_server_result(kr_server *s, int64_t id, double *results, double *times);
 
+/* kr_server_result for n completed requests: results concatenated in id
+ * order (sum of populations x KR_RESULT_WORDS f64), times n x 3; with
+ * release != 0 the requests are forgotten afterwards. */
+int kr_server_result_batch(kr_server *s, const int64_t *ids, int32_t n, double *results, double *times,
+                           int32_t release);
+
 /* Forget a completed request. */
 int kr_server_release(kr_server *s, int64_t id);
 
@@ -129,6 +144,7 @@ int kr_server_get_stats(kr_server *s, kr_server_stats *out);
 /* The first n normal numbers eps(seed, pair, 0..n) the device draws for
  * mirrored pair `pair` of a request (synchronous; for checking). */
 int kr_policy_eps(uint64_t seed, int32_t pair, int32_t n, float *out);
+
 void kr_server_destroy(kr_server *s);
 const char *kr_server_last_error(const kr_server *s);
 

@@ -673,6 +673,7 @@ int build_groups(kr_batch *b, Part &p, int max_steps) {
     if (e == cudaSuccess) e = cudaEventRecord(p.staged, st);
     if (e != cudaSuccess) return b->cuda_fail(e, "upload(groups)");
     p.staged_pending = true;
+    p.h2d_bytes += order.size() * b->cpc * sizeof(int);
   }
   p.n_groups = (int)order.size();
   p.dirty = false;

@@ -73,6 +73,7 @@ struct Part {
   cudaEvent_t staged = nullptr;   // the groups' host-to-device copy has run
   bool staged_pending = false;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;  // launch timing
+  uint64_t h2d_bytes = 0;         // group uploads so far
 };
 
 // slot data a spawn writes, built on the host

@@ -39,7 +39,7 @@ using namespace krb;
 
 constexpr int kMaxParams = KR_POLICY_HIDDEN * (6 * KR_BATCH_MAX_ARMS + 7) +
                            (KR_BATCH_MAX_ARMS * KR_BATCH_MAX_SEGS + KR_BATCH_MAX_ARMS) * (KR_POLICY_HIDDEN + 1);
-constexpr int kMaxAdmitPerRound = 64;   // requests admitted into one partition per round
+constexpr int kMaxThetaPerRound = 64;   // policy requests admitted into one partition per round
 constexpr uint64_t kFixedBytes = 8ull << 20;  // tables, maps, queues, events
 
 thread_local std::string g_serve_error;
@@ -101,6 +101,8 @@ struct Req {
   int64_t id = 0;
   kr_request r{};
   std::vector<float> theta;
+  std::vector<double> xs, ys, angles;   // per individual (empty: common pose)
+  std::vector<uint32_t> seeds;          // per individual control streams
   int part = -1;
   std::vector<int> slots;
   int rounds_left = 0;
@@ -115,7 +117,7 @@ struct Stage {
   SlotMeta *h_meta = nullptr, *d_meta = nullptr;   // part_cap
   int *h_slots = nullptr, *d_slots = nullptr;      // part_cap
   PJob *h_jobs = nullptr, *d_jobs = nullptr;       // part_cap
-  float *h_theta = nullptr, *d_theta = nullptr;    // kMaxAdmitPerRound x kMaxParams
+  float *h_theta = nullptr, *d_theta = nullptr;    // kMaxThetaPerRound x kMaxParams
   int *h_rslots = nullptr, *d_rslots = nullptr;    // part_cap
   double *h_res = nullptr, *d_res = nullptr;       // part_cap x KR_RESULT_WORDS
 };
@@ -140,7 +142,7 @@ uint64_t slot_bytes(const kr_server_desc &d) {
 uint64_t fixed_bytes(const kr_server_desc &d) {
   uint64_t b = kFixedBytes;
   if (d.n_maps > 0 && d.map_rect_off) b += (uint64_t)d.map_rect_off[d.n_maps] * 16 + (uint64_t)d.n_maps * 8;
-  if (d.policy) b += 2ull * kMaxAdmitPerRound * kMaxParams * 4;
+  if (d.policy) b += 2ull * kMaxThetaPerRound * kMaxParams * 4;
   return b;
 }
 
@@ -165,6 +167,7 @@ struct kr_server {
   int64_t next_id = 1;
   int64_t submitted = 0, admitted = 0, completed = 0, rounds = 0;
   double creature_steps = 0, device_ms = 0;
+  uint64_t h2d_bytes = 0, d2h_bytes = 0;
   std::chrono::steady_clock::time_point t0;
   std::string err;
 
@@ -251,10 +254,10 @@ void finish_round(kr_server *S, int p) {
     S->part_used[p] -= (int)n;
     S->completed++;
     S->done_ids.push_back(id);
-    auto &act = S->active[p];
-    act.erase(std::remove(act.begin(), act.end(), id), act.end());
   }
   if (!R.completing.empty()) {
+    auto &act = S->active[p];
+    act.erase(std::remove_if(act.begin(), act.end(), [&](int64_t id) { return S->reqs[id].done; }), act.end());
     std::vector<int> keep;
     keep.reserve(S->part_used[p]);
     for (int64_t id : S->active[p])
@@ -270,43 +273,54 @@ int admit(kr_server *S, int p) {
   Stage &st = S->stage[p];
   cudaStream_t stream = S->streams[p];
   const double t = S->now();
-  int n_new = 0, n_req = 0, theta_off = 0;
-  while (!S->queue.empty() && n_req < kMaxAdmitPerRound) {
+  int n_new = 0, n_theta = 0, theta_off = 0;
+  while (!S->queue.empty()) {
     Req &q = S->reqs[S->queue.front()];
     if (q.arrival > t) break;
     const int pop = q.r.population;
     if (pop > (int)S->free_slots.size() || S->part_used[p] + pop > S->part_cap) break;
-    // the creature data of one individual, replicated
+    const bool pol = !q.theta.empty();
+    if (pol && n_theta >= kMaxThetaPerRound) break;
+    // the creatures' initial data
+    const std::vector<int32_t> arms(pop, q.r.arms), segs(pop, q.r.segs), maps(pop, q.r.map_id), hor(pop, q.r.horizon);
+    std::vector<double> xs = q.xs, ys = q.ys, an = q.angles;
+    if (xs.empty()) { xs.assign(pop, q.r.x); ys.assign(pop, q.r.y); an.assign(pop, q.r.angle); }
+    std::vector<uint32_t> seeds = q.seeds;
+    if (seeds.empty()) {
+      seeds.resize(pop);
+      for (int i = 0; i < pop; i++) seeds[i] = (uint32_t)splitmix64(q.r.seed + (uint64_t)i);
+    }
+    const std::vector<float> tones(pop, q.r.tone);
     SpawnInit init;
     int bad = -1;
-    const uint32_t seed0 = 0;
-    int rc = prepare_spawn(S->b, 1, &q.r.arms, &q.r.segs, &q.r.map_id, &q.r.x, &q.r.y, &q.r.angle, &q.r.horizon,
-                           &seed0, &q.r.tone, q.theta.empty() ? KR_CTRL_STREAM : KR_CTRL_POLICY, &init, &bad);
+    int rc = prepare_spawn(S->b, pop, arms.data(), segs.data(), maps.data(), xs.data(), ys.data(), an.data(),
+                           hor.data(), seeds.data(), tones.data(), pol ? KR_CTRL_POLICY : KR_CTRL_STREAM, &init,
+                           &bad);
     if (rc != KR_OK) return S->batch_fail(rc);
     q.slots.resize(pop);
     for (int i = 0; i < pop; i++) {
       const int s = S->free_slots.back();
       S->free_slots.pop_back();
       q.slots[i] = s;
-      SlotMeta m = init.meta[0];
-      m.rng = (uint32_t)splitmix64(q.r.seed + (uint64_t)i);
-      std::copy(init.pose.begin(), init.pose.end(), st.h_pose + (size_t)n_new * kStateStride);
-      st.h_meta[n_new] = m;
+      std::copy(init.pose.begin() + (size_t)i * kStateStride, init.pose.begin() + (size_t)(i + 1) * kStateStride,
+                st.h_pose + (size_t)n_new * kStateStride);
+      st.h_meta[n_new] = init.meta[i];
       st.h_slots[n_new] = s;
-      if (!q.theta.empty()) {
+      if (pol) {
         PJob &j = st.h_jobs[n_new];
         j.slot = s; j.theta_off = theta_off; j.n_params = (int)q.theta.size(); j.pair = i / 2;
         j.sign = (i & 1) ? -1.f : 1.f; j.sigma = q.r.sigma; j.seed = q.r.seed;
       } else {
         st.h_jobs[n_new] = PJob{s, 0, 0, 0, 1.f, 0.f, 0};
       }
-      S->b->h_meta[s] = m;
-      S->b->h_remaining[s] = m.horizon;
+      S->b->h_meta[s] = init.meta[i];
+      S->b->h_remaining[s] = init.meta[i].horizon;
       n_new++;
     }
-    if (!q.theta.empty()) {
+    if (pol) {
       std::copy(q.theta.begin(), q.theta.end(), st.h_theta + theta_off);
       theta_off += (int)q.theta.size();
+      n_theta++;
     }
     q.part = p;
     q.admitted = t;
@@ -316,7 +330,6 @@ int admit(kr_server *S, int p) {
     for (int s : q.slots) S->parts[p].slots.push_back(s);
     S->queue.pop_front();
     S->admitted++;
-    n_req++;
   }
   if (n_new == 0) return KR_OK;
   cudaError_t e = cudaMemcpyAsync(st.d_pose, st.h_pose, (size_t)n_new * kStateStride * sizeof(float),
@@ -333,6 +346,8 @@ int admit(kr_server *S, int p) {
     }
   }
   if (e != cudaSuccess) return S->cuda_fail(e, "admission staging");
+  S->h2d_bytes += (uint64_t)n_new * (kStateStride * sizeof(float) + sizeof(SlotMeta) + sizeof(int));
+  if (S->d.policy && theta_off > 0) S->h2d_bytes += (uint64_t)theta_off * sizeof(float) + (uint64_t)n_new * sizeof(PJob);
   return KR_OK;
 }
 
@@ -375,6 +390,8 @@ int run_round(kr_server *S, int p) {
   }
   if (e == cudaSuccess) e = cudaEventRecord(R.done, stream);
   if (e != cudaSuccess) return S->cuda_fail(e, "round results");
+  S->h2d_bytes += (uint64_t)n_res * sizeof(int);
+  S->d2h_bytes += (uint64_t)n_res * KR_RESULT_WORDS * sizeof(double);
   R.inflight = true;
   S->rounds++;
   return KR_OK;
@@ -468,7 +485,7 @@ extern "C" int kr_server_create(const kr_server_desc *d, kr_server **out) {
     if (e == cudaSuccess) e = pinned_pair(&st.h_meta, &st.d_meta, pc);
     if (e == cudaSuccess) e = pinned_pair(&st.h_slots, &st.d_slots, pc);
     if (e == cudaSuccess) e = pinned_pair(&st.h_jobs, &st.d_jobs, pc);
-    if (e == cudaSuccess) e = pinned_pair(&st.h_theta, &st.d_theta, d->policy ? (size_t)kMaxAdmitPerRound * kMaxParams : 1);
+    if (e == cudaSuccess) e = pinned_pair(&st.h_theta, &st.d_theta, d->policy ? (size_t)kMaxThetaPerRound * kMaxParams : 1);
     if (e == cudaSuccess) e = pinned_pair(&st.h_rslots, &st.d_rslots, pc);
     if (e == cudaSuccess) e = pinned_pair(&st.h_res, &st.d_res, pc * KR_RESULT_WORDS);
   }
@@ -492,7 +509,7 @@ extern "C" int kr_server_submit(kr_server *S, const kr_request *r, int64_t *id) 
   if (r->arms < 1 || r->arms > KR_BATCH_MAX_ARMS || r->segs < 1 || r->segs > KR_BATCH_MAX_SEGS)
     return S->fail(KR_ERR_INVALID, "body shape outside 1..8 arms x 1..9 segments");
   if (r->map_id < 0 || r->map_id >= S->d.n_maps) return S->fail(KR_ERR_INDEX, "unknown map");
-  if (!(std::isfinite(r->x) && std::isfinite(r->y) && std::isfinite(r->angle)))
+  if (!r->xs && !(std::isfinite(r->x) && std::isfinite(r->y) && std::isfinite(r->angle)))
     return S->fail(KR_ERR_INVALID, "spawn pose not finite");
   Req q;
   q.id = S->next_id++;
@@ -508,6 +525,19 @@ extern "C" int kr_server_submit(kr_server *S, const kr_request *r, int64_t *id) 
     if (!(std::isfinite(r->sigma))) return S->fail(KR_ERR_INVALID, "sigma not finite");
     q.theta.assign(r->theta, r->theta + need);
   }
+  const bool px = r->xs != nullptr, py = r->ys != nullptr, pa = r->angles != nullptr;
+  if (px != py || px != pa) return S->fail(KR_ERR_INVALID, "per-individual poses need xs, ys and angles");
+  if (px) {
+    q.xs.assign(r->xs, r->xs + r->population);
+    q.ys.assign(r->ys, r->ys + r->population);
+    q.angles.assign(r->angles, r->angles + r->population);
+    for (int i = 0; i < r->population; i++)
+      if (!(std::isfinite(q.xs[i]) && std::isfinite(q.ys[i]) && std::isfinite(q.angles[i])))
+        return S->fail(KR_ERR_INVALID, "spawn pose not finite");
+  }
+  if (r->control_seeds) q.seeds.assign(r->control_seeds, r->control_seeds + r->population);
+  q.r.xs = q.r.ys = q.r.angles = nullptr;
+  q.r.control_seeds = nullptr;
   q.arrival = r->arrival < 0 ? S->now() : r->arrival;
   // FIFO by arrival time (requests submitted ahead of their arrival keep their order)
   auto it = S->queue.end();
@@ -517,6 +547,20 @@ extern "C" int kr_server_submit(kr_server *S, const kr_request *r, int64_t *id) 
   S->submitted++;
   if (id) *id = S->next_id - 1;
   return KR_OK;
+}
+
+extern "C" int kr_server_submit_batch(kr_server *S, const kr_request *reqs, int32_t n, int64_t *ids,
+                                      int32_t *n_submitted) {
+  if (!S || (n > 0 && !reqs)) return KR_ERR_INVALID;
+  int k = 0, rc = KR_OK;
+  for (; k < n; k++) {
+    int64_t id = 0;
+    rc = kr_server_submit(S, reqs + k, &id);
+    if (rc != KR_OK) break;
+    if (ids) ids[k] = id;
+  }
+  if (n_submitted) *n_submitted = k;
+  return rc;
 }
 
 extern "C" int kr_server_pump(kr_server *S, int32_t *busy_out) {
@@ -562,6 +606,26 @@ extern "C" int kr_server_result(kr_server *S, int64_t id, double *results, doubl
   return KR_OK;
 }
 
+extern "C" int kr_server_result_batch(kr_server *S, const int64_t *ids, int32_t n, double *results,
+                                      double *times, int32_t release) {
+  if (!S || (n > 0 && !ids)) return KR_ERR_INVALID;
+  for (int k = 0; k < n; k++) {
+    auto it = S->reqs.find(ids[k]);
+    if (it == S->reqs.end()) return S->fail(KR_ERR_INDEX, "unknown request " + std::to_string(ids[k]));
+    if (!it->second.done) return S->fail(KR_ERR_STATE, "request " + std::to_string(ids[k]) + " has not completed");
+  }
+  size_t off = 0;
+  for (int k = 0; k < n; k++) {
+    auto it = S->reqs.find(ids[k]);
+    const Req &q = it->second;
+    if (results) std::copy(q.results.begin(), q.results.end(), results + off);
+    off += q.results.size();
+    if (times) { times[3 * k] = q.arrival; times[3 * k + 1] = q.admitted; times[3 * k + 2] = q.completed; }
+    if (release) S->reqs.erase(it);
+  }
+  return KR_OK;
+}
+
 extern "C" int kr_server_release(kr_server *S, int64_t id) {
   if (!S) return KR_ERR_INVALID;
   auto it = S->reqs.find(id);
@@ -585,6 +649,8 @@ extern "C" int kr_server_get_stats(kr_server *S, kr_server_stats *o) {
   o->device_ms = S->device_ms;
   o->bytes_per_slot = S->bytes_per_slot;
   o->device_bytes = S->device_bytes;
+  o->h2d_bytes = S->h2d_bytes + S->parts[0].h2d_bytes + S->parts[1].h2d_bytes;
+  o->d2h_bytes = S->d2h_bytes;
   return KR_OK;
 }
 

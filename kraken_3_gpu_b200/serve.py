@@ -43,15 +43,28 @@ class ServerDesc(C.Structure):
 class Request(C.Structure):
     _fields_ = [("population", C.c_int32), ("horizon", C.c_int32), ("arms", C.c_int32),
                 ("segs", C.c_int32), ("map_id", C.c_int32), ("x", C.c_double), ("y", C.c_double),
-                ("angle", C.c_double), ("tone", C.c_float), ("theta", _F32P), ("n_params", C.c_int32),
+                ("angle", C.c_double), ("xs", _F64P), ("ys", _F64P), ("angles", _F64P),
+                ("control_seeds", C.POINTER(C.c_uint32)),
+                ("tone", C.c_float), ("theta", _F32P), ("n_params", C.c_int32),
                 ("sigma", C.c_float), ("seed", C.c_uint64), ("arrival", C.c_double)]
+
+
+class _RequestRaw(C.Structure):
+    """kr_request with the pointers as integers (same layout), for numpy."""
+    _fields_ = [(n, C.c_uint64 if t in (_F32P, _F64P, C.POINTER(C.c_uint32)) else t)
+                for n, t in Request._fields_]
+
+
+REQUEST_DTYPE = np.dtype(_RequestRaw)
+assert REQUEST_DTYPE.itemsize == C.sizeof(Request)
 
 
 class Stats(C.Structure):
     _fields_ = [("capacity", C.c_int32), ("partition_capacity", C.c_int32), ("live", C.c_int32),
                 ("queued", C.c_int32), ("submitted", C.c_int64), ("admitted", C.c_int64),
                 ("completed", C.c_int64), ("rounds", C.c_int64), ("creature_steps", C.c_double),
-                ("device_ms", C.c_double), ("bytes_per_slot", C.c_uint64), ("device_bytes", C.c_uint64)]
+                ("device_ms", C.c_double), ("bytes_per_slot", C.c_uint64), ("device_bytes", C.c_uint64),
+                ("h2d_bytes", C.c_uint64), ("d2h_bytes", C.c_uint64)]
 
 
 _bound = False
@@ -69,6 +82,8 @@ def _lib():
         "kr_server_now": (C.c_double, [vp]),
         "kr_server_submit": (C.c_int, [vp, C.POINTER(Request), _I64P]),
         "kr_server_pump": (C.c_int, [vp, _I32P]),
+        "kr_server_submit_batch": (C.c_int, [vp, vp, i32, _I64P, _I32P]),
+        "kr_server_result_batch": (C.c_int, [vp, _I64P, i32, _F64P, _F64P, i32]),
         "kr_server_drain": (C.c_int, [vp]),
         "kr_server_poll": (C.c_int, [vp, _I64P, i32, _I32P]),
         "kr_server_result": (C.c_int, [vp, C.c_int64, _F64P, _F64P]),
@@ -153,17 +168,66 @@ class Server:
     def now(self) -> float:
         return _lib().kr_server_now(self.h)
 
-    def submit(self, population, horizon, arms, segs, map_id, x, y, angle, theta=None, sigma=0.0,
-               seed=0, tone=0.5, arrival=-1.0) -> int:
+    def submit(self, population, horizon, arms, segs, map_id, x=0.0, y=0.0, angle=0.0, theta=None,
+               sigma=0.0, seed=0, tone=0.5, arrival=-1.0, xs=None, ys=None, angles=None,
+               control_seeds=None) -> int:
+        """Queue a request; x, y, angle is the common spawn pose, or xs, ys,
+        angles one pose per individual; control_seeds (no theta) one control
+        stream seed per individual."""
         th = None if theta is None else np.ascontiguousarray(theta, dtype=np.float32).ravel()
+        per = None
+        if xs is not None:
+            per = [np.ascontiguousarray(v, dtype=np.float64) for v in (xs, ys, angles)]
+        cs = None if control_seeds is None else np.ascontiguousarray(control_seeds, dtype=np.uint32)
+        ptrs = tuple(v.ctypes.data_as(_F64P) for v in per) if per else (None, None, None)
         r = Request(int(population), int(horizon), int(arms), int(segs), int(map_id), float(x),
-                    float(y), float(angle), float(tone),
+                    float(y), float(angle), *ptrs,
+                    cs.ctypes.data_as(C.POINTER(C.c_uint32)) if cs is not None else None,
+                    float(tone),
                     th.ctypes.data_as(_F32P) if th is not None else None,
                     0 if th is None else th.size, float(sigma), int(seed) & (2**64 - 1),
                     float(arrival))
         rid = C.c_int64()
         _check(_lib().kr_server_submit(self.h, C.byref(r), C.byref(rid)), self.h)
         return rid.value
+
+    def submit_many(self, horizon, arms, segs, map_id, xs, ys, angles, control_seeds=None,
+                    tone=0.5, arrival=-1.0):
+        """One single-creature request per row (its pose, control stream
+        seed and horizon), queued with one C call; returns the ids."""
+        n = len(horizon)
+        a = np.zeros(n, dtype=REQUEST_DTYPE)
+        keep = [np.ascontiguousarray(v, dtype=np.float64) for v in (xs, ys, angles)]
+        a["population"] = 1
+        a["horizon"] = horizon
+        a["arms"] = arms
+        a["segs"] = segs
+        a["map_id"] = map_id
+        for f, v in zip(("xs", "ys", "angles"), keep):
+            a[f] = v.ctypes.data + 8 * np.arange(n, dtype=np.uint64)
+        if control_seeds is not None:
+            cs = np.ascontiguousarray(control_seeds, dtype=np.uint32)
+            keep.append(cs)
+            a["control_seeds"] = cs.ctypes.data + 4 * np.arange(n, dtype=np.uint64)
+        a["tone"] = tone
+        a["arrival"] = arrival
+        ids = np.zeros(n, dtype=np.int64)
+        done = C.c_int32()
+        _check(_lib().kr_server_submit_batch(self.h, a.ctypes.data, n, ids.ctypes.data_as(_I64P),
+                                             C.byref(done)), self.h)
+        return ids
+
+    def results_many(self, ids, populations=None, release=False):
+        """Results of completed requests, concatenated in id order
+        (sum of populations, RESULT_WORDS), and their times (len(ids), 3)."""
+        ids = np.ascontiguousarray(ids, dtype=np.int64)
+        total = len(ids) if populations is None else int(np.sum(populations))
+        out = np.zeros((total, RESULT_WORDS), dtype=np.float64)
+        t = np.zeros((len(ids), 3), dtype=np.float64)
+        _check(_lib().kr_server_result_batch(self.h, ids.ctypes.data_as(_I64P), len(ids),
+                                             out.ctypes.data_as(_F64P), t.ctypes.data_as(_F64P),
+                                             1 if release else 0), self.h)
+        return out, t
 
     def pump(self) -> bool:
         busy = C.c_int32()

@@ -124,3 +124,29 @@ def test_server_rejects_bad_requests():
     with pytest.raises(_native.KrError):
         srv.submit(2, 50, 6, 7, 0, 100, 100, 0, theta=np.zeros(10, np.float32))
     srv.close()
+
+
+def test_served_uneven_workload_equals_batched_engine():
+    """The mixed workload submitted as requests (one per creature, its own
+    pose, control stream and horizon) gives the batched engine's results."""
+    w = workloads.uneven(n=60, n_maps=5, seed=13, h_min=30, h_max=120)
+    eng = batch.BatchEngine(w.maps, w.n)
+    workloads.spawn_all(eng, w)
+    eng.run(int(w.horizon.max()))
+    want = eng.read_fitness()
+    eng.close()
+    srv = serve.Server(w.maps, 1 << 30, max_slots=40, chunk_steps=24, policy=False)
+    half = w.n // 2
+    ids = []
+    for i in range(half):  # one call per request
+        ids.append(srv.submit(1, int(w.horizon[i]), int(w.arms[i]), int(w.segs[i]), int(w.map_id[i]),
+                              xs=[w.x[i]], ys=[w.y[i]], angles=[w.angle[i]], control_seeds=[w.seed[i]]))
+    s = slice(half, w.n)  # the rest in one batch call
+    ids += list(srv.submit_many(w.horizon[s], w.arms[s], w.segs[s], w.map_id[s], w.x[s], w.y[s],
+                                w.angle[s], control_seeds=w.seed[s]))
+    srv.drain()
+    got = np.concatenate([srv.result(r, 1)["results"] for r in ids[:half]])
+    rest, times = srv.results_many(ids[half:], release=True)
+    srv.close()
+    assert np.array_equal(np.concatenate([got, rest]), want)
+    assert np.all(times[:, 0] <= times[:, 1]) and np.all(times[:, 1] <= times[:, 2])
