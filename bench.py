@@ -1,20 +1,27 @@
 #!/usr/bin/env python
-"""Creature-steps/s of Kraken 3's XPBD creature step on B200.
+"""Creature-steps/s of Kraken 3's XPBD creature step on B200, persistent and
+served, beside the plain per-step launch; p50/p99 rollout latency.
 
 Workload (default): 16,384 creatures on 64 maps, bodies of 4-8 arms x 5-9
 segments, horizons U{200..2000} env steps, controls from per-creature
 mulberry32 streams redrawn every 6 steps (tone 0.5), S=2 substeps x I=4
 iterations at h = 1/120 -- seeded synthetic data in the shapes of the
-uneven-batching configuration.  One bench step = one full rollout of every
-creature to its horizon, restored from a device snapshot, run by the
-persistent kernel (one launch).  value = creature-steps / device time.
+uneven-batching configuration.
 
-Also measured on the same workload and GPU: the plain form (one launch per
-env step), the CUDA-graph form (the per-step launches replayed as a graph),
-the end-to-end rate through the public API with host buffers (spawn from
-host arrays, run, read results back), the FP32-issue roofline of the kernel
-and the CPU oracle (FP64 restatement of the reference's xpbd.js) on the host
-cores as a reported baseline.
+value: one bench step = one full rollout of every creature to its horizon by
+the persistent kernel (one launch, autotuned launch shape), state restored
+from a device snapshot, L2 flushed in between; creature-steps / device time.
+
+e2e: the same workload served through the rollout server's C ABI with host
+buffers -- one request per creature (its pose, control stream and horizon),
+results copied back -- with p50/p99 rollout latency.
+
+Beside them: the plain form (the same kernel, one launch per env step), its
+CUDA-graph replay, an ES request stream (Poisson 200 req/s, mirrored
+populations 8-512, horizons 300-3000, fused policy MLP) through a
+16,384-slot server with p50/p99 latency, the FP32-issue roofline of the
+kernel and the CPU oracle (FP64 restatement of the reference's xpbd.js) on
+the host cores as a reported baseline.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
 """
@@ -36,7 +43,7 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-METRIC = "creature-steps/s at 16k mixed envs (persistent served form; plain per-step launch beside it)"
+METRIC = "creature-steps/s at 16k mixed envs, served vs plain launch; p50/p99 rollout ms"
 UNIT = "creature-steps/s"
 
 
@@ -54,7 +61,12 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
-    ap.add_argument("--warps", type=int, default=0, help="warps per CTA (0: autotune)")
+    ap.add_argument("--shape", default="", help="lanes,warps,ctas launch shape (empty: autotune)")
+    ap.add_argument("--chunk", type=int, default=64, help="server env steps per round")
+    ap.add_argument("--no-es", action="store_true", help="skip the ES request stream")
+    ap.add_argument("--es-requests", type=int, default=200)
+    ap.add_argument("--traffic", type=float, default=None,
+                    help="ncu DRAM bytes per launch of the captured kernel, if measured")
     return ap.parse_args()
 
 
@@ -224,6 +236,68 @@ def reference_arm(args):
     print(json.dumps(line), flush=True)
 
 
+def served_uneven(serve, w, shape, chunk, sessions):
+    """The mixed workload through the rollout server's C ABI with host
+    buffers: one request per creature (its own pose, control stream and
+    horizon), all submitted at once; results read back to the host."""
+    srv = serve.Server(w.maps, 8 << 30, max_slots=w.n, chunk_steps=chunk, policy=False,
+                       lanes=shape[0], warps=shape[1], ctas=shape[2])
+    xs, ys, an = (np.ascontiguousarray(v, dtype=np.float64) for v in (w.x, w.y, w.angle))
+    seeds = np.ascontiguousarray(w.seed, dtype=np.uint32)
+    out = []
+    for _ in range(sessions):
+        s0 = srv.stats()
+        t0 = time.perf_counter()
+        ids = srv.submit_many(w.horizon, w.arms, w.segs, w.map_id, xs, ys, an, control_seeds=seeds)
+        srv.drain()
+        res, times = srv.results_many(ids, release=True)
+        wall = time.perf_counter() - t0
+        s1 = srv.stats()
+        out.append({"wall_s": wall, "lat": times[:, 2] - times[:, 0],
+                    "h2d": s1["h2d_bytes"] - s0["h2d_bytes"], "d2h": s1["d2h_bytes"] - s0["d2h_bytes"],
+                    "device_ms": s1["device_ms"] - s0["device_ms"]})
+    srv.close()
+    return out
+
+
+def served_es_stream(serve, w, shape, chunk, n_req, rate, seed=0):
+    """ES evaluation requests (mirrored populations 8-512, horizons
+    300-3000, body shapes and maps of the mixed workload, fused policy with
+    theta ~ N(0, 0.1^2), sigma 0.02) arriving as a Poisson stream."""
+    rng = np.random.default_rng(seed)
+    reqs, t = [], 0.0
+    for k in range(n_req):
+        t += rng.exponential(1.0 / rate)
+        i = int(rng.integers(0, w.n))
+        arms, segs = int(w.arms[i]), int(w.segs[i])
+        reqs.append(dict(population=2 * int(rng.integers(4, 257)), horizon=int(rng.integers(300, 3001)),
+                         arms=arms, segs=segs, map_id=int(w.map_id[i]), x=float(w.x[i]), y=float(w.y[i]),
+                         angle=float(w.angle[i]),
+                         theta=rng.normal(0, 0.1, serve.policy_params(arms, segs)).astype(np.float32),
+                         sigma=0.02, seed=k + 1, arrival=t))
+    units = sum(r["population"] * r["horizon"] for r in reqs)
+    srv = serve.Server(w.maps, 8 << 30, max_slots=16384, chunk_steps=chunk, policy=True,
+                       lanes=shape[0], warps=shape[1], ctas=shape[2])
+    t0 = srv.now() + 0.02
+    ids = []
+    for r in reqs:
+        r = dict(r)
+        r["arrival"] += t0
+        ids.append(srv.submit(**r))
+    srv.drain()
+    res = [srv.result(i, r["population"]) for i, r in zip(ids, reqs)]
+    st = srv.stats()
+    srv.close()
+    lat = np.array([x["completed"] - x["arrival"] for x in res])
+    span = max(x["completed"] for x in res) - min(x["arrival"] for x in res)
+    return {"value": units / span, "unit": UNIT, "requests": n_req, "rate_req_s": rate,
+            "creature_steps": units, "makespan_s": span,
+            "p50_rollout_ms": float(np.percentile(lat, 50) * 1e3),
+            "p99_rollout_ms": float(np.percentile(lat, 99) * 1e3),
+            "slots": st["capacity"], "chunk_steps": chunk,
+            "device_kernel_ms_summed": st["device_ms"]}
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -253,7 +327,7 @@ def main():
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
         return float(t.item())
 
-    from kraken_3_gpu_b200 import batch, workloads
+    from kraken_3_gpu_b200 import batch, serve, workloads
 
     w = workloads.uneven(n=args.n, n_maps=args.maps, seed=args.seed + 1000 * rank,
                          h_min=args.hmin, h_max=args.hmax)
@@ -264,23 +338,23 @@ def main():
     eng.set_stream(stream.cuda_stream)
     workloads.spawn_all(eng, w)
     eng.snapshot()
+    # L2 flush between timed rollouts (a write larger than the 126 MB L2)
+    flush = torch.empty(64 << 20, dtype=torch.float32, device="cuda")
 
-    # autotune the launch shape (creatures per CTA) on a short slice
-    launches = 0
-    if args.warps:
-        best_w = args.warps
+    # autotune the launch shape (lanes per creature, warps per CTA, CTAs per
+    # SM) on a 64-step slice of the workload; every shape gives the same bits
+    tune = {}
+    if args.shape:
+        best = tuple(int(v) for v in args.shape.split(","))
     else:
-        best_w, best_t = 8, float("inf")
-        for wp in (4, 8, 16):
-            eng.set_launch(wp, 0)
+        for shp in ((16, 8, 0), (16, 4, 4), (8, 8, 0), (32, 8, 0), (16, 16, 1)):
+            eng.set_launch(shp[1], shp[2], lanes_per_creature=shp[0])
             eng.restore()
-            eng.run(40)
-            launches += 1
+            eng.run(64)
             eng.sync()
-            t = eng.last_ms()
-            if t < best_t:
-                best_w, best_t = wp, t
-    eng.set_launch(best_w, 0)
+            tune[shp] = eng.last_ms()
+        best = min(tune, key=tune.get)
+    eng.set_launch(best[1], best[2], lanes_per_creature=best[0])
 
     # warm-up: full rollouts
     for _ in range(args.warmup):
@@ -291,32 +365,26 @@ def main():
     sampler = ClockSampler(local)
     sampler.start()
     time.sleep(0.3)
-    kernel_ms = []
     barrier()
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     e0.record(stream)
     for _ in range(args.steps):
+        flush.zero_()
         eng.restore()
         eng.run(max_h)
-        kernel_ms.append(None)
     e1.record(stream)
     e1.synchronize()
     barrier()
     elapsed_ms = e0.elapsed_time(e1)
-    # the kernel's own duration (last launch of each step, timed by events
-    # around the launch on the same stream)
-    eng.restore()
-    eng.run(max_h)
-    kms = eng.last_ms()
-    clocks = sampler.stop()
-    gpu_launches = args.steps * 1
+    kms = eng.last_ms()  # the last rollout's kernel alone (events on its stream)
     t_max = all_max(elapsed_ms)
     value = world * units * args.steps / (t_max / 1000.0)
     ms_per_step = t_max / args.steps
+    gpu_launches = args.steps
 
-    # plain form (one launch per env step) and the CUDA-graph step loop
     extra = {}
+    # plain form: the same kernel, one launch per env step
     if not args.no_plain:
         eng.restore()
         torch.cuda.synchronize()
@@ -327,35 +395,30 @@ def main():
         p1.record(stream)
         p1.synchronize()
         plain_ms = all_max(p0.elapsed_time(p1))
-        extra["plain_per_step_launch"] = {"value": world * units / (plain_ms / 1000.0),
+        extra["plain_per_step_launch"] = {"value": world * units / (plain_ms / 1000.0), "unit": UNIT,
                                           "ms_per_rollout": plain_ms, "launches": max_h}
         eng.restore()
-        torch.cuda.synchronize()
-        g0 = time.perf_counter()
         eng.run_graph(1, max_h, 1)
-        g_ms = all_max((time.perf_counter() - g0) * 1000.0)
-        extra["graph_step_loop"] = {"value": world * units / (g_ms / 1000.0),
-                                    "ms_per_rollout_incl_capture": g_ms}
+        g_ms = all_max(eng.last_ms())
+        extra["graph_step_loop"] = {"value": world * units / (g_ms / 1000.0), "unit": UNIT,
+                                    "ms_per_rollout_replay": g_ms, "launches_in_graph": max_h}
 
-    # end to end through the public API with host buffers: spawn from host
-    # arrays, run the rollout, read every creature's result back
-    e2e_iters = max(1, min(args.steps, 2))
-    eng2 = batch.BatchEngine(w.maps, w.n)
-    eng2.set_stream(stream.cuda_stream)
-    eng2.set_launch(best_w, 0)
-    workloads.spawn_all(eng2, w)
-    eng2.run(1)
-    torch.cuda.synchronize()
-    h0 = time.perf_counter()
-    for _ in range(e2e_iters):
-        workloads.spawn_all(eng2, w)
-        eng2.run(max_h)
-        fit = eng2.read_fitness()
-        st = eng2.read_state()
-    e2e_s = all_max(time.perf_counter() - h0)
-    h2d = w.n * (4 * 4 + 8 * 3 + 4 + 4) + w.n * 6 * 76 * 4  # spawn args + staged poses
-    d2h = fit.nbytes + sum(v.nbytes for v in st.values())
-    eng2.close()
+    # end to end: the workload served through the rollout server's C ABI with
+    # host buffers (requests in, results out), p50/p99 rollout latency
+    chunk = args.chunk
+    sess = served_uneven(serve, w, best, chunk, 1 + max(1, min(args.steps, 2)))[1:]
+    e2e_s = all_max(sum(x["wall_s"] for x in sess))
+    lat = np.concatenate([x["lat"] for x in sess])
+    clocks = sampler.stop()
+    e2e = {"value": world * units * len(sess) / e2e_s, "unit": UNIT,
+           "h2d_bytes_per_step": int(np.mean([x["h2d"] for x in sess])),
+           "d2h_bytes_per_step": int(np.mean([x["d2h"] for x in sess])),
+           "form": "served: rollout server C ABI, one request per creature, host buffers in and out",
+           "p50_rollout_ms": float(np.percentile(lat, 50) * 1e3),
+           "p99_rollout_ms": float(np.percentile(lat, 99) * 1e3), "chunk_steps": chunk}
+
+    if not args.no_es and rank == 0:
+        extra["served_es_stream"] = served_es_stream(serve, w, best, chunk, args.es_requests, 200.0)
 
     # roofline: f32 rounding ops per creature-step of the restated f32
     # algorithm (op-counting oracle build) x creature-steps per launch /
@@ -368,9 +431,10 @@ def main():
             ops = ops_per_creature_step(w)
             achieved = ops * units / (kms / 1000.0)
             roof = {"bound": "fp32", "achieved": achieved / 1e12, "peak": fma_rate / 1e12,
-                    "unit": "TFLOP/s", "frac": achieved / fma_rate, "traffic": None,
+                    "unit": "TFLOP/s", "frac": achieved / fma_rate, "traffic": args.traffic,
                     "ops_per_creature_step": ops, "kernel_ms": kms,
-                    "peak_note": "measured dependent-free f32 FMA issue rate (lane-ops/s) on this GPU"}
+                    "peak_note": "measured dependent-free f32 FMA issue rate (lane-ops/s) of this GPU; "
+                                 "MEASURED_PEAKS.json has no f32 figure"}
             threads = os.cpu_count() or 1
             cv, cn, ce = cpu_oracle_rate(w, args.cpu_seconds, threads)
             cpu = {"value": cv, "unit": UNIT, "cores": threads, "kind": "port",
@@ -383,16 +447,19 @@ def main():
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32", "data": "synthetic",
-            "config": {"workload": "uneven-16k", "creatures": w.n, "maps": args.maps,
-                       "bodies": "4-8 arms x 5-9 segs", "horizons": f"{args.hmin}-{args.hmax}",
-                       "creature_steps_per_rollout": units, "substeps": 2, "iterations": 4,
+            "config": {"workload": "uneven-16k: 16,384 creatures, 64 maps, 4-8 arms x 5-9 segments, "
+                                   f"horizons {args.hmin}-{args.hmax}",
+                       "creatures": w.n, "maps": args.maps, "creature_steps_per_rollout": units,
+                       "substeps": 2, "iterations": 4,
                        "controls": "device mulberry32 streams, redraw every 6 steps",
-                       "warps_per_cta": best_w, "parallelism": f"replicas x{world}",
-                       "l2": "state per rollout restored from a device snapshot; working set "
-                             f"{w.n * 2.4 / 1024:.0f} MB of state, compute-bound"},
-            "roofline": roof, "cpu_baseline": cpu, "clocks": clocks,
-            "e2e": {"value": world * units * e2e_iters / e2e_s, "unit": UNIT,
-                    "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+                       "form": "persistent kernel, one launch per rollout, state resident in HBM",
+                       "launch_shape": {"lanes_per_creature": best[0], "warps_per_cta": best[1],
+                                        "ctas_per_sm": best[2]},
+                       "autotune_ms": {",".join(map(str, k)): round(v, 3) for k, v in tune.items()},
+                       "parallelism": f"replicas x{world}",
+                       "l2": "flushed between timed rollouts (256 MB write); state restored from a device "
+                             "snapshot inside the timed region"},
+            "roofline": roof, "cpu_baseline": cpu, "clocks": clocks, "e2e": e2e,
             "gpu_launches": gpu_launches, **extra,
         }
         print(json.dumps(line), flush=True)

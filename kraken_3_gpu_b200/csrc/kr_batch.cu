@@ -53,9 +53,9 @@ struct BatchArgs {
   int obs_ring;
   double slip_max, cooldown, inv_h64, dt;
   // policy
-  const float *pw;       // n_individuals x n_params
+  const float *pw;       // n_individuals x pw_stride, device layout (see policy())
   const int *pw_idx;     // individual of each slot
-  int n_params;
+  int pw_stride;
 };
 
 // --- shared-memory layout, carved per template ------------------------------
@@ -218,37 +218,59 @@ __device__ unsigned proprio(const BatchArgs &A, const TplDev &td, const TplSmem 
   return att;
 }
 
+// HPL consecutive floats from 8- or 16-byte aligned memory
+template <int HPL>
+__device__ __forceinline__ void load_vec(const float *p, float *v) {
+  if constexpr (HPL == 2) {
+    const float2 a = __ldg(reinterpret_cast<const float2 *>(p));
+    v[0] = a.x; v[1] = a.y;
+  } else {
+#pragma unroll
+    for (int k = 0; k < HPL; k += 4) {
+      const float4 a = __ldg(reinterpret_cast<const float4 *>(p + k));
+      v[k] = a.x; v[k + 1] = a.y; v[k + 2] = a.z; v[k + 3] = a.w;
+    }
+  }
+}
+
 // fused policy (G lanes): proprio (n_in = 6A + 6) -> 64 tanh -> A*S motor
-// targets (tanh) + A adhesion values ((tanh + 1) / 2).  Weights of the
-// slot's individual, row-major with the bias last: W1 64 x (n_in + 1), then
-// W2 n_out x 65.  Every dot product accumulates in index order.
+// targets (tanh) + A adhesion values ((tanh + 1) / 2).  Device layout of an
+// individual (the transpose of the public row-major layout, so lanes read
+// consecutive words): W1T (n_in + 1) x 64, bias row last, then W2T 65 x
+// n_out, bias row last.  Lane l holds hidden units HPL*l .. HPL*l + HPL - 1.
+// Every dot product starts from the bias and accumulates in index order.
 template <int G>
 __device__ void policy(const BatchArgs &A, const TplDev &td, CreatureSmem &X, int slot,
                        const kr::Lanes<G> &L) {
-  constexpr int HPL = KR_POLICY_HIDDEN / G;  // hidden units per lane
+  constexpr int H = KR_POLICY_HIDDEN;
+  constexpr int HPL = H / G;  // hidden units per lane
   const int n_in = 6 * td.arms + 6, n_out = td.arms * td.segs + td.arms, lane = L.lane;
-  const float *w = A.pw + (size_t)A.pw_idx[slot] * A.n_params;
+  const float *w = A.pw + (size_t)A.pw_idx[slot] * A.pw_stride;
+  const float *col = w + HPL * lane;
   float hid[HPL];
+  load_vec<HPL>(col + (size_t)n_in * H, hid);
+#pragma unroll 4
+  for (int i = 0; i < n_in; i++) {
+    float wv[HPL];
+    load_vec<HPL>(col + (size_t)i * H, wv);
+    const float x = X.obs[i];
 #pragma unroll
-  for (int u = 0; u < HPL; u++) {
-    const float *row = w + (size_t)(lane + G * u) * (n_in + 1);
-    float acc = __ldg(row + n_in);
-    for (int i = 0; i < n_in; i++) acc = fmaf(__ldg(row + i), X.obs[i], acc);
-    hid[u] = tanhf(acc);
+    for (int u = 0; u < HPL; u++) hid[u] = fmaf(wv[u], x, hid[u]);
   }
-  const float *w2 = w + (size_t)KR_POLICY_HIDDEN * (n_in + 1);
+#pragma unroll
+  for (int u = 0; u < HPL; u++) hid[u] = tanhf(hid[u]);
+  const float *w2 = w + (size_t)H * (n_in + 1);
   for (int base = 0; base < n_out; base += G) {
     const int o = base + lane;
-    const float *row = w2 + (size_t)(o < n_out ? o : 0) * (KR_POLICY_HIDDEN + 1);
-    float acc = o < n_out ? __ldg(row + KR_POLICY_HIDDEN) : 0.f;
+    const bool ok = o < n_out;
+    const float *c2 = w2 + (ok ? o : 0);
+    float acc = ok ? __ldg(c2 + (size_t)H * n_out) : 0.f;
 #pragma unroll
-    for (int u = 0; u < HPL; u++) {
-      for (int j = 0; j < G; j++) {
-        const float hj = __shfl_sync(L.mask, hid[u], j, G);
-        if (o < n_out) acc = fmaf(__ldg(row + u * G + j), hj, acc);
-      }
+    for (int j = 0; j < H; j++) {
+      const float hj = __shfl_sync(L.mask, hid[j % HPL], j / HPL, G);
+      if (ok) acc = fmaf(__ldg(c2 + (size_t)j * n_out), hj, acc);
     }
-    if (o < n_out) {
+    if (ok) {
       const float y = tanhf(acc);
       X.ctrl[o] = o < td.arms * td.segs ? y : 0.5f * (y + 1.f);
     }
@@ -481,6 +503,11 @@ void free_part(Part &p) {
   p = Part{};
 }
 
+void transpose_policy(const float *pub, int arms, int segs, float *dev) {
+  const int n = policy_param_count(arms, segs);
+  for (int p = 0; p < n; p++) dev[policy_device_index(arms, segs, p)] = pub[p];
+}
+
 int ensure_template(kr_batch *b, int arms, int segs) {
   auto key = std::make_pair(arms, segs);
   auto it = b->tpl_index.find(key);
@@ -607,11 +634,11 @@ int build_groups(kr_batch *b, Part &p, int max_steps) {
   for (int s : live) {
     const SlotMeta &m = b->h_meta[s];
     if (m.ctrl != KR_CTRL_POLICY) continue;
-    const TplDev &t = b->h_tpl[m.tpl];
-    const int need = KR_POLICY_HIDDEN * (6 * t.arms + 7) + (t.arms * t.segs + t.arms) * (KR_POLICY_HIDDEN + 1);
-    if (!b->d_pw || b->n_params < need)
-      return b->fail(KR_ERR_STATE, "slot " + std::to_string(s) + ": policy control needs " + std::to_string(need) +
-                                       " parameters per individual (kr_batch_set_policy)");
+    if (!b->d_pw || b->h_pw_idx.size() != (size_t)b->capacity)
+      return b->fail(KR_ERR_STATE, "slot " + std::to_string(s) + ": policy control without kr_batch_set_policy");
+    if (b->h_pw_tpl[b->h_pw_idx[s]] != m.tpl)
+      return b->fail(KR_ERR_STATE, "slot " + std::to_string(s) + ": its individual's weights were laid out for "
+                                       "another body shape (kr_batch_set_policy after the spawn)");
   }
   std::stable_sort(live.begin(), live.end(), [&](int x, int y) {
     if (b->h_meta[x].tpl != b->h_meta[y].tpl) return b->h_meta[x].tpl < b->h_meta[y].tpl;
@@ -725,7 +752,7 @@ int launch_part(kr_batch *b, Part &p, int max_steps, bool timed) {
   A.slip_max = b->d.grip_slip_max; A.cooldown = b->d.grip_cooldown;
   A.inv_h64 = 1.0 / b->d.solver.h;
   A.dt = b->d.solver.h * b->d.solver.substeps;
-  A.pw = b->d_pw; A.pw_idx = b->d_pw_idx; A.n_params = b->n_params;
+  A.pw = b->d_pw; A.pw_idx = b->d_pw_idx; A.pw_stride = b->pw_stride;
   cudaError_t e;
   if ((e = cudaMemsetAsync(p.d_queue, 0, sizeof(int), st)) != cudaSuccess) return b->cuda_fail(e, "queue reset");
   if (timed) cudaEventRecord(p.ev0, st);
@@ -962,42 +989,58 @@ extern "C" int kr_batch_set_policy(kr_batch *b, const float *weights, int32_t n_
   if (!b) return KR_ERR_INVALID;
   if (!weights || !slot_individual || n_individuals <= 0 || n_params <= 0)
     return b->fail(KR_ERR_INVALID, "kr_batch_set_policy: null argument or empty policy");
+  // the body shape of every individual: the template of the live slots using it
+  std::vector<int> ind_tpl(n_individuals, -1);
   for (int s = 0; s < b->capacity; s++) {
     if (slot_individual[s] < 0 || slot_individual[s] >= n_individuals)
       return b->fail(KR_ERR_INDEX, "slot " + std::to_string(s) + " refers to individual " +
                                        std::to_string(slot_individual[s]) + " of " +
                                        std::to_string(n_individuals));
     const SlotMeta &m = b->h_meta[s];
-    if (m.horizon > 0) {
-      const kr::Template &t = b->tpls[m.tpl];
-      const int need = KR_POLICY_HIDDEN * (6 * t.arms + 7) + (t.arms * t.segs + t.arms) * (KR_POLICY_HIDDEN + 1);
-      if (n_params < need)
-        return b->fail(KR_ERR_INVALID, "slot " + std::to_string(s) + ": a " + std::to_string(t.arms) + "x" +
-                                           std::to_string(t.segs) + " body needs " + std::to_string(need) +
-                                           " policy parameters, got " + std::to_string(n_params));
-    }
+    if (m.horizon <= 0) continue;
+    const kr::Template &t = b->tpls[m.tpl];
+    const int need = policy_param_count(t.arms, t.segs);
+    if (n_params < need)
+      return b->fail(KR_ERR_INVALID, "slot " + std::to_string(s) + ": a " + std::to_string(t.arms) + "x" +
+                                         std::to_string(t.segs) + " body needs " + std::to_string(need) +
+                                         " policy parameters, got " + std::to_string(n_params));
+    int &it = ind_tpl[slot_individual[s]];
+    if (it >= 0 && it != m.tpl)
+      return b->fail(KR_ERR_INVALID, "individual " + std::to_string(slot_individual[s]) +
+                                         " is used by two body shapes");
+    it = m.tpl;
   }
-  const size_t need = (size_t)n_individuals * n_params;
+  const int stride = (n_params + 3) & ~3;  // 16-byte aligned individuals
+  std::vector<float> dev((size_t)n_individuals * stride, 0.f);
+  for (int k = 0; k < n_individuals; k++) {
+    if (ind_tpl[k] < 0) continue;
+    const kr::Template &t = b->tpls[ind_tpl[k]];
+    transpose_policy(weights + (size_t)k * n_params, t.arms, t.segs, dev.data() + (size_t)k * stride);
+  }
+  const size_t need = dev.size();
   cudaError_t e = cudaStreamSynchronize(b->stream);
   if (e != cudaSuccess) return b->cuda_fail(e, "kr_batch_set_policy sync");
-  if (!b->d_pw || (size_t)b->n_individuals * b->n_params < need) {
+  if (!b->d_pw || b->pw_capacity < need) {
     if (b->d_pw) cudaFree(b->d_pw);
     b->d_pw = nullptr;
     e = cudaMalloc(&b->d_pw, need * sizeof(float));
     if (e != cudaSuccess) return b->cuda_fail(e, "cudaMalloc(policy weights)");
+    b->pw_capacity = need;
   }
   if (!b->d_pw_idx) {
     e = cudaMalloc(&b->d_pw_idx, (size_t)b->capacity * sizeof(int));
     if (e != cudaSuccess) return b->cuda_fail(e, "cudaMalloc(policy index)");
   }
-  e = cudaMemcpyAsync(b->d_pw, weights, need * sizeof(float), cudaMemcpyHostToDevice, b->stream);
+  e = cudaMemcpyAsync(b->d_pw, dev.data(), need * sizeof(float), cudaMemcpyHostToDevice, b->stream);
   if (e == cudaSuccess)
     e = cudaMemcpyAsync(b->d_pw_idx, slot_individual, (size_t)b->capacity * sizeof(int),
                         cudaMemcpyHostToDevice, b->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
   if (e != cudaSuccess) return b->cuda_fail(e, "kr_batch_set_policy");
   b->n_individuals = n_individuals;
-  b->n_params = n_params;
+  b->pw_stride = stride;
+  b->h_pw_idx.assign(slot_individual, slot_individual + b->capacity);
+  b->h_pw_tpl = ind_tpl;
   return KR_OK;
 }
 

@@ -57,6 +57,21 @@ struct SlotMeta {
   double last_x, last_y;
 };
 
+// policy parameters of an arms x segs body (kraken_batch.h layout: W1
+// 64 x (n_in + 1) then W2 n_out x 65, row-major, bias last)
+__host__ __device__ inline int policy_param_count(int arms, int segs) {
+  return KR_POLICY_HIDDEN * (6 * arms + 7) + (arms * segs + arms) * (KR_POLICY_HIDDEN + 1);
+}
+
+// position of public parameter p in the device layout, the transposes
+// W1T (n_in + 1) x 64 and W2T 65 x n_out (lanes then read consecutive words)
+__host__ __device__ inline int policy_device_index(int arms, int segs, int p) {
+  const int n_in = 6 * arms + 6, n_out = arms * segs + arms, H = KR_POLICY_HIDDEN;
+  if (p < H * (n_in + 1)) return (p % (n_in + 1)) * H + p / (n_in + 1);
+  const int q = p - H * (n_in + 1);
+  return H * (n_in + 1) + (q % (H + 1)) * n_out + q / (H + 1);
+}
+
 // A set of slots launched together on one stream: every slot (the public
 // engine calls) or an explicit list (the rollout server's partitions).
 struct Part {
@@ -132,10 +147,13 @@ struct kr_batch {
   std::vector<int> tpl_cpg;     // creatures per group of each template
   size_t smem_dyn = 0;          // dynamic shared memory per CTA
   bool shape_dirty = true;
-  // policy: n_params floats per individual, individual of each slot
+  // policy: pw_stride floats per individual (device layout), individual of
+  // each slot, the body shape each individual's weights are laid out for
   float *d_pw = nullptr;
   int *d_pw_idx = nullptr;
-  int n_params = 0, n_individuals = 0;
+  size_t pw_capacity = 0;
+  int pw_stride = 0, n_individuals = 0;
+  std::vector<int> h_pw_idx, h_pw_tpl;
 
   int fail(int code, const std::string &m) { err = m; return code; }
   int cuda_fail(cudaError_t e, const char *what) {
@@ -168,6 +186,8 @@ int prepare_spawn(kr_batch *b, int n, const int32_t *arms, const int32_t *segs, 
 cudaError_t launch_spawn(kr_batch *b, const int *d_slots, const float *d_pose, const SlotMeta *d_meta,
                          int n, cudaStream_t stream);
 cudaStream_t part_stream(const kr_batch *b, const Part &p);
+// public -> device layout of one individual's policy parameters
+void transpose_policy(const float *pub, int arms, int segs, float *dev);
 void free_part(Part &p);
 
 }  // namespace krb

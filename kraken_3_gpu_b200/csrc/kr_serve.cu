@@ -44,10 +44,6 @@ constexpr uint64_t kFixedBytes = 8ull << 20;  // tables, maps, queues, events
 
 thread_local std::string g_serve_error;
 
-int policy_params(int arms, int segs) {
-  return KR_POLICY_HIDDEN * (6 * arms + 7) + (arms * segs + arms) * (KR_POLICY_HIDDEN + 1);
-}
-
 __host__ __device__ inline uint64_t splitmix64(uint64_t z) {
   z += 0x9e3779b97f4a7c15ULL;
   z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ULL;
@@ -69,20 +65,22 @@ __global__ void eps_kernel(uint64_t seed, int pair, int n, float *out) {
 }
 
 struct PJob {
-  int slot, theta_off, n_params, pair;
+  int slot, theta_off, arms, segs, pair;
   float sign, sigma;
   uint64_t seed;
 };
 
-// weights of newly admitted individuals: theta +- sigma * eps
+// weights of newly admitted individuals: theta +- sigma * eps for public
+// parameter p, stored at its place in the device layout
 __global__ void perturb_kernel(float *w, int stride, const float *theta, const PJob *jobs, int n) {
   if ((int)blockIdx.x >= n) return;
   const PJob j = jobs[blockIdx.x];
   float *dst = w + (size_t)j.slot * stride;
   const float *th = theta + j.theta_off;
-  for (int p = threadIdx.x; p < j.n_params; p += blockDim.x) {
+  const int np = policy_param_count(j.arms, j.segs);
+  for (int p = threadIdx.x; p < np; p += blockDim.x) {
     const float d = __fmul_rn(j.sigma, eps_normal(j.seed, j.pair, p));
-    dst[p] = __fadd_rn(th[p], j.sign < 0.f ? -d : d);
+    dst[policy_device_index(j.arms, j.segs, p)] = __fadd_rn(th[p], j.sign < 0.f ? -d : d);
   }
 }
 
@@ -308,13 +306,14 @@ int admit(kr_server *S, int p) {
       st.h_slots[n_new] = s;
       if (pol) {
         PJob &j = st.h_jobs[n_new];
-        j.slot = s; j.theta_off = theta_off; j.n_params = (int)q.theta.size(); j.pair = i / 2;
+        j.slot = s; j.theta_off = theta_off; j.arms = q.r.arms; j.segs = q.r.segs; j.pair = i / 2;
         j.sign = (i & 1) ? -1.f : 1.f; j.sigma = q.r.sigma; j.seed = q.r.seed;
       } else {
-        st.h_jobs[n_new] = PJob{s, 0, 0, 0, 1.f, 0.f, 0};
+        st.h_jobs[n_new] = PJob{s, 0, 0, 0, 0, 1.f, 0.f, 0};
       }
       S->b->h_meta[s] = init.meta[i];
       S->b->h_remaining[s] = init.meta[i].horizon;
+      if (pol) S->b->h_pw_tpl[s] = init.meta[i].tpl;
       n_new++;
     }
     if (pol) {
@@ -470,8 +469,11 @@ extern "C" int kr_server_create(const kr_server_desc *d, kr_server **out) {
     if (e == cudaSuccess) e = cudaMalloc(&b->d_pw_idx, (size_t)cap * sizeof(int));
     if (e == cudaSuccess) e = cudaMemcpy(b->d_pw_idx, idx.data(), idx.size() * sizeof(int), cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemset(b->d_pw, 0, (size_t)cap * kMaxParams * sizeof(float));
-    b->n_params = kMaxParams;
+    b->pw_stride = kMaxParams;  // a multiple of 4: 16-byte aligned individuals
+    b->pw_capacity = (size_t)cap * kMaxParams;
     b->n_individuals = cap;
+    b->h_pw_idx = idx;
+    b->h_pw_tpl.assign(cap, -1);
     if (e != cudaSuccess) { S->cuda_fail(e, "policy weights"); return bail(KR_ERR_CUDA); }
   }
   for (int p = 0; p < 2; p++) {
@@ -517,7 +519,7 @@ extern "C" int kr_server_submit(kr_server *S, const kr_request *r, int64_t *id) 
   q.r.theta = nullptr;
   if (r->theta) {
     if (!S->d.policy) return S->fail(KR_ERR_STATE, "server created without policy weights");
-    const int need = policy_params(r->arms, r->segs);
+    const int need = policy_param_count(r->arms, r->segs);
     if (r->n_params < need)
       return S->fail(KR_ERR_INVALID, "theta has " + std::to_string(r->n_params) + " parameters, a " +
                                          std::to_string(r->arms) + "x" + std::to_string(r->segs) + " body needs " +

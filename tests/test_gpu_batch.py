@@ -137,9 +137,9 @@ def test_fused_policy_matches_mlp_on_recorded_proprio(lanes):
     w = _small_uneven(n=12, h=6)
     rng = np.random.default_rng(3)
     n_params = batch.policy_params(8, 9)
-    n_ind = 4
+    n_ind = w.n  # one individual per creature (weights are laid out per body shape)
     weights = rng.normal(0.0, 0.3, size=(n_ind, n_params)).astype(np.float32)
-    slot_ind = rng.integers(0, n_ind, size=w.n).astype(np.int32)
+    slot_ind = rng.permutation(n_ind).astype(np.int32)
     eng = batch.BatchEngine(w.maps, w.n, obs_ring=8, control="policy")
     eng.set_launch(4, 0, lanes_per_creature=lanes)
     workloads.spawn_all(eng, w)
@@ -159,8 +159,8 @@ def test_fused_policy_matches_mlp_on_recorded_proprio(lanes):
 def test_fused_policy_same_bits_for_every_launch_shape():
     w = _small_uneven(n=20, h=25)
     rng = np.random.default_rng(4)
-    weights = rng.normal(0.0, 0.2, size=(3, batch.policy_params(8, 9))).astype(np.float32)
-    slot_ind = rng.integers(0, 3, size=w.n).astype(np.int32)
+    weights = rng.normal(0.0, 0.2, size=(w.n, batch.policy_params(8, 9))).astype(np.float32)
+    slot_ind = rng.permutation(w.n).astype(np.int32)
     out = []
     for lanes, warps in ((32, 8), (16, 4), (8, 16)):
         eng = batch.BatchEngine(w.maps, w.n, control="policy")
@@ -173,3 +173,16 @@ def test_fused_policy_same_bits_for_every_launch_shape():
     for s in out[1:]:
         for f in ("px", "py", "ang", "grips"):
             assert np.array_equal(out[0][f], s[f]), f
+
+
+def test_policy_individual_shared_by_two_body_shapes_is_rejected():
+    from kraken_3_gpu_b200 import _native
+    w = _small_uneven(n=12, h=6)
+    assert len(set(zip(w.arms.tolist(), w.segs.tolist()))) > 1
+    eng = batch.BatchEngine(w.maps, w.n, control="policy")
+    workloads.spawn_all(eng, w)
+    weights = np.zeros((1, batch.policy_params(8, 9)), np.float32)
+    with pytest.raises(_native.KrError) as e:
+        eng.set_policy(weights, np.zeros(w.n, np.int32))
+    assert "two body shapes" in str(e.value)
+    eng.close()
