@@ -87,9 +87,11 @@ def test_chunked_runs_and_graph_equal_one_run():
 
 
 @pytest.mark.parametrize("lanes,warps,ctas", [(32, 1, 1), (32, 16, 1), (16, 4, 2), (16, 8, 0),
-                                               (8, 2, 4), (8, 16, 1)])
+                                               (8, 2, 4), (8, 16, 1), (16, 4, 5), (16, 4, 6),
+                                               (32, 8, 3)])
 def test_launch_shape_does_not_change_results(lanes, warps, ctas):
-    """One to four creatures per warp, any CTA size: the same bits."""
+    """One to four creatures per warp, any CTA size or CTAs per SM: the
+    same bits."""
     w = _small_uneven(n=40, h=30)
     base = batch.BatchEngine(w.maps, w.n, obs_ring=32)
     workloads.spawn_all(base, w)
