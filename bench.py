@@ -65,6 +65,7 @@ def parse():
     ap.add_argument("--chunk", type=int, default=64, help="server env steps per round")
     ap.add_argument("--no-es", action="store_true", help="skip the ES request stream")
     ap.add_argument("--es-requests", type=int, default=200)
+    ap.add_argument("--no-config1", action="store_true", help="skip the 1,024-creature drop-in comparison")
     ap.add_argument("--traffic", type=float, default=None,
                     help="ncu DRAM bytes per launch of the captured kernel, if measured")
     return ap.parse_args()
@@ -298,6 +299,73 @@ def served_es_stream(serve, w, shape, chunk, n_req, rate, seed=0):
             "device_kernel_ms_summed": st["device_ms"]}
 
 
+def config1_forms(torch, stream, plain_steps=200, steps=1000):
+    """The plain batched drop-in configuration: 1,024 default creatures on
+    map seed 1 (createSim spawn rule).  The reference's plain form -- per env
+    step the 80 B constraint blocks up (uploadControls), one step, bodies and
+    constraints down (download), gpuworld.js:312-396 -- through the drop-in C
+    ABI with host buffers (the CPU reflex the reference runs between steps is
+    not timed); the same drop-in with state resident (kr_step per env step
+    only); and the persistent batched engine on the same creatures."""
+    import ctypes as C
+    from kraken_3_gpu_b200 import _native, batch, core, gpuworld, workloads
+    sim = core.create_sim(seed=1, creatures=1024)
+    w = sim["world"]
+    n = len(sim["creatures"])
+    g = gpuworld.create(w, sim["map"])
+    gpuworld.upload(g)
+    L = _native.lib()
+    h = g.handle
+    _native.check(L.kr_set_stream(h, C.c_void_p(stream.cuda_stream)), h)
+    cons = np.ascontiguousarray(g.consData).view(np.uint32)
+    body = np.zeros(g.nB * gpuworld.BODY_STRIDE, dtype=np.float32)
+    cp, bp = cons.ctypes.data_as(C.POINTER(C.c_uint32)), body.ctypes.data_as(C.POINTER(C.c_float))
+    for _ in range(5):
+        L.kr_upload_controls(h, cp); L.kr_step(h, 1); L.kr_download(h, bp, cp)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(plain_steps):
+        _native.check(L.kr_upload_controls(h, cp), h)
+        _native.check(L.kr_step(h, 1), h)
+        _native.check(L.kr_download(h, bp, cp), h)
+    loop_s = time.perf_counter() - t0
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(plain_steps):
+        L.kr_step(h, 1)
+    e1.record(stream)
+    e1.synchronize()
+    step_ms = e0.elapsed_time(e1)
+    gpuworld.destroy(g)
+    mant = [c.mantle for c in sim["creatures"]]
+    eng = batch.BatchEngine([workloads._rects(sim["map"])], n)
+    eng.set_stream(stream.cuda_stream)
+    ones = np.ones(n, np.int32)
+    eng.spawn(0, 6 * ones, 7 * ones, 0 * ones, w.px[mant], w.py[mant], w.ang[mant], steps * ones,
+              seed=np.arange(n, dtype=np.uint32))
+    eng.snapshot()
+    pers_ms, shape = float("inf"), None
+    for shp in ((32, 4, 0), (16, 8, 0)):
+        eng.set_launch(shp[1], shp[2], lanes_per_creature=shp[0])
+        eng.restore()
+        eng.run(64)
+        eng.restore()
+        eng.run(steps)
+        eng.sync()
+        if eng.last_ms() < pers_ms:
+            pers_ms, shape = eng.last_ms(), shp
+    eng.close()
+    return {"creatures": n, "map_seed": 1,
+            "dropin_per_step_loop": {"value": n * plain_steps / loop_s, "unit": UNIT, "steps": plain_steps,
+                                     "h2d_bytes_per_step": int(cons.nbytes),
+                                     "d2h_bytes_per_step": int(cons.nbytes + body.nbytes)},
+            "dropin_per_step_kernel": {"value": n * plain_steps / (step_ms / 1000.0), "unit": UNIT,
+                                       "steps": plain_steps},
+            "persistent": {"value": n * steps / (pers_ms / 1000.0), "unit": UNIT, "steps": steps,
+                           "launch_shape": list(shape)}}
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -419,6 +487,8 @@ def main():
 
     if not args.no_es and rank == 0:
         extra["served_es_stream"] = served_es_stream(serve, w, best, chunk, args.es_requests, 200.0)
+    if not args.no_config1 and rank == 0:
+        extra["plain_dropin_1024"] = config1_forms(torch, stream)
 
     # roofline: f32 rounding ops per creature-step of the restated f32
     # algorithm (op-counting oracle build) x creature-steps per launch /

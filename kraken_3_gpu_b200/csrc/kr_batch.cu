@@ -644,13 +644,32 @@ int build_groups(kr_batch *b, Part &p, int max_steps) {
     if (b->h_meta[x].tpl != b->h_meta[y].tpl) return b->h_meta[x].tpl < b->h_meta[y].tpl;
     return rem[x] > rem[y];
   });
+  // Group size per template.  When the live creatures fill less than one
+  // wave of the resident CTAs, smaller groups (whole warps) spread them over
+  // every SM instead of packing a few SMs.
+  const int cpw = 32 / b->G;
+  const int ctas = b->ctas_per_sm > 0 ? b->ctas_per_sm : std::max(1, 16 / b->W);
+  const long slots = (long)b->n_sm * ctas;
+  std::vector<int> n_t(b->h_tpl.size(), 0), size_t_(b->h_tpl.size(), 0);
+  for (int s : live) n_t[b->h_meta[s].tpl]++;
+  long full_groups = 0;
+  for (size_t t = 0; t < n_t.size(); t++)
+    if (n_t[t]) full_groups += (n_t[t] + b->tpl_cpg[t] - 1) / b->tpl_cpg[t];
+  for (size_t t = 0; t < n_t.size(); t++) {
+    size_t_[t] = b->tpl_cpg[t];
+    if (!n_t[t] || full_groups >= slots || live.empty()) continue;
+    const long want = std::max<long>(1, (long)((double)slots * n_t[t] / (double)live.size()));
+    int sz = (int)((n_t[t] + want - 1) / want);
+    sz = ((sz + cpw - 1) / cpw) * cpw;
+    size_t_[t] = std::max(cpw, std::min(b->tpl_cpg[t], sz));
+  }
   std::vector<std::pair<double, int>> order;  // (work, first index into live)
   std::vector<int> starts, sizes;
   for (size_t i = 0; i < live.size();) {
     const int t = b->h_meta[live[i]].tpl;
     const size_t st = i;
     int n = 0;
-    while (i < live.size() && n < b->tpl_cpg[t] && b->h_meta[live[i]].tpl == t) { i++; n++; }
+    while (i < live.size() && n < size_t_[t] && b->h_meta[live[i]].tpl == t) { i++; n++; }
     const double work = (double)std::min(max_steps, rem[live[st]]) * tpl_cost(b->h_tpl[t]);
     order.push_back({work, (int)starts.size()});
     starts.push_back((int)st);
@@ -733,6 +752,22 @@ int launch_part(kr_batch *b, Part &p, int max_steps, bool timed) {
   if (b->tpls.empty()) return KR_OK;
   if (b->d.control_mode == KR_CTRL_POLICY && !b->d_pw)
     return b->fail(KR_ERR_STATE, "policy control without kr_batch_set_policy");
+  if (b->auto_shape && p.dirty) {
+    // few creatures (under 16 per SM): one per warp, the shortest step
+    // latency; else two per warp, the most creature-steps per issue slot
+    long live = 0;
+    if (p.all) {
+      for (int s = 0; s < b->capacity; s++) live += b->h_meta[s].horizon > 0 && b->h_remaining[s] > 0;
+    } else {
+      for (int s : p.slots) live += b->h_remaining[s] > 0;
+    }
+    const int g = live < 16L * b->n_sm ? 32 : 16, w = g == 32 ? 4 : 8;
+    if (g != b->G || w != b->W) {
+      b->G = g;
+      b->W = w;
+      b->shape_dirty = true;
+    }
+  }
   if (p.dirty || b->shape_dirty) {
     int rc = build_groups(b, p, max_steps);
     if (rc != KR_OK) return rc;
@@ -1060,6 +1095,7 @@ extern "C" int kr_batch_set_launch(kr_batch *b, int32_t lanes_per_creature, int3
   b->G = lanes_per_creature;
   b->W = warps_per_cta;
   b->ctas_per_sm = ctas_per_sm;
+  b->auto_shape = false;
   return KR_OK;
 }
 

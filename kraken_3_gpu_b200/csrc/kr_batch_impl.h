@@ -143,6 +143,7 @@ struct kr_batch {
   // launch shape
   int G = 16, W = 8, ctas_per_sm = 0, n_sm = 0;
   int smem_per_sm = 0, smem_reserved = 0, smem_optin = 0;
+  bool auto_shape = true;       // until kr_batch_set_launch: G and W from the live count
   int cpc = 16;                 // creature entries per group: W * 32 / G
   std::vector<int> tpl_cpg;     // creatures per group of each template
   size_t smem_dyn = 0;          // dynamic shared memory per CTA
