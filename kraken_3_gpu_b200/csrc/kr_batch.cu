@@ -138,7 +138,7 @@ __device__ inline void carve_creature(kr::Island &S, CreatureSmem &X, const TplS
   S.plx = P.plx; S.ply = P.ply; S.pr = P.pr; S.pbody = P.pbody; S.boff = P.boff; S.bcnt = P.bcnt;
   S.lvl = P.lvl;
   S.tb = nullptr; S.comp = nullptr; S.tgt = nullptr; S.brk = nullptr;
-  S.nb = td.nb; S.nc = td.nc; S.np = td.np; S.nlv = td.nlv;
+  S.nb = td.nb; S.nc = td.nc; S.np = td.np;
 }
 
 __device__ inline double mulberry_next(uint32_t &s) {
@@ -280,12 +280,13 @@ __device__ void policy(const BatchArgs &A, const TplDev &td, CreatureSmem &X, in
 
 // One creature (slot) advanced by its G lanes for up to A.max_steps env steps.
 template <int G>
-__device__ void run_creature(const BatchArgs &A, const TplDev &td, const TplSmem &P, float *base,
+__device__ void run_creature(const BatchArgs &A, const TplDev &td, int nlv, const TplSmem &P, float *base,
                              int slot, const kr::Lanes<G> &L) {
   const int lane = L.lane;
   kr::Island S;
   CreatureSmem X;
   carve_creature(S, X, P, base, td);
+  S.nlv = nlv;
   SlotMeta m = A.meta[slot];
   const int steps = min(A.max_steps, m.horizon - m.step);
   if (steps <= 0) return;
@@ -405,6 +406,7 @@ __device__ void run_creature(const BatchArgs &A, const TplDev &td, const TplSmem
 template <int G>
 __global__ void __launch_bounds__(32 * kMaxW, 1) batch_kernel(BatchArgs A) {
   constexpr int CPW = 32 / G;  // creatures per warp
+  constexpr int V = G == 32 ? 0 : G == 16 ? 1 : 2;  // kr::schedule_index(G): the schedule for G lanes
   extern __shared__ __align__(16) float smem[];
   __shared__ int s_group;
   const int warp = threadIdx.x >> 5, wl = threadIdx.x & 31;
@@ -426,18 +428,18 @@ __global__ void __launch_bounds__(32 * kMaxW, 1) batch_kernel(BatchArgs A) {
       P.boff[i] = A.T.boff[td.o_b + i]; P.bcnt[i] = A.T.bcnt[td.o_b + i];
     }
     for (int k = threadIdx.x; k < td.nc; k += blockDim.x) {
-      const int o = td.o_c + k;
+      const int o = td.o_c[V] + k;
       P.ab[k] = A.T.ab[o]; P.type[k] = A.T.type[o]; P.motor[k] = A.T.motor[o]; P.garm[k] = A.T.garm[o];
       P.lax[k] = A.T.lax[o]; P.lay[k] = A.T.lay[o]; P.lbx[k] = A.T.lbx[o]; P.lby[k] = A.T.lby[o];
       P.rest[k] = A.T.rest[o]; P.minA[k] = A.T.minA[o]; P.maxA[k] = A.T.maxA[o];
     }
-    for (int l = threadIdx.x; l <= td.nlv; l += blockDim.x) P.lvl[l] = A.T.lvl[td.o_l + l];
+    for (int l = threadIdx.x; l <= td.nlv[V]; l += blockDim.x) P.lvl[l] = A.T.lvl[td.o_l[V] + l];
     for (int p = threadIdx.x; p < td.np; p += blockDim.x) {
       P.plx[p] = A.T.plx[td.o_p + p]; P.ply[p] = A.T.ply[td.o_p + p]; P.pr[p] = A.T.pr[td.o_p + p];
       P.pbody[p] = A.T.pbody[td.o_p + p];
     }
     for (int a = threadIdx.x; a < td.arms; a += blockDim.x) {
-      P.arm_tip[a] = A.T.arm_tip[td.o_a + a]; P.arm_grip[a] = A.T.arm_grip[td.o_a + a];
+      P.arm_tip[a] = A.T.arm_tip[td.o_a + a]; P.arm_grip[a] = A.T.arm_grip[td.o_g[V] + a];
       P.arm_seg0[a] = A.T.arm_seg0[td.o_a + a];
     }
     for (int q = threadIdx.x; q < td.arms * td.segs; q += blockDim.x) P.arm_segs[q] = A.T.arm_segs[td.o_s + q];
@@ -446,7 +448,7 @@ __global__ void __launch_bounds__(32 * kMaxW, 1) batch_kernel(BatchArgs A) {
     if (slot >= 0) {
       float *base = smem + tpl_smem_words(td.nb, td.nc, td.np) +
                     c * creature_smem_words(td.nb, td.nc, td.np, td.arms, td.segs);
-      run_creature<G>(A, td, P, base, slot, L);
+      run_creature<G>(A, td, td.nlv[V], P, base, slot, L);
     }
   }
 }
@@ -527,28 +529,30 @@ int upload_templates(kr_batch *b) {
   b->h_tpl.clear();
   for (const auto &t : b->tpls) {
     TplDev d{};
-    d.nb = t.nb; d.nc = t.nc; d.np = t.np; d.nlv = t.nlv; d.arms = t.arms; d.segs = t.segs;
+    d.nb = t.nb; d.nc = t.nc; d.np = t.np; d.arms = t.arms; d.segs = t.segs;
     d.r_max = t.r_max; d.reach = t.reach;
-    d.o_b = (int)im.size(); d.o_c = (int)ab.size(); d.o_l = (int)lvl.size(); d.o_p = (int)plx.size();
-    d.o_a = (int)tip.size(); d.o_s = (int)segs.size();
+    d.o_b = (int)im.size(); d.o_p = (int)plx.size(); d.o_a = (int)tip.size(); d.o_s = (int)segs.size();
     im.insert(im.end(), t.im.begin(), t.im.end()); ii.insert(ii.end(), t.ii.begin(), t.ii.end());
     boff.insert(boff.end(), t.boff.begin(), t.boff.end()); bcnt.insert(bcnt.end(), t.bcnt.begin(), t.bcnt.end());
-    ab.insert(ab.end(), t.ab.begin(), t.ab.end()); type.insert(type.end(), t.type.begin(), t.type.end());
-    motor.insert(motor.end(), t.motor.begin(), t.motor.end());
-    {
+    for (int v = 0; v < kr::kSchedules; v++) {
+      const kr::Schedule &S = t.sched[v];
+      d.nlv[v] = S.nlv;
+      d.o_c[v] = (int)ab.size(); d.o_l[v] = (int)lvl.size(); d.o_g[v] = (int)grip.size();
+      ab.insert(ab.end(), S.ab.begin(), S.ab.end()); type.insert(type.end(), S.type.begin(), S.type.end());
+      motor.insert(motor.end(), S.motor.begin(), S.motor.end());
       std::vector<int> ga(t.nc, -1);
-      for (int a = 0; a < t.arms; a++) ga[t.arm_grip[a]] = a;
+      for (int a = 0; a < t.arms; a++) ga[S.arm_grip[a]] = a;
       garm.insert(garm.end(), ga.begin(), ga.end());
+      lax.insert(lax.end(), S.lax.begin(), S.lax.end()); lay.insert(lay.end(), S.lay.begin(), S.lay.end());
+      lbx.insert(lbx.end(), S.lbx.begin(), S.lbx.end()); lby.insert(lby.end(), S.lby.begin(), S.lby.end());
+      rest.insert(rest.end(), S.rest.begin(), S.rest.end());
+      minA.insert(minA.end(), S.minA.begin(), S.minA.end()); maxA.insert(maxA.end(), S.maxA.begin(), S.maxA.end());
+      lvl.insert(lvl.end(), S.lvl.begin(), S.lvl.end());
+      grip.insert(grip.end(), S.arm_grip.begin(), S.arm_grip.end());
     }
-    lax.insert(lax.end(), t.lax.begin(), t.lax.end()); lay.insert(lay.end(), t.lay.begin(), t.lay.end());
-    lbx.insert(lbx.end(), t.lbx.begin(), t.lbx.end()); lby.insert(lby.end(), t.lby.begin(), t.lby.end());
-    rest.insert(rest.end(), t.rest.begin(), t.rest.end());
-    minA.insert(minA.end(), t.minA.begin(), t.minA.end()); maxA.insert(maxA.end(), t.maxA.begin(), t.maxA.end());
-    lvl.insert(lvl.end(), t.lvl.begin(), t.lvl.end());
     plx.insert(plx.end(), t.plx.begin(), t.plx.end()); ply.insert(ply.end(), t.ply.begin(), t.ply.end());
     pr.insert(pr.end(), t.pr.begin(), t.pr.end()); pbody.insert(pbody.end(), t.pbody.begin(), t.pbody.end());
     tip.insert(tip.end(), t.arm_tip.begin(), t.arm_tip.end());
-    grip.insert(grip.end(), t.arm_grip.begin(), t.arm_grip.end());
     seg0.insert(seg0.end(), t.arm_seg0.begin(), t.arm_seg0.end());
     segs.insert(segs.end(), t.arm_segs.begin(), t.arm_segs.end());
     b->h_tpl.push_back(d);

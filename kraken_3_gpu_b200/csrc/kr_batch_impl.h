@@ -23,12 +23,16 @@ constexpr int kStateStride = 6 * kBodyPad;                     // px py vx vy an
 constexpr int kCtrlStride = KR_BATCH_MAX_ARMS * (KR_BATCH_MAX_SEGS + 1);  // 80
 
 // Template record on the device: sizes and offsets into the flat arrays.
+// Constraint slots, level offsets and arm grip slots exist once per solve
+// schedule (kr::schedule_index of the lanes per creature).
 struct TplDev {
-  int nb, nc, np, nlv, arms, segs;
+  int nb, nc, np, arms, segs;
+  int nlv[kr::kSchedules];
   float r_max;
   float pad0;
   double reach;
-  int o_b, o_c, o_l, o_p, o_a, o_s;
+  int o_b, o_p, o_a, o_s;
+  int o_c[kr::kSchedules], o_l[kr::kSchedules], o_g[kr::kSchedules];
 };
 
 struct TplArrays {
@@ -39,7 +43,7 @@ struct TplArrays {
   const int *lvl;
   const float *plx, *ply, *pr;
   const int *pbody;
-  const int *arm_tip, *arm_grip, *arm_seg0, *arm_segs;
+  const int *arm_tip, *arm_grip, *arm_seg0, *arm_segs;  // arm_grip: per schedule
 };
 
 // Per-slot record (device resident; the host keeps a mirror of the static

@@ -29,6 +29,73 @@ struct RawCon {
 
 double rect_inertia(double m, double w, double h) { return m * (w * w + h * h) / 12; }
 
+// Levels balanced for G lanes.  Input: the solve list (type and bodies of
+// each entry, in list order) and its as-early-as-possible levels.  Any level
+// assignment in which every pair of entries sharing a body keeps its list
+// order gives bit-identical results (a level holds body-disjoint entries, so
+// their order inside it is free).  This one keeps the number of levels and
+// each level's constraint type (so a level's lanes never diverge between
+// the pin and the angle solve) and fills levels from the first: each level
+// takes the entries that cannot go later, then fills its last pass of G
+// lanes with the most urgent of the others whose predecessors are placed.
+// Returns false (leaving `out` unset) if the list's levels mix types.
+bool balance_levels(const std::vector<int> &ty, const std::vector<int> &ea, const std::vector<int> &eb,
+                    const std::vector<int> &asap0, int L, int G, std::vector<int> *out) {
+  const int n = (int)ty.size();
+  std::vector<int> ltype(L, -1);
+  for (int i = 0; i < n; i++) {
+    if (ltype[asap0[i]] >= 0 && ltype[asap0[i]] != ty[i]) return false;
+    ltype[asap0[i]] = ty[i];
+  }
+  std::vector<std::vector<int>> pred(n), succ(n);
+  std::vector<int> last_of;
+  for (int i = 0; i < n; i++) {
+    for (int b : {ea[i], eb[i]}) {
+      if (b < 0) continue;
+      if ((int)last_of.size() <= b) last_of.resize(b + 1, -1);
+      if (last_of[b] >= 0) { pred[i].push_back(last_of[b]); succ[last_of[b]].push_back(i); }
+      last_of[b] = i;
+    }
+  }
+  std::vector<int> asap(n), alap(n);
+  for (int i = 0; i < n; i++) {
+    int lo = 0;
+    for (int p : pred[i]) lo = std::max(lo, asap[p] + 1);
+    while (lo < L && ltype[lo] != ty[i]) lo++;
+    if (lo >= L) return false;
+    asap[i] = lo;
+  }
+  for (int i = n - 1; i >= 0; i--) {
+    int hi = L - 1;
+    for (int j : succ[i]) hi = std::min(hi, alap[j] - 1);
+    while (hi >= 0 && ltype[hi] != ty[i]) hi--;
+    if (hi < asap[i]) return false;
+    alap[i] = hi;
+  }
+  std::vector<int> lvl(n, -1);
+  for (int l = 0; l < L; l++) {
+    std::vector<int> mand, rest;
+    for (int i = 0; i < n; i++) {
+      if (lvl[i] >= 0 || ty[i] != ltype[l] || asap[i] > l) continue;
+      bool ready = true;
+      for (int p : pred[i]) ready = ready && lvl[p] >= 0 && lvl[p] < l;
+      if (!ready) continue;
+      (alap[i] == l ? mand : rest).push_back(i);
+    }
+    std::stable_sort(rest.begin(), rest.end(), [&](int x, int y) { return alap[x] < alap[y]; });
+    const int cap = std::max(1, (int)(mand.size() + G - 1) / G) * G;
+    for (int i : mand) lvl[i] = l;
+    for (size_t k = 0; k < rest.size() && (int)(mand.size() + k) < cap; k++) lvl[rest[k]] = l;
+  }
+  for (int i = 0; i < n; i++) {
+    if (lvl[i] < 0) return false;
+    for (int j : succ[i])
+      if (lvl[i] >= lvl[j]) return false;
+  }
+  *out = lvl;
+  return true;
+}
+
 }  // namespace
 
 bool build_template(int arms, int segs, Template *t, std::string *err) {
@@ -137,30 +204,52 @@ bool build_template(int arms, int segs, Template *t, std::string *err) {
     *err = "body shape needs " + std::to_string(nlv) + " levels";
     return false;
   }
-  std::vector<int> cnt(nlv + 1, 0);
-  for (int q = 0; q < nc; q++) cnt[level[q] + 1]++;
-  for (int L = 0; L < nlv; L++) cnt[L + 1] += cnt[L];
-  std::vector<int> order(nc), cur(cnt.begin(), cnt.end() - 1);
-  for (int q = 0; q < nc; q++) order[cur[level[q]]++] = list[q];
-  t->nb = nb; t->nc = nc; t->np = np; t->nlv = nlv;
-  t->lvl = cnt;
+  t->nb = nb; t->nc = nc; t->np = np;
   t->im.resize(nb); t->ii.resize(nb);
   for (int i = 0; i < nb; i++) { t->im[i] = (float)im[i]; t->ii[i] = (float)ii[i]; }
-  std::vector<int> slot_of(nc);
-  for (int s = 0; s < nc; s++) {
-    const RawCon &c = cons[order[s]];
-    slot_of[order[s]] = s;
-    const uint32_t b = c.b >= 0 ? (uint32_t)c.b : 0xffffu;
-    t->ab.push_back((int)((uint32_t)c.a | (b << 16)));
-    t->type.push_back(c.type);
-    t->lax.push_back((float)c.lax); t->lay.push_back((float)c.lay);
-    t->lbx.push_back((float)c.lbx); t->lby.push_back((float)c.lby);
-    t->rest.push_back((float)c.rest);
-    t->minA.push_back((float)c.minA); t->maxA.push_back((float)c.maxA);
-    t->motor.push_back(c.motor);
+  // the list's types and bodies, for the balanced schedules
+  std::vector<int> lty(nc), la(nc), lb(nc);
+  for (int q = 0; q < nc; q++) {
+    const RawCon &c = cons[list[q]];
+    lty[q] = c.type == 1 ? 1 : 0;
+    la[q] = c.a;
+    lb[q] = c.b;
   }
-  t->arm_grip.resize(arms);
-  for (int a = 0; a < arms; a++) t->arm_grip[a] = slot_of[grip_raw[a]];
+  for (int v = 0; v < kSchedules; v++) {
+    const int G = v == 0 ? 32 : v == 1 ? 16 : 8;
+    std::vector<int> lv = level, bal;
+    if (balance_levels(lty, la, lb, level, nlv, G, &bal)) lv = bal;
+    Schedule &S = t->sched[v];
+    S.nlv = nlv;
+    std::vector<int> cnt(nlv + 1, 0);
+    for (int q = 0; q < nc; q++) cnt[lv[q] + 1]++;
+    for (int L = 0; L < nlv; L++) cnt[L + 1] += cnt[L];
+    std::vector<int> order(nc), cur(cnt.begin(), cnt.end() - 1);
+    for (int q = 0; q < nc; q++) order[cur[lv[q]]++] = list[q];
+    S.lvl = cnt;
+    std::vector<int> slot_of(nc);
+    for (int s = 0; s < nc; s++) {
+      const RawCon &c = cons[order[s]];
+      slot_of[order[s]] = s;
+      const uint32_t b = c.b >= 0 ? (uint32_t)c.b : 0xffffu;
+      S.ab.push_back((int)((uint32_t)c.a | (b << 16)));
+      S.type.push_back(c.type);
+      S.lax.push_back((float)c.lax); S.lay.push_back((float)c.lay);
+      S.lbx.push_back((float)c.lbx); S.lby.push_back((float)c.lby);
+      S.rest.push_back((float)c.rest);
+      S.minA.push_back((float)c.minA); S.maxA.push_back((float)c.maxA);
+      S.motor.push_back(c.motor);
+    }
+    S.arm_grip.resize(arms);
+    for (int a = 0; a < arms; a++) S.arm_grip[a] = slot_of[grip_raw[a]];
+  }
+  const Schedule &S0 = t->sched[0];
+  t->nlv = nlv;
+  t->lvl = S0.lvl;
+  t->ab = S0.ab; t->type = S0.type; t->motor = S0.motor;
+  t->lax = S0.lax; t->lay = S0.lay; t->lbx = S0.lbx; t->lby = S0.lby;
+  t->rest = S0.rest; t->minA = S0.minA; t->maxA = S0.maxA;
+  t->arm_grip = S0.arm_grip;
   // points grouped per body, creation order within a body (groupCollPoints)
   t->boff.assign(nb, 0);
   t->bcnt.assign(nb, 0);

@@ -21,18 +21,38 @@ constexpr int kMaxTplCons = kMaxArms * (2 * kMaxSegs + 1);        // 152
 constexpr int kMaxTplPts = 8 + 2 * kMaxArms * kMaxSegs;           // 152
 constexpr int kMaxTplLevels = 64;
 
+// Solve schedules per lane-group size: 32, 16 and 8 lanes per creature.
+constexpr int kSchedules = 3;
+constexpr int schedule_index(int lanes) { return lanes == 32 ? 0 : lanes == 16 ? 1 : 2; }
+
+// One solve schedule of the constraint list: the constraint slots level by
+// level (each level body-disjoint and of one constraint type) with their
+// static data.
+struct Schedule {
+  int nlv = 0;
+  std::vector<int> lvl;                 // nlv + 1 level offsets
+  std::vector<int> ab;                  // local a | local b << 16 (b = 0xffff: world)
+  std::vector<int> type;                // 0 pin, 1 angle, 2 grip
+  std::vector<int> motor;               // a * segs + j for motor j of arm a, else -1
+  std::vector<float> lax, lay, lbx, lby, rest, minA, maxA;
+  std::vector<int> arm_grip;            // slot of each arm's grip
+};
+
 struct Template {
   int arms = 0, segs = 0;
   int nb = 0, nc = 0, np = 0, nlv = 0;
   // bodies
   std::vector<float> im, ii;            // f32 as uploaded (gpuworld.js:258-259)
   std::vector<int> boff, bcnt;          // collision points per body
-  // constraints in schedule order (level by level)
+  // constraints in schedule order (level by level), as in sched[0]
   std::vector<int> ab;                  // local a | local b << 16 (b = 0xffff: world)
   std::vector<int> type;                // 0 pin, 1 angle, 2 grip
   std::vector<float> lax, lay, lbx, lby, rest, minA, maxA;
   std::vector<int> motor;               // a * segs + j for motor j of arm a, else -1
   std::vector<int> lvl;                 // nlv + 1 level offsets
+  // per lane-group size (schedule_index): the same constraints in levels
+  // balanced for that many lanes
+  Schedule sched[kSchedules];
   // collision points grouped per body in creation order
   std::vector<float> plx, ply, pr;
   std::vector<int> pbody;
