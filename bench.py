@@ -419,7 +419,7 @@ def main():
     if args.shape:
         best = tuple(int(v) for v in args.shape.split(","))
     else:
-        for shp in ((16, 8, 0), (16, 4, 4), (8, 8, 0), (32, 8, 0), (16, 16, 1)):
+        for shp in ((8, 8, 0), (8, 16, 1), (16, 8, 0), (16, 16, 1), (32, 8, 0)):
             eng.set_launch(shp[1], shp[2], lanes_per_creature=shp[0])
             eng.restore()
             eng.run(64)

@@ -758,14 +758,15 @@ int launch_part(kr_batch *b, Part &p, int max_steps, bool timed) {
     return b->fail(KR_ERR_STATE, "policy control without kr_batch_set_policy");
   if (b->auto_shape && p.dirty) {
     // few creatures (under 16 per SM): one per warp, the shortest step
-    // latency; else two per warp, the most creature-steps per issue slot
+    // latency; up to 96 per SM two per warp; beyond, four per warp, the
+    // most creature-steps per issue slot (measured on the 16k workload)
     long live = 0;
     if (p.all) {
       for (int s = 0; s < b->capacity; s++) live += b->h_meta[s].horizon > 0 && b->h_remaining[s] > 0;
     } else {
       for (int s : p.slots) live += b->h_remaining[s] > 0;
     }
-    const int g = live < 16L * b->n_sm ? 32 : 16, w = g == 32 ? 4 : 8;
+    const int g = live < 16L * b->n_sm ? 32 : live < 96L * b->n_sm ? 16 : 8, w = g == 32 ? 4 : 8;
     if (g != b->G || w != b->W) {
       b->G = g;
       b->W = w;
