@@ -241,12 +241,12 @@ def reference_arm(args):
     print(json.dumps(line), flush=True)
 
 
-def served_uneven(serve, w, shape, chunk, sessions):
+def served_uneven(serve, w, chunk, sessions):
     """The mixed workload through the rollout server's C ABI with host
     buffers: one request per creature (its own pose, control stream and
-    horizon), all submitted at once; results read back to the host."""
-    srv = serve.Server(w.maps, 8 << 30, max_slots=w.n, chunk_steps=chunk, policy=False,
-                       lanes=shape[0], warps=shape[1], ctas=shape[2])
+    horizon), all submitted at once; results read back to the host.  The
+    server picks each round's launch shape from its partition's live count."""
+    srv = serve.Server(w.maps, 8 << 30, max_slots=w.n, chunk_steps=chunk, policy=False)
     xs, ys, an = (np.ascontiguousarray(v, dtype=np.float64) for v in (w.x, w.y, w.angle))
     seeds = np.ascontiguousarray(w.seed, dtype=np.uint32)
     out = []
@@ -265,7 +265,7 @@ def served_uneven(serve, w, shape, chunk, sessions):
     return out
 
 
-def served_es_stream(serve, w, shape, chunk, n_req, rate, seed=0):
+def served_es_stream(serve, w, chunk, n_req, rate, seed=0):
     """ES evaluation requests (mirrored populations 8-512, horizons
     300-3000, body shapes and maps of the mixed workload, fused policy with
     theta ~ N(0, 0.1^2), sigma 0.02) arriving as a Poisson stream."""
@@ -281,8 +281,7 @@ def served_es_stream(serve, w, shape, chunk, n_req, rate, seed=0):
                          theta=rng.normal(0, 0.1, serve.policy_params(arms, segs)).astype(np.float32),
                          sigma=0.02, seed=k + 1, arrival=t))
     units = sum(r["population"] * r["horizon"] for r in reqs)
-    srv = serve.Server(w.maps, 8 << 30, max_slots=16384, chunk_steps=chunk, policy=True,
-                       lanes=shape[0], warps=shape[1], ctas=shape[2])
+    srv = serve.Server(w.maps, 8 << 30, max_slots=16384, chunk_steps=chunk, policy=True)
     t0 = srv.now() + 0.02
     ids = []
     for r in reqs:
@@ -478,7 +477,7 @@ def main():
     # end to end: the workload served through the rollout server's C ABI with
     # host buffers (requests in, results out), p50/p99 rollout latency
     chunk = args.chunk
-    sess = served_uneven(serve, w, best, chunk, 1 + max(1, min(args.steps, 2)))[1:]
+    sess = served_uneven(serve, w, chunk, 1 + max(1, min(args.steps, 2)))[1:]
     e2e_s = all_max(sum(x["wall_s"] for x in sess))
     lat = np.concatenate([x["lat"] for x in sess])
     clocks = sampler.stop()
@@ -490,7 +489,7 @@ def main():
            "p99_rollout_ms": float(np.percentile(lat, 99) * 1e3), "chunk_steps": chunk}
 
     if not args.no_es and rank == 0:
-        extra["served_es_stream"] = served_es_stream(serve, w, best, chunk, args.es_requests, 200.0)
+        extra["served_es_stream"] = served_es_stream(serve, w, chunk, args.es_requests, 200.0)
     if not args.no_config1 and rank == 0:
         extra["plain_dropin_1024"] = config1_forms(torch, stream)
 
