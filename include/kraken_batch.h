@@ -137,8 +137,9 @@ int kr_probe_fp32_rate(double *fma_per_s);
  * per SM (0 = 16 / warps).  A CTA gets an equal share of the SM's shared
  * memory; a group of one body template holds as many creatures as fit in it.
  * Until this is called the engine picks the shape per launch: 32 lanes x 4
- * warps below 16 live creatures per SM, 16 lanes x 8 warps below 96, else
- * 8 lanes x 8 warps.  Results do not depend on the launch shape. */
+ * warps below 16 live creatures per SM, 16 lanes x 8 warps below 96 (8
+ * lanes when most creatures run the fused policy or an observation ring is
+ * kept), else 8 lanes x 8 warps.  Results do not depend on the launch shape. */
 int kr_batch_set_launch(kr_batch *b, int32_t lanes_per_creature, int32_t warps_per_cta,
                         int32_t ctas_per_sm);
 

@@ -69,9 +69,12 @@ __host__ __device__ constexpr int r4(int n) { return (n + 3) & ~3; }
 __host__ __device__ inline int tpl_smem_words(int nb, int nc, int np) {
   return 5 * r4(nb) + 11 * r4(nc) + 4 * r4(np) + kLvlWords + kArmWords;
 }
-// one creature: bodies, grip and motor state, lambda, collision scratch
+// one creature: predicted bodies and their sin/cos, grip and motor state,
+// lambda, collision scratch (the committed state -- positions, angles,
+// velocities -- is read and written in place in the slot's HBM block: it is
+// touched once per substep, not in the solver's inner loops)
 __host__ __device__ inline int creature_smem_words(int nb, int nc, int np, int arms, int segs) {
-  return 11 * r4(nb) + 2 * r4(nc) + r4(arms * segs) + r4(arms * segs + arms) + 4 * arms + 3 * r4(np) +
+  return 5 * r4(nb) + 2 * r4(nc) + r4(arms * segs) + r4(arms * segs + arms) + 4 * arms + 3 * r4(np) +
          kr::kMaxCulled / 2;
 }
 
@@ -112,11 +115,13 @@ struct CreatureSmem {
 };
 
 __device__ inline void carve_creature(kr::Island &S, CreatureSmem &X, const TplSmem &P, float *p,
-                                      const TplDev &td) {
+                                      float *state, const TplDev &td) {
   const int mb = r4(td.nb), mc = r4(td.nc), mp = r4(td.np), AS = td.arms * td.segs;
-  S.px = p; p += mb; S.py = p; p += mb; S.ppx = p; p += mb; S.ppy = p; p += mb;
-  S.vx = p; p += mb; S.vy = p; p += mb; S.ang = p; p += mb; S.angP = p; p += mb;
-  S.av = p; p += mb; S.bs = p; p += mb; S.bc = p; p += mb;
+  // committed state in place in the slot's block (SoA, kBodyPad per field)
+  S.px = state; S.py = state + kBodyPad; S.vx = state + 2 * kBodyPad; S.vy = state + 3 * kBodyPad;
+  S.ang = state + 4 * kBodyPad; S.av = state + 5 * kBodyPad;
+  S.ppx = p; p += mb; S.ppy = p; p += mb; S.angP = p; p += mb;
+  S.bs = p; p += mb; S.bc = p; p += mb;
   S.lamX = p; p += mc; S.lamY = p; p += mc;
   S.lam = S.lamX;  // pins use lamX/lamY, angles lam: never both on one slot
   S.tgt_m = p; p += r4(AS);
@@ -285,20 +290,15 @@ __device__ void run_creature(const BatchArgs &A, const TplDev &td, int nlv, cons
   const int lane = L.lane;
   kr::Island S;
   CreatureSmem X;
-  carve_creature(S, X, P, base, td);
+  carve_creature(S, X, P, base, A.state + (size_t)slot * kStateStride, td);
   S.nlv = nlv;
   SlotMeta m = A.meta[slot];
   const int steps = min(A.max_steps, m.horizon - m.step);
   if (steps <= 0) return;
   const int arms = td.arms, AS = td.arms * td.segs;
-  const float *st = A.state + (size_t)slot * kStateStride;
   float4 *gst = A.grip + (size_t)slot * KR_BATCH_MAX_ARMS;
   float2 *glam = A.glam + (size_t)slot * KR_BATCH_MAX_ARMS;
   double *cdp = A.cd + (size_t)slot * KR_BATCH_MAX_ARMS;
-  for (int i = lane; i < td.nb; i += G) {
-    S.px[i] = st[i]; S.py[i] = st[kBodyPad + i]; S.vx[i] = st[2 * kBodyPad + i];
-    S.vy[i] = st[3 * kBodyPad + i]; S.ang[i] = st[4 * kBodyPad + i]; S.av[i] = st[5 * kBodyPad + i];
-  }
   for (int k = lane; k < td.nc; k += G) { S.lamX[k] = 0.f; S.lamY[k] = 0.f; }
   S.comp_m = m.comp;
   double cd = 0.0;  // reflex cooldown of arm `lane`
@@ -386,12 +386,7 @@ __device__ void run_creature(const BatchArgs &A, const TplDev &td, int nlv, cons
     }
     m.step = t + 1;
   }
-  // write back
-  float *sw = A.state + (size_t)slot * kStateStride;
-  for (int i = lane; i < td.nb; i += G) {
-    sw[i] = S.px[i]; sw[kBodyPad + i] = S.py[i]; sw[2 * kBodyPad + i] = S.vx[i];
-    sw[3 * kBodyPad + i] = S.vy[i]; sw[4 * kBodyPad + i] = S.ang[i]; sw[5 * kBodyPad + i] = S.av[i];
-  }
+  // write back (the committed state is already in place)
   if (lane < arms) {
     const int k = P.arm_grip[lane];
     gst[lane] = reinterpret_cast<const float4 *>(S.anc)[lane];
@@ -759,14 +754,23 @@ int launch_part(kr_batch *b, Part &p, int max_steps, bool timed) {
   if (b->auto_shape && p.dirty) {
     // few creatures (under 16 per SM): one per warp, the shortest step
     // latency; up to 96 per SM two per warp; beyond, four per warp, the
-    // most creature-steps per issue slot (measured on the 16k workload)
-    long live = 0;
+    // most creature-steps per issue slot (measured on the 16k workload).
+    // Proprioception and the fused policy run per arm, so creatures that
+    // need them pack four per warp from 16 per SM on.
+    long live = 0, per_arm = 0;
+    auto count = [&](int s) {
+      if (b->h_remaining[s] <= 0 || b->h_meta[s].horizon <= 0) return;
+      live++;
+      per_arm += b->h_meta[s].ctrl == KR_CTRL_POLICY;
+    };
     if (p.all) {
-      for (int s = 0; s < b->capacity; s++) live += b->h_meta[s].horizon > 0 && b->h_remaining[s] > 0;
+      for (int s = 0; s < b->capacity; s++) count(s);
     } else {
-      for (int s : p.slots) live += b->h_remaining[s] > 0;
+      for (int s : p.slots) count(s);
     }
-    const int g = live < 16L * b->n_sm ? 32 : live < 96L * b->n_sm ? 16 : 8, w = g == 32 ? 4 : 8;
+    const bool arm_heavy = b->d.obs_ring > 0 || 2 * per_arm > live;
+    const int g = live < 16L * b->n_sm ? 32 : (arm_heavy || live >= 96L * b->n_sm) ? 8 : 16;
+    const int w = g == 32 ? 4 : 8;
     if (g != b->G || w != b->W) {
       b->G = g;
       b->W = w;
