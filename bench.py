@@ -200,10 +200,8 @@ def ops_per_creature_step(w, sample: int = 48, steps: int = 60) -> float:
 # distributed plumbing
 # ---------------------------------------------------------------------------
 def dist_env():
-    rank = int(os.environ.get("RANK", 0))
-    world = int(os.environ.get("WORLD_SIZE", 1))
-    local = int(os.environ.get("LOCAL_RANK", 0))
-    return rank, world, local
+    from kraken_3_gpu_b200 import replicas
+    return replicas.dist_env()
 
 
 def reference_arm(args):
@@ -376,31 +374,21 @@ def main():
         return
     import torch
 
+    from kraken_3_gpu_b200 import batch, replicas, serve, workloads
+
     rank, world, local = dist_env()
     torch.cuda.set_device(local)
     # one explicit stream for the engine, the events and the copies
     torch.cuda.set_stream(torch.cuda.Stream())
-    if world > 1:
-        import datetime
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
-                                device_id=torch.device("cuda", local))
+    replicas.init("nccl", world, local)
 
     def barrier():
-        if world > 1:
-            torch.distributed.barrier()
-        torch.cuda.synchronize()
+        replicas.barrier(world)
 
     def all_max(x: float) -> float:
-        if world == 1:
-            return x
-        t = torch.tensor([x], device="cuda", dtype=torch.float64)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        return float(t.item())
+        return replicas.max_over_ranks(x, world)
 
-    from kraken_3_gpu_b200 import batch, serve, workloads
-
-    w = workloads.uneven(n=args.n, n_maps=args.maps, seed=args.seed + 1000 * rank,
+    w = workloads.uneven(n=args.n, n_maps=args.maps, seed=replicas.shard_seed(args.seed, rank),
                          h_min=args.hmin, h_max=args.hmax)
     units = w.creature_steps()
     max_h = int(w.horizon.max())
@@ -450,7 +438,7 @@ def main():
     elapsed_ms = e0.elapsed_time(e1)
     kms = eng.last_ms()  # the last rollout's kernel alone (events on its stream)
     t_max = all_max(elapsed_ms)
-    value = world * units * args.steps / (t_max / 1000.0)
+    value = replicas.job_rate(units * args.steps, world, t_max / 1000.0)
     ms_per_step = t_max / args.steps
     gpu_launches = args.steps
 
@@ -540,8 +528,7 @@ def main():
         }
         print(json.dumps(line), flush=True)
     eng.close()
-    if world > 1:
-        torch.distributed.destroy_process_group()
+    replicas.finish(world)
 
 
 if __name__ == "__main__":
