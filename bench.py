@@ -405,15 +405,11 @@ def main():
     tune = {}
     if args.shape:
         best = tuple(int(v) for v in args.shape.split(","))
+        eng.set_launch(best[1], best[2], lanes_per_creature=best[0])
     else:
-        for shp in ((8, 8, 0), (8, 16, 1), (16, 8, 0), (16, 16, 1), (32, 8, 0)):
-            eng.set_launch(shp[1], shp[2], lanes_per_creature=shp[0])
-            eng.restore()
-            eng.run(64)
-            eng.sync()
-            tune[shp] = eng.last_ms()
-        best = min(tune, key=tune.get)
-    eng.set_launch(best[1], best[2], lanes_per_creature=best[0])
+        g, wp, c, ms = eng.autotune(64)  # the library's autotuner: slots left as they were
+        best = (g, wp, c)
+        tune = {best: ms}
 
     # warm-up: full rollouts
     for _ in range(args.warmup):

@@ -148,6 +148,15 @@ int kr_batch_set_launch(kr_batch *b, int32_t lanes_per_creature, int32_t warps_p
 int kr_batch_get_launch(kr_batch *b, int32_t *lanes_per_creature, int32_t *warps_per_cta,
                         int32_t *ctas_per_sm, int32_t *smem_bytes);
 
+/* Autotuner: runs `steps` env steps of the live slots with each candidate
+ * launch shape (8, 16 and 32 lanes per creature with 4-16 warps per CTA),
+ * puts every slot's state back after each trial (slots end as they were;
+ * the kr_batch_snapshot copy is not touched) and keeps the fastest shape
+ * (kr_batch_set_launch).  The chosen shape and its time are returned; any
+ * pointer may be NULL.  Synchronous. */
+int kr_batch_autotune(kr_batch *b, int32_t steps, int32_t *lanes_per_creature, int32_t *warps_per_cta,
+                      int32_t *ctas_per_sm, float *best_ms);
+
 /* Device time of the last kr_batch_run launch in ms (synchronous). */
 int kr_batch_last_ms(kr_batch *b, float *ms);
 

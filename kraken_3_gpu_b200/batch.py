@@ -66,6 +66,7 @@ def _lib():
         "kr_batch_read_controls": (C.c_int, [vp, i32, i32, _F32P]),
         "kr_batch_set_launch": (C.c_int, [vp, i32, i32, i32]),
         "kr_batch_get_launch": (C.c_int, [vp, _I32P, _I32P, _I32P, _I32P]),
+        "kr_batch_autotune": (C.c_int, [vp, i32, _I32P, _I32P, _I32P, _F32P]),
         "kr_batch_last_ms": (C.c_int, [vp, _F32P]),
         "kr_batch_sync": (C.c_int, [vp]),
         "kr_batch_set_stream": (C.c_int, [vp, vp]),
@@ -169,6 +170,15 @@ class BatchEngine:
         CTAs per SM (0: 16 / warps).  Results do not depend on it."""
         _check(_lib().kr_batch_set_launch(self.h, lanes_per_creature, warps_per_cta, ctas_per_sm),
                self.h)
+
+    def autotune(self, steps=64):
+        """Time every candidate launch shape on `steps` env steps of the live
+        slots (state put back after each trial), keep the fastest; returns
+        (lanes_per_creature, warps_per_cta, ctas_per_sm, ms)."""
+        v = [C.c_int32() for _ in range(3)]
+        ms = C.c_float()
+        _check(_lib().kr_batch_autotune(self.h, steps, *[C.byref(x) for x in v], C.byref(ms)), self.h)
+        return v[0].value, v[1].value, v[2].value, ms.value
 
     def get_launch(self):
         v = [C.c_int32() for _ in range(4)]

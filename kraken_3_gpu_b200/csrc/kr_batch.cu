@@ -1178,6 +1178,77 @@ extern "C" int kr_batch_run_graph(kr_batch *b, int32_t max_steps, int32_t launch
   return KR_OK;
 }
 
+extern "C" int kr_batch_autotune(kr_batch *b, int32_t steps, int32_t *lanes_out, int32_t *warps_out,
+                                 int32_t *ctas_out, float *best_ms_out) {
+  if (!b) return KR_ERR_INVALID;
+  if (steps < 1) return b->fail(KR_ERR_INVALID, "autotune steps < 1");
+  static const int kCand[][3] = {{8, 8, 0}, {8, 16, 1}, {8, 4, 4}, {16, 8, 0}, {16, 16, 1}, {32, 4, 0}, {32, 8, 0}};
+  const size_t C = (size_t)b->capacity;
+  // scratch copy of every slot (the trials run, then the state goes back)
+  float *t_state = nullptr, *t_ctrl = nullptr;
+  float4 *t_grip = nullptr;
+  float2 *t_glam = nullptr;
+  double *t_cd = nullptr;
+  SlotMeta *t_meta = nullptr;
+  cudaError_t e = cudaMalloc(&t_state, C * kStateStride * sizeof(float));
+  if (e == cudaSuccess) e = cudaMalloc(&t_grip, C * KR_BATCH_MAX_ARMS * sizeof(float4));
+  if (e == cudaSuccess) e = cudaMalloc(&t_glam, C * KR_BATCH_MAX_ARMS * sizeof(float2));
+  if (e == cudaSuccess) e = cudaMalloc(&t_cd, C * KR_BATCH_MAX_ARMS * sizeof(double));
+  if (e == cudaSuccess) e = cudaMalloc(&t_ctrl, C * kCtrlStride * sizeof(float));
+  if (e == cudaSuccess) e = cudaMalloc(&t_meta, C * sizeof(SlotMeta));
+  auto copy_slots = [&](bool save) {
+    cudaError_t r = cudaSuccess;
+    auto cp = [&](void *keep, void *live, size_t bytes) {
+      if (r == cudaSuccess)
+        r = cudaMemcpyAsync(save ? keep : live, save ? live : keep, bytes, cudaMemcpyDeviceToDevice, b->stream);
+    };
+    cp(t_state, b->d_state, C * kStateStride * sizeof(float));
+    cp(t_grip, b->d_grip, C * KR_BATCH_MAX_ARMS * sizeof(float4));
+    cp(t_glam, b->d_glam, C * KR_BATCH_MAX_ARMS * sizeof(float2));
+    cp(t_cd, b->d_cd, C * KR_BATCH_MAX_ARMS * sizeof(double));
+    cp(t_ctrl, b->d_ctrl, C * kCtrlStride * sizeof(float));
+    cp(t_meta, b->d_meta, C * sizeof(SlotMeta));
+    return r;
+  };
+  const std::vector<int> rem0 = b->h_remaining;
+  const int G0 = b->G, W0 = b->W, C0 = b->ctas_per_sm;
+  const bool auto0 = b->auto_shape;
+  int best = -1, rc = KR_OK;
+  float best_ms = 0.f;
+  if (e == cudaSuccess) e = copy_slots(true);
+  for (int c = 0; c < (int)(sizeof(kCand) / sizeof(kCand[0])) && e == cudaSuccess && rc == KR_OK; c++) {
+    rc = kr_batch_set_launch(b, kCand[c][0], kCand[c][1], kCand[c][2]);
+    if (rc != KR_OK) break;
+    b->main.dirty = true;
+    rc = launch_part(b, b->main, steps, true);
+    if (rc == KR_ERR_CAPACITY) { rc = KR_OK; b->h_remaining = rem0; e = copy_slots(false); continue; }
+    if (rc != KR_OK) break;
+    float ms = 0.f;
+    e = cudaEventSynchronize(b->main.ev1);
+    if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, b->main.ev0, b->main.ev1);
+    if (e == cudaSuccess && (best < 0 || ms < best_ms)) { best = c; best_ms = ms; }
+    b->h_remaining = rem0;
+    if (e == cudaSuccess) e = copy_slots(false);
+  }
+  if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
+  cudaFree(t_state); cudaFree(t_grip); cudaFree(t_glam); cudaFree(t_cd); cudaFree(t_ctrl); cudaFree(t_meta);
+  b->h_remaining = rem0;
+  b->main.dirty = true;
+  if (rc != KR_OK) return rc;
+  if (e != cudaSuccess) return b->cuda_fail(e, "kr_batch_autotune");
+  if (best < 0) {  // nothing live: keep the shape as it was
+    b->G = G0; b->W = W0; b->ctas_per_sm = C0; b->auto_shape = auto0; b->shape_dirty = true;
+  } else {
+    rc = kr_batch_set_launch(b, kCand[best][0], kCand[best][1], kCand[best][2]);
+    if (rc != KR_OK) return rc;
+  }
+  if (lanes_out) *lanes_out = b->G;
+  if (warps_out) *warps_out = b->W;
+  if (ctas_out) *ctas_out = b->ctas_per_sm;
+  if (best_ms_out) *best_ms_out = best_ms;
+  return KR_OK;
+}
+
 extern "C" int kr_batch_live(kr_batch *b, int32_t *live) {
   if (!b || !live) return KR_ERR_INVALID;
   std::vector<SlotMeta> m(b->capacity);

@@ -188,3 +188,28 @@ def test_policy_individual_shared_by_two_body_shapes_is_rejected():
         eng.set_policy(weights, np.zeros(w.n, np.int32))
     assert "two body shapes" in str(e.value)
     eng.close()
+
+
+def test_autotune_leaves_slots_as_they_were():
+    w = _small_uneven(n=48, h=40)
+    ref = batch.BatchEngine(w.maps, w.n)
+    workloads.spawn_all(ref, w)
+    ref.run(15)
+    ref.run(25)
+    eng = batch.BatchEngine(w.maps, w.n)
+    workloads.spawn_all(eng, w)
+    eng.run(15)
+    before = eng.read_state()
+    lanes, warps, ctas, ms = eng.autotune(10)
+    assert lanes in (8, 16, 32) and ms > 0
+    assert eng.get_launch()["lanes_per_creature"] == lanes
+    after = eng.read_state()
+    for f in ("px", "py", "ang", "vx", "vy", "av", "grips", "steps"):
+        assert np.array_equal(before[f], after[f]), f
+    eng.run(25)
+    a, b = ref.read_state(), eng.read_state()
+    for f in ("px", "py", "ang", "grips", "steps"):
+        assert np.array_equal(a[f], b[f]), f
+    assert np.array_equal(ref.read_fitness(), eng.read_fitness())
+    ref.close()
+    eng.close()
