@@ -118,8 +118,21 @@ int kr_batch_read_obs(kr_batch *b, int32_t first, int32_t n, float *obs);
 int kr_batch_read_controls(kr_batch *b, int32_t first, int32_t n, float *controls);
 
 /* Per-slot accumulators (synchronous): n x 4 f64 -- path length of the
- * mantle, x and y of the mantle, attach events. */
+ * mantle, x and y of the mantle, attach events (arms newly anchored after a
+ * step). */
 int kr_batch_read_fitness(kr_batch *b, int32_t first, int32_t n, double *out);
+
+/* The reference's fitness metrics of every slot (synchronous): n x
+ * KR_METRIC_WORDS f64, accumulated on the device after every env step as
+ * postStep does (src/sim/core.js:297-356, f64 on the f32 state), with the
+ * score of src/sim/fitness.js:115-172 (no prey; maxAngSpeed 18, dt 1/60).
+ * The spawn reach is measureReach (fitness.js:74-88) of the spawn point on
+ * the map's rects as given (f32 values), rays up to 3.5 reaches of the body.
+ * Words: score, steps, path length, max displacement, spawn reach, angular
+ * accumulation, forward progress, grip-pull progress, anchored steps, free
+ * move, energy spent, grip cycles, strides, attach events, mantle x, y. */
+#define KR_METRIC_WORDS 16
+int kr_batch_read_metrics(kr_batch *b, int32_t first, int32_t n, double *out);
 
 /* Keep a device copy of every slot's state (bodies, grips, reflex
  * cooldowns, current controls, step counters) and put it back later -- the

@@ -38,6 +38,7 @@
 #include <stdint.h>
 
 #include "kraken_b200.h"
+#include "kraken_batch.h"
 
 #ifdef __cplusplus
 extern "C" {
@@ -78,9 +79,10 @@ typedef struct kr_request {
   double arrival;               /* server time the request arrives (< 0: now) */
 } kr_request;
 
-/* results per individual: path length of the mantle, final mantle x, y,
- * attach events */
-#define KR_RESULT_WORDS 4
+/* results per individual: the metrics record of kraken_batch.h
+ * (KR_METRIC_WORDS f64: the reference's score first, then postStep's
+ * accumulators, the final mantle position last) */
+#define KR_RESULT_WORDS KR_METRIC_WORDS
 
 typedef struct kr_server_stats {
   int32_t capacity;             /* slots */

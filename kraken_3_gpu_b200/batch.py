@@ -26,6 +26,12 @@ OBS_STRIDE = 56
 CTRL_STRIDE = MAX_ARMS * (MAX_SEGS + 1)
 POLICY_HIDDEN = 64
 CONTROL_MODES = {"stream": 0, "buffer": 1, "policy": 2}
+# the reference's fitness metrics (postStep, src/sim/core.js:297-356) and score
+# (src/sim/fitness.js:115-172), in kr_batch_read_metrics order
+METRIC_FIELDS = ("score", "steps", "pathLen", "maxDisplacement", "spawnReach", "angularAccum",
+                 "forwardProg", "gripPullProg", "anchoredSteps", "freeMove", "energySpent",
+                 "gripCycles", "strides", "attachEvents", "x", "y")
+METRIC_WORDS = len(METRIC_FIELDS)
 
 _F32P = C.POINTER(C.c_float)
 _F64P = C.POINTER(C.c_double)
@@ -64,6 +70,7 @@ def _lib():
         "kr_batch_read_obs": (C.c_int, [vp, i32, i32, _F32P]),
         "kr_batch_read_fitness": (C.c_int, [vp, i32, i32, _F64P]),
         "kr_batch_read_controls": (C.c_int, [vp, i32, i32, _F32P]),
+        "kr_batch_read_metrics": (C.c_int, [vp, i32, i32, _F64P]),
         "kr_batch_set_launch": (C.c_int, [vp, i32, i32, i32]),
         "kr_batch_get_launch": (C.c_int, [vp, _I32P, _I32P, _I32P, _I32P]),
         "kr_batch_autotune": (C.c_int, [vp, i32, _I32P, _I32P, _I32P, _F32P]),
@@ -235,6 +242,14 @@ class BatchEngine:
         n = self.capacity - first if n is None else n
         out = np.zeros((n, CTRL_STRIDE), dtype=np.float32)
         _check(_lib().kr_batch_read_controls(self.h, first, n, out.ctypes.data_as(_F32P)), self.h)
+        return out
+
+    def read_metrics(self, first=0, n=None):
+        """(n, METRIC_WORDS) f64: the reference's score and postStep metrics
+        of each slot (METRIC_FIELDS order)."""
+        n = self.capacity - first if n is None else n
+        out = np.zeros((n, METRIC_WORDS), dtype=np.float64)
+        _check(_lib().kr_batch_read_metrics(self.h, first, n, out.ctypes.data_as(_F64P)), self.h)
         return out
 
     def read_fitness(self, first=0, n=None):

@@ -51,7 +51,8 @@ struct BatchArgs {
   int ctrl_period;
   float *obs;            // capacity x ring x KR_OBS_STRIDE
   int obs_ring;
-  double slip_max, cooldown, inv_h64, dt;
+  double slip_max, cooldown, inv_h64, dt, h64;
+  int substeps;
   // policy
   const float *pw;       // n_individuals x pw_stride, device layout (see policy())
   const int *pw_idx;     // individual of each slot
@@ -346,7 +347,6 @@ __device__ void run_creature(const BatchArgs &A, const TplDev &td, int nlv, cons
       const double lim = (mo % td.segs) == 0 ? kPiD * 0.62 : kPiD * 0.42;
       S.tgt_m[mo] = (float)fmax(-lim, fmin(lim, (double)X.ctrl[mo]));
     }
-    bool attached_now = false;
     if (lane < arms) {
       const int a = lane, k = P.arm_grip[a], tip = P.arm_tip[a];
       float *an = S.anc + 4 * a;
@@ -363,7 +363,6 @@ __device__ void run_creature(const BatchArgs &A, const TplDev &td, int nlv, cons
             an[2] = (float)(40.0 + 860.0 * adh);
             an[3] = 0.f;
             S.lamX[k] = 0.f; S.lamY[k] = 0.f;
-            attached_now = true;
           } else {
             c = A.cooldown;
           }
@@ -374,14 +373,37 @@ __device__ void run_creature(const BatchArgs &A, const TplDev &td, int nlv, cons
       }
       cd = c;
     }
-    m.attach_events += __popc(L.ballot(attached_now));
     L.sync();
     // 4. the XPBD step
     kr::island_step<kr::CompactAccess, G>(A.K, S, rects, nR, cull_d, L);
-    // 5. bookkeeping
+    // 5. postStep, core.js:297-356 (f64 on the f32 state, as the
+    //    reference's hybrid loop runs it on the mirrored state)
     if (lane == 0) {
-      const double x = S.px[0], y = S.py[0];
-      m.path_len += hypot(x - m.last_x, y - m.last_y);
+      const double x = S.px[0], y = S.py[0], angle = S.ang[0], av = S.av[0];
+      const double dx = x - m.last_x, dy = y - m.last_y;
+      const double step_dist = hypot(dx, dy);
+      m.path_len += step_dist;
+      m.angular_accum += fabs(av) * A.h64 * A.substeps;
+      const double fa = angle - kPiD * 0.5;
+      const double fwd = dx * cos(fa) + dy * sin(fa);
+      if (fwd > 0) m.forward_prog += fwd;
+      int anchored = 0;
+      unsigned now = 0;
+      for (int a = 0; a < arms; a++)
+        if (S.anc[4 * a + 3] == 0.f) { anchored++; now |= 1u << a; }
+      const double d_spawn = hypot(x - m.spawn_x, y - m.spawn_y);
+      if (anchored > 0) {
+        m.anchored_steps++;
+        if (d_spawn > m.spawn_dist_max) { m.grip_pull_prog += d_spawn - m.spawn_dist_max; m.spawn_dist_max = d_spawn; }
+      }
+      if (anchored == 0 && step_dist > 0.3) m.free_move += step_dist;
+      m.energy += (m.tone_d * 0.0006 + step_dist * 0.0004) * arms;
+      if (anchored > 0 && !(m.arm_anchored & 0x100u)) m.grip_cycles++;
+      const int newly = __popc(now & ~m.arm_anchored & 0xffu);
+      m.attach_events += newly;
+      if (newly > 0 && anchored - newly > 0) m.strides += newly;
+      m.arm_anchored = now | (anchored > 0 ? 0x100u : 0u);
+      m.max_disp = fmax(m.max_disp, d_spawn);
       m.last_x = x; m.last_y = y;
     }
     m.step = t + 1;
@@ -489,6 +511,81 @@ double tpl_cost(const TplDev &d) { return (double)d.nc + 0.5 * (double)d.np; }
 namespace krb {
 
 cudaStream_t part_stream(const kr_batch *b, const Part &p) { return p.stream ? p.stream : b->stream; }
+
+// signed distance of makeSdf (src/world/map.js:91-118) in f64
+static bool sdf_d(const double *r, int n, double x, double y, double *d) {
+  double best = INFINITY;
+  for (int i = 0; i < n; i++, r += 4) {
+    const double cx = std::max(r[0], std::min(x, r[0] + r[2]));
+    const double cy = std::max(r[1], std::min(y, r[1] + r[3]));
+    const double dx = x - cx, dy = y - cy, d2 = dx * dx + dy * dy;
+    if (d2 > 1e-12) {
+      if (d2 < best * best) best = std::sqrt(d2);
+    } else {
+      const double m = std::min(std::min(x - r[0], r[0] + r[2] - x), std::min(y - r[1], r[1] + r[3] - y));
+      if (-m < best) best = -m;
+    }
+  }
+  if (!std::isfinite(best)) return false;
+  *d = best;
+  return true;
+}
+
+// measureReach, src/sim/fitness.js:74-88: the free space around a spawn
+// point along 16 rays (12 px steps up to 3.5 arm reaches of the body)
+double measure_reach(const double *rects, int n, double reach, double x, double y) {
+  double sum = 0, best = 0;
+  for (int k = 0; k < 16; k++) {
+    const double a = ((double)k / 16) * 3.141592653589793 * 2;
+    double d = 0, h = 0;
+    while (d < reach * 3.5) {
+      d += 12;
+      if (!sdf_d(rects, n, x + std::cos(a) * d, y + std::sin(a) * d, &h) || h <= 0) break;
+    }
+    sum += d;
+    if (d > best) best = d;
+  }
+  return std::max(70.0, (sum / 16) * 0.55 + best * 0.45);
+}
+
+// score, src/sim/fitness.js:115-172 without prey (preyHit = preyNear = 0),
+// maxAngSpeed 18 and dt 1/60 as the trainer calls it: the terms in
+// TERM_ORDER, summed in f64 in that order
+static double fitness_score(const SlotMeta &c) {
+  const double steps = std::max(1, c.step), path = c.path_len, disp = c.max_disp;
+  const double reach = c.spawn_reach > 0 ? c.spawn_reach : 300;
+  const double reach_frac = std::min(1.2, disp / reach);
+  const double directed = path > 1 ? std::min(1.0, disp / path) : 0;
+  const double spin_budget = steps * 18 * (1.0 / 60);
+  const double heading_hold = 1 - std::min(1.0, c.angular_accum / std::max(1e-6, spin_budget));
+  const double mean_speed = path / steps / 60;
+  const double efficiency = c.forward_prog / std::max(0.5, c.energy > 0 ? c.energy : 0.5);
+  const double progress_base = c.grip_pull_prog * 2.6 + reach_frac * 320;
+  const double stride_frac = std::min((double)c.strides, 60.0) / 60.0;
+  const double prog_gate = std::min(1.0, disp / std::max(1e-6, 0.25 * reach));
+  const double t[12] = {c.grip_pull_prog * 2.6,
+                        progress_base * 0.5 * stride_frac,
+                        reach_frac * 320,
+                        directed * 70 * prog_gate,
+                        heading_hold * 28 * prog_gate,
+                        std::min(1.0, mean_speed) * 14 * prog_gate,
+                        std::min(20.0, efficiency) * 3 * prog_gate,
+                        -(c.angular_accum * 0.55 * 0.02),
+                        -(c.free_move * 0.05),
+                        -(c.energy * 0.30),
+                        0.0,
+                        0.0};
+  double s = 0;
+  for (double v : t) s += v;
+  return std::isfinite(s) ? s : 0;
+}
+
+void slot_metrics(const SlotMeta &m, double *o) {
+  o[0] = fitness_score(m); o[1] = m.step; o[2] = m.path_len; o[3] = m.max_disp; o[4] = m.spawn_reach;
+  o[5] = m.angular_accum; o[6] = m.forward_prog; o[7] = m.grip_pull_prog; o[8] = m.anchored_steps;
+  o[9] = m.free_move; o[10] = m.energy; o[11] = m.grip_cycles; o[12] = m.strides; o[13] = m.attach_events;
+  o[14] = m.last_x; o[15] = m.last_y;
+}
 
 void free_part(Part &p) {
   if (p.d_groups) cudaFree(p.d_groups);
@@ -796,6 +893,8 @@ int launch_part(kr_batch *b, Part &p, int max_steps, bool timed) {
   A.slip_max = b->d.grip_slip_max; A.cooldown = b->d.grip_cooldown;
   A.inv_h64 = 1.0 / b->d.solver.h;
   A.dt = b->d.solver.h * b->d.solver.substeps;
+  A.h64 = b->d.solver.h;
+  A.substeps = b->d.solver.substeps;
   A.pw = b->d_pw; A.pw_idx = b->d_pw_idx; A.pw_stride = b->pw_stride;
   cudaError_t e;
   if ((e = cudaMemsetAsync(p.d_queue, 0, sizeof(int), st)) != cudaSuccess) return b->cuda_fail(e, "queue reset");
@@ -855,6 +954,11 @@ int prepare_spawn(kr_batch *b, int n, const int32_t *arms, const int32_t *segs, 
     m.comp = (float)(1.0 / (2000.0 + tn * (400000.0 - 2000.0)));
     m.last_x = (double)(float)x[i];
     m.last_y = (double)(float)y[i];
+    m.tone_d = tn;
+    m.spawn_x = x[i];
+    m.spawn_y = y[i];
+    const int o = b->h_map_off[map_id[i]], nr = b->h_map_off[map_id[i] + 1] - o;
+    m.spawn_reach = measure_reach(b->h_rects.data() + 4 * (size_t)o, nr, T.reach, x[i], y[i]);
   }
   *first_bad = -1;
   if (b->tpls.size() != tpl_before) return upload_templates(b);
@@ -952,6 +1056,8 @@ extern "C" int kr_batch_create(const kr_batch_desc *desc, kr_batch **out) {
     const double c = ht + 2.0 + kr::kCullSlack + 1.0;
     b->h_map_cull[m] = std::isfinite(c) && c < 1e30 ? (float)c : 1e30f;
   }
+  b->h_rects.assign(d.rects, d.rects + 4 * (size_t)n_rects);
+  b->h_map_off = off;
   if ((e = upload_vec(&b->d_rects, r4)) != cudaSuccess) return bail(e, "upload(rects)");
   if ((e = upload_vec(&b->d_map_off, off)) != cudaSuccess) return bail(e, "upload(map offsets)");
   if ((e = upload_vec(&b->d_map_cull, b->h_map_cull)) != cudaSuccess) return bail(e, "upload(map cull)");
@@ -1327,6 +1433,17 @@ extern "C" int kr_batch_read_fitness(kr_batch *b, int32_t first, int32_t n, doub
     out[4 * i] = m[i].path_len; out[4 * i + 1] = m[i].last_x; out[4 * i + 2] = m[i].last_y;
     out[4 * i + 3] = m[i].attach_events;
   }
+  return KR_OK;
+}
+
+extern "C" int kr_batch_read_metrics(kr_batch *b, int32_t first, int32_t n, double *out) {
+  if (!b || !out) return KR_ERR_INVALID;
+  if (first < 0 || n < 0 || first + n > b->capacity) return b->fail(KR_ERR_INVALID, "read range outside the slots");
+  std::vector<SlotMeta> m(n);
+  cudaError_t e = cudaMemcpyAsync(m.data(), b->d_meta + first, m.size() * sizeof(SlotMeta), cudaMemcpyDeviceToHost, b->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
+  if (e != cudaSuccess) return b->cuda_fail(e, "kr_batch_read_metrics");
+  for (int i = 0; i < n; i++) slot_metrics(m[i], out + (size_t)i * KR_METRIC_WORDS);
   return KR_OK;
 }
 

@@ -53,12 +53,17 @@ struct SlotMeta {
   uint32_t rng;
   float comp;       // muscle compliance (f32 as packControls writes it)
   float tone;
-  int attach_events;
+  int attach_events;  // arms newly anchored after a step
   int ctrl;         // KR_CTRL_* of this slot
   int pad;
   double prev_vx, prev_vy;
   double path_len;
   double last_x, last_y;
+  // postStep accumulators, core.js:297-356
+  double tone_d, spawn_x, spawn_y, spawn_reach;
+  double angular_accum, forward_prog, grip_pull_prog, spawn_dist_max, free_move, energy, max_disp;
+  int anchored_steps, grip_cycles, strides;
+  unsigned arm_anchored;  // bit a: arm a anchored after the last step; bit 8: any
 };
 
 // policy parameters of an arms x segs body (kraken_batch.h layout: W1
@@ -122,6 +127,8 @@ struct kr_batch {
   int *d_map_off = nullptr;
   float *d_map_cull = nullptr;
   std::vector<float> h_map_cull;
+  std::vector<double> h_rects;         // every map's rects x y w h as the device holds them
+  std::vector<int> h_map_off;
   // slots
   float *d_state = nullptr;
   float4 *d_grip = nullptr;
@@ -191,6 +198,8 @@ int prepare_spawn(kr_batch *b, int n, const int32_t *arms, const int32_t *segs, 
 cudaError_t launch_spawn(kr_batch *b, const int *d_slots, const float *d_pose, const SlotMeta *d_meta,
                          int n, cudaStream_t stream);
 cudaStream_t part_stream(const kr_batch *b, const Part &p);
+// the metrics record of a slot (kraken_batch.h, KR_METRIC_WORDS), score included
+void slot_metrics(const SlotMeta &m, double *out);
 // public -> device layout of one individual's policy parameters
 void transpose_policy(const float *pub, int arms, int segs, float *dev);
 void free_part(Part &p);

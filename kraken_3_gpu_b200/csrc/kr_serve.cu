@@ -84,15 +84,11 @@ __global__ void perturb_kernel(float *w, int stride, const float *theta, const P
   }
 }
 
-// results of the creatures in slots[0..n)
-__global__ void gather_kernel(const SlotMeta *meta, const int *slots, int n, double *out) {
+// the records of the creatures in slots[0..n) (results are derived on the host)
+__global__ void gather_kernel(const SlotMeta *meta, const int *slots, int n, SlotMeta *out) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
-  const SlotMeta m = meta[slots[i]];
-  out[KR_RESULT_WORDS * i] = m.path_len;
-  out[KR_RESULT_WORDS * i + 1] = m.last_x;
-  out[KR_RESULT_WORDS * i + 2] = m.last_y;
-  out[KR_RESULT_WORDS * i + 3] = (double)m.attach_events;
+  out[i] = meta[slots[i]];
 }
 
 struct Req {
@@ -117,7 +113,7 @@ struct Stage {
   PJob *h_jobs = nullptr, *d_jobs = nullptr;       // part_cap
   float *h_theta = nullptr, *d_theta = nullptr;    // kMaxThetaPerRound x kMaxParams
   int *h_rslots = nullptr, *d_rslots = nullptr;    // part_cap
-  double *h_res = nullptr, *d_res = nullptr;       // part_cap x KR_RESULT_WORDS
+  SlotMeta *h_res = nullptr, *d_res = nullptr;     // part_cap records of completing slots
 };
 
 struct Round {
@@ -133,7 +129,7 @@ uint64_t slot_bytes(const kr_server_desc &d) {
   b += (uint64_t)d.obs_ring * KR_OBS_STRIDE * 4;
   if (d.policy) b += (uint64_t)kMaxParams * 4 + 4;
   // partition staging and work groups (two partitions of half the slots)
-  b += (uint64_t)kStateStride * 4 + sizeof(SlotMeta) + 4 + sizeof(PJob) + 4 + KR_RESULT_WORDS * 8 + 2 * 4;
+  b += (uint64_t)kStateStride * 4 + sizeof(SlotMeta) + 4 + sizeof(PJob) + 4 + sizeof(SlotMeta) + 2 * 4;
   return b;
 }
 
@@ -240,7 +236,8 @@ void finish_round(kr_server *S, int p) {
   for (int64_t id : R.completing) {
     Req &q = S->reqs[id];
     const size_t n = q.slots.size();
-    q.results.assign(S->stage[p].h_res + off * KR_RESULT_WORDS, S->stage[p].h_res + (off + n) * KR_RESULT_WORDS);
+    q.results.resize(n * KR_RESULT_WORDS);
+    for (size_t i = 0; i < n; i++) slot_metrics(S->stage[p].h_res[off + i], q.results.data() + i * KR_RESULT_WORDS);
     off += n;
     q.completed = t;
     q.done = true;
@@ -384,13 +381,12 @@ int run_round(kr_server *S, int p) {
       e = cudaGetLastError();
     }
     if (e == cudaSuccess)
-      e = cudaMemcpyAsync(st.h_res, st.d_res, (size_t)n_res * KR_RESULT_WORDS * sizeof(double),
-                          cudaMemcpyDeviceToHost, stream);
+      e = cudaMemcpyAsync(st.h_res, st.d_res, (size_t)n_res * sizeof(SlotMeta), cudaMemcpyDeviceToHost, stream);
   }
   if (e == cudaSuccess) e = cudaEventRecord(R.done, stream);
   if (e != cudaSuccess) return S->cuda_fail(e, "round results");
   S->h2d_bytes += (uint64_t)n_res * sizeof(int);
-  S->d2h_bytes += (uint64_t)n_res * KR_RESULT_WORDS * sizeof(double);
+  S->d2h_bytes += (uint64_t)n_res * sizeof(SlotMeta);
   R.inflight = true;
   S->rounds++;
   return KR_OK;
@@ -489,7 +485,7 @@ extern "C" int kr_server_create(const kr_server_desc *d, kr_server **out) {
     if (e == cudaSuccess) e = pinned_pair(&st.h_jobs, &st.d_jobs, pc);
     if (e == cudaSuccess) e = pinned_pair(&st.h_theta, &st.d_theta, d->policy ? (size_t)kMaxThetaPerRound * kMaxParams : 1);
     if (e == cudaSuccess) e = pinned_pair(&st.h_rslots, &st.d_rslots, pc);
-    if (e == cudaSuccess) e = pinned_pair(&st.h_res, &st.d_res, pc * KR_RESULT_WORDS);
+    if (e == cudaSuccess) e = pinned_pair(&st.h_res, &st.d_res, pc);
   }
   if (e == cudaSuccess) e = cudaDeviceSynchronize();
   if (e != cudaSuccess) { S->cuda_fail(e, "server setup"); return bail(KR_ERR_CUDA); }

@@ -22,8 +22,8 @@ import numpy as np
 from . import _native
 from .batch import policy_params  # noqa: F401  (parameter count of a body's policy)
 
-RESULT_WORDS = 4
-RESULT_FIELDS = ("path_len", "x", "y", "attach_events")
+from .batch import METRIC_FIELDS as RESULT_FIELDS  # noqa: E402
+RESULT_WORDS = len(RESULT_FIELDS)
 
 _F32P = C.POINTER(C.c_float)
 _F64P = C.POINTER(C.c_double)

@@ -114,6 +114,11 @@ def lib(opcount: bool = False) -> C.CDLL:
         "or_sim_reflex_state": (None, [vp, i, dp, dp]),
         "or_read_proprio": (i, [vp, i, dp]),
         "or_sim_step": (None, [vp]), "or_sim_step32": (None, [vp]),
+        "or_measure_reach": (d, [dp, i, d, d, d]),
+        "or_sim_set_spawn_reach": (None, [vp, i, d]),
+        "or_sim_pre_step": (None, [vp]), "or_sim_post_step": (None, [vp]),
+        "or_sim_metrics": (None, [vp, i, C.POINTER(Metrics)]),
+        "or_score": (d, [C.POINTER(Metrics)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -364,6 +369,22 @@ class Kraken:
         return self.world.con(self.grips[arm])
 
 
+METRIC_FIELDS = ("score", "steps", "pathLen", "maxDisplacement", "spawnReach", "angularAccum",
+                 "forwardProg", "gripPullProg", "anchoredSteps", "freeMove", "energySpent",
+                 "gripCycles", "strides", "attachEvents", "x", "y")
+
+
+class Metrics(C.Structure):
+    """or_metrics: postStep's accumulators (core.js:297-356) and score."""
+    _fields_ = [(f, C.c_double) for f in METRIC_FIELDS] + [("spawnDistMax", C.c_double)]
+
+
+def measure_reach(rects, reach, x, y) -> float:
+    """measureReach (fitness.js:74-88) over rects x y w h, rays up to 3.5 reach."""
+    r = np.ascontiguousarray(rects, dtype=np.float64).reshape(-1, 4)
+    return lib().or_measure_reach(_dp(r), len(r), reach, x, y)
+
+
 class Sim:
     """createSim (core.js:37-74) with prey 0; physics, colouring and reflex only.
 
@@ -437,3 +458,20 @@ class Sim:
 
     def step32(self):
         self.L.or_sim_step32(self.ptr)
+
+    def pre_step(self):
+        """preStep of every creature (core.js:291-294)."""
+        self.L.or_sim_pre_step(self.ptr)
+
+    def post_step(self):
+        """postStep of every creature (core.js:297-356)."""
+        self.L.or_sim_post_step(self.ptr)
+
+    def set_spawn_reach(self, ci, reach):
+        self.L.or_sim_set_spawn_reach(self.ptr, ci, reach)
+
+    def metrics(self, ci) -> dict:
+        """postStep accumulators and score (fitness.js:115-172) of creature ci."""
+        m = Metrics()
+        self.L.or_sim_metrics(self.ptr, ci, C.byref(m))
+        return {f: getattr(m, f) for f in METRIC_FIELDS}

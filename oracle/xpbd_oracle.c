@@ -1217,6 +1217,9 @@ typedef struct {
   double tone;
   double adhesion[OR_MAX_ARMS], cd[OR_MAX_ARMS];
   double prevVx, prevVy;
+  or_metrics m;
+  double sx, sy;                       /* preStep's position */
+  int armWasAnchored[OR_MAX_ARMS], wasAnchored;
 } or_creature;
 
 struct or_sim {
@@ -1450,4 +1453,117 @@ int or_read_proprio(or_sim *s, int ci, double *out) {
 }
 
 void or_sim_step(or_sim *s) { or_step(s->w); }
+
+/* measureReach, fitness.js:74-88: the free space around (x, y) along 16
+ * rays marched in 12 px steps up to 3.5 arm reaches, until the SDF of the
+ * map is not positive */
+double or_measure_reach(const double *rects, int nR, double reach, double x, double y) {
+  double sum = 0, best = 0;
+  const int N = 16;
+  for (int k = 0; k < N; k++) {
+    const double a = ((double)k / N) * JS_PI * 2;
+    double d = 0;
+    while (d < reach * 3.5) {
+      d += 12;
+      double hd, nx, ny;
+      if (!or_sdf(rects, nR, x + cos(a) * d, y + sin(a) * d, &hd, &nx, &ny) || hd <= 0) break;
+    }
+    sum += d;
+    if (d > best) best = d;
+  }
+  const double r = (sum / N) * 0.55 + best * 0.45;
+  return r > 70 ? r : 70;
+}
+
+void or_sim_set_spawn_reach(or_sim *s, int ci, double reach) { s->cr[ci].m.spawnReach = reach; }
+
+/* preStep, core.js:291-294 */
+void or_sim_pre_step(or_sim *s) {
+  for (int i = 0; i < s->nCr; i++) {
+    or_creature *c = &s->cr[i];
+    c->sx = PX(s->w)[c->k.mantle];
+    c->sy = PY(s->w)[c->k.mantle];
+  }
+}
+
+/* postStep, core.js:297-356 (no prey) */
+void or_sim_post_step(or_sim *s) {
+  const or_world *w = s->w;
+  for (int i = 0; i < s->nCr; i++) {
+    or_creature *c = &s->cr[i];
+    or_metrics *m = &c->m;
+    const int mt = c->k.mantle, A = c->k.nArms;
+    const double x = PX(w)[mt], y = PY(w)[mt], angle = ANG(w)[mt], av = AV(w)[mt];
+    m->steps++;
+    const double dx = x - c->sx, dy = y - c->sy;
+    const double stepDist = hypot(dx, dy);
+    m->pathLen += stepDist;
+    m->angularAccum += fabs(av) * w->h * w->substeps;
+    const double fa = angle - JS_PI * 0.5;
+    const double fwd = dx * cos(fa) + dy * sin(fa);
+    if (fwd > 0) m->forwardProg += fwd;
+    int anchored = 0;
+    for (int a = 0; a < A; a++) anchored += w->cons[c->k.grip[a]].broken ? 0 : 1;
+    const double dSpawn = hypot(x - c->k.spawnX, y - c->k.spawnY);
+    if (anchored > 0) {
+      m->anchoredSteps++;
+      if (dSpawn > m->spawnDistMax) { m->gripPullProg += dSpawn - m->spawnDistMax; m->spawnDistMax = dSpawn; }
+    }
+    if (anchored == 0 && stepDist > 0.3) m->freeMove += stepDist;
+    m->energySpent += (c->tone * 0.0006 + stepDist * 0.0004) * A;
+    if (anchored > 0 && !c->wasAnchored) m->gripCycles++;
+    c->wasAnchored = anchored > 0;
+    int newly = 0;
+    for (int a = 0; a < A; a++) {
+      const int now = w->cons[c->k.grip[a]].broken ? 0 : 1;
+      if (now && !c->armWasAnchored[a]) { newly++; m->attachEvents++; }
+      c->armWasAnchored[a] = now;
+    }
+    if (newly > 0 && anchored - newly > 0) m->strides += newly;
+    if (dSpawn > m->maxDisplacement) m->maxDisplacement = dSpawn;
+    m->x = x; m->y = y;
+  }
+}
+
+/* score, fitness.js:115-172: the terms in TERM_ORDER, summed in f64 in that
+ * order (no prey: preyHit and preyNear are 0); maxAngSpeed 18, dt 1/60 */
+double or_score(const or_metrics *c) {
+  const double W_gripPull = 2.6, W_strideBonus = 0.5, W_strideCap = 60, W_reach = 320, W_directed = 70,
+               W_headingHold = 28, W_meanSpeed = 14, W_efficiency = 3, W_progGateKnee = 0.25, W_spin = 0.55,
+               W_drift = 0.05, W_energy = 0.30;
+  const double steps = c->steps > 1 ? c->steps : 1;
+  const double path = c->pathLen, disp = c->maxDisplacement;
+  const double reach = c->spawnReach > 0 ? c->spawnReach : 300;
+  const double reachFrac = fmin(1.2, disp / reach);
+  const double directed = path > 1 ? fmin(1, disp / path) : 0;
+  const double spinBudget = steps * 18 * (1.0 / 60);
+  const double headingHold = 1 - fmin(1, c->angularAccum / fmax(1e-6, spinBudget));
+  const double meanSpeed = path / steps / 60;
+  const double efficiency = c->forwardProg / fmax(0.5, c->energySpent > 0 ? c->energySpent : 0.5);
+  const double progressBase = c->gripPullProg * W_gripPull + reachFrac * W_reach;
+  const double strideFrac = fmin(c->strides, W_strideCap) / W_strideCap;
+  const double progGate = fmin(1, disp / fmax(1e-6, W_progGateKnee * reach));
+  const double t[12] = {
+    c->gripPullProg * W_gripPull,
+    progressBase * W_strideBonus * strideFrac,
+    reachFrac * W_reach,
+    directed * W_directed * progGate,
+    headingHold * W_headingHold * progGate,
+    fmin(1, meanSpeed) * W_meanSpeed * progGate,
+    fmin(20, efficiency) * W_efficiency * progGate,
+    -(c->angularAccum * W_spin * 0.02),
+    -(c->freeMove * W_drift),
+    -(c->energySpent * W_energy),
+    0.0,
+    0.0,
+  };
+  double sc = 0;
+  for (int i = 0; i < 12; i++) sc += t[i];
+  return isfinite(sc) ? sc : 0;
+}
+
+void or_sim_metrics(const or_sim *s, int ci, or_metrics *out) {
+  *out = s->cr[ci].m;
+  out->score = or_score(out);
+}
 void or_sim_step32(or_sim *s) { or_step32(s->w); }

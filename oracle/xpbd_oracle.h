@@ -139,6 +139,20 @@ int or_read_proprio(or_sim *s, int ci, double *out);
 void or_sim_step(or_sim *s);        /* world.step() of the whole sim */
 void or_sim_step32(or_sim *s);      /* f32 emulation step */
 
+/* fitness metrics of a creature: postStep's accumulators (core.js:297-356)
+ * and score (fitness.js:115-172) */
+typedef struct {
+  double score, steps, pathLen, maxDisplacement, spawnReach, angularAccum, forwardProg, gripPullProg;
+  double anchoredSteps, freeMove, energySpent, gripCycles, strides, attachEvents, x, y;
+  double spawnDistMax;
+} or_metrics;
+double or_measure_reach(const double *rects, int nR, double reach, double x, double y);
+void or_sim_set_spawn_reach(or_sim *s, int ci, double reach);
+void or_sim_pre_step(or_sim *s);    /* preStep of every creature */
+void or_sim_post_step(or_sim *s);   /* postStep of every creature */
+double or_score(const or_metrics *m);
+void or_sim_metrics(const or_sim *s, int ci, or_metrics *out);
+
 #ifdef __cplusplus
 }
 #endif

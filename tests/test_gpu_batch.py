@@ -106,7 +106,7 @@ def test_launch_shape_does_not_change_results(lanes, warps, ctas):
     for f in ("px", "py", "ang", "vx", "vy", "av", "grips", "steps"):
         assert np.array_equal(s0[f], s1[f]), f
     assert np.array_equal(base.read_obs(), other.read_obs())
-    assert np.array_equal(base.read_fitness(), other.read_fitness())
+    assert np.array_equal(base.read_metrics(), other.read_metrics())
     base.close()
     other.close()
 
@@ -210,6 +210,6 @@ def test_autotune_leaves_slots_as_they_were():
     a, b = ref.read_state(), eng.read_state()
     for f in ("px", "py", "ang", "grips", "steps"):
         assert np.array_equal(a[f], b[f]), f
-    assert np.array_equal(ref.read_fitness(), eng.read_fitness())
+    assert np.array_equal(ref.read_metrics(), eng.read_metrics())
     ref.close()
     eng.close()

@@ -18,7 +18,7 @@ def mixed16k():
 
 def _state(eng):
     st = eng.read_state()
-    return st, eng.read_fitness()
+    return st, eng.read_metrics()
 
 
 def test_mixed_16k_deterministic_and_shape_invariant(mixed16k):
@@ -48,7 +48,7 @@ def test_mixed_16k_served_equals_persistent(mixed16k):
     eng = batch.BatchEngine(w.maps, w.n)
     workloads.spawn_all(eng, w)
     eng.run(int(w.horizon.max()))
-    want = eng.read_fitness()
+    want = eng.read_metrics()
     eng.close()
     srv = serve.Server(w.maps, 8 << 30, max_slots=w.n, chunk_steps=64, policy=False)
     ids = srv.submit_many(w.horizon, w.arms, w.segs, w.map_id, w.x, w.y, w.angle, control_seeds=w.seed)

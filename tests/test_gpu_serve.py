@@ -62,7 +62,7 @@ def test_server_equals_engine_with_explicit_mirrored_weights():
     eng.spawn(0, [arms] * pop, [segs] * pop, [2] * pop, [x] * pop, [y] * pop, [0.7] * pop, [H] * pop)
     eng.set_policy(W, np.arange(pop, dtype=np.int32))
     eng.run(H)
-    want = eng.read_fitness()
+    want = eng.read_metrics()
     eng.close()
     assert np.array_equal(got, want)
     assert not np.array_equal(got[0], got[1])  # the mirrored pair differs
@@ -133,7 +133,7 @@ def test_served_uneven_workload_equals_batched_engine():
     eng = batch.BatchEngine(w.maps, w.n)
     workloads.spawn_all(eng, w)
     eng.run(int(w.horizon.max()))
-    want = eng.read_fitness()
+    want = eng.read_metrics()
     eng.close()
     srv = serve.Server(w.maps, 1 << 30, max_slots=40, chunk_steps=24, policy=False)
     half = w.n // 2
