@@ -59,7 +59,8 @@ def test_measure_reach_open_space_and_walls():
     # 3.5 reaches = 414.75 px: every ray runs out in the open, 35 full steps
     assert open_ == 35 * 12
     assert 70 <= near < open_
-    assert ob.measure_reach(box, 118.5, 500, 500, ) == ob.measure_reach(box, 118.5, 500, 500)
+    # a longer body reaches farther: rays run up to 3.5 of its reaches
+    assert ob.measure_reach(box, 24 + 9 * 13.5, 500, 500) > open_
 
 
 def test_post_step_counts_steps_and_path():
