@@ -378,33 +378,37 @@ __device__ void run_creature(const BatchArgs &A, const TplDev &td, int nlv, cons
     kr::island_step<kr::CompactAccess, G>(A.K, S, rects, nR, cull_d, L);
     // 5. postStep, core.js:297-356 (f64 on the f32 state, as the
     //    reference's hybrid loop runs it on the mirrored state)
+    //    The accumulators are read and written through the slot's HBM
+    //    record by lane 0 (they do not live in every lane's registers).
     if (lane == 0) {
+      SlotMeta &g = A.meta[slot];
       const double x = S.px[0], y = S.py[0], angle = S.ang[0], av = S.av[0];
-      const double dx = x - m.last_x, dy = y - m.last_y;
+      const double dx = x - g.last_x, dy = y - g.last_y;
       const double step_dist = hypot(dx, dy);
-      m.path_len += step_dist;
-      m.angular_accum += fabs(av) * A.h64 * A.substeps;
+      g.path_len += step_dist;
+      g.angular_accum += fabs(av) * A.h64 * A.substeps;
       const double fa = angle - kPiD * 0.5;
       const double fwd = dx * cos(fa) + dy * sin(fa);
-      if (fwd > 0) m.forward_prog += fwd;
+      if (fwd > 0) g.forward_prog += fwd;
       int anchored = 0;
       unsigned now = 0;
       for (int a = 0; a < arms; a++)
         if (S.anc[4 * a + 3] == 0.f) { anchored++; now |= 1u << a; }
-      const double d_spawn = hypot(x - m.spawn_x, y - m.spawn_y);
+      const double d_spawn = hypot(x - g.spawn_x, y - g.spawn_y);
       if (anchored > 0) {
-        m.anchored_steps++;
-        if (d_spawn > m.spawn_dist_max) { m.grip_pull_prog += d_spawn - m.spawn_dist_max; m.spawn_dist_max = d_spawn; }
+        g.anchored_steps++;
+        if (d_spawn > g.spawn_dist_max) { g.grip_pull_prog += d_spawn - g.spawn_dist_max; g.spawn_dist_max = d_spawn; }
       }
-      if (anchored == 0 && step_dist > 0.3) m.free_move += step_dist;
-      m.energy += (m.tone_d * 0.0006 + step_dist * 0.0004) * arms;
-      if (anchored > 0 && !(m.arm_anchored & 0x100u)) m.grip_cycles++;
-      const int newly = __popc(now & ~m.arm_anchored & 0xffu);
-      m.attach_events += newly;
-      if (newly > 0 && anchored - newly > 0) m.strides += newly;
-      m.arm_anchored = now | (anchored > 0 ? 0x100u : 0u);
-      m.max_disp = fmax(m.max_disp, d_spawn);
-      m.last_x = x; m.last_y = y;
+      if (anchored == 0 && step_dist > 0.3) g.free_move += step_dist;
+      g.energy += (g.tone_d * 0.0006 + step_dist * 0.0004) * arms;
+      const unsigned was = g.arm_anchored;
+      if (anchored > 0 && !(was & 0x100u)) g.grip_cycles++;
+      const int newly = __popc(now & ~was & 0xffu);
+      g.attach_events += newly;
+      if (newly > 0 && anchored - newly > 0) g.strides += newly;
+      g.arm_anchored = now | (anchored > 0 ? 0x100u : 0u);
+      g.max_disp = fmax(g.max_disp, d_spawn);
+      g.last_x = x; g.last_y = y;
     }
     m.step = t + 1;
   }
@@ -417,7 +421,13 @@ __device__ void run_creature(const BatchArgs &A, const TplDev &td, int nlv, cons
   }
   float *cout = A.ctrl_cur + (size_t)slot * kCtrlStride;
   for (int q = lane; q < AS + arms; q += G) cout[q] = X.ctrl[q];
-  if (lane == 0) A.meta[slot] = m;
+  if (lane == 0) {  // the fields this loop keeps in registers; postStep's are in place
+    SlotMeta &g = A.meta[slot];
+    g.step = m.step;
+    g.rng = m.rng;
+    g.prev_vx = m.prev_vx;
+    g.prev_vy = m.prev_vy;
+  }
 }
 
 template <int G>
