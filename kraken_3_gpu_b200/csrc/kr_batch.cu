@@ -482,10 +482,22 @@ __global__ void __launch_bounds__(32 * kMaxW, 1) batch_kernel(BatchArgs A) {
 
 // writes n prepared creatures into slots[0..n): pose, released grips, zero
 // lambda / cooldown / controls, meta
+// one block per spawned creature: copies its pose and metadata into the slot,
+// clears its grips and controls, and measures its spawn reach (16 threads,
+// one ray each; init's spawn_reach holds the body's arm reach on entry)
 __global__ void spawn_kernel(float *state, float4 *grip, float2 *glam, double *cd, SlotMeta *meta,
-                             float *ctrl, const int *slots, const float *pose, const SlotMeta *init, int n) {
+                             float *ctrl, const int *slots, const float *pose, const SlotMeta *init, int n,
+                             const double *rects, const int *map_off, RayDirs rays) {
+  __shared__ double ray_d[16];
   const int i = blockIdx.x;
   if (i >= n) return;
+  if (threadIdx.x < 16) {
+    const SlotMeta &m = init[i];
+    const int o = map_off[m.map], nr = map_off[m.map + 1] - o;
+    ray_d[threadIdx.x] = reach_ray(rects + 4 * (size_t)o, nr, m.spawn_reach, m.spawn_x, m.spawn_y,
+                                   rays.c[threadIdx.x], rays.s[threadIdx.x]);
+  }
+  __syncthreads();
   const int slot = slots[i];
   const float *src = pose + (size_t)i * kStateStride;
   float *dst = state + (size_t)slot * kStateStride;
@@ -496,7 +508,17 @@ __global__ void spawn_kernel(float *state, float4 *grip, float2 *glam, double *c
     cd[(size_t)slot * KR_BATCH_MAX_ARMS + threadIdx.x] = 0.0;
   }
   for (int q = threadIdx.x; q < kCtrlStride; q += blockDim.x) ctrl[(size_t)slot * kCtrlStride + q] = 0.f;
-  if (threadIdx.x == 0) meta[slot] = init[i];
+  if (threadIdx.x == 0) {
+    SlotMeta m = init[i];
+    double sum = 0, best = 0;
+    for (int k = 0; k < 16; k++) {
+      sum += ray_d[k];
+      if (ray_d[k] > best) best = ray_d[k];
+    }
+    const double v = (sum / 16) * 0.55 + best * 0.45;
+    m.spawn_reach = 70.0 < v ? v : 70.0;
+    meta[slot] = m;
+  }
 }
 
 }  // namespace
@@ -521,42 +543,6 @@ double tpl_cost(const TplDev &d) { return (double)d.nc + 0.5 * (double)d.np; }
 namespace krb {
 
 cudaStream_t part_stream(const kr_batch *b, const Part &p) { return p.stream ? p.stream : b->stream; }
-
-// signed distance of makeSdf (src/world/map.js:91-118) in f64
-static bool sdf_d(const double *r, int n, double x, double y, double *d) {
-  double best = INFINITY;
-  for (int i = 0; i < n; i++, r += 4) {
-    const double cx = std::max(r[0], std::min(x, r[0] + r[2]));
-    const double cy = std::max(r[1], std::min(y, r[1] + r[3]));
-    const double dx = x - cx, dy = y - cy, d2 = dx * dx + dy * dy;
-    if (d2 > 1e-12) {
-      if (d2 < best * best) best = std::sqrt(d2);
-    } else {
-      const double m = std::min(std::min(x - r[0], r[0] + r[2] - x), std::min(y - r[1], r[1] + r[3] - y));
-      if (-m < best) best = -m;
-    }
-  }
-  if (!std::isfinite(best)) return false;
-  *d = best;
-  return true;
-}
-
-// measureReach, src/sim/fitness.js:74-88: the free space around a spawn
-// point along 16 rays (12 px steps up to 3.5 arm reaches of the body)
-double measure_reach(const double *rects, int n, double reach, double x, double y) {
-  double sum = 0, best = 0;
-  for (int k = 0; k < 16; k++) {
-    const double a = ((double)k / 16) * 3.141592653589793 * 2;
-    double d = 0, h = 0;
-    while (d < reach * 3.5) {
-      d += 12;
-      if (!sdf_d(rects, n, x + std::cos(a) * d, y + std::sin(a) * d, &h) || h <= 0) break;
-    }
-    sum += d;
-    if (d > best) best = d;
-  }
-  return std::max(70.0, (sum / 16) * 0.55 + best * 0.45);
-}
 
 // score, src/sim/fitness.js:115-172 without prey (preyHit = preyNear = 0),
 // maxAngSpeed 18 and dt 1/60 as the trainer calls it: the terms in
@@ -967,8 +953,7 @@ int prepare_spawn(kr_batch *b, int n, const int32_t *arms, const int32_t *segs, 
     m.tone_d = tn;
     m.spawn_x = x[i];
     m.spawn_y = y[i];
-    const int o = b->h_map_off[map_id[i]], nr = b->h_map_off[map_id[i] + 1] - o;
-    m.spawn_reach = measure_reach(b->h_rects.data() + 4 * (size_t)o, nr, T.reach, x[i], y[i]);
+    m.spawn_reach = T.reach;  // replaced by measureReach in spawn_kernel
   }
   *first_bad = -1;
   if (b->tpls.size() != tpl_before) return upload_templates(b);
@@ -979,7 +964,7 @@ cudaError_t launch_spawn(kr_batch *b, const int *d_slots, const float *d_pose, c
                          int n, cudaStream_t stream) {
   if (n <= 0) return cudaSuccess;
   spawn_kernel<<<n, 128, 0, stream>>>(b->d_state, b->d_grip, b->d_glam, b->d_cd, b->d_meta, b->d_ctrl,
-                                      d_slots, d_pose, d_meta, n);
+                                      d_slots, d_pose, d_meta, n, b->d_rects64, b->d_map_off, b->rays);
   return cudaGetLastError();
 }
 
@@ -1070,6 +1055,12 @@ extern "C" int kr_batch_create(const kr_batch_desc *desc, kr_batch **out) {
   b->h_map_off = off;
   if ((e = upload_vec(&b->d_rects, r4)) != cudaSuccess) return bail(e, "upload(rects)");
   if ((e = upload_vec(&b->d_map_off, off)) != cudaSuccess) return bail(e, "upload(map offsets)");
+  if ((e = upload_vec(&b->d_rects64, b->h_rects)) != cudaSuccess) return bail(e, "upload(rects f64)");
+  for (int k = 0; k < 16; k++) {
+    const double a = ((double)k / 16) * 3.141592653589793 * 2;
+    b->rays.c[k] = std::cos(a);
+    b->rays.s[k] = std::sin(a);
+  }
   if ((e = upload_vec(&b->d_map_cull, b->h_map_cull)) != cudaSuccess) return bail(e, "upload(map cull)");
   const size_t C = (size_t)d.capacity;
   if ((e = cudaMalloc(&b->d_state, C * kStateStride * sizeof(float))) != cudaSuccess) return bail(e, "cudaMalloc(state)");
@@ -1495,7 +1486,7 @@ extern "C" void kr_batch_destroy(kr_batch *b) {
   for (void *p : b->d_tpl_arrays)
     if (p) cudaFree(p);
   free_part(b->main);
-  void *ptrs[] = {b->d_tpl, const_cast<int *>(b->T.arm_segs), b->d_rects, b->d_map_off, b->d_map_cull,
+  void *ptrs[] = {b->d_tpl, const_cast<int *>(b->T.arm_segs), b->d_rects, b->d_map_off, b->d_map_cull, b->d_rects64,
                   b->d_state, b->d_grip, b->d_glam, b->d_cd, b->d_ctrl, b->d_meta, b->d_obs,
                   b->d_pw, b->d_pw_idx, b->s_state, b->s_grip, b->s_glam, b->s_cd,
                   b->s_ctrl, b->s_meta, b->s_groups};

@@ -81,6 +81,42 @@ __host__ __device__ inline int policy_device_index(int arms, int segs, int p) {
   return H * (n_in + 1) + (q % (H + 1)) * n_out + q / (H + 1);
 }
 
+// measureReach (src/sim/fitness.js:74-88) along one ray from (x, y) with
+// direction (c, s): march in 12 px steps while the makeSdf distance
+// (src/world/map.js:91-118, f64 over the map's rects x y w h) stays positive,
+// up to 3.5 reach; the distance marched.  Host and device run this same code
+// (IEEE f64 add, multiply and sqrt; min / max as std::min / std::max).
+__host__ __device__ inline double reach_ray(const double *rects, int n, double reach, double x, double y,
+                                            double c, double s) {
+  double d = 0;
+  while (d < reach * 3.5) {
+    d += 12;
+    const double px = x + c * d, py = y + s * d;
+    double best = INFINITY;
+    const double *r = rects;
+    for (int i = 0; i < n; i++, r += 4) {
+      const double xr = r[0] + r[2], yb = r[1] + r[3];
+      const double mx = xr < px ? xr : px, my = yb < py ? yb : py;
+      const double cx = r[0] < mx ? mx : r[0], cy = r[1] < my ? my : r[1];
+      const double dx = px - cx, dy = py - cy, d2 = dx * dx + dy * dy;
+      if (d2 > 1e-12) {
+        if (d2 < best * best) best = sqrt(d2);
+      } else {
+        const double a = px - r[0], b = xr - px, e = py - r[1], f = yb - py;
+        const double ab = b < a ? b : a, ef = f < e ? f : e, m = ef < ab ? ef : ab;
+        if (-m < best) best = -m;
+      }
+    }
+    if (!(best < INFINITY && best > -INFINITY) || best <= 0) break;
+  }
+  return d;
+}
+
+// the 16 ray directions of measureReach, angle k / 16 * 2 pi, from the host's libm
+struct RayDirs {
+  double c[16], s[16];
+};
+
 // A set of slots launched together on one stream: every slot (the public
 // engine calls) or an explicit list (the rollout server's partitions).
 struct Part {
@@ -129,6 +165,8 @@ struct kr_batch {
   std::vector<float> h_map_cull;
   std::vector<double> h_rects;         // every map's rects x y w h as the device holds them
   std::vector<int> h_map_off;
+  double *d_rects64 = nullptr;         // h_rects on the device (measureReach at spawn)
+  krb::RayDirs rays{};
   // slots
   float *d_state = nullptr;
   float4 *d_grip = nullptr;

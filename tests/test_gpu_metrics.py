@@ -63,3 +63,17 @@ def test_server_results_are_the_metrics_record():
     assert got.shape == (w.n, serve.RESULT_WORDS)
     assert np.array_equal(got, want)
     assert np.all(got[:, 1] == w.horizon)  # steps
+
+
+def test_spawn_reach_bit_exact_on_many_maps():
+    """measureReach runs in the spawn kernel; it equals the oracle's f64 march
+    exactly, creature by creature, over 64 maps of varying density."""
+    w = workloads.uneven(n=2048, n_maps=64, seed=9, h_min=1, h_max=1)
+    eng = batch.BatchEngine(w.maps, w.n)
+    workloads.spawn_all(eng, w)
+    got = eng.read_metrics()[:, batch.METRIC_FIELDS.index("spawnReach")]
+    eng.close()
+    for i in range(w.n):
+        rects32 = w.maps[w.map_id[i]].astype(np.float32).astype(np.float64)
+        want = ob.measure_reach(rects32, kraken.arm_reach(int(w.segs[i])), w.x[i], w.y[i])
+        assert got[i] == want, (i, got[i], want)
