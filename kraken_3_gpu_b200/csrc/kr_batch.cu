@@ -37,7 +37,7 @@ struct BatchArgs {
   float *state;          // capacity x kStateStride
   float4 *grip;          // capacity x 8: lbx lby brk broken
   float2 *glam;          // capacity x 8: grip lambda after the last substep
-  double *cd;            // capacity x 8
+  double2 *cd;           // capacity x 8: reflex cooldown, break force (f64, as applyControl sets it)
   float *ctrl_cur;       // capacity x kCtrlStride: the controls in use
   SlotMeta *meta;
   const float4 *rects;   // x y x+w y+h
@@ -158,10 +158,13 @@ __device__ inline double mulberry_next(uint32_t &s) {
 __device__ inline double clamp_sym(double v, double m) { return v > m ? m : (v < -m ? -m : v); }
 
 // proprioception of the current state, readProprio (core.js:129-175), f64;
-// writes 6A+6 values into X.obs and returns the attached-arm bitmask
+// writes 6A+6 values into X.obs and returns the attached-arm bitmask.  The
+// grip load divides by the arm's break force in f64, cdp[a].y (the JS
+// object's breakForce, which the GPU mirror never overwrites with the f32
+// copy the solver holds).
 template <int G>
 __device__ unsigned proprio(const BatchArgs &A, const TplDev &td, const TplSmem &P, kr::Island &S,
-                            CreatureSmem &X, SlotMeta &m, const kr::Lanes<G> &L) {
+                            CreatureSmem &X, SlotMeta &m, const double2 *cdp, const kr::Lanes<G> &L) {
   const int arms = td.arms, segs = td.segs, lane = L.lane;
   const float4 *grip_st = reinterpret_cast<const float4 *>(S.anc);
   const double cx = S.px[0], cy = S.py[0], cvx = S.vx[0], cvy = S.vy[0];
@@ -206,7 +209,7 @@ __device__ unsigned proprio(const BatchArgs &A, const TplDev &td, const TplSmem 
     const float4 g = grip_st[a];
     double force = 0.0;
     if (g.w == 0.f) force = hypot((double)S.lamX[P.arm_grip[a]], (double)S.lamY[P.arm_grip[a]]) * A.inv_h64;
-    X.obs[4 * arms + a] = g.w != 0.f ? 0.f : (float)fmin(1.0, force / fmax(1.0, (double)g.z));
+    X.obs[4 * arms + a] = g.w != 0.f ? 0.f : (float)fmin(1.0, force / fmax(1.0, cdp[a].y));
     X.obs[5 * arms + a] = g.w != 0.f ? 0.f : 1.f;
   }
   if (lane == 0) {
@@ -299,17 +302,17 @@ __device__ void run_creature(const BatchArgs &A, const TplDev &td, int nlv, cons
   const int arms = td.arms, AS = td.arms * td.segs;
   float4 *gst = A.grip + (size_t)slot * KR_BATCH_MAX_ARMS;
   float2 *glam = A.glam + (size_t)slot * KR_BATCH_MAX_ARMS;
-  double *cdp = A.cd + (size_t)slot * KR_BATCH_MAX_ARMS;
+  double2 *cdp = A.cd + (size_t)slot * KR_BATCH_MAX_ARMS;
   for (int k = lane; k < td.nc; k += G) { S.lamX[k] = 0.f; S.lamY[k] = 0.f; }
   S.comp_m = m.comp;
-  double cd = 0.0;  // reflex cooldown of arm `lane`
+  double cd = 0.0;  // reflex cooldown of arm `lane` (its f64 break force stays in cdp)
   L.sync();
   if (lane < arms) {
     reinterpret_cast<float4 *>(S.anc)[lane] = gst[lane];
     const float2 gl = glam[lane];
     const int k = P.arm_grip[lane];
     S.lamX[k] = gl.x; S.lamY[k] = gl.y;
-    cd = cdp[lane];
+    cd = cdp[lane].x;
   }
   const float *cin = A.ctrl_cur + (size_t)slot * kCtrlStride;
   for (int q = lane; q < AS + arms; q += G) X.ctrl[q] = cin[q];
@@ -321,7 +324,7 @@ __device__ void run_creature(const BatchArgs &A, const TplDev &td, int nlv, cons
     const int t = m.step;
     // 1. proprioception of the current state
     if (A.obs_ring > 0 || m.ctrl == KR_CTRL_POLICY) {
-      const unsigned att = proprio<G>(A, td, P, S, X, m, L);
+      const unsigned att = proprio<G>(A, td, P, S, X, m, cdp, L);
       if (A.obs_ring > 0) {
         float *o = A.obs + ((size_t)slot * A.obs_ring + (t % A.obs_ring)) * KR_OBS_STRIDE;
         for (int q = lane; q < 6 * arms + 6; q += G) o[q] = X.obs[q];
@@ -360,7 +363,9 @@ __device__ void run_creature(const BatchArgs &A, const TplDev &td, int nlv, cons
             const double ta = (double)S.ang[tip];
             an[0] = (float)((double)S.px[tip] + kSegHalf * cos(ta));
             an[1] = (float)((double)S.py[tip] + kSegHalf * sin(ta));
-            an[2] = (float)(40.0 + 860.0 * adh);
+            const double brk = 40.0 + 860.0 * adh;
+            cdp[a].y = brk;
+            an[2] = (float)brk;
             an[3] = 0.f;
             S.lamX[k] = 0.f; S.lamY[k] = 0.f;
           } else {
@@ -368,7 +373,9 @@ __device__ void run_creature(const BatchArgs &A, const TplDev &td, int nlv, cons
           }
         }
       } else {
-        an[2] = (float)(40.0 + 860.0 * adh);
+        const double brk = 40.0 + 860.0 * adh;
+        cdp[a].y = brk;
+        an[2] = (float)brk;
         if (adh < 0.04) an[3] = 1.f;
       }
       cd = c;
@@ -417,7 +424,7 @@ __device__ void run_creature(const BatchArgs &A, const TplDev &td, int nlv, cons
     const int k = P.arm_grip[lane];
     gst[lane] = reinterpret_cast<const float4 *>(S.anc)[lane];
     glam[lane] = make_float2(S.lamX[k], S.lamY[k]);
-    cdp[lane] = cd;
+    cdp[lane].x = cd;
   }
   float *cout = A.ctrl_cur + (size_t)slot * kCtrlStride;
   for (int q = lane; q < AS + arms; q += G) cout[q] = X.ctrl[q];
@@ -485,7 +492,7 @@ __global__ void __launch_bounds__(32 * kMaxW, 1) batch_kernel(BatchArgs A) {
 // one block per spawned creature: copies its pose and metadata into the slot,
 // clears its grips and controls, and measures its spawn reach (16 threads,
 // one ray each; init's spawn_reach holds the body's arm reach on entry)
-__global__ void spawn_kernel(float *state, float4 *grip, float2 *glam, double *cd, SlotMeta *meta,
+__global__ void spawn_kernel(float *state, float4 *grip, float2 *glam, double2 *cd, SlotMeta *meta,
                              float *ctrl, const int *slots, const float *pose, const SlotMeta *init, int n,
                              const double *rects, const int *map_off, RayDirs rays) {
   __shared__ double ray_d[16];
@@ -505,7 +512,7 @@ __global__ void spawn_kernel(float *state, float4 *grip, float2 *glam, double *c
   if (threadIdx.x < KR_BATCH_MAX_ARMS) {
     grip[(size_t)slot * KR_BATCH_MAX_ARMS + threadIdx.x] = make_float4(0.f, 0.f, 0.f, 1.f);
     glam[(size_t)slot * KR_BATCH_MAX_ARMS + threadIdx.x] = make_float2(0.f, 0.f);
-    cd[(size_t)slot * KR_BATCH_MAX_ARMS + threadIdx.x] = 0.0;
+    cd[(size_t)slot * KR_BATCH_MAX_ARMS + threadIdx.x] = make_double2(0.0, 0.0);
   }
   for (int q = threadIdx.x; q < kCtrlStride; q += blockDim.x) ctrl[(size_t)slot * kCtrlStride + q] = 0.f;
   if (threadIdx.x == 0) {
@@ -1066,7 +1073,7 @@ extern "C" int kr_batch_create(const kr_batch_desc *desc, kr_batch **out) {
   if ((e = cudaMalloc(&b->d_state, C * kStateStride * sizeof(float))) != cudaSuccess) return bail(e, "cudaMalloc(state)");
   if ((e = cudaMalloc(&b->d_grip, C * KR_BATCH_MAX_ARMS * sizeof(float4))) != cudaSuccess) return bail(e, "cudaMalloc(grips)");
   if ((e = cudaMalloc(&b->d_glam, C * KR_BATCH_MAX_ARMS * sizeof(float2))) != cudaSuccess) return bail(e, "cudaMalloc(grip lambda)");
-  if ((e = cudaMalloc(&b->d_cd, C * KR_BATCH_MAX_ARMS * sizeof(double))) != cudaSuccess) return bail(e, "cudaMalloc(cooldown)");
+  if ((e = cudaMalloc(&b->d_cd, C * KR_BATCH_MAX_ARMS * sizeof(double2))) != cudaSuccess) return bail(e, "cudaMalloc(cooldown)");
   if ((e = cudaMalloc(&b->d_ctrl, C * kCtrlStride * sizeof(float))) != cudaSuccess) return bail(e, "cudaMalloc(controls)");
   if ((e = cudaMemset(b->d_ctrl, 0, C * kCtrlStride * sizeof(float))) != cudaSuccess) return bail(e, "cudaMemset(controls)");
   if ((e = cudaMalloc(&b->d_meta, C * sizeof(SlotMeta))) != cudaSuccess) return bail(e, "cudaMalloc(meta)");
@@ -1295,12 +1302,12 @@ extern "C" int kr_batch_autotune(kr_batch *b, int32_t steps, int32_t *lanes_out,
   float *t_state = nullptr, *t_ctrl = nullptr;
   float4 *t_grip = nullptr;
   float2 *t_glam = nullptr;
-  double *t_cd = nullptr;
+  double2 *t_cd = nullptr;
   SlotMeta *t_meta = nullptr;
   cudaError_t e = cudaMalloc(&t_state, C * kStateStride * sizeof(float));
   if (e == cudaSuccess) e = cudaMalloc(&t_grip, C * KR_BATCH_MAX_ARMS * sizeof(float4));
   if (e == cudaSuccess) e = cudaMalloc(&t_glam, C * KR_BATCH_MAX_ARMS * sizeof(float2));
-  if (e == cudaSuccess) e = cudaMalloc(&t_cd, C * KR_BATCH_MAX_ARMS * sizeof(double));
+  if (e == cudaSuccess) e = cudaMalloc(&t_cd, C * KR_BATCH_MAX_ARMS * sizeof(double2));
   if (e == cudaSuccess) e = cudaMalloc(&t_ctrl, C * kCtrlStride * sizeof(float));
   if (e == cudaSuccess) e = cudaMalloc(&t_meta, C * sizeof(SlotMeta));
   auto copy_slots = [&](bool save) {
@@ -1312,7 +1319,7 @@ extern "C" int kr_batch_autotune(kr_batch *b, int32_t steps, int32_t *lanes_out,
     cp(t_state, b->d_state, C * kStateStride * sizeof(float));
     cp(t_grip, b->d_grip, C * KR_BATCH_MAX_ARMS * sizeof(float4));
     cp(t_glam, b->d_glam, C * KR_BATCH_MAX_ARMS * sizeof(float2));
-    cp(t_cd, b->d_cd, C * KR_BATCH_MAX_ARMS * sizeof(double));
+    cp(t_cd, b->d_cd, C * KR_BATCH_MAX_ARMS * sizeof(double2));
     cp(t_ctrl, b->d_ctrl, C * kCtrlStride * sizeof(float));
     cp(t_meta, b->d_meta, C * sizeof(SlotMeta));
     return r;
@@ -1530,7 +1537,7 @@ extern "C" int kr_batch_restore(kr_batch *b) {
   cudaError_t e = cudaMemcpyAsync(b->d_state, b->s_state, C * kStateStride * sizeof(float), cudaMemcpyDeviceToDevice, b->stream);
   if (e == cudaSuccess) e = cudaMemcpyAsync(b->d_grip, b->s_grip, C * KR_BATCH_MAX_ARMS * sizeof(float4), cudaMemcpyDeviceToDevice, b->stream);
   if (e == cudaSuccess) e = cudaMemcpyAsync(b->d_glam, b->s_glam, C * KR_BATCH_MAX_ARMS * sizeof(float2), cudaMemcpyDeviceToDevice, b->stream);
-  if (e == cudaSuccess) e = cudaMemcpyAsync(b->d_cd, b->s_cd, C * KR_BATCH_MAX_ARMS * sizeof(double), cudaMemcpyDeviceToDevice, b->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(b->d_cd, b->s_cd, C * KR_BATCH_MAX_ARMS * sizeof(double2), cudaMemcpyDeviceToDevice, b->stream);
   if (e == cudaSuccess) e = cudaMemcpyAsync(b->d_ctrl, b->s_ctrl, C * kCtrlStride * sizeof(float), cudaMemcpyDeviceToDevice, b->stream);
   if (e == cudaSuccess) e = cudaMemcpyAsync(b->d_meta, b->s_meta, C * sizeof(SlotMeta), cudaMemcpyDeviceToDevice, b->stream);
   if (e != cudaSuccess) return b->cuda_fail(e, "kr_batch_restore");

@@ -171,7 +171,7 @@ struct kr_batch {
   float *d_state = nullptr;
   float4 *d_grip = nullptr;
   float2 *d_glam = nullptr;
-  double *d_cd = nullptr;
+  double2 *d_cd = nullptr;           // per arm: reflex cooldown, f64 break force
   float *d_ctrl = nullptr;
   krb::SlotMeta *d_meta = nullptr;
   float *d_obs = nullptr;
@@ -183,7 +183,7 @@ struct kr_batch {
   float *s_state = nullptr;
   float4 *s_grip = nullptr;
   float2 *s_glam = nullptr;
-  double *s_cd = nullptr;
+  double2 *s_cd = nullptr;
   float *s_ctrl = nullptr;
   krb::SlotMeta *s_meta = nullptr;
   std::vector<int> s_remaining;

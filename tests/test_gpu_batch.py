@@ -47,6 +47,7 @@ def test_uneven_batch_bit_exact_vs_f32_oracle():
     st = eng.read_state()
     obs = eng.read_obs()
     assert np.all(st["steps"] == 40)
+    exact = total = 0
     for i in range(w.n):
         sim, grips, o_obs = _oracle_run(w, i, 40, record_obs=True)
         nb = sim.world.n
@@ -59,8 +60,13 @@ def test_uneven_batch_bit_exact_vs_f32_oracle():
         for s in range(40):
             p = obs[i, s, : 6 * A + 6]
             assert np.allclose(p, o_obs[s], atol=1e-6, rtol=0), (i, s)
+            exact += int(np.sum(p == o_obs[s].astype(np.float32)))
+            total += 6 * A + 6
             flags = int(obs[i, s, batch.OBS_STRIDE - 1].view(np.uint32))
             assert flags == sum(1 << a for a in range(A) if o_obs[s][5 * A + a] == 1.0)
+    # the f64 libm (atan2, sin, cos, hypot) may move an f32 rounding by one ulp
+    # now and then; everything else is the oracle's value bit for bit
+    assert exact >= 0.999 * total, (exact, total)
     eng.close()
 
 
