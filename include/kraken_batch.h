@@ -37,6 +37,15 @@ extern "C" {
 #define KR_CTRL_STREAM 0   /* per-creature mulberry32 stream, redrawn every period steps */
 #define KR_CTRL_BUFFER 1   /* host-provided buffer, one record per creature (kr_batch_set_controls) */
 #define KR_CTRL_POLICY 2   /* fused per-creature MLP on the proprioception vector */
+#define KR_CTRL_NET 3      /* the reference trainer's own recurrent net on proprioception + senses */
+
+/* KR_CTRL_NET sizes: net.js's HIDDEN, echo.js's ECHO_RAYS, lights per map
+ * (at most), and the strides of kr_batch_read_net */
+#define KR_NET_HIDDEN 24
+#define KR_NET_RAYS 12
+#define KR_NET_MAX_LIGHTS 8
+#define KR_NET_IN_STRIDE 128
+#define KR_NET_OUT_STRIDE 32
 
 typedef struct kr_batch kr_batch;
 
@@ -51,6 +60,14 @@ typedef struct kr_batch_desc {
   double grip_cooldown;        /* s, core.js:31 */
   int32_t control_mode;        /* KR_CTRL_* */
   int32_t control_period;      /* KR_CTRL_STREAM: steps between redraws (>= 1) */
+  /* KR_CTRL_NET only (NULL otherwise): every map's moving lights as makeMap
+   * draws them (src/world/map.js:60-69), x y r ir ph sp per light (f64),
+   * map_light_off (n_maps + 1 offsets, in lights, at most KR_NET_MAX_LIGHTS
+   * per map) and map_size (n_maps x width, height: the lights' clamp).
+   * NULL lights: no lights (the light sense reads the ambient level). */
+  const double *lights;
+  const int32_t *map_light_off;
+  const double *map_size;
 } kr_batch_desc;
 
 int kr_batch_create(const kr_batch_desc *desc, kr_batch **out);
@@ -83,6 +100,39 @@ int kr_batch_set_controls(kr_batch *b, const float *controls);
 #define KR_POLICY_HIDDEN 64
 int kr_batch_set_policy(kr_batch *b, const float *weights, int32_t n_individuals, int32_t n_params,
                         const int32_t *slot_individual);
+
+/* KR_CTRL_NET: the reference trainer's own controller (src/sim/train.js:
+ * 233-249, src/sim/gputrain.js:72-90) per slot and env step, on the device:
+ * the input vector -- readProprio (6A + 6 values), readSenses (core.js:
+ * 233-242: echo 2 x 12, chemoreception 6, light 3, hearing 4, tip contact A;
+ * without prey or other entities the chemoreception and hearing read 0) and
+ * the previous step's A_out = 3A + 2 outputs, n_in = 10A + 45 values, each
+ * rounded to f32 as the trainer's Float32Array holds it -- through net.js's
+ * forwardInto (src/brain/net.js:71-98: two tanh layers of KR_NET_HIDDEN and
+ * a tanh output layer, f64 sums of f32 products, tanh clamped to +-1 beyond
+ * +-20, activations rounded to f32), decode (net.js:124-133: tone, per arm
+ * shoulder, curl and adhesion, echo emission above 0.3) and applyControl
+ * with that tone.  After the XPBD step and postStep the senses advance as
+ * tickSenses does (core.js:245-267): the map's lights move (tickMapLights,
+ * map.js:75-83), the echo's cooldown runs and arrived echoes are written, an
+ * emission marches 12 rays against the map (echo.js:67-127), the light and
+ * contact senses are sampled.  A slot starts as a creature of a fresh sim:
+ * time 0, lights at the positions of the map description, sense buffers
+ * and recurrent outputs 0.  For A = 6 the network is net.js's 105 -> 24 ->
+ * 24 -> 20 with its 3,644 weights; other arm counts use the same layout with
+ * n_in = 10A + 45 and A_out outputs.
+ *
+ * genomes holds n_individuals weight vectors of n_params floats in net.js's
+ * layout (weightCount: n_in x 24, 24, 24 x 24, 24, 24 x A_out, A_out);
+ * n_params must be the count for the arms of every spawned slot that uses
+ * the vector; slot s uses vector slot_individual[s] (capacity entries). */
+int kr_batch_set_net(kr_batch *b, const float *genomes, int32_t n_individuals, int32_t n_params,
+                     const int32_t *slot_individual);
+
+/* KR_CTRL_NET: the input vector and outputs of each slot's last env step
+ * (synchronous): inputs n x KR_NET_IN_STRIDE f32 (n_in used), outputs n x
+ * KR_NET_OUT_STRIDE f32 (A_out used).  Either pointer may be NULL. */
+int kr_batch_read_net(kr_batch *b, int32_t first, int32_t n, float *inputs, float *outputs);
 
 /* Advance every live slot by min(max_steps, horizon - step) env steps with
  * one persistent launch.  Asynchronous; returns once enqueued. */

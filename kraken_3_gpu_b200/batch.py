@@ -25,7 +25,29 @@ MAX_BODIES = 1 + MAX_ARMS * MAX_SEGS
 OBS_STRIDE = 56
 CTRL_STRIDE = MAX_ARMS * (MAX_SEGS + 1)
 POLICY_HIDDEN = 64
-CONTROL_MODES = {"stream": 0, "buffer": 1, "policy": 2}
+CONTROL_MODES = {"stream": 0, "buffer": 1, "policy": 2, "net": 3}
+# KR_CTRL_NET: net.js HIDDEN, echo.js ECHO_RAYS, lights per map, read strides
+NET_HIDDEN = 24
+NET_RAYS = 12
+NET_MAX_LIGHTS = 8
+NET_IN_STRIDE = 128
+NET_OUT_STRIDE = 32
+
+
+def net_inputs(arms):
+    """Input size of the reference net for an arms-armed body (105 at 6 arms)."""
+    return 10 * arms + 45
+
+
+def net_outputs(arms):
+    """Outputs of the reference net: tone, 3 per arm, echo (20 at 6 arms)."""
+    return 3 * arms + 2
+
+
+def net_param_count(arms):
+    """net.js weightCount (3,644 at 6 arms)."""
+    ni, no, h = net_inputs(arms), net_outputs(arms), NET_HIDDEN
+    return ni * h + h + h * h + h + h * no + no
 # the reference's fitness metrics (postStep, src/sim/core.js:297-356) and score
 # (src/sim/fitness.js:115-172), in kr_batch_read_metrics order
 METRIC_FIELDS = ("score", "steps", "pathLen", "maxDisplacement", "spawnReach", "angularAccum",
@@ -44,7 +66,8 @@ class BatchDesc(C.Structure):
                 ("rects", _F32P), ("map_rect_off", _I32P), ("capacity", C.c_int32),
                 ("obs_ring", C.c_int32), ("grip_slip_max", C.c_double),
                 ("grip_cooldown", C.c_double), ("control_mode", C.c_int32),
-                ("control_period", C.c_int32)]
+                ("control_period", C.c_int32), ("lights", _F64P), ("map_light_off", _I32P),
+                ("map_size", _F64P)]
 
 
 _bound = False
@@ -62,6 +85,8 @@ def _lib():
                                      _I32P, _U32P, _F32P]),
         "kr_batch_set_controls": (C.c_int, [vp, _F32P]),
         "kr_batch_set_policy": (C.c_int, [vp, _F32P, i32, i32, _I32P]),
+        "kr_batch_set_net": (C.c_int, [vp, _F32P, i32, i32, _I32P]),
+        "kr_batch_read_net": (C.c_int, [vp, i32, i32, _F32P, _F32P]),
         "kr_batch_run": (C.c_int, [vp, i32]),
         "kr_batch_run_graph": (C.c_int, [vp, i32, i32, i32]),
         "kr_batch_run_launches": (C.c_int, [vp, i32, i32]),
@@ -106,7 +131,11 @@ class BatchEngine:
 
     def __init__(self, maps, capacity, obs_ring=0, control="stream", control_period=6,
                  substeps=2, iterations=4, h=1 / 120, lin_drag=3.0, ang_drag=3.0,
-                 max_speed=360.0, max_ang_speed=18.0, grip_slip_max=150.0, grip_cooldown=0.05):
+                 max_speed=360.0, max_ang_speed=18.0, grip_slip_max=150.0, grip_cooldown=0.05,
+                 lights=None, map_size=(1440.0, 810.0)):
+        """maps: per map an (n, 4) array of rects x y w h.  control="net":
+        lights, per map an (n, 6) array x y r ir ph sp (or None: no lights),
+        and map_size (width, height) of every map, the lights' clamp."""
         L = _lib()
         rect_list = [np.asarray(m, dtype=np.float32).reshape(-1, 4) for m in maps]
         off = np.zeros(len(rect_list) + 1, dtype=np.int32)
@@ -122,6 +151,20 @@ class BatchEngine:
                       len(rect_list), rects.ctypes.data_as(_F32P), off.ctypes.data_as(_I32P),
                       self.capacity, self.obs_ring, grip_slip_max, grip_cooldown,
                       CONTROL_MODES[control], control_period)
+        if control == "net" and lights is not None:
+            lv = [np.asarray(l, dtype=np.float64).reshape(-1, 6) for l in lights]
+            if len(lv) != len(rect_list):
+                raise ValueError("one light array per map")
+            loff = np.zeros(len(lv) + 1, dtype=np.int32)
+            for i, l in enumerate(lv):
+                loff[i + 1] = loff[i] + len(l)
+            self._lights = np.ascontiguousarray(np.concatenate(lv) if lv else np.zeros((0, 6)))
+            self._light_off = loff
+            self._map_size = np.ascontiguousarray(np.tile(np.asarray(map_size, np.float64),
+                                                          (len(lv), 1)))
+            d.lights = self._lights.ctypes.data_as(_F64P)
+            d.map_light_off = self._light_off.ctypes.data_as(_I32P)
+            d.map_size = self._map_size.ctypes.data_as(_F64P)
         self.h = C.c_void_p()
         rc = L.kr_batch_create(C.byref(d), C.byref(self.h))
         _check(rc, None)
@@ -165,6 +208,25 @@ class BatchEngine:
         idx = _arr(slot_individual, np.int32)
         _check(_lib().kr_batch_set_policy(self.h, w.ctypes.data_as(_F32P), w.shape[0], w.shape[1],
                                           idx.ctypes.data_as(_I32P)), self.h)
+
+    def set_net(self, genomes, slot_individual):
+        """control="net": genomes (n_individuals, net_param_count(arms)) f32 in
+        net.js's layout; slot s uses genome slot_individual[s]."""
+        g = _arr(genomes, np.float32)
+        g = g.reshape(g.shape[0], -1)
+        idx = _arr(slot_individual, np.int32)
+        _check(_lib().kr_batch_set_net(self.h, g.ctypes.data_as(_F32P), g.shape[0], g.shape[1],
+                                       idx.ctypes.data_as(_I32P)), self.h)
+
+    def read_net(self, first=0, n=None):
+        """control="net": (inputs (n, NET_IN_STRIDE), outputs (n, NET_OUT_STRIDE))
+        f32 of each slot's last env step (net_inputs / net_outputs used)."""
+        n = self.capacity - first if n is None else n
+        x = np.zeros((n, NET_IN_STRIDE), dtype=np.float32)
+        o = np.zeros((n, NET_OUT_STRIDE), dtype=np.float32)
+        _check(_lib().kr_batch_read_net(self.h, first, n, x.ctypes.data_as(_F32P),
+                                        o.ctypes.data_as(_F32P)), self.h)
+        return x, o
 
     def snapshot(self):
         _check(_lib().kr_batch_snapshot(self.h), self.h)

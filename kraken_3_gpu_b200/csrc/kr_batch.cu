@@ -53,10 +53,16 @@ struct BatchArgs {
   int obs_ring;
   double slip_max, cooldown, inv_h64, dt, h64;
   int substeps;
-  // policy
-  const float *pw;       // n_individuals x pw_stride, device layout (see policy())
+  // policy (KR_CTRL_POLICY: device layout, see policy(); KR_CTRL_NET: net.js layout)
+  const float *pw;       // n_individuals x pw_stride
   const int *pw_idx;     // individual of each slot
   int pw_stride;
+  // KR_CTRL_NET
+  NetRec *net;           // capacity records
+  const double *rects64; // x y w h per rect, f64 of the f32 values (offsets map_off)
+  const double *lights;  // x y r ir ph sp per light
+  const int *light_off;  // n_maps + 1, or null: no lights
+  const double *map_size;
 };
 
 // --- shared-memory layout, carved per template ------------------------------
@@ -287,6 +293,203 @@ __device__ void policy(const BatchArgs &A, const TplDev &td, CreatureSmem &X, in
   L.sync();
 }
 
+// net.js's activation: tanh, clamped to +-1 beyond +-20, stored in a Float32Array
+__device__ __forceinline__ float net_act(double s) { return (float)(s > 20 ? 1.0 : (s < -20 ? -1.0 : tanh(s))); }
+
+// What the KR_CTRL_NET steps read of BatchArgs, passed by value so that the
+// non-inlined calls take no address of the kernel's arguments or state.
+struct NetArgs {
+  NetRec *net;
+  SlotMeta *meta;
+  const float *pw;
+  const int *pw_idx;
+  int pw_stride;
+  const double *rects64;
+  const int *map_off;
+  const double *lights;
+  const int *light_off;
+  const double *map_size;
+  double dt;
+};
+
+__device__ __forceinline__ NetArgs net_args(const BatchArgs &A) {
+  return NetArgs{A.net, A.meta, A.pw, A.pw_idx, A.pw_stride, A.rects64, A.map_off, A.lights, A.light_off,
+                 A.map_size, A.dt};
+}
+
+// KR_CTRL_NET, before the step: the trainer's input vector (train.js:236-241:
+// readProprio -- already in obs --, readSenses, the previous outputs),
+// forwardInto (net.js:71-98; the second layer's bias is read at b2 + j, as
+// the reference reads it) and decode + applyControl's tone (net.js:124-133,
+// core.js:185-199).  Writes the per-motor controls and adhesion values to
+// ctrl and the emission wish to the record; returns the compliance of the
+// tone.  G lanes: input entries, then hidden / output units, strided.
+template <int G>
+__device__ __noinline__ float net_control(NetArgs N, int arms, int segs, const float *obs, float *ctrl, int slot,
+                                          kr::Lanes<G> L) {
+  NetRec &R = N.net[slot];
+  const int lane = L.lane;
+  const int np = 6 * arms + 6, ni = net_inputs(arms), no = net_outputs(arms), H = KR_NET_HIDDEN;
+  constexpr int E = 2 * KR_NET_RAYS;  // echo entries, then chem 6, light 3, hearing 4, contact
+  for (int q = lane; q < ni; q += G) {
+    float v;
+    const int r = q - np;
+    if (q < np) v = obs[q];
+    else if (r < E) v = (r & 1) ? R.inten[r >> 1] : R.range[r >> 1];
+    else if (r < E + 6) v = 0.f;                              // chemoreception: no scent sources
+    else if (r < E + 9) v = R.light_v[r - E - 6];
+    else if (r < E + 13) v = 0.f;                             // hearing: no noise sources
+    else if (r < E + 13 + arms) v = (float)R.contact[r - E - 13];
+    else v = R.out[r - E - 13 - arms];                        // recurrent: last step's outputs
+    R.x[q] = v;
+  }
+  L.sync();
+  const float *w = N.pw + (size_t)N.pw_idx[slot] * N.pw_stride;
+  const int b1 = ni * H, b2 = b1 + H, b3 = b2 + H * H, b4 = b3 + H, b5 = b4 + H * no;
+  for (int j = lane; j < H; j += G) {
+    double acc = w[b1 + j];
+    const float *row = w + (size_t)j * ni;
+    for (int i = 0; i < ni; i++) acc += (double)R.x[i] * (double)row[i];
+    R.h[j] = net_act(acc);
+  }
+  L.sync();
+  for (int j = lane; j < H; j += G) {
+    double acc = w[b2 + j];
+    const float *row = w + b3 - H * H + j * H;
+    for (int i = 0; i < H; i++) acc += (double)R.h[i] * (double)row[i];
+    R.h[H + j] = net_act(acc);
+  }
+  L.sync();
+  for (int j = lane; j < no; j += G) {
+    double acc = w[b5 + j];
+    const float *row = w + b4 + j * H;
+    for (int i = 0; i < H; i++) acc += (double)R.h[H + i] * (double)row[i];
+    R.out[j] = net_act(acc);
+  }
+  L.sync();
+  // decode: motor 0 of arm a takes its shoulder output, the distal motors its curl
+  const int AS = arms * segs;
+  for (int q = lane; q < AS; q += G) {
+    const int a = q / segs;
+    ctrl[q] = R.out[(q % segs) == 0 ? 1 + 3 * a : 2 + 3 * a];
+  }
+  for (int a = lane; a < arms; a += G) {
+    const float v = R.out[3 + 3 * a];
+    ctrl[AS + a] = v > 0.f ? v : 0.f;
+  }
+  const double tone = fmax(0.0, fmin(1.0, 0.5 + 0.5 * (double)R.out[0]));
+  if (lane == 0) {
+    N.meta[slot].tone_d = tone;
+    R.wants_emit = (double)R.out[no - 1] > 0.3 ? 1 : 0;
+  }
+  L.sync();
+  return (float)(1.0 / (2000.0 + tone * (400000.0 - 2000.0)));  // toneToCompliance
+}
+
+// sampleAt, src/senses/light.js:99-106
+__device__ __forceinline__ double light_at(const double *lp, const double *xy, int nl, double x, double y) {
+  double v = 0.05;
+  for (int l = 0; l < nl; l++) {
+    const double d = hypot(x - xy[2 * l], y - xy[2 * l + 1]);
+    v += fmax(0.0, 1 - d / lp[6 * l + 2]) * lp[6 * l + 3];
+  }
+  return fmin(1.0, v);
+}
+
+// KR_CTRL_NET, after postStep: sim.time += dt, tickMapLights (map.js:75-83)
+// on the creature's copy of its map's lights, then tickSenses (core.js:
+// 245-267) without entities: the echo's tick (echo.js:120-127) and, when
+// the net asked for it and the cooldown allows, an emission (echo.js:67-85:
+// 12 rays over the fan, lanes strided, arrivals inserted in arrival order
+// after equal times, as the stable sort after the push orders them); the
+// light sense (light.js:90-97) and the tip contact per arm.
+template <int G>
+__device__ __noinline__ void net_senses(NetArgs N, int arms, const int *arm_tip, const float *px, const float *py,
+                                        const float *ang, int map, int slot, kr::Lanes<G> L) {
+  NetRec &R = N.net[slot];
+  const int lane = L.lane;
+  const int ro = N.map_off[map], nR = N.map_off[map + 1] - ro;
+  const double *rects = N.rects64 + 4 * (size_t)ro;
+  const double x = px[0], y = py[0];
+  const double heading = (double)ang[0] - kPiD * 0.5;
+  const double dt = N.dt;
+  int emit = 0;
+  if (lane == 0) {
+    const double time = R.time + dt;
+    R.time = time;
+    const int lo = N.light_off ? N.light_off[map] : 0, nl = N.light_off ? N.light_off[map + 1] - lo : 0;
+    const double *lp = N.lights + 6 * (size_t)lo;
+    const double mw = nl ? N.map_size[2 * map] : 0, mh = nl ? N.map_size[2 * map + 1] : 0;
+    for (int l = 0; l < nl; l++) {
+      const double a = time * lp[6 * l + 5] + lp[6 * l + 4];
+      R.light_xy[2 * l] = fmax(60.0, fmin(mw - 60, R.light_xy[2 * l] + cos(a) * 18 * dt));
+      R.light_xy[2 * l + 1] = fmax(60.0, fmin(mh - 60, R.light_xy[2 * l + 1] + sin(a * 0.8) * 18 * dt));
+    }
+    if (R.cooldown > 0) R.cooldown -= dt;
+    int k = 0;
+    while (k < R.n_pending && R.p_at[k] <= time) {
+      R.range[R.p_ray[k]] = R.p_range[k];
+      R.inten[R.p_ray[k]] = R.p_inten[k];
+      k++;
+    }
+    for (int q = k; q < R.n_pending; q++) {
+      R.p_at[q - k] = R.p_at[q]; R.p_ray[q - k] = R.p_ray[q];
+      R.p_range[q - k] = R.p_range[q]; R.p_inten[q - k] = R.p_inten[q];
+    }
+    R.n_pending -= k;
+    if (R.wants_emit && !(R.cooldown > 0)) {
+      R.cooldown = kEchoInterval;
+      R.emit_count++;
+      emit = 1;
+    }
+    // light.js sample: left / right receptors 26 px across the heading
+    const double perp = heading + kPiD / 2;
+    const double lx = x + cos(perp) * 26, ly = y + sin(perp) * 26;
+    const double rx = x - cos(perp) * 26, ry = y - sin(perp) * 26;
+    R.light_v[0] = (float)light_at(lp, R.light_xy, nl, lx, ly);
+    R.light_v[1] = (float)light_at(lp, R.light_xy, nl, rx, ry);
+    R.light_v[2] = (float)light_at(lp, R.light_xy, nl, x, y);
+  }
+  emit = __shfl_sync(L.mask, emit, 0, G);
+  if (emit) {
+    for (int i = lane; i < KR_NET_RAYS; i += G) {
+      const double t = (double)i / (KR_NET_RAYS - 1);
+      const double a = heading + (t - 0.5) * (kPiD * 0.85);
+      R.ray_d[i] = echo_march(rects, nR, x, y, cos(a), sin(a), kEchoRange);
+    }
+    L.sync();
+    if (lane == 0) {
+      const double time = R.time;
+      for (int i = 0; i < KR_NET_RAYS; i++) {
+        const double d = R.ray_d[i];
+        if (d >= kEchoRange) continue;
+        const double inten = fmin(1.0, (kEchoRange * 0.22) / fmax(8.0, d * d / kEchoRange));
+        const double at = time + (2 * d) / kEchoSpeed;
+        if (R.n_pending >= kEchoPending) { R.dropped++; continue; }
+        int q = R.n_pending;
+        while (q > 0 && R.p_at[q - 1] > at) {
+          R.p_at[q] = R.p_at[q - 1]; R.p_ray[q] = R.p_ray[q - 1];
+          R.p_range[q] = R.p_range[q - 1]; R.p_inten[q] = R.p_inten[q - 1];
+          q--;
+        }
+        R.p_at[q] = at; R.p_ray[q] = i;
+        R.p_range[q] = (float)(d / kEchoRange); R.p_inten[q] = (float)inten;
+        R.n_pending++;
+      }
+    }
+  }
+  // tip contact: near = max(0, 1 - d / 9) of the map's SDF at the tip point
+  for (int a = lane; a < arms; a += G) {
+    const int tip = arm_tip[a];
+    const double ta = ang[tip];
+    const double tx = (double)px[tip] + kSegHalf * cos(ta), ty = (double)py[tip] + kSegHalf * sin(ta);
+    double d;
+    const double near = sdf64(rects, nR, tx, ty, &d) ? fmax(0.0, 1 - d / 9) : 0.0;
+    R.contact[a] = R.contact[a] * 0.7 + near * 0.3;
+  }
+  L.sync();
+}
+
 // One creature (slot) advanced by its G lanes for up to A.max_steps env steps.
 template <int G>
 __device__ void run_creature(const BatchArgs &A, const TplDev &td, int nlv, const TplSmem &P, float *base,
@@ -323,7 +526,7 @@ __device__ void run_creature(const BatchArgs &A, const TplDev &td, int nlv, cons
   for (int s = 0; s < steps; s++) {
     const int t = m.step;
     // 1. proprioception of the current state
-    if (A.obs_ring > 0 || m.ctrl == KR_CTRL_POLICY) {
+    if (A.obs_ring > 0 || m.ctrl == KR_CTRL_POLICY || m.ctrl == KR_CTRL_NET) {
       const unsigned att = proprio<G>(A, td, P, S, X, m, cdp, L);
       if (A.obs_ring > 0) {
         float *o = A.obs + ((size_t)slot * A.obs_ring + (t % A.obs_ring)) * KR_OBS_STRIDE;
@@ -343,6 +546,8 @@ __device__ void run_creature(const BatchArgs &A, const TplDev &td, int nlv, cons
       }
     } else if (m.ctrl == KR_CTRL_POLICY) {
       policy<G>(A, td, X, slot, L);
+    } else if (m.ctrl == KR_CTRL_NET) {
+      S.comp_m = net_control<G>(net_args(A), arms, td.segs, X.obs, X.ctrl, slot, L);
     }
     L.sync();
     // 3. applyControl: targets (clamped) and the reflex, core.js:183-220
@@ -417,6 +622,7 @@ __device__ void run_creature(const BatchArgs &A, const TplDev &td, int nlv, cons
       g.max_disp = fmax(g.max_disp, d_spawn);
       g.last_x = x; g.last_y = y;
     }
+    if (m.ctrl == KR_CTRL_NET) net_senses<G>(net_args(A), arms, P.arm_tip, S.px, S.py, S.ang, m.map, slot, L);
     m.step = t + 1;
   }
   // write back (the committed state is already in place)
@@ -487,17 +693,28 @@ __global__ void __launch_bounds__(32 * kMaxW, 1) batch_kernel(BatchArgs A) {
   }
 }
 
-// writes n prepared creatures into slots[0..n): pose, released grips, zero
-// lambda / cooldown / controls, meta
 // one block per spawned creature: copies its pose and metadata into the slot,
 // clears its grips and controls, and measures its spawn reach (16 threads,
-// one ray each; init's spawn_reach holds the body's arm reach on entry)
+// one ray each; init's spawn_reach holds the body's arm reach on entry);
+// with net records, clears the slot's record and places its copy of the
+// map's lights
 __global__ void spawn_kernel(float *state, float4 *grip, float2 *glam, double2 *cd, SlotMeta *meta,
                              float *ctrl, const int *slots, const float *pose, const SlotMeta *init, int n,
-                             const double *rects, const int *map_off, RayDirs rays) {
+                             const double *rects, const int *map_off, RayDirs rays, NetRec *net,
+                             const double *lights, const int *light_off) {
   __shared__ double ray_d[16];
   const int i = blockIdx.x;
   if (i >= n) return;
+  if (net) {
+    NetRec *R = net + slots[i];
+    uint32_t *words = reinterpret_cast<uint32_t *>(R);
+    for (int q = threadIdx.x; q < (int)(sizeof(NetRec) / 4); q += blockDim.x) words[q] = 0u;
+    __syncthreads();
+    if (light_off && threadIdx.x < 2 * KR_NET_MAX_LIGHTS) {
+      const int map = init[i].map, lo = light_off[map], nl = light_off[map + 1] - lo, l = threadIdx.x >> 1;
+      if (l < nl) R->light_xy[threadIdx.x] = lights[6 * (size_t)(lo + l) + (threadIdx.x & 1)];
+    }
+  }
   if (threadIdx.x < 16) {
     const SlotMeta &m = init[i];
     const int o = map_off[m.map], nr = map_off[m.map + 1] - o;
@@ -732,6 +949,14 @@ int build_groups(kr_batch *b, Part &p, int max_steps) {
   }
   for (int s : live) {
     const SlotMeta &m = b->h_meta[s];
+    if (m.ctrl == KR_CTRL_NET) {
+      if (!b->d_pw || b->h_pw_idx.size() != (size_t)b->capacity)
+        return b->fail(KR_ERR_STATE, "slot " + std::to_string(s) + ": net control without kr_batch_set_net");
+      if (b->h_pw_arms[b->h_pw_idx[s]] != b->tpls[m.tpl].arms)
+        return b->fail(KR_ERR_STATE, "slot " + std::to_string(s) + ": its genome was set for another arm "
+                                         "count (kr_batch_set_net after the spawn)");
+      continue;
+    }
     if (m.ctrl != KR_CTRL_POLICY) continue;
     if (!b->d_pw || b->h_pw_idx.size() != (size_t)b->capacity)
       return b->fail(KR_ERR_STATE, "slot " + std::to_string(s) + ": policy control without kr_batch_set_policy");
@@ -861,7 +1086,7 @@ int launch_part(kr_batch *b, Part &p, int max_steps, bool timed) {
     auto count = [&](int s) {
       if (b->h_remaining[s] <= 0 || b->h_meta[s].horizon <= 0) return;
       live++;
-      per_arm += b->h_meta[s].ctrl == KR_CTRL_POLICY;
+      per_arm += b->h_meta[s].ctrl == KR_CTRL_POLICY || b->h_meta[s].ctrl == KR_CTRL_NET;
     };
     if (p.all) {
       for (int s = 0; s < b->capacity; s++) count(s);
@@ -899,6 +1124,8 @@ int launch_part(kr_batch *b, Part &p, int max_steps, bool timed) {
   A.h64 = b->d.solver.h;
   A.substeps = b->d.solver.substeps;
   A.pw = b->d_pw; A.pw_idx = b->d_pw_idx; A.pw_stride = b->pw_stride;
+  A.net = b->d_net; A.rects64 = b->d_rects64; A.lights = b->d_lights; A.light_off = b->d_light_off;
+  A.map_size = b->d_map_size;
   cudaError_t e;
   if ((e = cudaMemsetAsync(p.d_queue, 0, sizeof(int), st)) != cudaSuccess) return b->cuda_fail(e, "queue reset");
   if (timed) cudaEventRecord(p.ev0, st);
@@ -971,7 +1198,8 @@ cudaError_t launch_spawn(kr_batch *b, const int *d_slots, const float *d_pose, c
                          int n, cudaStream_t stream) {
   if (n <= 0) return cudaSuccess;
   spawn_kernel<<<n, 128, 0, stream>>>(b->d_state, b->d_grip, b->d_glam, b->d_cd, b->d_meta, b->d_ctrl,
-                                      d_slots, d_pose, d_meta, n, b->d_rects64, b->d_map_off, b->rays);
+                                      d_slots, d_pose, d_meta, n, b->d_rects64, b->d_map_off, b->rays,
+                                      b->d_net, b->d_lights, b->d_light_off);
   return cudaGetLastError();
 }
 
@@ -997,7 +1225,23 @@ extern "C" int kr_batch_create(const kr_batch_desc *desc, kr_batch **out) {
   if (d.n_maps < 1 || !d.rects || !d.map_rect_off) { g_batch_error = "need at least one map"; return KR_ERR_INVALID; }
   if (d.capacity < 1 || d.capacity > (1 << 24)) { g_batch_error = "capacity out of range"; return KR_ERR_INVALID; }
   if (d.obs_ring < 0 || d.obs_ring > 4096) { g_batch_error = "obs_ring out of range 0..4096"; return KR_ERR_INVALID; }
-  if (d.control_mode < 0 || d.control_mode > 2) { g_batch_error = "unknown control mode"; return KR_ERR_INVALID; }
+  if (d.control_mode < 0 || d.control_mode > KR_CTRL_NET) { g_batch_error = "unknown control mode"; return KR_ERR_INVALID; }
+  if (d.control_mode == KR_CTRL_NET && d.lights) {
+    if (!d.map_light_off || !d.map_size) { g_batch_error = "lights without map_light_off / map_size"; return KR_ERR_INVALID; }
+    for (int m = 0; m < d.n_maps; m++) {
+      const int n = d.map_light_off[m + 1] - d.map_light_off[m];
+      if (d.map_light_off[m] < 0 || n < 0 || n > KR_NET_MAX_LIGHTS) {
+        g_batch_error = "map " + std::to_string(m) + ": " + std::to_string(n) + " lights (0.." +
+                        std::to_string(KR_NET_MAX_LIGHTS) + ")";
+        return KR_ERR_INVALID;
+      }
+      for (int l = d.map_light_off[m]; l < d.map_light_off[m + 1]; l++)
+        if (!(d.lights[6 * (size_t)l + 2] > 0)) {
+          g_batch_error = "map " + std::to_string(m) + ": light radius must be positive";
+          return KR_ERR_INVALID;
+        }
+    }
+  }
   if (d.control_mode == KR_CTRL_STREAM && d.control_period < 1) { g_batch_error = "control_period < 1"; return KR_ERR_INVALID; }
   for (int m = 0; m < d.n_maps; m++) {
     const int n = d.map_rect_off[m + 1] - d.map_rect_off[m];
@@ -1016,6 +1260,9 @@ extern "C" int kr_batch_create(const kr_batch_desc *desc, kr_batch **out) {
   b->d = d;
   b->d.rects = nullptr;
   b->d.map_rect_off = nullptr;
+  b->d.lights = nullptr;
+  b->d.map_light_off = nullptr;
+  b->d.map_size = nullptr;
   b->capacity = d.capacity;
   b->n_maps = d.n_maps;
   kr::SolverConsts &K = b->K;
@@ -1081,6 +1328,19 @@ extern "C" int kr_batch_create(const kr_batch_desc *desc, kr_batch **out) {
   if (d.obs_ring > 0) {
     if ((e = cudaMalloc(&b->d_obs, C * d.obs_ring * KR_OBS_STRIDE * sizeof(float))) != cudaSuccess) return bail(e, "cudaMalloc(obs)");
     if ((e = cudaMemset(b->d_obs, 0, C * d.obs_ring * KR_OBS_STRIDE * sizeof(float))) != cudaSuccess) return bail(e, "cudaMemset(obs)");
+  }
+  if (d.control_mode == KR_CTRL_NET) {
+    if ((e = cudaMalloc(&b->d_net, C * sizeof(NetRec))) != cudaSuccess) return bail(e, "cudaMalloc(net records)");
+    if ((e = cudaMemset(b->d_net, 0, C * sizeof(NetRec))) != cudaSuccess) return bail(e, "cudaMemset(net records)");
+    if (d.lights) {
+      const int nl = d.map_light_off[d.n_maps];
+      std::vector<double> lv(d.lights, d.lights + 6 * (size_t)nl);
+      std::vector<int> lo(d.map_light_off, d.map_light_off + d.n_maps + 1);
+      std::vector<double> ms(d.map_size, d.map_size + 2 * (size_t)d.n_maps);
+      if ((e = upload_vec(&b->d_lights, lv)) != cudaSuccess) return bail(e, "upload(lights)");
+      if ((e = upload_vec(&b->d_light_off, lo)) != cudaSuccess) return bail(e, "upload(light offsets)");
+      if ((e = upload_vec(&b->d_map_size, ms)) != cudaSuccess) return bail(e, "upload(map sizes)");
+    }
   }
   b->h_meta.assign(C, SlotMeta{});
   b->h_remaining.assign(C, 0);
@@ -1202,6 +1462,80 @@ extern "C" int kr_batch_set_policy(kr_batch *b, const float *weights, int32_t n_
   return KR_OK;
 }
 
+extern "C" int kr_batch_set_net(kr_batch *b, const float *genomes, int32_t n_individuals, int32_t n_params,
+                                const int32_t *slot_individual) {
+  if (!b) return KR_ERR_INVALID;
+  if (b->d.control_mode != KR_CTRL_NET) return b->fail(KR_ERR_STATE, "kr_batch_set_net on an engine without KR_CTRL_NET");
+  if (!genomes || !slot_individual || n_individuals <= 0 || n_params <= 0)
+    return b->fail(KR_ERR_INVALID, "kr_batch_set_net: null argument or empty genome set");
+  // the arm count of every individual: that of the spawned slots using it
+  std::vector<int> ind_arms(n_individuals, -1);
+  for (int s = 0; s < b->capacity; s++) {
+    if (slot_individual[s] < 0 || slot_individual[s] >= n_individuals)
+      return b->fail(KR_ERR_INDEX, "slot " + std::to_string(s) + " refers to individual " +
+                                       std::to_string(slot_individual[s]) + " of " + std::to_string(n_individuals));
+    const SlotMeta &m = b->h_meta[s];
+    if (m.horizon <= 0) continue;
+    const int arms = b->tpls[m.tpl].arms, need = net_param_count(arms);
+    if (n_params != need)
+      return b->fail(KR_ERR_INVALID, "slot " + std::to_string(s) + ": a " + std::to_string(arms) +
+                                         "-armed body's net has " + std::to_string(need) + " weights, got " +
+                                         std::to_string(n_params));
+    int &ia = ind_arms[slot_individual[s]];
+    if (ia >= 0 && ia != arms)
+      return b->fail(KR_ERR_INVALID, "individual " + std::to_string(slot_individual[s]) +
+                                         " is used by two arm counts");
+    ia = arms;
+  }
+  const int stride = (n_params + 3) & ~3;
+  std::vector<float> dev((size_t)n_individuals * stride, 0.f);
+  for (int k = 0; k < n_individuals; k++)
+    std::memcpy(dev.data() + (size_t)k * stride, genomes + (size_t)k * n_params, n_params * sizeof(float));
+  const size_t need = dev.size();
+  cudaError_t e = cudaStreamSynchronize(b->stream);
+  if (e != cudaSuccess) return b->cuda_fail(e, "kr_batch_set_net sync");
+  if (!b->d_pw || b->pw_capacity < need) {
+    if (b->d_pw) cudaFree(b->d_pw);
+    b->d_pw = nullptr;
+    e = cudaMalloc(&b->d_pw, need * sizeof(float));
+    if (e != cudaSuccess) return b->cuda_fail(e, "cudaMalloc(genomes)");
+    b->pw_capacity = need;
+  }
+  if (!b->d_pw_idx) {
+    e = cudaMalloc(&b->d_pw_idx, (size_t)b->capacity * sizeof(int));
+    if (e != cudaSuccess) return b->cuda_fail(e, "cudaMalloc(genome index)");
+  }
+  e = cudaMemcpyAsync(b->d_pw, dev.data(), need * sizeof(float), cudaMemcpyHostToDevice, b->stream);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(b->d_pw_idx, slot_individual, (size_t)b->capacity * sizeof(int), cudaMemcpyHostToDevice,
+                        b->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
+  if (e != cudaSuccess) return b->cuda_fail(e, "kr_batch_set_net");
+  b->n_individuals = n_individuals;
+  b->pw_stride = stride;
+  b->h_pw_idx.assign(slot_individual, slot_individual + b->capacity);
+  b->h_pw_arms = ind_arms;
+  return KR_OK;
+}
+
+extern "C" int kr_batch_read_net(kr_batch *b, int32_t first, int32_t n, float *inputs, float *outputs) {
+  if (!b) return KR_ERR_INVALID;
+  if (!b->d_net) return b->fail(KR_ERR_STATE, "kr_batch_read_net on an engine without KR_CTRL_NET");
+  if (first < 0 || n < 0 || first + n > b->capacity) return b->fail(KR_ERR_INVALID, "read range outside the slots");
+  if (n == 0) return KR_OK;
+  const NetRec *src = b->d_net + first;
+  cudaError_t e = cudaSuccess;
+  if (inputs)
+    e = cudaMemcpy2DAsync(inputs, KR_NET_IN_STRIDE * sizeof(float), src->x, sizeof(NetRec),
+                          KR_NET_IN_STRIDE * sizeof(float), n, cudaMemcpyDeviceToHost, b->stream);
+  if (e == cudaSuccess && outputs)
+    e = cudaMemcpy2DAsync(outputs, KR_NET_OUT_STRIDE * sizeof(float), src->out, sizeof(NetRec),
+                          KR_NET_OUT_STRIDE * sizeof(float), n, cudaMemcpyDeviceToHost, b->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
+  if (e != cudaSuccess) return b->cuda_fail(e, "kr_batch_read_net");
+  return KR_OK;
+}
+
 extern "C" int kr_batch_set_launch(kr_batch *b, int32_t lanes_per_creature, int32_t warps_per_cta,
                                    int32_t ctas_per_sm) {
   if (!b) return KR_ERR_INVALID;
@@ -1304,12 +1638,14 @@ extern "C" int kr_batch_autotune(kr_batch *b, int32_t steps, int32_t *lanes_out,
   float2 *t_glam = nullptr;
   double2 *t_cd = nullptr;
   SlotMeta *t_meta = nullptr;
+  NetRec *t_net = nullptr;
   cudaError_t e = cudaMalloc(&t_state, C * kStateStride * sizeof(float));
   if (e == cudaSuccess) e = cudaMalloc(&t_grip, C * KR_BATCH_MAX_ARMS * sizeof(float4));
   if (e == cudaSuccess) e = cudaMalloc(&t_glam, C * KR_BATCH_MAX_ARMS * sizeof(float2));
   if (e == cudaSuccess) e = cudaMalloc(&t_cd, C * KR_BATCH_MAX_ARMS * sizeof(double2));
   if (e == cudaSuccess) e = cudaMalloc(&t_ctrl, C * kCtrlStride * sizeof(float));
   if (e == cudaSuccess) e = cudaMalloc(&t_meta, C * sizeof(SlotMeta));
+  if (e == cudaSuccess && b->d_net) e = cudaMalloc(&t_net, C * sizeof(NetRec));
   auto copy_slots = [&](bool save) {
     cudaError_t r = cudaSuccess;
     auto cp = [&](void *keep, void *live, size_t bytes) {
@@ -1322,6 +1658,7 @@ extern "C" int kr_batch_autotune(kr_batch *b, int32_t steps, int32_t *lanes_out,
     cp(t_cd, b->d_cd, C * KR_BATCH_MAX_ARMS * sizeof(double2));
     cp(t_ctrl, b->d_ctrl, C * kCtrlStride * sizeof(float));
     cp(t_meta, b->d_meta, C * sizeof(SlotMeta));
+    if (b->d_net) cp(t_net, b->d_net, C * sizeof(NetRec));
     return r;
   };
   const std::vector<int> rem0 = b->h_remaining;
@@ -1346,6 +1683,7 @@ extern "C" int kr_batch_autotune(kr_batch *b, int32_t steps, int32_t *lanes_out,
   }
   if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
   cudaFree(t_state); cudaFree(t_grip); cudaFree(t_glam); cudaFree(t_cd); cudaFree(t_ctrl); cudaFree(t_meta);
+  if (t_net) cudaFree(t_net);
   b->h_remaining = rem0;
   b->main.dirty = true;
   if (rc != KR_OK) return rc;
@@ -1496,7 +1834,8 @@ extern "C" void kr_batch_destroy(kr_batch *b) {
   void *ptrs[] = {b->d_tpl, const_cast<int *>(b->T.arm_segs), b->d_rects, b->d_map_off, b->d_map_cull, b->d_rects64,
                   b->d_state, b->d_grip, b->d_glam, b->d_cd, b->d_ctrl, b->d_meta, b->d_obs,
                   b->d_pw, b->d_pw_idx, b->s_state, b->s_grip, b->s_glam, b->s_cd,
-                  b->s_ctrl, b->s_meta, b->s_groups};
+                  b->s_ctrl, b->s_meta, b->s_groups, b->d_net, b->s_net, b->d_lights, b->d_light_off,
+                  b->d_map_size};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   if (b->own_stream && b->stream) cudaStreamDestroy(b->stream);
@@ -1523,6 +1862,7 @@ extern "C" int kr_batch_snapshot(kr_batch *b) {
   if (e == cudaSuccess) e = copy_all(&b->s_cd, b->d_cd, C * KR_BATCH_MAX_ARMS, b->stream);
   if (e == cudaSuccess) e = copy_all(&b->s_ctrl, b->d_ctrl, C * kCtrlStride, b->stream);
   if (e == cudaSuccess) e = copy_all(&b->s_meta, b->d_meta, C, b->stream);
+  if (e == cudaSuccess && b->d_net) e = copy_all(&b->s_net, b->d_net, C, b->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
   if (e != cudaSuccess) return b->cuda_fail(e, "kr_batch_snapshot");
   b->s_remaining = b->h_remaining;
@@ -1540,6 +1880,8 @@ extern "C" int kr_batch_restore(kr_batch *b) {
   if (e == cudaSuccess) e = cudaMemcpyAsync(b->d_cd, b->s_cd, C * KR_BATCH_MAX_ARMS * sizeof(double2), cudaMemcpyDeviceToDevice, b->stream);
   if (e == cudaSuccess) e = cudaMemcpyAsync(b->d_ctrl, b->s_ctrl, C * kCtrlStride * sizeof(float), cudaMemcpyDeviceToDevice, b->stream);
   if (e == cudaSuccess) e = cudaMemcpyAsync(b->d_meta, b->s_meta, C * sizeof(SlotMeta), cudaMemcpyDeviceToDevice, b->stream);
+  if (e == cudaSuccess && b->d_net && b->s_net)
+    e = cudaMemcpyAsync(b->d_net, b->s_net, C * sizeof(NetRec), cudaMemcpyDeviceToDevice, b->stream);
   if (e != cudaSuccess) return b->cuda_fail(e, "kr_batch_restore");
   b->h_remaining = b->s_remaining;
   // the work groups of the snapshot state: built once, then copied back

@@ -81,36 +81,100 @@ __host__ __device__ inline int policy_device_index(int arms, int segs, int p) {
   return H * (n_in + 1) + (q % (H + 1)) * n_out + q / (H + 1);
 }
 
+// makeSdf's distance (src/world/map.js:91-118) in f64 over rects x y w h:
+// false where the JS returns null (no finite winner).  Host and device run
+// this same code (IEEE f64 add, multiply and sqrt; min / max as std::min /
+// std::max).
+__host__ __device__ inline bool sdf64(const double *rects, int n, double px, double py, double *out) {
+  double best = INFINITY;
+  const double *r = rects;
+  for (int i = 0; i < n; i++, r += 4) {
+    const double xr = r[0] + r[2], yb = r[1] + r[3];
+    const double mx = xr < px ? xr : px, my = yb < py ? yb : py;
+    const double cx = r[0] < mx ? mx : r[0], cy = r[1] < my ? my : r[1];
+    const double dx = px - cx, dy = py - cy, d2 = dx * dx + dy * dy;
+    if (d2 > 1e-12) {
+      if (d2 < best * best) best = sqrt(d2);
+    } else {
+      const double a = px - r[0], b = xr - px, e = py - r[1], f = yb - py;
+      const double ab = b < a ? b : a, ef = f < e ? f : e, m = ef < ab ? ef : ab;
+      if (-m < best) best = -m;
+    }
+  }
+  if (!(best < INFINITY && best > -INFINITY)) return false;
+  *out = best;
+  return true;
+}
+
 // measureReach (src/sim/fitness.js:74-88) along one ray from (x, y) with
-// direction (c, s): march in 12 px steps while the makeSdf distance
-// (src/world/map.js:91-118, f64 over the map's rects x y w h) stays positive,
-// up to 3.5 reach; the distance marched.  Host and device run this same code
-// (IEEE f64 add, multiply and sqrt; min / max as std::min / std::max).
+// direction (c, s): march in 12 px steps while the makeSdf distance stays
+// positive, up to 3.5 reach; the distance marched.
 __host__ __device__ inline double reach_ray(const double *rects, int n, double reach, double x, double y,
                                             double c, double s) {
   double d = 0;
   while (d < reach * 3.5) {
     d += 12;
-    const double px = x + c * d, py = y + s * d;
-    double best = INFINITY;
-    const double *r = rects;
-    for (int i = 0; i < n; i++, r += 4) {
-      const double xr = r[0] + r[2], yb = r[1] + r[3];
-      const double mx = xr < px ? xr : px, my = yb < py ? yb : py;
-      const double cx = r[0] < mx ? mx : r[0], cy = r[1] < my ? my : r[1];
-      const double dx = px - cx, dy = py - cy, d2 = dx * dx + dy * dy;
-      if (d2 > 1e-12) {
-        if (d2 < best * best) best = sqrt(d2);
-      } else {
-        const double a = px - r[0], b = xr - px, e = py - r[1], f = yb - py;
-        const double ab = b < a ? b : a, ef = f < e ? f : e, m = ef < ab ? ef : ab;
-        if (-m < best) best = -m;
-      }
-    }
-    if (!(best < INFINITY && best > -INFINITY) || best <= 0) break;
+    double h;
+    if (!sdf64(rects, n, x + c * d, y + s * d, &h) || h <= 0) break;
   }
   return d;
 }
+
+// raymarch, src/senses/echo.js:94-110: the distance to the first surface
+// along the ray (cx, cy) = (cos, sin) of its angle, adaptive steps, at most
+// 96, maxd when nothing is hit
+__host__ __device__ inline double echo_march(const double *rects, int n, double x, double y, double cx,
+                                             double cy, double maxd) {
+  double t = 0;
+  for (int i = 0; i < 96; i++) {
+    if (t >= maxd) return maxd;
+    double d;
+    if (!sdf64(rects, n, x + cx * t, y + cy * t, &d)) return maxd;
+    if (d <= 0) return t;
+    const double adv = d * 0.85;
+    t += adv > 1.0 ? adv : 1.0;
+    if (d < 0.5) return t;
+  }
+  return maxd;
+}
+
+// net.js weightCount for an arms-armed body: n_in = 10 arms + 45 inputs,
+// KR_NET_HIDDEN twice, 3 arms + 2 outputs
+__host__ __device__ inline int net_inputs(int arms) { return 10 * arms + 45; }
+__host__ __device__ inline int net_outputs(int arms) { return 3 * arms + 2; }
+__host__ __device__ inline int net_param_count(int arms) {
+  const int ni = net_inputs(arms), no = net_outputs(arms), H = KR_NET_HIDDEN;
+  return ni * H + H + H * H + H + H * no + no;
+}
+
+// echo.js constants (ECHO_RANGE, SOUND_SPEED, ECHO_INTERVAL) and the
+// pending-echo capacity: an echo arrives within 2 range / speed = 0.756 s of
+// its emission and emissions are at least 0.42 s apart, so at most two
+// emissions (24 echoes) are pending at once
+constexpr double kEchoRange = 340.0, kEchoSpeed = 900.0, kEchoInterval = 0.42;
+constexpr int kEchoPending = 32;
+
+// Per-slot state of KR_CTRL_NET (f64 where the reference keeps f64 state;
+// values the trainer only reads through its Float32Array input are kept in
+// f32): the sim time (sim.time and map.t advance alike), the echo (cooldown,
+// pending echoes sorted by arrival, last arrived range / intensity per ray),
+// the creature's copy of its map's lights, the light and contact senses,
+// and the network's last input, hidden and output vectors.
+struct NetRec {
+  double time, cooldown;
+  double contact[KR_BATCH_MAX_ARMS];
+  double light_xy[2 * KR_NET_MAX_LIGHTS];
+  double p_at[kEchoPending];
+  double ray_d[KR_NET_RAYS];
+  float p_range[kEchoPending], p_inten[kEchoPending];
+  int p_ray[kEchoPending];
+  float range[KR_NET_RAYS], inten[KR_NET_RAYS];
+  float light_v[4];          // left, right, total
+  int n_pending, emit_count, wants_emit, dropped;
+  float x[KR_NET_IN_STRIDE];
+  float h[2 * KR_NET_HIDDEN];
+  float out[KR_NET_OUT_STRIDE];
+};
 
 // the 16 ray directions of measureReach, angle k / 16 * 2 pi, from the host's libm
 struct RayDirs {
@@ -165,8 +229,14 @@ struct kr_batch {
   std::vector<float> h_map_cull;
   std::vector<double> h_rects;         // every map's rects x y w h as the device holds them
   std::vector<int> h_map_off;
-  double *d_rects64 = nullptr;         // h_rects on the device (measureReach at spawn)
+  double *d_rects64 = nullptr;         // h_rects on the device (measureReach, senses)
   krb::RayDirs rays{};
+  // KR_CTRL_NET: lights per map (x y r ir ph sp), offsets, sizes; per-slot state
+  double *d_lights = nullptr;
+  int *d_light_off = nullptr;
+  double *d_map_size = nullptr;
+  krb::NetRec *d_net = nullptr, *s_net = nullptr;
+  std::vector<int> h_pw_arms;          // arms of each net individual (-1: unused)
   // slots
   float *d_state = nullptr;
   float4 *d_grip = nullptr;

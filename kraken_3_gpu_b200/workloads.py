@@ -17,7 +17,7 @@ from dataclasses import dataclass
 import numpy as np
 
 from .kraken import arm_reach
-from .world_map import find_spawn, make_map, mulberry32
+from .world_map import find_spawn, light_array, make_map, mulberry32
 
 WIDTH, HEIGHT = 1440, 810
 TONE = 0.5  # creature default tone, core.js:81 (compliance 1 / 201000)
@@ -56,6 +56,7 @@ class Workload:
     angle: np.ndarray
     horizon: np.ndarray
     seed: np.ndarray      # control stream seed per creature
+    lights: list = None   # per map (n, 6) f64: x y r ir ph sp (makeMap's moving lights)
 
     @property
     def n(self) -> int:
@@ -88,7 +89,8 @@ def uneven(n=16384, n_maps=64, seed=2, h_min=200, h_max=2000, arms=(4, 8), segs=
         X[i], Y[i] = sp["x"], sp["y"]
         ANG[i] = r() * math.pi * 2
     seeds = (np.arange(n, dtype=np.uint64) * 2654435761 + seed).astype(np.uint32)
-    return Workload("uneven", [_rects(m) for m in maps_js], A, S, M, X, Y, ANG, H, seeds)
+    return Workload("uneven", [_rects(m) for m in maps_js], A, S, M, X, Y, ANG, H, seeds,
+                    [np.array(light_array(m), dtype=np.float64).reshape(-1, 6) for m in maps_js])
 
 
 def uniform(n=1024, steps=1000, map_seed=1, seed=1, jitter=20.0) -> Workload:
@@ -103,7 +105,7 @@ def uniform(n=1024, steps=1000, map_seed=1, seed=1, jitter=20.0) -> Workload:
     ones = np.ones(n, np.int32)
     seeds = (np.arange(n, dtype=np.uint64) * 2654435761 + seed).astype(np.uint32)
     return Workload("uniform", [_rects(m)], 6 * ones, 7 * ones, 0 * ones, X, Y, ANG,
-                    steps * ones, seeds)
+                    steps * ones, seeds, [np.array(light_array(m), dtype=np.float64).reshape(-1, 6)])
 
 
 def spawn_all(engine, w: Workload, first=0):

@@ -25,8 +25,8 @@ def mulberry32(seed: int):
 
 
 def make_map(width, height, **opts):
-    """makeMap, map.js:22-71 (rects and the SDF; lights, which the physics
-    never reads, are not generated)."""
+    """makeMap, map.js:22-71: rects, the SDF and the moving lights (drawn
+    after the rects from the same stream; only the light sense reads them)."""
     o = {"wallThickness": 14, "corridorCols": 4, "corridorRows": 3, "density": 0.48,
          "seed": 1, **opts}
     rects = []
@@ -66,8 +66,22 @@ def make_map(width, height, **opts):
             g_end = g_start + g_sz
             if g_end < xs + cw - 14:
                 rects.append({"x": g_end, "y": yl - wt / 2, "w": xs + cw - g_end, "h": wt})
+    lights = []
+    for _ in range(o.get("lights", 4)):
+        x = T + rnd() * max(1, width - T * 2)      # findSpawnRaw, map.js:72-74
+        y = T + rnd() * max(1, height - T * 2)
+        r = 220 + rnd() * 70
+        ir = 0.7 + rnd() * 0.12
+        ph = rnd() * math.pi * 2
+        sp = 0.11 + rnd() * 0.06
+        lights.append({"x": x, "y": y, "r": r, "ir": ir, "ph": ph, "sp": sp})
     return {"width": width, "height": height, "rects": rects, "sdf": make_sdf(rects),
-            "lights": [], "t": 0}
+            "lights": lights, "t": 0}
+
+
+def light_array(m):
+    """A map's lights as rows x y r ir ph sp (the engine's and the oracle's layout)."""
+    return [[l["x"], l["y"], l["r"], l["ir"], l["ph"], l["sp"]] for l in m["lights"]]
 
 
 def make_sdf(rects):

@@ -119,6 +119,14 @@ def lib(opcount: bool = False) -> C.CDLL:
         "or_sim_pre_step": (None, [vp]), "or_sim_post_step": (None, [vp]),
         "or_sim_metrics": (None, [vp, i, C.POINTER(Metrics)]),
         "or_score": (d, [C.POINTER(Metrics)]),
+        "or_net_new": (vp, [vp, dp, i]),
+        "or_net_free": (None, [vp]),
+        "or_net_param_count": (i, [i]),
+        "or_net_forward": (None, [C.POINTER(C.c_float), C.POINTER(C.c_float), C.POINTER(C.c_float),
+                                  C.POINTER(C.c_float), i, i]),
+        "or_net_step": (i, [vp, C.POINTER(C.c_float), i, ip, i]),
+        "or_net_io": (None, [vp, i, C.POINTER(C.c_float), C.POINTER(C.c_float)]),
+        "or_net_echo": (None, [vp, i, ip, ip]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -475,3 +483,61 @@ class Sim:
         m = Metrics()
         self.L.or_sim_metrics(self.ptr, ci, C.byref(m))
         return {f: getattr(m, f) for f in METRIC_FIELDS}
+
+
+def _fp(a: np.ndarray):
+    return a.ctypes.data_as(C.POINTER(C.c_float))
+
+
+def net_param_count(arms: int) -> int:
+    """net.js weightCount for an arms-armed body (n_in = 10 arms + 45)."""
+    return lib().or_net_param_count(arms)
+
+
+def net_forward(w, x, n_out):
+    """forwardInto (net.js:71-98) of one genome on one input vector."""
+    w = np.ascontiguousarray(w, dtype=np.float32)
+    x = np.ascontiguousarray(x, dtype=np.float32)
+    out = np.zeros(n_out, np.float32)
+    scratch = np.zeros(48, np.float32)
+    lib().or_net_forward(_fp(w), _fp(x), _fp(out), _fp(scratch), len(x), n_out)
+    return out
+
+
+class NetSim:
+    """The trainer's controller over a :class:`Sim`'s creatures: senses
+    without entities, the recurrent net and trainStep (train.js:233-249).
+    ``lights`` are the map's lights, rows x y r ir ph sp."""
+
+    def __init__(self, sim: Sim, lights=None):
+        self.sim = sim
+        self.L = sim.L
+        lv = np.ascontiguousarray(np.zeros((0, 6)) if lights is None else lights, dtype=np.float64)
+        self.ptr = self.L.or_net_new(sim.ptr, _dp(lv), len(lv))
+        if not self.ptr:
+            raise ValueError("too many lights")
+
+    def __del__(self):
+        if getattr(self, "ptr", None):
+            self.L.or_net_free(self.ptr)
+            self.ptr = None
+
+    def step(self, genomes, individual, f32=True):
+        g = np.ascontiguousarray(genomes, dtype=np.float32)
+        ind = np.ascontiguousarray(individual, dtype=np.int32)
+        rc = self.L.or_net_step(self.ptr, _fp(g), g.shape[-1], ind.ctypes.data_as(C.POINTER(C.c_int)),
+                                1 if f32 else 0)
+        if rc != 0:
+            raise ValueError("genome size does not match a creature's arm count")
+
+    def io(self, ci):
+        A = self.sim.creatures[ci].n_arms
+        x = np.zeros(10 * A + 45, np.float32)
+        out = np.zeros(3 * A + 2, np.float32)
+        self.L.or_net_io(self.ptr, ci, _fp(x), _fp(out))
+        return x, out
+
+    def echo(self, ci):
+        e, p = C.c_int(), C.c_int()
+        self.L.or_net_echo(self.ptr, ci, C.byref(e), C.byref(p))
+        return e.value, p.value

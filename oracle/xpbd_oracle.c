@@ -1567,3 +1567,239 @@ void or_sim_metrics(const or_sim *s, int ci, or_metrics *out) {
   out->score = or_score(out);
 }
 void or_sim_step32(or_sim *s) { or_step32(s->w); }
+
+/* ======================================================================
+ * The trainer's controller: senses without entities (src/senses/echo.js,
+ * light.js; tip contact core.js:260-266), the recurrent net (src/brain/
+ * net.js:71-133) and one training step (src/sim/train.js:233-249 with
+ * stepSim, core.js:358-382).  A sim's creatures share its time and lights.
+ * ==================================================================== */
+#define OR_ECHO_RAYS 12
+#define OR_ECHO_RANGE 340.0
+#define OR_SOUND_SPEED 900.0
+#define OR_ECHO_INTERVAL 0.42
+#define OR_MAX_LIGHTS 8
+#define OR_NET_H 24
+#define OR_NET_IN_MAX 128
+#define OR_NET_OUT_MAX 32
+
+typedef struct { double at; int i; double dist, intensity; } or_echo_pending;
+
+typedef struct {
+  double cooldown, range_[OR_ECHO_RAYS], intensity[OR_ECHO_RAYS];
+  or_echo_pending pend[64];
+  int npend, emitCount, wantsEmit;
+  double light_l, light_r, light_t;
+  double contact[OR_MAX_ARMS];
+  float x[OR_NET_IN_MAX], h[2 * OR_NET_H], out[OR_NET_OUT_MAX];
+} or_senses;
+
+struct or_net_sim {
+  or_sim *s;          /* borrowed */
+  double time;
+  int nL;
+  double L[OR_MAX_LIGHTS][6];  /* x y r ir ph sp; x, y move */
+  or_senses *cs;
+  int n;
+};
+typedef struct or_net_sim or_net_sim;
+
+/* a fresh trainer state for every creature of s and the map's lights */
+or_net_sim *or_net_new(or_sim *s, const double *lights, int nL) {
+  if (nL < 0 || nL > OR_MAX_LIGHTS) return NULL;
+  or_net_sim *n = (or_net_sim *)calloc(1, sizeof(or_net_sim));
+  n->s = s;
+  n->nL = nL;
+  for (int l = 0; l < nL; l++)
+    for (int k = 0; k < 6; k++) n->L[l][k] = lights[6 * l + k];
+  n->n = s->nCr;
+  n->cs = (or_senses *)calloc((size_t)(s->nCr > 0 ? s->nCr : 1), sizeof(or_senses));
+  return n;
+}
+
+void or_net_free(or_net_sim *n) {
+  if (!n) return;
+  free(n->cs);
+  free(n);
+}
+
+int or_net_param_count(int arms) {
+  const int ni = 10 * arms + 45, no = 3 * arms + 2, H = OR_NET_H;
+  return ni * H + H + H * H + H + H * no + no;
+}
+
+/* forwardInto, net.js:71-98: f64 sums of the Float32Array's values,
+ * activations stored back to f32; the second layer reads its bias at
+ * b2 + j as the reference does */
+static float net_act(double s) { return (float)(s > 20 ? 1 : (s < -20 ? -1 : tanh(s))); }
+
+void or_net_forward(const float *w, const float *x, float *out, float *scratch, int nIn, int nOut) {
+  const int H = OR_NET_H, h1 = 0, h2 = H;
+  const int b1 = nIn * H, b2 = b1 + H, b3 = b2 + H * H, b4 = b3 + H, b5 = b4 + H * nOut;
+  for (int j = 0; j < H; j++) {
+    double s = w[b1 + j];
+    const int row = j * nIn;
+    for (int i = 0; i < nIn; i++) s += (double)x[i] * (double)w[row + i];
+    scratch[h1 + j] = net_act(s);
+  }
+  for (int j = 0; j < H; j++) {
+    double s = w[b2 + j];
+    const int row = b3 - H * H + j * H;
+    for (int i = 0; i < H; i++) s += (double)scratch[h1 + i] * (double)w[row + i];
+    scratch[h2 + j] = net_act(s);
+  }
+  for (int j = 0; j < nOut; j++) {
+    double s = w[b5 + j];
+    const int row = b4 + j * H;
+    for (int i = 0; i < H; i++) s += (double)scratch[h2 + i] * (double)w[row + i];
+    out[j] = net_act(s);
+  }
+}
+
+/* raymarch, echo.js:94-110 */
+static double echo_raymarch(const or_sim *s, double x, double y, double angle, double maxDist) {
+  const double dx = cos(angle), dy = sin(angle);
+  double t = 0;
+  for (int i = 0; i < 96; i++) {
+    if (t >= maxDist) return maxDist;
+    double d, nx, ny;
+    if (!or_sdf(s->rects, s->nR, x + dx * t, y + dy * t, &d, &nx, &ny)) return maxDist;
+    if (d <= 0) return t;
+    t += fmax(1, d * 0.85);
+    if (d < 0.5) return t;
+  }
+  return maxDist;
+}
+
+/* sampleAt, light.js:99-106 */
+static double light_sample(const or_net_sim *n, double x, double y) {
+  double v = 0.05;
+  for (int l = 0; l < n->nL; l++) {
+    const double d = hypot(x - n->L[l][0], y - n->L[l][1]);
+    v += fmax(0, 1 - d / n->L[l][2]) * n->L[l][3];
+  }
+  return fmin(1, v);
+}
+
+/* tickSenses, core.js:245-267, with no entities */
+static void tick_senses(or_net_sim *n, int ci) {
+  or_sim *s = n->s;
+  or_world *w = s->w;
+  or_creature *c = &s->cr[ci];
+  or_senses *e = &n->cs[ci];
+  const int m = c->k.mantle;
+  const double x = PX(w)[m], y = PY(w)[m], angle = ANG(w)[m];
+  const double dt = w->h * w->substeps, time = n->time;
+  const double heading = angle - JS_PI * 0.5;
+  /* tick, echo.js:120-127 */
+  if (e->cooldown > 0) e->cooldown -= dt;
+  while (e->npend && e->pend[0].at <= time) {
+    const or_echo_pending p = e->pend[0];
+    memmove(e->pend, e->pend + 1, sizeof(or_echo_pending) * (size_t)(e->npend - 1));
+    e->npend--;
+    e->range_[p.i] = p.dist / OR_ECHO_RANGE;
+    e->intensity[p.i] = p.intensity;
+  }
+  /* emit, echo.js:67-85 */
+  if (e->wantsEmit && !(e->cooldown > 0)) {
+    e->cooldown = OR_ECHO_INTERVAL;
+    e->emitCount++;
+    for (int i = 0; i < OR_ECHO_RAYS; i++) {
+      const double t = (double)i / (OR_ECHO_RAYS - 1);
+      const double a = heading + (t - 0.5) * (JS_PI * 0.85);
+      const double d = echo_raymarch(s, x, y, a, OR_ECHO_RANGE);
+      if (d >= OR_ECHO_RANGE) continue;
+      const double inten = fmin(1, (OR_ECHO_RANGE * 0.22) / fmax(8, d * d / OR_ECHO_RANGE));
+      if (e->npend < 64) {
+        or_echo_pending p = {time + (2 * d) / OR_SOUND_SPEED, i, d, inten};
+        e->pend[e->npend++] = p;
+      }
+    }
+    /* the stable sort by arrival time */
+    for (int a = 1; a < e->npend; a++) {
+      const or_echo_pending p = e->pend[a];
+      int b = a;
+      while (b > 0 && e->pend[b - 1].at > p.at) { e->pend[b] = e->pend[b - 1]; b--; }
+      e->pend[b] = p;
+    }
+    e->wantsEmit = 0;
+  }
+  /* sample, light.js:90-97 */
+  const double perp = heading + JS_PI / 2;
+  e->light_l = light_sample(n, x + cos(perp) * 26, y + sin(perp) * 26);
+  e->light_r = light_sample(n, x - cos(perp) * 26, y - sin(perp) * 26);
+  e->light_t = light_sample(n, x, y);
+  /* tip contact, core.js:260-266 */
+  for (int a = 0; a < c->k.nArms; a++) {
+    double tx, ty, d, nx, ny;
+    or_tip_position(w, &c->k, a, &tx, &ty);
+    const double near = or_sdf(s->rects, s->nR, tx, ty, &d, &nx, &ny) ? fmax(0, 1 - d / 9) : 0;
+    e->contact[a] = e->contact[a] * 0.7 + near * 0.3;
+  }
+}
+
+/* One trainStep (train.js:233-249): per creature readProprio, readSenses,
+ * the previous outputs, forwardInto with genome genomes[ind[ci]] (n_params
+ * floats each), decode (net.js:124-133) and applyControl; then preStep, the
+ * physics step (f32 emulation when f32, else f64), postStep, time, the
+ * lights (tickMapLights, map.js:75-83) and tickSenses.  Returns -1 when a
+ * creature's genome has the wrong size. */
+int or_net_step(or_net_sim *n, const float *genomes, int n_params, const int *ind, int f32) {
+  or_sim *s = n->s;
+  or_world *w = s->w;
+  for (int ci = 0; ci < s->nCr && ci < n->n; ci++) {
+    or_creature *c = &s->cr[ci];
+    or_senses *e = &n->cs[ci];
+    const int A = c->k.nArms, no = 3 * A + 2;
+    if (or_net_param_count(A) != n_params) return -1;
+    double p[6 * OR_MAX_ARMS + 6];
+    const int np = or_read_proprio(s, ci, p);
+    int i = 0;
+    for (int k = 0; k < np; k++) e->x[i++] = (float)p[k];
+    for (int r = 0; r < OR_ECHO_RAYS; r++) {
+      e->x[i++] = (float)e->range_[r];
+      e->x[i++] = (float)e->intensity[r];
+    }
+    for (int k = 0; k < 6; k++) e->x[i++] = 0.f;  /* chemoreception: no scent sources */
+    e->x[i++] = (float)e->light_l;
+    e->x[i++] = (float)e->light_r;
+    e->x[i++] = (float)e->light_t;
+    for (int k = 0; k < 4; k++) e->x[i++] = 0.f;  /* hearing: no noise sources */
+    for (int a = 0; a < A; a++) e->x[i++] = (float)e->contact[a];
+    for (int k = 0; k < no; k++) e->x[i++] = e->out[k];
+    or_net_forward(genomes + (size_t)ind[ci] * n_params, e->x, e->out, e->h, i, no);
+    double shoulder[OR_MAX_ARMS], curl[OR_MAX_ARMS], adh[OR_MAX_ARMS];
+    for (int a = 0; a < A; a++) {
+      shoulder[a] = e->out[1 + 3 * a];
+      curl[a] = e->out[2 + 3 * a];
+      adh[a] = e->out[3 + 3 * a] > 0 ? e->out[3 + 3 * a] : 0;
+    }
+    e->wantsEmit = e->out[no - 1] > 0.3;
+    or_apply_control(s, ci, 0.5 + 0.5 * e->out[0], shoulder, curl, adh);
+  }
+  or_sim_pre_step(s);
+  if (f32) or_step32(w); else or_step(w);
+  or_sim_post_step(s);
+  const double dt = w->h * w->substeps;
+  n->time += dt;
+  for (int l = 0; l < n->nL; l++) {
+    const double a = n->time * n->L[l][5] + n->L[l][4];
+    n->L[l][0] = fmax(60, fmin(s->width - 60, n->L[l][0] + cos(a) * 18 * dt));
+    n->L[l][1] = fmax(60, fmin(s->height - 60, n->L[l][1] + sin(a * 0.8) * 18 * dt));
+  }
+  for (int ci = 0; ci < s->nCr && ci < n->n; ci++) tick_senses(n, ci);
+  return 0;
+}
+
+/* the last input vector and outputs of creature ci (n_in and n_out values) */
+void or_net_io(const or_net_sim *n, int ci, float *x, float *out) {
+  const int A = n->s->cr[ci].k.nArms;
+  memcpy(x, n->cs[ci].x, sizeof(float) * (size_t)(10 * A + 45));
+  memcpy(out, n->cs[ci].out, sizeof(float) * (size_t)(3 * A + 2));
+}
+
+/* echo state of creature ci: emissions so far and pending echoes */
+void or_net_echo(const or_net_sim *n, int ci, int *emits, int *pending) {
+  *emits = n->cs[ci].emitCount;
+  *pending = n->cs[ci].npend;
+}

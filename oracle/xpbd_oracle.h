@@ -150,6 +150,16 @@ double or_measure_reach(const double *rects, int nR, double reach, double x, dou
 void or_sim_set_spawn_reach(or_sim *s, int ci, double reach);
 void or_sim_pre_step(or_sim *s);    /* preStep of every creature */
 void or_sim_post_step(or_sim *s);   /* postStep of every creature */
+
+/* the trainer's controller: senses without entities, net.js, trainStep */
+typedef struct or_net_sim or_net_sim;
+or_net_sim *or_net_new(or_sim *s, const double *lights, int nL);  /* lights: x y r ir ph sp */
+void or_net_free(or_net_sim *n);
+int or_net_param_count(int arms);
+void or_net_forward(const float *w, const float *x, float *out, float *scratch, int nIn, int nOut);
+int or_net_step(or_net_sim *n, const float *genomes, int n_params, const int *ind, int f32);
+void or_net_io(const or_net_sim *n, int ci, float *x, float *out);
+void or_net_echo(const or_net_sim *n, int ci, int *emits, int *pending);
 double or_score(const or_metrics *m);
 void or_sim_metrics(const or_sim *s, int ci, or_metrics *out);
 

@@ -1,0 +1,111 @@
+"""KR_CTRL_NET on the device against the oracle's trainStep (src/sim/
+train.js:233-249): the reference net (src/brain/net.js) on proprioception,
+senses (echo, light, contact; no entities) and its own previous outputs,
+driving the f32 XPBD step, creature by creature over uneven bodies and maps.
+
+Physics and the f32 data path are bit-exact; the f64 libm calls (tanh,
+sin, cos, atan2, hypot) of the controller may differ from glibc in the last
+f64 bit, which can move an f32 rounding of an input or output by one ulp and
+then grows through the closed loop -- so step 1 is compared within 1e-6 and
+nearly all exact, the last step by the distance that chaos allows."""
+import numpy as np
+import pytest
+
+from kraken_3_gpu_b200 import batch, workloads
+from tests.test_net_host import _net_sim, random_genome
+
+pytestmark = pytest.mark.gpu
+
+
+def _genomes(w, seed, echo_bias=None):
+    rng = np.random.default_rng(seed)
+    G = []
+    for i in range(w.n):
+        A = int(w.arms[i])
+        g = random_genome(batch.net_inputs(A), batch.net_outputs(A), rng)
+        if echo_bias is not None:
+            g[-1] = echo_bias
+        G.append(g)
+    return G
+
+
+def _run_net(w, G, steps, lanes=None):
+    """The engine over all creatures (one arm count: one genome size)."""
+    eng = batch.BatchEngine(w.maps, w.n, control="net", lights=w.lights)
+    workloads.spawn_all(eng, w)
+    if lanes:
+        eng.set_launch(4, 0, lanes_per_creature=lanes)
+    assert len({batch.net_param_count(int(a)) for a in w.arms}) == 1
+    eng.set_net(np.stack(G), np.arange(w.n, dtype=np.int32))
+    eng.run(steps)
+    x, o = eng.read_net()
+    metrics = eng.read_metrics()
+    eng.close()
+    return x, o, metrics
+
+
+def test_net_first_step():
+    """Step 1 (zero senses and outputs in, the spawn pose): inputs and
+    outputs within 1e-6 (the proprioception's f64 libm), nearly all exact."""
+    w = workloads.uneven(n=8, n_maps=2, seed=23, h_min=1, h_max=1, arms=(5, 5), segs=(5, 9))
+    G = _genomes(w, 4)
+    x, o, _ = _run_net(w, G, 1)
+    exact = total = 0
+    for i in range(w.n):
+        sim, net, hist = _net_sim(w, i, 1, G[i])
+        xi, oi = hist[-1]
+        A = int(w.arms[i])
+        ni, no = batch.net_inputs(A), batch.net_outputs(A)
+        assert np.allclose(x[i, :ni], xi, atol=1e-6, rtol=0) and np.allclose(o[i, :no], oi, atol=1e-6, rtol=0)
+        exact += int(np.sum(x[i, :ni] == xi)) + int(np.sum(o[i, :no] == oi))
+        total += ni + no
+    assert exact >= 0.98 * total, (exact, total)
+
+
+@pytest.mark.parametrize("lanes", [32, 16, 8])
+def test_net_engine_tracks_oracle_trainer(lanes):
+    """60 steps per creature: every step's inputs within 1e-4 of the oracle
+    for the first 10 steps, mantle within 0.05 px after 60 (the north-star
+    f64 tolerance class), identical echo usage."""
+    w = workloads.uneven(n=12, n_maps=3, seed=21, h_min=60, h_max=60, arms=(6, 6), segs=(5, 9))
+    G = _genomes(w, 3, echo_bias=1.5)
+    eng = batch.BatchEngine(w.maps, w.n, control="net", lights=w.lights)
+    workloads.spawn_all(eng, w)
+    eng.set_launch(4, 0, lanes_per_creature=lanes)
+    eng.set_net(np.stack(G), np.arange(w.n, dtype=np.int32))
+    X = []
+    for t in range(60):
+        eng.run(1)
+        X.append(eng.read_net()[0].copy())
+    metrics = eng.read_metrics()
+    eng.close()
+    for i in range(w.n):
+        sim, net, hist = _net_sim(w, i, 60, G[i])
+        ni = batch.net_inputs(int(w.arms[i]))
+        for t in range(10):
+            assert np.allclose(X[t][i, :ni], hist[t][0], atol=1e-4, rtol=0), (i, t)
+        want = sim.metrics(0)
+        got = dict(zip(batch.METRIC_FIELDS, metrics[i]))
+        assert abs(got["x"] - want["x"]) < 0.05 and abs(got["y"] - want["y"]) < 0.05, (i, got["x"], want["x"])
+        assert got["steps"] == 60
+    P, E = 6 * 6 + 6, 2 * batch.NET_RAYS
+    assert np.any(X[-1][:, P:P + E] > 0)                       # echoes arrived
+    assert np.any(X[-1][:, P + E + 6:P + E + 9] > np.float32(0.05))  # lit somewhere
+
+
+def test_net_same_for_every_launch_shape_and_alone():
+    """A creature's net rollout does not depend on the launch shape, its
+    neighbours or its slot."""
+    w = workloads.uneven(n=16, n_maps=3, seed=25, h_min=80, h_max=80, arms=(7, 7), segs=(5, 9))
+    G = _genomes(w, 6, echo_bias=1.0)
+    x, o, metrics = _run_net(w, G, 80, lanes=8)
+    for lanes in (16, 32):
+        x2, o2, m2 = _run_net(w, G, 80, lanes=lanes)
+        assert np.array_equal(x2, x) and np.array_equal(o2, o) and np.array_equal(m2, metrics)
+    for i in (0, 7, 15):
+        sub = workloads.Workload("one", w.maps, w.arms[i:i + 1], w.segs[i:i + 1], w.map_id[i:i + 1],
+                                 w.x[i:i + 1], w.y[i:i + 1], w.angle[i:i + 1], w.horizon[i:i + 1],
+                                 w.seed[i:i + 1], w.lights)
+        x1, o1, m1 = _run_net(sub, [G[i]], 80)
+        assert np.array_equal(x1[0], x[i]) and np.array_equal(o1[0], o[i])
+        assert np.array_equal(m1[0], metrics[i])
