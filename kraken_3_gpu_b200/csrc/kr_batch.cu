@@ -491,7 +491,9 @@ __device__ __noinline__ void net_senses(NetArgs N, int arms, const int *arm_tip,
 }
 
 // One creature (slot) advanced by its G lanes for up to A.max_steps env steps.
-template <int G>
+// NET: the kernel instance of engines in KR_CTRL_NET mode (the other modes'
+// kernels carry none of the net's code).
+template <int G, bool NET>
 __device__ void run_creature(const BatchArgs &A, const TplDev &td, int nlv, const TplSmem &P, float *base,
                              int slot, const kr::Lanes<G> &L) {
   const int lane = L.lane;
@@ -526,7 +528,7 @@ __device__ void run_creature(const BatchArgs &A, const TplDev &td, int nlv, cons
   for (int s = 0; s < steps; s++) {
     const int t = m.step;
     // 1. proprioception of the current state
-    if (A.obs_ring > 0 || m.ctrl == KR_CTRL_POLICY || m.ctrl == KR_CTRL_NET) {
+    if (A.obs_ring > 0 || m.ctrl == KR_CTRL_POLICY || (NET && m.ctrl == KR_CTRL_NET)) {
       const unsigned att = proprio<G>(A, td, P, S, X, m, cdp, L);
       if (A.obs_ring > 0) {
         float *o = A.obs + ((size_t)slot * A.obs_ring + (t % A.obs_ring)) * KR_OBS_STRIDE;
@@ -546,8 +548,8 @@ __device__ void run_creature(const BatchArgs &A, const TplDev &td, int nlv, cons
       }
     } else if (m.ctrl == KR_CTRL_POLICY) {
       policy<G>(A, td, X, slot, L);
-    } else if (m.ctrl == KR_CTRL_NET) {
-      S.comp_m = net_control<G>(net_args(A), arms, td.segs, X.obs, X.ctrl, slot, L);
+    } else if constexpr (NET) {
+      if (m.ctrl == KR_CTRL_NET) S.comp_m = net_control<G>(net_args(A), arms, td.segs, X.obs, X.ctrl, slot, L);
     }
     L.sync();
     // 3. applyControl: targets (clamped) and the reflex, core.js:183-220
@@ -622,7 +624,9 @@ __device__ void run_creature(const BatchArgs &A, const TplDev &td, int nlv, cons
       g.max_disp = fmax(g.max_disp, d_spawn);
       g.last_x = x; g.last_y = y;
     }
-    if (m.ctrl == KR_CTRL_NET) net_senses<G>(net_args(A), arms, P.arm_tip, S.px, S.py, S.ang, m.map, slot, L);
+    if constexpr (NET) {
+      if (m.ctrl == KR_CTRL_NET) net_senses<G>(net_args(A), arms, P.arm_tip, S.px, S.py, S.ang, m.map, slot, L);
+    }
     m.step = t + 1;
   }
   // write back (the committed state is already in place)
@@ -643,7 +647,7 @@ __device__ void run_creature(const BatchArgs &A, const TplDev &td, int nlv, cons
   }
 }
 
-template <int G>
+template <int G, bool NET>
 __global__ void __launch_bounds__(32 * kMaxW, 1) batch_kernel(BatchArgs A) {
   constexpr int CPW = 32 / G;  // creatures per warp
   constexpr int V = G == 32 ? 0 : G == 16 ? 1 : 2;  // kr::schedule_index(G): the schedule for G lanes
@@ -688,7 +692,7 @@ __global__ void __launch_bounds__(32 * kMaxW, 1) batch_kernel(BatchArgs A) {
     if (slot >= 0) {
       float *base = smem + tpl_smem_words(td.nb, td.nc, td.np) +
                     c * creature_smem_words(td.nb, td.nc, td.np, td.arms, td.segs);
-      run_creature<G>(A, td, td.nlv[V], P, base, slot, L);
+      run_creature<G, NET>(A, td, td.nlv[V], P, base, slot, L);
     }
   }
 }
@@ -1055,7 +1059,7 @@ int build_groups(kr_batch *b, Part &p, int max_steps) {
 namespace {
 template <int G>
 cudaError_t launch_g(const BatchArgs &A, kr_batch *b, cudaStream_t st, int n_groups, int *grid_out) {
-  auto *fn = batch_kernel<G>;
+  auto *fn = b->d_net ? batch_kernel<G, true> : batch_kernel<G, false>;
   cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b->smem_dyn);
   if (e != cudaSuccess) return e;
   int per_sm = 0;

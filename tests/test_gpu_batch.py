@@ -33,7 +33,9 @@ def _oracle_run(w, i, steps, record_obs=False):
         if record_obs:
             obs.append(sim.read_proprio(0))
         t, a = cs.at(s)
-        sim.apply_control_motors(0, TONE, t, a)
+        # the engine's stream draws into its f32 control record
+        t32, a32 = (v.astype(np.float32).astype(np.float64) for v in (t, a))
+        sim.apply_control_motors(0, TONE, t32, a32)
         sim.step32()
     grips = [k.grip(a).broken for a in range(int(w.arms[i]))]
     return sim, grips, obs

@@ -5,9 +5,10 @@ driving the f32 XPBD step, creature by creature over uneven bodies and maps.
 
 Physics and the f32 data path are bit-exact; the f64 libm calls (tanh,
 sin, cos, atan2, hypot) of the controller may differ from glibc in the last
-f64 bit, which can move an f32 rounding of an input or output by one ulp and
-then grows through the closed loop -- so step 1 is compared within 1e-6 and
-nearly all exact, the last step by the distance that chaos allows."""
+f64 bit, which would move an f32 rounding of an input or output by one ulp
+and then grow through the closed loop.  Measured: every creature of the
+60-step scenario bit-identical to the oracle at every step; the tests allow
+one creature with such a rounding, bounded by the f64 tolerance class."""
 import numpy as np
 import pytest
 
@@ -63,34 +64,46 @@ def test_net_first_step():
 
 
 @pytest.mark.parametrize("lanes", [32, 16, 8])
-def test_net_engine_tracks_oracle_trainer(lanes):
-    """60 steps per creature: every step's inputs within 1e-4 of the oracle
-    for the first 10 steps, mantle within 0.05 px after 60 (the north-star
-    f64 tolerance class), identical echo usage."""
+def test_net_engine_matches_oracle_trainer(lanes):
+    """60 trainer steps per creature, every step's input vector and outputs
+    compared: bit-identical for (nearly) every creature; a creature whose
+    f64 libm call rounded differently once stays within 1e-4 for the first
+    10 steps and within 0.05 px of the oracle's mantle after 60."""
     w = workloads.uneven(n=12, n_maps=3, seed=21, h_min=60, h_max=60, arms=(6, 6), segs=(5, 9))
     G = _genomes(w, 3, echo_bias=1.5)
     eng = batch.BatchEngine(w.maps, w.n, control="net", lights=w.lights)
     workloads.spawn_all(eng, w)
     eng.set_launch(4, 0, lanes_per_creature=lanes)
     eng.set_net(np.stack(G), np.arange(w.n, dtype=np.int32))
-    X = []
+    X, O = [], []
     for t in range(60):
         eng.run(1)
-        X.append(eng.read_net()[0].copy())
+        x, o = eng.read_net()
+        X.append(x.copy())
+        O.append(o.copy())
     metrics = eng.read_metrics()
     eng.close()
+    identical = 0
     for i in range(w.n):
         sim, net, hist = _net_sim(w, i, 60, G[i])
-        ni = batch.net_inputs(int(w.arms[i]))
-        for t in range(10):
-            assert np.allclose(X[t][i, :ni], hist[t][0], atol=1e-4, rtol=0), (i, t)
+        ni, no = batch.net_inputs(6), batch.net_outputs(6)
+        same = all(np.array_equal(X[t][i, :ni], hist[t][0]) and np.array_equal(O[t][i, :no], hist[t][1])
+                   for t in range(60))
+        identical += same
         want = sim.metrics(0)
         got = dict(zip(batch.METRIC_FIELDS, metrics[i]))
-        assert abs(got["x"] - want["x"]) < 0.05 and abs(got["y"] - want["y"]) < 0.05, (i, got["x"], want["x"])
+        if same:
+            for f in ("x", "y", "pathLen", "energySpent", "gripCycles", "attachEvents"):
+                assert np.isclose(got[f], want[f], rtol=1e-10, atol=1e-9), (i, f, got[f], want[f])
+        else:
+            for t in range(10):
+                assert np.allclose(X[t][i, :ni], hist[t][0], atol=1e-4, rtol=0), (i, t)
+            assert abs(got["x"] - want["x"]) < 0.05 and abs(got["y"] - want["y"]) < 0.05, i
         assert got["steps"] == 60
+    assert identical >= w.n - 1, identical
     P, E = 6 * 6 + 6, 2 * batch.NET_RAYS
-    assert np.any(X[-1][:, P:P + E] > 0)                       # echoes arrived
-    assert np.any(X[-1][:, P + E + 6:P + E + 9] > np.float32(0.05))  # lit somewhere
+    assert np.any(X[-1][:, P:P + E] > 0)                              # echoes arrived
+    assert np.any(X[-1][:, P + E + 6:P + E + 9] > np.float32(0.05))   # lit somewhere
 
 
 def test_net_same_for_every_launch_shape_and_alone():
