@@ -70,6 +70,7 @@ def parse():
     ap.add_argument("--no-es", action="store_true", help="skip the ES request stream")
     ap.add_argument("--es-requests", type=int, default=200)
     ap.add_argument("--no-config1", action="store_true", help="skip the 1,024-creature drop-in comparison")
+    ap.add_argument("--no-net", action="store_true", help="skip the reference-net controller rollout")
     ap.add_argument("--traffic", type=float, default=None,
                     help="ncu DRAM bytes per launch of the captured kernel, if measured")
     return ap.parse_args()
@@ -367,6 +368,42 @@ def config1_forms(torch, stream, plain_steps=200, steps=1000):
                            "launch_shape": list(shape)}}
 
 
+def net_controller(stream, w, seed=7):
+    """The same workload driven by the reference trainer's own controller
+    (KR_CTRL_NET: net.js's recurrent net on proprioception + echo, light and
+    contact senses), one randomGenome-initialised genome per creature (net.js:
+    41-55: N(0, 1/fan_in) weights, zero biases); one persistent launch over the
+    whole horizons, kernel time by CUDA events."""
+    from kraken_3_gpu_b200 import batch, workloads
+    rng = np.random.default_rng(seed)
+    width = batch.net_param_count(int(w.arms.max()))
+    genomes = np.zeros((w.n, width), np.float32)
+    H = batch.NET_HIDDEN
+    for i in range(w.n):
+        A = int(w.arms[i])
+        ni, no = batch.net_inputs(A), batch.net_outputs(A)
+        k = 0
+        for n, s in ((ni * H, 1 / np.sqrt(ni)), (H, 0.0), (H * H, 1 / np.sqrt(H)), (H, 0.0),
+                     (H * no, 1 / np.sqrt(H)), (no, 0.0)):
+            genomes[i, k:k + n] = rng.normal(0, 1, n) * s
+            k += n
+    eng = batch.BatchEngine(w.maps, w.n, control="net", lights=w.lights)
+    eng.set_stream(stream.cuda_stream)
+    workloads.spawn_all(eng, w)
+    eng.set_net(genomes, np.arange(w.n, dtype=np.int32))
+    eng.snapshot()
+    eng.run(64)
+    eng.restore()
+    eng.run(int(w.horizon.max()))
+    eng.sync()
+    ms = eng.last_ms()
+    shape = eng.get_launch()
+    eng.close()
+    return {"value": w.creature_steps() / (ms / 1000.0), "unit": UNIT, "kernel_ms": ms,
+            "controller": "net.js 10A+45 -> 24 -> 24 -> 3A+2 per creature, senses and recurrent outputs on the device",
+            "launch_shape": [shape["lanes_per_creature"], shape["warps_per_cta"], shape["ctas_per_sm"]]}
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -476,6 +513,8 @@ def main():
         extra["served_es_stream"] = served_es_stream(serve, w, chunk, args.es_requests, 200.0)
     if not args.no_config1 and rank == 0:
         extra["plain_dropin_1024"] = config1_forms(torch, stream)
+    if not args.no_net and rank == 0:
+        extra["net_controller"] = net_controller(stream, w)
 
     # roofline: f32 rounding ops per creature-step of the restated f32
     # algorithm (op-counting oracle build) x creature-steps per launch /

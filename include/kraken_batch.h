@@ -122,10 +122,12 @@ int kr_batch_set_policy(kr_batch *b, const float *weights, int32_t n_individuals
  * 24 -> 20 with its 3,644 weights; other arm counts use the same layout with
  * n_in = 10A + 45 and A_out outputs.
  *
- * genomes holds n_individuals weight vectors of n_params floats in net.js's
- * layout (weightCount: n_in x 24, 24, 24 x 24, 24, 24 x A_out, A_out);
- * n_params must be the count for the arms of every spawned slot that uses
- * the vector; slot s uses vector slot_individual[s] (capacity entries). */
+ * genomes holds n_individuals weight vectors at a stride of n_params floats,
+ * each in net.js's layout (weightCount: n_in x 24, 24, 24 x 24, 24, 24 x
+ * A_out, A_out) for the arm count of the spawned slots that use it (its
+ * first weightCount floats are read; n_params must be at least that for
+ * every such slot, so one call serves bodies of several arm counts); slot s
+ * uses vector slot_individual[s] (capacity entries). */
 int kr_batch_set_net(kr_batch *b, const float *genomes, int32_t n_individuals, int32_t n_params,
                      const int32_t *slot_individual);
 

@@ -210,8 +210,9 @@ class BatchEngine:
                                           idx.ctypes.data_as(_I32P)), self.h)
 
     def set_net(self, genomes, slot_individual):
-        """control="net": genomes (n_individuals, net_param_count(arms)) f32 in
-        net.js's layout; slot s uses genome slot_individual[s]."""
+        """control="net": genomes (n_individuals, n) f32, each row in net.js's
+        layout for its slots' arm count (first net_param_count(arms) floats
+        read, n at least that); slot s uses genome slot_individual[s]."""
         g = _arr(genomes, np.float32)
         g = g.reshape(g.shape[0], -1)
         idx = _arr(slot_individual, np.int32)

@@ -1481,7 +1481,7 @@ extern "C" int kr_batch_set_net(kr_batch *b, const float *genomes, int32_t n_ind
     const SlotMeta &m = b->h_meta[s];
     if (m.horizon <= 0) continue;
     const int arms = b->tpls[m.tpl].arms, need = net_param_count(arms);
-    if (n_params != need)
+    if (n_params < need)
       return b->fail(KR_ERR_INVALID, "slot " + std::to_string(s) + ": a " + std::to_string(arms) +
                                          "-armed body's net has " + std::to_string(need) + " weights, got " +
                                          std::to_string(n_params));

@@ -31,13 +31,17 @@ def _genomes(w, seed, echo_bias=None):
 
 
 def _run_net(w, G, steps, lanes=None):
-    """The engine over all creatures (one arm count: one genome size)."""
+    """The engine over all creatures; genomes of several arm counts padded
+    to one row width."""
     eng = batch.BatchEngine(w.maps, w.n, control="net", lights=w.lights)
     workloads.spawn_all(eng, w)
     if lanes:
         eng.set_launch(4, 0, lanes_per_creature=lanes)
-    assert len({batch.net_param_count(int(a)) for a in w.arms}) == 1
-    eng.set_net(np.stack(G), np.arange(w.n, dtype=np.int32))
+    width = max(len(g) for g in G)
+    padded = np.zeros((len(G), width), np.float32)
+    for k, g in enumerate(G):
+        padded[k, :len(g)] = g
+    eng.set_net(padded, np.arange(w.n, dtype=np.int32))
     eng.run(steps)
     x, o = eng.read_net()
     metrics = eng.read_metrics()
@@ -108,8 +112,8 @@ def test_net_engine_matches_oracle_trainer(lanes):
 
 def test_net_same_for_every_launch_shape_and_alone():
     """A creature's net rollout does not depend on the launch shape, its
-    neighbours or its slot."""
-    w = workloads.uneven(n=16, n_maps=3, seed=25, h_min=80, h_max=80, arms=(7, 7), segs=(5, 9))
+    neighbours (of other arm counts too) or its slot."""
+    w = workloads.uneven(n=16, n_maps=3, seed=25, h_min=80, h_max=80, arms=(4, 8), segs=(5, 9))
     G = _genomes(w, 6, echo_bias=1.0)
     x, o, metrics = _run_net(w, G, 80, lanes=8)
     for lanes in (16, 32):
