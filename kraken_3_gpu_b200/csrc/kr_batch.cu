@@ -344,28 +344,52 @@ __device__ __noinline__ float net_control(NetArgs N, int arms, int segs, const f
     R.x[q] = v;
   }
   L.sync();
-  const float *w = N.pw + (size_t)N.pw_idx[slot] * N.pw_stride;
-  const int b1 = ni * H, b2 = b1 + H, b3 = b2 + H * H, b4 = b3 + H, b5 = b4 + H * no;
-  for (int j = lane; j < H; j += G) {
-    double acc = w[b1 + j];
-    const float *row = w + (size_t)j * ni;
-    for (int i = 0; i < ni; i++) acc += (double)R.x[i] * (double)row[i];
-    R.h[j] = net_act(acc);
+  // device layout (net_transpose): W1T, b1, W2T, b2, W3T, b3 -- lane j of a
+  // row reads word j, so a warp's loads are consecutive words.  Each lane
+  // carries its units j = lane + u G as independent f64 chains; every sum
+  // still runs over i in ascending order from its bias.
+  const float *w1 = N.pw + (size_t)N.pw_idx[slot] * N.pw_stride;
+  const float *b1 = w1 + (size_t)ni * H, *w2 = b1 + H, *b2 = w2 + H * H, *w3 = b2 + H, *b3 = w3 + H * no;
+  constexpr int U = (KR_NET_HIDDEN + G - 1) / G, UO = (KR_NET_OUT_STRIDE + G - 1) / G;
+  double acc[U > UO ? U : UO];
+#pragma unroll
+  for (int u = 0; u < U; u++) acc[u] = lane + u * G < H ? (double)b1[lane + u * G] : 0.0;
+  for (int i = 0; i < ni; i++) {
+    const double xi = R.x[i];
+    const float *r = w1 + i * H;
+#pragma unroll
+    for (int u = 0; u < U; u++)
+      if (lane + u * G < H) acc[u] += xi * (double)r[lane + u * G];
   }
+#pragma unroll
+  for (int u = 0; u < U; u++)
+    if (lane + u * G < H) R.h[lane + u * G] = net_act(acc[u]);
   L.sync();
-  for (int j = lane; j < H; j += G) {
-    double acc = w[b2 + j];
-    const float *row = w + b3 - H * H + j * H;
-    for (int i = 0; i < H; i++) acc += (double)R.h[i] * (double)row[i];
-    R.h[H + j] = net_act(acc);
+#pragma unroll
+  for (int u = 0; u < U; u++) acc[u] = lane + u * G < H ? (double)b2[lane + u * G] : 0.0;
+  for (int i = 0; i < H; i++) {
+    const double hi = R.h[i];
+    const float *r = w2 + i * H;
+#pragma unroll
+    for (int u = 0; u < U; u++)
+      if (lane + u * G < H) acc[u] += hi * (double)r[lane + u * G];
   }
+#pragma unroll
+  for (int u = 0; u < U; u++)
+    if (lane + u * G < H) R.h[H + lane + u * G] = net_act(acc[u]);
   L.sync();
-  for (int j = lane; j < no; j += G) {
-    double acc = w[b5 + j];
-    const float *row = w + b4 + j * H;
-    for (int i = 0; i < H; i++) acc += (double)R.h[H + i] * (double)row[i];
-    R.out[j] = net_act(acc);
+#pragma unroll
+  for (int u = 0; u < UO; u++) acc[u] = lane + u * G < no ? (double)b3[lane + u * G] : 0.0;
+  for (int i = 0; i < H; i++) {
+    const double hi = R.h[H + i];
+    const float *r = w3 + i * no;
+#pragma unroll
+    for (int u = 0; u < UO; u++)
+      if (lane + u * G < no) acc[u] += hi * (double)r[lane + u * G];
   }
+#pragma unroll
+  for (int u = 0; u < UO; u++)
+    if (lane + u * G < no) R.out[lane + u * G] = net_act(acc[u]);
   L.sync();
   // decode: motor 0 of arm a takes its shoulder output, the distal motors its curl
   const int AS = arms * segs;
@@ -1466,6 +1490,26 @@ extern "C" int kr_batch_set_policy(kr_batch *b, const float *weights, int32_t n_
   return KR_OK;
 }
 
+// net.js's genome layout (forwardInto, net.js:71-98: W1 rows of n_in, b1,
+// W2 rows of 24 -- whose bias the reference reads at b2 + j, i.e. from the
+// first row --, an unread block of 24, W3 rows of 24, b3) to the device
+// layout W1T (n_in x 24), b1, W2T (24 x 24), the second layer's bias as read,
+// W3T (24 x n_out), b3: the same weightCount floats
+static void net_transpose(const float *w, int arms, float *dev) {
+  const int ni = net_inputs(arms), no = net_outputs(arms), H = KR_NET_HIDDEN;
+  const int b1 = ni * H, b2 = b1 + H, b3 = b2 + H * H, b4 = b3 + H, b5 = b4 + H * no;
+  float *w1 = dev, *d1 = w1 + ni * H, *w2 = d1 + H, *d2 = w2 + H * H, *w3 = d2 + H, *d3 = w3 + H * no;
+  for (int j = 0; j < H; j++)
+    for (int i = 0; i < ni; i++) w1[i * H + j] = w[j * ni + i];
+  for (int j = 0; j < H; j++) d1[j] = w[b1 + j];
+  for (int j = 0; j < H; j++)
+    for (int i = 0; i < H; i++) w2[i * H + j] = w[b3 - H * H + j * H + i];
+  for (int j = 0; j < H; j++) d2[j] = w[b2 + j];
+  for (int j = 0; j < no; j++)
+    for (int i = 0; i < H; i++) w3[i * no + j] = w[b4 + j * H + i];
+  for (int j = 0; j < no; j++) d3[j] = w[b5 + j];
+}
+
 extern "C" int kr_batch_set_net(kr_batch *b, const float *genomes, int32_t n_individuals, int32_t n_params,
                                 const int32_t *slot_individual) {
   if (!b) return KR_ERR_INVALID;
@@ -1494,7 +1538,7 @@ extern "C" int kr_batch_set_net(kr_batch *b, const float *genomes, int32_t n_ind
   const int stride = (n_params + 3) & ~3;
   std::vector<float> dev((size_t)n_individuals * stride, 0.f);
   for (int k = 0; k < n_individuals; k++)
-    std::memcpy(dev.data() + (size_t)k * stride, genomes + (size_t)k * n_params, n_params * sizeof(float));
+    if (ind_arms[k] >= 0) net_transpose(genomes + (size_t)k * n_params, ind_arms[k], dev.data() + (size_t)k * stride);
   const size_t need = dev.size();
   cudaError_t e = cudaStreamSynchronize(b->stream);
   if (e != cudaSuccess) return b->cuda_fail(e, "kr_batch_set_net sync");
