@@ -180,7 +180,9 @@ __device__ unsigned proprio(const BatchArgs &A, const TplDev &td, const TplSmem 
   for (int q = lane; q < npair; q += G) {
     const int a = q / (segs - 1), i = q % (segs - 1) + 1;
     const double d = (double)S.ang[P.arm_segs[a * segs + i]] - (double)S.ang[P.arm_segs[a * segs + i - 1]];
-    X.pair[q] = atan2(sin(d), cos(d));
+    double sd, cd;
+    sincos(d, &sd, &cd);
+    X.pair[q] = atan2(sd, cd);
   }
   L.sync();
   double ext = 0.0, curl = 0.0, sh = 0.0, tx = 0.0, ty = 0.0;
@@ -192,10 +194,12 @@ __device__ unsigned proprio(const BatchArgs &A, const TplDev &td, const TplSmem 
     curl = segs > 1 ? s / (segs - 1) : 0.0;
     const int s0 = P.arm_seg0[a], tip = P.arm_tip[a];
     const double d = (double)S.ang[s0] - angle;
-    sh = atan2(sin(d), cos(d));
-    const double ta = (double)S.ang[tip];
-    tx = (double)S.px[tip] + kSegHalf * cos(ta);
-    ty = (double)S.py[tip] + kSegHalf * sin(ta);
+    double sd, cd, st, ct;
+    sincos(d, &sd, &cd);
+    sh = atan2(sd, cd);
+    sincos((double)S.ang[tip], &st, &ct);
+    tx = (double)S.px[tip] + kSegHalf * ct;
+    ty = (double)S.py[tip] + kSegHalf * st;
     ext = fmin(1.0, hypot(tx - (double)S.px[s0], ty - (double)S.py[s0]) / fmax(1.0, td.reach));
     attached = grip_st[a].w == 0.f;
   }
@@ -203,7 +207,8 @@ __device__ unsigned proprio(const BatchArgs &A, const TplDev &td, const TplSmem 
   // sums in arm order, like the sequential loop
   double ext_sum = 0.0;
   for (int a = 0; a < arms; a++) ext_sum += __shfl_sync(L.mask, ext, a, G);
-  const double ca = cos(-angle), sa = sin(-angle);
+  double ca, sa;
+  sincos(-angle, &sa, &ca);
   const double SL = kPiD * 0.62, JL = kPiD * 0.42;
   if (lane < arms) {
     const int a = lane;
@@ -410,16 +415,6 @@ __device__ __noinline__ float net_control(NetArgs N, int arms, int segs, const f
   return (float)(1.0 / (2000.0 + tone * (400000.0 - 2000.0)));  // toneToCompliance
 }
 
-// sampleAt, src/senses/light.js:99-106
-__device__ __forceinline__ double light_at(const double *lp, const double *xy, int nl, double x, double y) {
-  double v = 0.05;
-  for (int l = 0; l < nl; l++) {
-    const double d = hypot(x - xy[2 * l], y - xy[2 * l + 1]);
-    v += fmax(0.0, 1 - d / lp[6 * l + 2]) * lp[6 * l + 3];
-  }
-  return fmin(1.0, v);
-}
-
 // KR_CTRL_NET, after postStep: sim.time += dt, tickMapLights (map.js:75-83)
 // on the creature's copy of its map's lights, then tickSenses (core.js:
 // 245-267) without entities: the echo's tick (echo.js:120-127) and, when
@@ -437,17 +432,38 @@ __device__ __noinline__ void net_senses(NetArgs N, int arms, const int *arm_tip,
   const double x = px[0], y = py[0];
   const double heading = (double)ang[0] - kPiD * 0.5;
   const double dt = N.dt;
+  const double time = R.time + dt;
+  const int lo = N.light_off ? N.light_off[map] : 0, nl = N.light_off ? N.light_off[map + 1] - lo : 0;
+  const double *lp = N.lights + 6 * (size_t)lo;
+  // the lights move (light l on lane l), then every (sample point, light)
+  // contribution on its own lane; lane 0 sums them in light order below
+  if (lane < nl) {
+    const int l = lane;
+    const double mw = N.map_size[2 * map], mh = N.map_size[2 * map + 1];
+    const double a = time * lp[6 * l + 5] + lp[6 * l + 4];
+    R.light_xy[2 * l] = fmax(60.0, fmin(mw - 60, R.light_xy[2 * l] + cos(a) * 18 * dt));
+    R.light_xy[2 * l + 1] = fmax(60.0, fmin(mh - 60, R.light_xy[2 * l + 1] + sin(a * 0.8) * 18 * dt));
+  }
+  L.sync();
+  {
+    double sp, cp;
+    sincos(heading + kPiD / 2, &sp, &cp);  // light.js: receptors 26 px across the heading
+    for (int q = lane; q < 3 * nl; q += G) {
+      const int s = q / nl, l = q % nl;
+      const double qx = s == 0 ? x + cp * 26 : (s == 1 ? x - cp * 26 : x);
+      const double qy = s == 0 ? y + sp * 26 : (s == 1 ? y - sp * 26 : y);
+      const double d = hypot(qx - R.light_xy[2 * l], qy - R.light_xy[2 * l + 1]);
+      R.lc[q] = fmax(0.0, 1 - d / lp[6 * l + 2]) * lp[6 * l + 3];
+    }
+  }
+  L.sync();
   int emit = 0;
   if (lane == 0) {
-    const double time = R.time + dt;
     R.time = time;
-    const int lo = N.light_off ? N.light_off[map] : 0, nl = N.light_off ? N.light_off[map + 1] - lo : 0;
-    const double *lp = N.lights + 6 * (size_t)lo;
-    const double mw = nl ? N.map_size[2 * map] : 0, mh = nl ? N.map_size[2 * map + 1] : 0;
-    for (int l = 0; l < nl; l++) {
-      const double a = time * lp[6 * l + 5] + lp[6 * l + 4];
-      R.light_xy[2 * l] = fmax(60.0, fmin(mw - 60, R.light_xy[2 * l] + cos(a) * 18 * dt));
-      R.light_xy[2 * l + 1] = fmax(60.0, fmin(mh - 60, R.light_xy[2 * l + 1] + sin(a * 0.8) * 18 * dt));
+    for (int s = 0; s < 3; s++) {  // sampleAt, light.js:99-106
+      double v = 0.05;
+      for (int l = 0; l < nl; l++) v += R.lc[s * nl + l];
+      R.light_v[s] = (float)fmin(1.0, v);
     }
     if (R.cooldown > 0) R.cooldown -= dt;
     int k = 0;
@@ -466,20 +482,15 @@ __device__ __noinline__ void net_senses(NetArgs N, int arms, const int *arm_tip,
       R.emit_count++;
       emit = 1;
     }
-    // light.js sample: left / right receptors 26 px across the heading
-    const double perp = heading + kPiD / 2;
-    const double lx = x + cos(perp) * 26, ly = y + sin(perp) * 26;
-    const double rx = x - cos(perp) * 26, ry = y - sin(perp) * 26;
-    R.light_v[0] = (float)light_at(lp, R.light_xy, nl, lx, ly);
-    R.light_v[1] = (float)light_at(lp, R.light_xy, nl, rx, ry);
-    R.light_v[2] = (float)light_at(lp, R.light_xy, nl, x, y);
   }
   emit = __shfl_sync(L.mask, emit, 0, G);
   if (emit) {
     for (int i = lane; i < KR_NET_RAYS; i += G) {
       const double t = (double)i / (KR_NET_RAYS - 1);
       const double a = heading + (t - 0.5) * (kPiD * 0.85);
-      R.ray_d[i] = echo_march(rects, nR, x, y, cos(a), sin(a), kEchoRange);
+      double sa, ca;
+      sincos(a, &sa, &ca);
+      R.ray_d[i] = echo_march(rects, nR, x, y, ca, sa, kEchoRange);
     }
     L.sync();
     if (lane == 0) {
@@ -505,8 +516,9 @@ __device__ __noinline__ void net_senses(NetArgs N, int arms, const int *arm_tip,
   // tip contact: near = max(0, 1 - d / 9) of the map's SDF at the tip point
   for (int a = lane; a < arms; a += G) {
     const int tip = arm_tip[a];
-    const double ta = ang[tip];
-    const double tx = (double)px[tip] + kSegHalf * cos(ta), ty = (double)py[tip] + kSegHalf * sin(ta);
+    double st, ct;
+    sincos((double)ang[tip], &st, &ct);
+    const double tx = (double)px[tip] + kSegHalf * ct, ty = (double)py[tip] + kSegHalf * st;
     double d;
     const double near = sdf64(rects, nR, tx, ty, &d) ? fmax(0.0, 1 - d / 9) : 0.0;
     R.contact[a] = R.contact[a] * 0.7 + near * 0.3;
@@ -626,7 +638,9 @@ __device__ void run_creature(const BatchArgs &A, const TplDev &td, int nlv, cons
       g.path_len += step_dist;
       g.angular_accum += fabs(av) * A.h64 * A.substeps;
       const double fa = angle - kPiD * 0.5;
-      const double fwd = dx * cos(fa) + dy * sin(fa);
+      double sf, cf;
+      sincos(fa, &sf, &cf);
+      const double fwd = dx * cf + dy * sf;
       if (fwd > 0) g.forward_prog += fwd;
       int anchored = 0;
       unsigned now = 0;

@@ -170,6 +170,7 @@ struct NetRec {
   int p_ray[kEchoPending];
   float range[KR_NET_RAYS], inten[KR_NET_RAYS];
   float light_v[4];          // left, right, total
+  double lc[3 * KR_NET_MAX_LIGHTS];  // per sample point and light: its contribution
   int n_pending, emit_count, wants_emit, dropped;
   float x[KR_NET_IN_STRIDE];
   float h[2 * KR_NET_HIDDEN];
