@@ -61,6 +61,15 @@ typedef struct kr_server_desc {
   int32_t ctas_per_sm;
   double grip_slip_max;         /* px/s, core.js:30 */
   double grip_cooldown;         /* s, core.js:31 */
+  /* 1: requests with theta run the reference trainer's own controller
+   * (KR_CTRL_NET of kraken_batch.h) -- theta is a net.js genome for the
+   * request's arm count, perturbed per individual exactly as the fused
+   * policy's theta is; needs policy == 0.  lights / map_light_off / map_size
+   * as in kr_batch_desc; NULL lights: none. */
+  int32_t net;
+  const double *lights;
+  const int32_t *map_light_off;
+  const double *map_size;
 } kr_server_desc;
 
 typedef struct kr_request {
@@ -72,7 +81,8 @@ typedef struct kr_request {
   const double *xs, *ys, *angles;     /* or one pose per individual (all three, or NULL) */
   const uint32_t *control_seeds;      /* no theta: stream seed per individual (NULL: from seed) */
   float tone;                   /* muscle tone 0..1 */
-  const float *theta;           /* NULL: control streams; else n_params floats (kraken_batch.h layout) */
+  const float *theta;           /* NULL: control streams; else n_params floats (kraken_batch.h policy
+                                   layout, or with net: a net.js genome, kr_batch_set_net) */
   int32_t n_params;
   float sigma;
   uint64_t seed;                /* eps (policy) or control streams (no theta) */

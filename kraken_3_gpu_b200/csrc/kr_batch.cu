@@ -1504,24 +1504,15 @@ extern "C" int kr_batch_set_policy(kr_batch *b, const float *weights, int32_t n_
   return KR_OK;
 }
 
-// net.js's genome layout (forwardInto, net.js:71-98: W1 rows of n_in, b1,
-// W2 rows of 24 -- whose bias the reference reads at b2 + j, i.e. from the
-// first row --, an unread block of 24, W3 rows of 24, b3) to the device
-// layout W1T (n_in x 24), b1, W2T (24 x 24), the second layer's bias as read,
-// W3T (24 x n_out), b3: the same weightCount floats
+// net.js's genome layout to the device layout (net_device_slots)
 static void net_transpose(const float *w, int arms, float *dev) {
-  const int ni = net_inputs(arms), no = net_outputs(arms), H = KR_NET_HIDDEN;
-  const int b1 = ni * H, b2 = b1 + H, b3 = b2 + H * H, b4 = b3 + H, b5 = b4 + H * no;
-  float *w1 = dev, *d1 = w1 + ni * H, *w2 = d1 + H, *d2 = w2 + H * H, *w3 = d2 + H, *d3 = w3 + H * no;
-  for (int j = 0; j < H; j++)
-    for (int i = 0; i < ni; i++) w1[i * H + j] = w[j * ni + i];
-  for (int j = 0; j < H; j++) d1[j] = w[b1 + j];
-  for (int j = 0; j < H; j++)
-    for (int i = 0; i < H; i++) w2[i * H + j] = w[b3 - H * H + j * H + i];
-  for (int j = 0; j < H; j++) d2[j] = w[b2 + j];
-  for (int j = 0; j < no; j++)
-    for (int i = 0; i < H; i++) w3[i * no + j] = w[b4 + j * H + i];
-  for (int j = 0; j < no; j++) d3[j] = w[b5 + j];
+  const int n = net_param_count(arms);
+  for (int p = 0; p < n; p++) {
+    int d0 = 0, d1 = 0;
+    const int k = net_device_slots(arms, p, &d0, &d1);
+    if (k > 0) dev[d0] = w[p];
+    if (k > 1) dev[d1] = w[p];
+  }
 }
 
 extern "C" int kr_batch_set_net(kr_batch *b, const float *genomes, int32_t n_individuals, int32_t n_params,

@@ -147,6 +147,30 @@ __host__ __device__ inline int net_param_count(int arms) {
   return ni * H + H + H * H + H + H * no + no;
 }
 
+// Device layout of a net genome: the blocks of net.js's layout at the same
+// offsets (W1 | b1 | W2 | unread | W3 | b3, forwardInto's b1..b5), each
+// weight matrix transposed (input-major, so the lanes of one input read
+// consecutive words) and the unread block replaced by the layer-2 bias as
+// forwardInto reads it, w[b2 + j] -- which is also W2's first row.  Public
+// parameter p goes to *d0 and, for that first row, also to *d1; returns the
+// number of places (0 for the unread block).
+__host__ __device__ inline int net_device_slots(int arms, int p, int *d0, int *d1) {
+  const int ni = net_inputs(arms), no = net_outputs(arms), H = KR_NET_HIDDEN;
+  const int b1 = ni * H, b2 = b1 + H, b3 = b2 + H * H, b4 = b3 + H, b5 = b4 + H * no;
+  if (p < b1) { *d0 = (p % ni) * H + p / ni; return 1; }
+  if (p < b2) { *d0 = p; return 1; }
+  if (p < b3) {
+    const int q = p - b2;
+    *d0 = b2 + (q % H) * H + q / H;
+    if (q < H) { *d1 = b3 + q; return 2; }
+    return 1;
+  }
+  if (p < b4) return 0;
+  if (p < b5) { const int q = p - b4; *d0 = b4 + (q % H) * no + q / H; return 1; }
+  *d0 = p;
+  return 1;
+}
+
 // echo.js constants (ECHO_RANGE, SOUND_SPEED, ECHO_INTERVAL) and the
 // pending-echo capacity: an echo arrives within 2 range / speed = 0.756 s of
 // its emission and emissions are at least 0.42 s apart, so at most two

@@ -39,6 +39,9 @@ using namespace krb;
 
 constexpr int kMaxParams = KR_POLICY_HIDDEN * (6 * KR_BATCH_MAX_ARMS + 7) +
                            (KR_BATCH_MAX_ARMS * KR_BATCH_MAX_SEGS + KR_BATCH_MAX_ARMS) * (KR_POLICY_HIDDEN + 1);
+constexpr int kMaxNetParams = ((10 * KR_BATCH_MAX_ARMS + 45) * KR_NET_HIDDEN + 2 * KR_NET_HIDDEN +
+                               KR_NET_HIDDEN * KR_NET_HIDDEN + (3 * KR_BATCH_MAX_ARMS + 2) * (KR_NET_HIDDEN + 1) + 3) &
+                              ~3;  // net.js genome of the largest body, 16-byte multiple
 constexpr int kMaxThetaPerRound = 64;   // policy requests admitted into one partition per round
 constexpr uint64_t kFixedBytes = 8ull << 20;  // tables, maps, queues, events
 
@@ -71,16 +74,25 @@ struct PJob {
 };
 
 // weights of newly admitted individuals: theta +- sigma * eps for public
-// parameter p, stored at its place in the device layout
-__global__ void perturb_kernel(float *w, int stride, const float *theta, const PJob *jobs, int n) {
+// parameter p, stored at its place(s) in the device layout of the fused
+// policy or, with net, of the reference net (net_device_slots)
+__global__ void perturb_kernel(float *w, int stride, const float *theta, const PJob *jobs, int n, int net) {
   if ((int)blockIdx.x >= n) return;
   const PJob j = jobs[blockIdx.x];
   float *dst = w + (size_t)j.slot * stride;
   const float *th = theta + j.theta_off;
-  const int np = policy_param_count(j.arms, j.segs);
+  const int np = net ? net_param_count(j.arms) : policy_param_count(j.arms, j.segs);
   for (int p = threadIdx.x; p < np; p += blockDim.x) {
     const float d = __fmul_rn(j.sigma, eps_normal(j.seed, j.pair, p));
-    dst[policy_device_index(j.arms, j.segs, p)] = __fadd_rn(th[p], j.sign < 0.f ? -d : d);
+    const float v = __fadd_rn(th[p], j.sign < 0.f ? -d : d);
+    if (!net) {
+      dst[policy_device_index(j.arms, j.segs, p)] = v;
+      continue;
+    }
+    int d0 = 0, d1 = 0;
+    const int k = net_device_slots(j.arms, p, &d0, &d1);
+    if (k > 0) dst[d0] = v;
+    if (k > 1) dst[d1] = v;
   }
 }
 
@@ -123,11 +135,15 @@ struct Round {
   bool timed = false;
 };
 
+// weights per slot: the fused policy's or the reference net's largest body
+int weight_stride(const kr_server_desc &d) { return d.net ? kMaxNetParams : kMaxParams; }
+
 uint64_t slot_bytes(const kr_server_desc &d) {
   uint64_t b = (uint64_t)kStateStride * 4 + KR_BATCH_MAX_ARMS * (16 + 8 + 8) + (uint64_t)kCtrlStride * 4 +
                sizeof(SlotMeta);
   b += (uint64_t)d.obs_ring * KR_OBS_STRIDE * 4;
   if (d.policy) b += (uint64_t)kMaxParams * 4 + 4;
+  if (d.net) b += (uint64_t)kMaxNetParams * 4 + 4 + sizeof(NetRec);
   // partition staging and work groups (two partitions of half the slots)
   b += (uint64_t)kStateStride * 4 + sizeof(SlotMeta) + 4 + sizeof(PJob) + 4 + sizeof(SlotMeta) + 2 * 4;
   return b;
@@ -136,7 +152,8 @@ uint64_t slot_bytes(const kr_server_desc &d) {
 uint64_t fixed_bytes(const kr_server_desc &d) {
   uint64_t b = kFixedBytes;
   if (d.n_maps > 0 && d.map_rect_off) b += (uint64_t)d.map_rect_off[d.n_maps] * 16 + (uint64_t)d.n_maps * 8;
-  if (d.policy) b += 2ull * kMaxThetaPerRound * kMaxParams * 4;
+  if (d.policy || d.net) b += 2ull * kMaxThetaPerRound * weight_stride(d) * 4;
+  if (d.net && d.lights && d.map_light_off) b += (uint64_t)d.map_light_off[d.n_maps] * 48 + (uint64_t)d.n_maps * 20;
   return b;
 }
 
@@ -187,6 +204,7 @@ int check_desc(const kr_server_desc *d, std::string *why) {
   if (d->obs_ring < 0 || d->obs_ring > 4096) { *why = "obs_ring outside 0..4096"; return KR_ERR_INVALID; }
   if (d->max_slots < 0) { *why = "max_slots < 0"; return KR_ERR_INVALID; }
   if (d->n_maps < 1 || !d->rects || !d->map_rect_off) { *why = "need at least one map"; return KR_ERR_INVALID; }
+  if (d->policy && d->net) { *why = "policy and net are exclusive (theta is one or the other)"; return KR_ERR_INVALID; }
   return KR_OK;
 }
 
@@ -275,6 +293,7 @@ int admit(kr_server *S, int p) {
     const int pop = q.r.population;
     if (pop > (int)S->free_slots.size() || S->part_used[p] + pop > S->part_cap) break;
     const bool pol = !q.theta.empty();
+    const int ctrl = !pol ? KR_CTRL_STREAM : S->d.net ? KR_CTRL_NET : KR_CTRL_POLICY;
     if (pol && n_theta >= kMaxThetaPerRound) break;
     // the creatures' initial data
     const std::vector<int32_t> arms(pop, q.r.arms), segs(pop, q.r.segs), maps(pop, q.r.map_id), hor(pop, q.r.horizon);
@@ -289,8 +308,7 @@ int admit(kr_server *S, int p) {
     SpawnInit init;
     int bad = -1;
     int rc = prepare_spawn(S->b, pop, arms.data(), segs.data(), maps.data(), xs.data(), ys.data(), an.data(),
-                           hor.data(), seeds.data(), tones.data(), pol ? KR_CTRL_POLICY : KR_CTRL_STREAM, &init,
-                           &bad);
+                           hor.data(), seeds.data(), tones.data(), ctrl, &init, &bad);
     if (rc != KR_OK) return S->batch_fail(rc);
     q.slots.resize(pop);
     for (int i = 0; i < pop; i++) {
@@ -310,7 +328,8 @@ int admit(kr_server *S, int p) {
       }
       S->b->h_meta[s] = init.meta[i];
       S->b->h_remaining[s] = init.meta[i].horizon;
-      if (pol) S->b->h_pw_tpl[s] = init.meta[i].tpl;
+      if (pol && S->d.net) S->b->h_pw_arms[s] = q.r.arms;
+      else if (pol) S->b->h_pw_tpl[s] = init.meta[i].tpl;
       n_new++;
     }
     if (pol) {
@@ -333,17 +352,19 @@ int admit(kr_server *S, int p) {
   if (e == cudaSuccess) e = cudaMemcpyAsync(st.d_meta, st.h_meta, (size_t)n_new * sizeof(SlotMeta), cudaMemcpyHostToDevice, stream);
   if (e == cudaSuccess) e = cudaMemcpyAsync(st.d_slots, st.h_slots, (size_t)n_new * sizeof(int), cudaMemcpyHostToDevice, stream);
   if (e == cudaSuccess) e = launch_spawn(S->b, st.d_slots, st.d_pose, st.d_meta, n_new, stream);
-  if (e == cudaSuccess && S->d.policy && theta_off > 0) {
+  const bool weights = S->d.policy || S->d.net;
+  if (e == cudaSuccess && weights && theta_off > 0) {
     e = cudaMemcpyAsync(st.d_theta, st.h_theta, (size_t)theta_off * sizeof(float), cudaMemcpyHostToDevice, stream);
     if (e == cudaSuccess) e = cudaMemcpyAsync(st.d_jobs, st.h_jobs, (size_t)n_new * sizeof(PJob), cudaMemcpyHostToDevice, stream);
     if (e == cudaSuccess) {
-      perturb_kernel<<<n_new, 256, 0, stream>>>(S->b->d_pw, kMaxParams, st.d_theta, st.d_jobs, n_new);
+      perturb_kernel<<<n_new, 256, 0, stream>>>(S->b->d_pw, weight_stride(S->d), st.d_theta, st.d_jobs, n_new,
+                                                S->d.net);
       e = cudaGetLastError();
     }
   }
   if (e != cudaSuccess) return S->cuda_fail(e, "admission staging");
   S->h2d_bytes += (uint64_t)n_new * (kStateStride * sizeof(float) + sizeof(SlotMeta) + sizeof(int));
-  if (S->d.policy && theta_off > 0) S->h2d_bytes += (uint64_t)theta_off * sizeof(float) + (uint64_t)n_new * sizeof(PJob);
+  if (weights && theta_off > 0) S->h2d_bytes += (uint64_t)theta_off * sizeof(float) + (uint64_t)n_new * sizeof(PJob);
   return KR_OK;
 }
 
@@ -425,8 +446,13 @@ extern "C" int kr_server_create(const kr_server_desc *d, kr_server **out) {
   bd.obs_ring = d->obs_ring;
   bd.grip_slip_max = d->grip_slip_max;
   bd.grip_cooldown = d->grip_cooldown;
-  bd.control_mode = KR_CTRL_STREAM;  // per slot: policy for requests with theta
+  bd.control_mode = d->net ? KR_CTRL_NET : KR_CTRL_STREAM;  // per slot: policy / net for requests with theta
   bd.control_period = 6;
+  if (d->net) {
+    bd.lights = d->lights;
+    bd.map_light_off = d->map_light_off;
+    bd.map_size = d->map_size;
+  }
   kr_batch *b = nullptr;
   rc = kr_batch_create(&bd, &b);
   if (rc != KR_OK) { g_serve_error = std::string("engine: ") + kr_batch_last_error(nullptr); return rc; }
@@ -434,6 +460,9 @@ extern "C" int kr_server_create(const kr_server_desc *d, kr_server **out) {
   S->d = *d;
   S->d.rects = nullptr;
   S->d.map_rect_off = nullptr;
+  S->d.lights = nullptr;
+  S->d.map_light_off = nullptr;
+  S->d.map_size = nullptr;
   S->b = b;
   S->capacity = cap;
   S->part_cap = cap / 2;
@@ -458,18 +487,20 @@ extern "C" int kr_server_create(const kr_server_desc *d, kr_server **out) {
   if (rc == KR_OK) rc = plan_shape(b);
   if (rc != KR_OK) { S->batch_fail(rc); return bail(rc); }
   cudaError_t e = cudaSuccess;
-  if (d->policy) {
-    e = cudaMalloc(&b->d_pw, (size_t)cap * kMaxParams * sizeof(float));
+  if (d->policy || d->net) {
+    const int ws = weight_stride(*d);  // a multiple of 4: 16-byte aligned individuals
+    e = cudaMalloc(&b->d_pw, (size_t)cap * ws * sizeof(float));
     std::vector<int> idx(cap);
     for (int s = 0; s < cap; s++) idx[s] = s;
     if (e == cudaSuccess) e = cudaMalloc(&b->d_pw_idx, (size_t)cap * sizeof(int));
     if (e == cudaSuccess) e = cudaMemcpy(b->d_pw_idx, idx.data(), idx.size() * sizeof(int), cudaMemcpyHostToDevice);
-    if (e == cudaSuccess) e = cudaMemset(b->d_pw, 0, (size_t)cap * kMaxParams * sizeof(float));
-    b->pw_stride = kMaxParams;  // a multiple of 4: 16-byte aligned individuals
-    b->pw_capacity = (size_t)cap * kMaxParams;
+    if (e == cudaSuccess) e = cudaMemset(b->d_pw, 0, (size_t)cap * ws * sizeof(float));
+    b->pw_stride = ws;
+    b->pw_capacity = (size_t)cap * ws;
     b->n_individuals = cap;
     b->h_pw_idx = idx;
     b->h_pw_tpl.assign(cap, -1);
+    b->h_pw_arms.assign(cap, -1);
     if (e != cudaSuccess) { S->cuda_fail(e, "policy weights"); return bail(KR_ERR_CUDA); }
   }
   for (int p = 0; p < 2; p++) {
@@ -483,7 +514,9 @@ extern "C" int kr_server_create(const kr_server_desc *d, kr_server **out) {
     if (e == cudaSuccess) e = pinned_pair(&st.h_meta, &st.d_meta, pc);
     if (e == cudaSuccess) e = pinned_pair(&st.h_slots, &st.d_slots, pc);
     if (e == cudaSuccess) e = pinned_pair(&st.h_jobs, &st.d_jobs, pc);
-    if (e == cudaSuccess) e = pinned_pair(&st.h_theta, &st.d_theta, d->policy ? (size_t)kMaxThetaPerRound * kMaxParams : 1);
+    if (e == cudaSuccess)
+      e = pinned_pair(&st.h_theta, &st.d_theta,
+                      d->policy || d->net ? (size_t)kMaxThetaPerRound * weight_stride(*d) : 1);
     if (e == cudaSuccess) e = pinned_pair(&st.h_rslots, &st.d_rslots, pc);
     if (e == cudaSuccess) e = pinned_pair(&st.h_res, &st.d_res, pc);
   }
@@ -514,8 +547,8 @@ extern "C" int kr_server_submit(kr_server *S, const kr_request *r, int64_t *id) 
   q.r = *r;
   q.r.theta = nullptr;
   if (r->theta) {
-    if (!S->d.policy) return S->fail(KR_ERR_STATE, "server created without policy weights");
-    const int need = policy_param_count(r->arms, r->segs);
+    if (!S->d.policy && !S->d.net) return S->fail(KR_ERR_STATE, "server created without policy or net weights");
+    const int need = S->d.net ? net_param_count(r->arms) : policy_param_count(r->arms, r->segs);
     if (r->n_params < need)
       return S->fail(KR_ERR_INVALID, "theta has " + std::to_string(r->n_params) + " parameters, a " +
                                          std::to_string(r->arms) + "x" + std::to_string(r->segs) + " body needs " +

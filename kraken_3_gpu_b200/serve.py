@@ -20,7 +20,7 @@ import ctypes as C
 import numpy as np
 
 from . import _native
-from .batch import policy_params  # noqa: F401  (parameter count of a body's policy)
+from .batch import net_param_count, policy_params  # noqa: F401  (parameter counts of a body's controllers)
 
 from .batch import METRIC_FIELDS as RESULT_FIELDS  # noqa: E402
 RESULT_WORDS = len(RESULT_FIELDS)
@@ -37,7 +37,8 @@ class ServerDesc(C.Structure):
                 ("obs_ring", C.c_int32), ("chunk_steps", C.c_int32), ("policy", C.c_int32),
                 ("lanes_per_creature", C.c_int32), ("warps_per_cta", C.c_int32),
                 ("ctas_per_sm", C.c_int32), ("grip_slip_max", C.c_double),
-                ("grip_cooldown", C.c_double)]
+                ("grip_cooldown", C.c_double), ("net", C.c_int32), ("lights", _F64P),
+                ("map_light_off", _I32P), ("map_size", _F64P)]
 
 
 class Request(C.Structure):
@@ -109,7 +110,7 @@ def _check(rc, h):
 
 def _desc(maps, hbm_budget, max_slots, obs_ring, chunk_steps, policy, lanes, warps, ctas,
           substeps, iterations, h, lin_drag, ang_drag, max_speed, max_ang_speed, grip_slip_max,
-          grip_cooldown):
+          grip_cooldown, net, lights, map_size):
     rect_list = [np.asarray(m, dtype=np.float32).reshape(-1, 4) for m in maps]
     off = np.zeros(len(rect_list) + 1, dtype=np.int32)
     for i, r in enumerate(rect_list):
@@ -121,12 +122,30 @@ def _desc(maps, hbm_budget, max_slots, obs_ring, chunk_steps, policy, lanes, war
                    len(rect_list), rects.ctypes.data_as(_F32P), off.ctypes.data_as(_I32P),
                    int(hbm_budget), int(max_slots), int(obs_ring), int(chunk_steps), int(policy),
                    int(lanes), int(warps), int(ctas), grip_slip_max, grip_cooldown)
-    return d, (rects, off)
+    keep = [rects, off]
+    if net:
+        d.net = 1
+        d.policy = 0
+        if lights is not None:
+            lv = [np.asarray(l, dtype=np.float64).reshape(-1, 6) for l in lights]
+            if len(lv) != len(rect_list):
+                raise ValueError("one light array per map")
+            loff = np.zeros(len(lv) + 1, dtype=np.int32)
+            for i, l in enumerate(lv):
+                loff[i + 1] = loff[i] + len(l)
+            lights_a = np.ascontiguousarray(np.concatenate(lv) if lv else np.zeros((0, 6)))
+            size_a = np.ascontiguousarray(np.tile(np.asarray(map_size, np.float64), (len(lv), 1)))
+            d.lights = lights_a.ctypes.data_as(_F64P)
+            d.map_light_off = loff.ctypes.data_as(_I32P)
+            d.map_size = size_a.ctypes.data_as(_F64P)
+            keep += [lights_a, loff, size_a]
+    return d, keep
 
 
 _DEFAULTS = dict(max_slots=0, obs_ring=0, chunk_steps=32, policy=True, lanes=0, warps=0, ctas=0,
                  substeps=2, iterations=4, h=1 / 120, lin_drag=3.0, ang_drag=3.0, max_speed=360.0,
-                 max_ang_speed=18.0, grip_slip_max=150.0, grip_cooldown=0.05)
+                 max_ang_speed=18.0, grip_slip_max=150.0, grip_cooldown=0.05, net=False, lights=None,
+                 map_size=(1440.0, 810.0))
 
 
 def plan(maps, hbm_budget, **kw):

@@ -126,3 +126,37 @@ def test_net_same_for_every_launch_shape_and_alone():
         x1, o1, m1 = _run_net(sub, [G[i]], 80)
         assert np.array_equal(x1[0], x[i]) and np.array_equal(o1[0], o[i])
         assert np.array_equal(m1[0], metrics[i])
+
+
+def test_server_net_request_equals_engine_with_host_perturbed_genomes():
+    """A mirrored ES request under the reference net: the server perturbs the
+    genome on the device into the net's device layout; the engine given the
+    same theta +- sigma * eps (eps from the device generator, f32 arithmetic
+    on the host) in net.js's own layout gives the same bits."""
+    from kraken_3_gpu_b200 import serve
+    w = workloads.uneven(n=4, n_maps=3, seed=31, h_min=10, h_max=10)
+    arms, segs, pop, H, m = 6, 7, 6, 70, 1
+    x, y = float(w.x[0]), float(w.y[0])
+    m = int(w.map_id[0])
+    rng = np.random.default_rng(8)
+    n_par = batch.net_param_count(arms)
+    theta = random_genome(batch.net_inputs(arms), batch.net_outputs(arms), rng)
+    theta[-1] = 1.0  # the echo fires
+    sigma, seed = 0.05, 123
+    srv = serve.Server(w.maps, 1 << 30, max_slots=32, chunk_steps=16, net=True, lights=w.lights)
+    rid = srv.submit(pop, H, arms, segs, m, x, y, 0.4, theta=theta, sigma=sigma, seed=seed)
+    srv.drain()
+    got = srv.result(rid, pop)["results"]
+    srv.close()
+    G = []
+    for i in range(pop):
+        d = np.float32(sigma) * serve.policy_eps(seed, i // 2, n_par)
+        G.append(theta + d if i % 2 == 0 else theta - d)
+    eng = batch.BatchEngine(w.maps, pop, control="net", lights=w.lights)
+    eng.spawn(0, [arms] * pop, [segs] * pop, [m] * pop, [x] * pop, [y] * pop, [0.4] * pop, [H] * pop)
+    eng.set_net(np.stack(G), np.arange(pop, dtype=np.int32))
+    eng.run(H)
+    want = eng.read_metrics()
+    eng.close()
+    assert np.array_equal(got, want)
+    assert not np.array_equal(got[0], got[1])  # the mirrored pair differs

@@ -41,3 +41,18 @@ def test_eps_restatement_is_standard_normal():
     e = serve_ref.eps(7, 3, 4000)
     assert abs(e.mean()) < 0.06 and abs(e.std() - 1.0) < 0.05
     assert not np.array_equal(e, serve_ref.eps(7, 4, 4000))
+
+
+def test_plan_counts_net_genomes_and_records():
+    """A net server keeps a genome of the largest body (net.js layout, 16-byte
+    rows) and the per-slot sense / net record in every slot; policy and net
+    are exclusive."""
+    maps = _maps()
+    _, without = serve.plan(maps, 1 << 30, policy=False)
+    _, with_net = serve.plan(maps, 1 << 30, net=True)
+    stride = (serve.net_param_count(8) + 3) // 4 * 4
+    assert with_net - without > 4 * stride + 4
+    assert with_net - without - (4 * stride + 4) < 4096  # the record: sense state and the net's vectors
+    lights = [[[100.0, 100.0, 250.0, 0.7, 0.0, 0.1]]] * len(maps)
+    cap_l, per_l = serve.plan(maps, 1 << 30, net=True, lights=lights)
+    assert per_l == with_net
