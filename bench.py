@@ -264,10 +264,12 @@ def served_uneven(serve, w, chunk, sessions):
     return out
 
 
-def served_es_stream(serve, w, chunk, n_req, rate, seed=0):
+def served_es_stream(serve, w, chunk, n_req, rate, seed=0, net=False):
     """ES evaluation requests (mirrored populations 8-512, horizons
     300-3000, body shapes and maps of the mixed workload, fused policy with
-    theta ~ N(0, 0.1^2), sigma 0.02) arriving as a Poisson stream."""
+    theta ~ N(0, 0.1^2), sigma 0.02) arriving as a Poisson stream.  net: the
+    requests' theta is a genome of the reference net (net.js), which then
+    drives every individual with its senses."""
     rng = np.random.default_rng(seed)
     reqs, t = [], 0.0
     for k in range(n_req):
@@ -277,10 +279,12 @@ def served_es_stream(serve, w, chunk, n_req, rate, seed=0):
         reqs.append(dict(population=2 * int(rng.integers(4, 257)), horizon=int(rng.integers(300, 3001)),
                          arms=arms, segs=segs, map_id=int(w.map_id[i]), x=float(w.x[i]), y=float(w.y[i]),
                          angle=float(w.angle[i]),
-                         theta=rng.normal(0, 0.1, serve.policy_params(arms, segs)).astype(np.float32),
+                         theta=rng.normal(0, 0.1, serve.net_param_count(arms) if net else
+                                          serve.policy_params(arms, segs)).astype(np.float32),
                          sigma=0.02, seed=k + 1, arrival=t))
     units = sum(r["population"] * r["horizon"] for r in reqs)
-    srv = serve.Server(w.maps, 8 << 30, max_slots=16384, chunk_steps=chunk, policy=True)
+    srv = (serve.Server(w.maps, 8 << 30, max_slots=16384, chunk_steps=chunk, net=True, lights=w.lights) if net
+           else serve.Server(w.maps, 8 << 30, max_slots=16384, chunk_steps=chunk, policy=True))
     t0 = srv.now() + 0.02
     ids = []
     for r in reqs:
@@ -515,6 +519,8 @@ def main():
         extra["plain_dropin_1024"] = config1_forms(torch, stream)
     if not args.no_net and rank == 0:
         extra["net_controller"] = net_controller(stream, w)
+        if not args.no_es:
+            extra["served_es_stream_net"] = served_es_stream(serve, w, chunk, args.es_requests, 200.0, net=True)
 
     # roofline: f32 rounding ops per creature-step of the restated f32
     # algorithm (op-counting oracle build) x creature-steps per launch /
