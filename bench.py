@@ -71,6 +71,8 @@ def parse():
     ap.add_argument("--es-requests", type=int, default=200)
     ap.add_argument("--no-config1", action="store_true", help="skip the 1,024-creature drop-in comparison")
     ap.add_argument("--no-net", action="store_true", help="skip the reference-net controller rollout")
+    ap.add_argument("--net-only", action="store_true",
+                    help="only the reference-net controller rollout of the workload (one JSON line)")
     ap.add_argument("--traffic", type=float, default=None,
                     help="ncu DRAM bytes per launch of the captured kernel, if measured")
     return ap.parse_args()
@@ -431,6 +433,15 @@ def main():
 
     w = workloads.uneven(n=args.n, n_maps=args.maps, seed=replicas.shard_seed(args.seed, rank),
                          h_min=args.hmin, h_max=args.hmax)
+    if args.net_only:
+        line = net_controller(torch.cuda.current_stream(), w)
+        line.update({"metric": "creature-steps/s under the reference net controller", "n_gpus": 1,
+                     "config": {"workload": f"uneven: {w.n} creatures, {len(w.maps)} maps, horizons "
+                                            f"{args.hmin}-{args.hmax}"}})
+        if rank == 0:
+            print(json.dumps(line))
+        replicas.finish(world)
+        return
     units = w.creature_steps()
     max_h = int(w.horizon.max())
     stream = torch.cuda.current_stream()
