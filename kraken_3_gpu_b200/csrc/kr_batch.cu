@@ -625,7 +625,7 @@ __device__ void run_creature(const BatchArgs &A, const TplDev &td, int nlv, cons
     }
     L.sync();
     // 4. the XPBD step
-    kr::island_step<kr::CompactAccess, G>(A.K, S, rects, nR, cull_d, L);
+    kr::island_step<kr::CompactAccess, G>(A.K, S, rects, nR, cull_d, L, td.off_max + 1.f);
     // 5. postStep, core.js:297-356 (f64 on the f32 state, as the
     //    reference's hybrid loop runs it on the mirrored state)
     //    The accumulators are read and written through the slot's HBM
@@ -884,7 +884,7 @@ int upload_templates(kr_batch *b) {
   for (const auto &t : b->tpls) {
     TplDev d{};
     d.nb = t.nb; d.nc = t.nc; d.np = t.np; d.arms = t.arms; d.segs = t.segs;
-    d.r_max = t.r_max; d.reach = t.reach;
+    d.r_max = t.r_max; d.off_max = t.off_max; d.reach = t.reach;
     d.o_b = (int)im.size(); d.o_p = (int)plx.size(); d.o_a = (int)tip.size(); d.o_s = (int)segs.size();
     im.insert(im.end(), t.im.begin(), t.im.end()); ii.insert(ii.end(), t.ii.begin(), t.ii.end());
     boff.insert(boff.end(), t.boff.begin(), t.boff.end()); bcnt.insert(bcnt.end(), t.bcnt.begin(), t.bcnt.end());

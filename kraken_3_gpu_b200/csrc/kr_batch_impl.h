@@ -29,7 +29,7 @@ struct TplDev {
   int nb, nc, np, arms, segs;
   int nlv[kr::kSchedules];
   float r_max;
-  float pad0;
+  float off_max;   // largest distance of a collision point from its body's centre
   double reach;
   int o_b, o_p, o_a, o_s;
   int o_c[kr::kSchedules], o_l[kr::kSchedules], o_g[kr::kSchedules];

@@ -435,9 +435,43 @@ __device__ __forceinline__ void solve_angle(const SolverConsts &K, Island &S, in
 //      it; after the first correction the remaining points of that body are
 //      re-evaluated at the moved pose, exactly as the sequential loop does.
 // cull_d = D + kCullSlack with D as in the comment above kMaxCulled.
+//
+// reach >= 0 bounds every collision point's distance from its body's centre
+// (plus rounding: 1 px).  Then a pass whose culled list would be empty --
+// no rect within cull_d of the box of the bodies' centres widened by reach,
+// which holds the box of the points -- corrects no point: every evaluation
+// returns "far", nothing moves, and the scratch it writes (bs, bc, pdx, pdy,
+// pflag) is read by nothing after the pass.  It returns before any of that
+// work.  reach < 0: no such bound (the drop-in world).
 template <int G>
 __device__ __forceinline__ void collide_island(Island &S, const float4 *__restrict__ rects, int nR,
-                                               float cull_d, const Lanes<G> &L) {
+                                               float cull_d, const Lanes<G> &L, float reach) {
+  if (reach >= 0.f) {
+    float lx = __int_as_float(0x7f800000), ly = lx, hx = -lx, hy = -lx;
+    for (int j = L.lane; j < S.nb; j += G) {
+      lx = fminf(lx, S.ppx[j]); hx = fmaxf(hx, S.ppx[j]);
+      ly = fminf(ly, S.ppy[j]); hy = fmaxf(hy, S.ppy[j]);
+    }
+    lx = L.min(lx); ly = L.min(ly);
+    hx = L.max(hx); hy = L.max(hy);
+    const float e = reach + cull_d;
+    const float x0 = lx - e, x1 = hx + e, y0 = ly - e, y1 = hy + e;
+    // finite and below 1e6 px (f32 spacing <= 1/16 px there, so the 1 px in
+    // reach covers the rounding of the point positions and of these bounds)
+    if (x0 <= x1 && y0 <= y1 && fmaxf(fmaxf(fabsf(x0), fabsf(x1)), fmaxf(fabsf(y0), fabsf(y1))) < 1e6f) {
+      bool near = false;
+      for (int base = 0; base < nR && !near; base += G) {
+        const int i = base + L.lane;
+        bool keep = false;
+        if (i < nR) {
+          const float4 r = __ldg(rects + i);
+          keep = !(r.z < x0 || r.x > x1 || r.w < y0 || r.y > y1);
+        }
+        near = L.ballot(keep) != 0u;
+      }
+      if (!near) return;
+    }
+  }
   for (int j = L.lane; j < S.nb; j += G) {
     float s, c;
     sincos_r(S.angP[j], &s, &c);
@@ -577,7 +611,7 @@ __device__ __forceinline__ void grip_break(const SolverConsts &K, Island &S, int
 template <class Acc, int G>
 __device__ __forceinline__ void island_step(const SolverConsts &K, Island &S,
                                             const float4 *__restrict__ rects, int nR, float cull_d,
-                                            const Lanes<G> &L) {
+                                            const Lanes<G> &L, float reach) {
   for (int s = 0; s < K.substeps; s++) {
     for (int k = L.lane; k < S.nc; k += G) { S.lamX[k] = 0.f; S.lamY[k] = 0.f; S.lam[k] = 0.f; }
     for (int i = L.lane; i < S.nb; i += G) integrate_body(K, S, i);
@@ -592,7 +626,7 @@ __device__ __forceinline__ void island_step(const SolverConsts &K, Island &S,
         }
         L.sync();
       }
-      collide_island<G>(S, rects, nR, cull_d, L);
+      collide_island<G>(S, rects, nR, cull_d, L, reach);
     }
     for (int i = L.lane; i < S.nb; i += G) finalize_body(K, S, i);
     L.sync();

@@ -263,6 +263,8 @@ bool build_template(int arms, int segs, Template *t, std::string *err) {
     t->plx[q] = (float)plx[p]; t->ply[q] = (float)ply[p]; t->pr[q] = (float)pr[p];
     t->pbody[q] = pbody[p];
     t->r_max = std::max(t->r_max, (float)pr[p]);
+    const double off = std::sqrt((double)t->plx[q] * t->plx[q] + (double)t->ply[q] * t->ply[q]);
+    t->off_max = std::max(t->off_max, (float)off);
   }
   return true;
 }

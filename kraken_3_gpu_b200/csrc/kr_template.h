@@ -62,6 +62,7 @@ struct Template {
   std::vector<int> arm_seg0;            // first segment body
   std::vector<int> arm_segs;            // arms x segs body ids
   float r_max = 0.f;                    // largest collision radius
+  float off_max = 0.f;                  // largest distance of a collision point from its body's centre
   double reach = 0.0;                   // ARM_REACH for this segment count
 };
 

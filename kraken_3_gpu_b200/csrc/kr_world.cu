@@ -151,7 +151,7 @@ __device__ __forceinline__ void plain_step_body(const StepArgs &A) {
   }
   __syncwarp();
 
-  kr::island_step<kr::SlotAccess, 32>(A.K, S, A.rects, A.nR, A.cull_d, kr::Lanes<32>(lane));
+  kr::island_step<kr::SlotAccess, 32>(A.K, S, A.rects, A.nR, A.cull_d, kr::Lanes<32>(lane), -1.f);
 
   // write back bodies, consumed forces and constraint multipliers / flags
   for (int i = lane; i < S.nb; i += 32) {
