@@ -519,8 +519,18 @@ __device__ __noinline__ void net_senses(NetArgs N, int arms, const int *arm_tip,
     double st, ct;
     sincos((double)ang[tip], &st, &ct);
     const double tx = (double)px[tip] + kSegHalf * ct, ty = (double)py[tip] + kSegHalf * st;
+    // near is 0 unless a rect lies within 9 px: a rect whose box is 10 px
+    // away or more cannot make it positive, so the SDF runs only when some
+    // box is closer (the result is the same either way)
+    bool close = false;
+    for (int i = 0; i < nR && !close; i++) {
+      const double *r = rects + 4 * i;
+      const bool far = r[2] >= 0 && r[3] >= 0 &&
+                       (tx <= r[0] - 10 || tx >= r[0] + r[2] + 10 || ty <= r[1] - 10 || ty >= r[1] + r[3] + 10);
+      close = !far;  // NaN coordinates or extents count as close: the SDF then decides
+    }
     double d;
-    const double near = sdf64(rects, nR, tx, ty, &d) ? fmax(0.0, 1 - d / 9) : 0.0;
+    const double near = close && sdf64(rects, nR, tx, ty, &d) ? fmax(0.0, 1 - d / 9) : 0.0;
     R.contact[a] = R.contact[a] * 0.7 + near * 0.3;
   }
   L.sync();
