@@ -434,44 +434,137 @@ __device__ __forceinline__ void solve_angle(const SolverConsts &K, Island &S, in
 //      the sequential one as long as no earlier point of that body moved
 //      it; after the first correction the remaining points of that body are
 //      re-evaluated at the moved pose, exactly as the sequential loop does.
-// cull_d = D + kCullSlack with D as in the comment above kMaxCulled.
-//
-// reach >= 0 bounds every collision point's distance from its body's centre
-// (plus rounding: 1 px).  Then a pass whose culled list would be empty --
-// no rect within cull_d of the box of the bodies' centres widened by reach,
-// which holds the box of the points -- corrects no point: every evaluation
-// returns "far", nothing moves, and the scratch it writes (bs, bc, pdx, pdy,
-// pflag) is read by nothing after the pass.  It returns before any of that
-// work.  reach < 0: no such bound (the drop-in world).
+// The collision pass with the culled list taken from the box of the bodies'
+// centres widened by reach (>= every collision point's distance from its
+// body's centre, plus 1 px for rounding): the rects within cull_d of that
+// box, in ascending order.  The box holds every point the pass evaluates, so
+// the list keeps every rect within cull_d of them and the fold over it is
+// exact by the argument above kMaxCulled.  A body with no listed rect within
+// reach + cull_d of its centre has no point that any rect can correct: its
+// sin/cos, point positions and SDF evaluations are skipped (bc[j] = 2, an
+// impossible cosine, marks it) -- its points are unflagged, as the full
+// evaluation would leave them.  With an empty list the pass changes nothing
+// and ends at once.  Returns false, having changed nothing, when the box is
+// not finite or reaches 1e6 px (where 1 px no longer covers f32 rounding) or
+// the list would exceed kMaxCulled; the caller then runs the pass below.
+template <int G>
+__device__ __forceinline__ bool collide_bodies(Island &S, const float4 *__restrict__ rects, int nR, float cull_d,
+                                               const Lanes<G> &L, float reach) {
+  float lx = __int_as_float(0x7f800000), ly = lx, hx = -lx, hy = -lx;
+  for (int j = L.lane; j < S.nb; j += G) {
+    lx = fminf(lx, S.ppx[j]); hx = fmaxf(hx, S.ppx[j]);
+    ly = fminf(ly, S.ppy[j]); hy = fmaxf(hy, S.ppy[j]);
+  }
+  lx = L.min(lx); ly = L.min(ly);
+  hx = L.max(hx); hy = L.max(hy);
+  const float e = reach + cull_d;
+  const float x0 = lx - e, x1 = hx + e, y0 = ly - e, y1 = hy + e;
+  if (!(x0 <= x1 && y0 <= y1 && fmaxf(fmaxf(fabsf(x0), fabsf(x1)), fmaxf(fabsf(y0), fabsf(y1))) < 1e6f))
+    return false;
+  int ncull = 0;
+  for (int base = 0; base < nR; base += G) {
+    const int i = base + L.lane;
+    bool keep = false;
+    if (i < nR) {
+      const float4 r = __ldg(rects + i);
+      keep = !(r.z < x0 || r.x > x1 || r.w < y0 || r.y > y1);
+    }
+    const unsigned m = L.ballot(keep);
+    const int at = ncull + __popc(m & ((1u << L.lane) - 1u));
+    if (keep && at < kMaxCulled) S.cull[at] = static_cast<short>(i);
+    ncull += __popc(m);
+    if (ncull > kMaxCulled) {
+      L.sync();
+      return false;
+    }
+  }
+  if (ncull == 0) return true;
+  L.sync();
+  for (int j = L.lane; j < S.nb; j += G) {
+    const float cx = S.ppx[j], cy = S.ppy[j];
+    bool near = false;
+    for (int q = 0; q < ncull && !near; q++) {
+      const float4 r = __ldg(rects + S.cull[q]);
+      near = !(r.z < cx - e || r.x > cx + e || r.w < cy - e || r.y > cy + e);
+    }
+    if (near) {
+      float sn, cs;
+      sincos_r(S.angP[j], &sn, &cs);
+      S.bs[j] = sn;
+      S.bc[j] = cs;
+    } else {
+      S.bc[j] = 2.f;
+    }
+  }
+  L.sync();
+  for (int p = L.lane; p < S.np; p += G) {
+    const int j = S.pbody[p];
+    const float ca = S.bc[j];
+    int flag = 0;
+    float cx = 0.f, cy = 0.f;
+    if (ca != 2.f && S.im[j] != 0.f) {
+      const float sa = S.bs[j], ox = S.plx[p], oy = S.ply[p];
+      const float wx = fadd(S.ppx[j], fsub(fmul(ox, ca), fmul(oy, sa)));
+      const float wy = fadd(S.ppy[j], fadd(fmul(ox, sa), fmul(oy, ca)));
+      float d, nx, ny;
+      if (sdf(rects, S.cull, ncull, wx, wy, &d, &nx, &ny)) {
+        const float pen = fsub(S.pr[p], d);
+        if (pen > kSlackPos) {
+          flag = 1;
+          cx = fmul(nx, pen);
+          cy = fmul(ny, pen);
+        }
+      }
+    }
+    S.pflag[p] = flag;
+    S.pdx[p] = cx;
+    S.pdy[p] = cy;
+  }
+  L.sync();
+  const float sx0 = lx - reach - kCullSlack, sx1 = hx + reach + kCullSlack;
+  const float sy0 = ly - reach - kCullSlack, sy1 = hy + reach + kCullSlack;
+  for (int j = L.lane; j < S.nb; j += G) {
+    if (S.im[j] == 0.f || S.bc[j] == 2.f) continue;
+    const int o = S.boff[j], cnt = S.bcnt[j];
+    float px = S.ppx[j], py = S.ppy[j];
+    const float ca = S.bc[j], sa = S.bs[j];
+    bool moved = false;
+    for (int q = 0; q < cnt; q++) {
+      const int p = o + q;
+      if (!moved) {
+        if (S.pflag[p]) {
+          px = fadd(px, S.pdx[p]);
+          py = fadd(py, S.pdy[p]);
+          moved = true;
+        }
+        continue;
+      }
+      const float ox = S.plx[p], oy = S.ply[p];
+      const float wx = fadd(px, fsub(fmul(ox, ca), fmul(oy, sa)));
+      const float wy = fadd(py, fadd(fmul(ox, sa), fmul(oy, ca)));
+      const bool in_box = wx >= sx0 && wx <= sx1 && wy >= sy0 && wy <= sy1;
+      float d, nx, ny;
+      if (!sdf(rects, in_box ? S.cull : nullptr, in_box ? ncull : nR, wx, wy, &d, &nx, &ny)) continue;
+      const float pen = fsub(S.pr[p], d);
+      if (pen <= kSlackPos) continue;
+      px = fadd(px, fmul(nx, pen));
+      py = fadd(py, fmul(ny, pen));
+    }
+    S.ppx[j] = px;
+    S.ppy[j] = py;
+  }
+  L.sync();
+  return true;
+}
+
+// cull_d = D + kCullSlack with D as in the comment above kMaxCulled.  reach
+// >= 0 (the batched engine's templates): collide_bodies; reach < 0 (the
+// drop-in world, arbitrary collision points): the culled list from the box
+// of the evaluated points.
 template <int G>
 __device__ __forceinline__ void collide_island(Island &S, const float4 *__restrict__ rects, int nR,
                                                float cull_d, const Lanes<G> &L, float reach) {
-  if (reach >= 0.f) {
-    float lx = __int_as_float(0x7f800000), ly = lx, hx = -lx, hy = -lx;
-    for (int j = L.lane; j < S.nb; j += G) {
-      lx = fminf(lx, S.ppx[j]); hx = fmaxf(hx, S.ppx[j]);
-      ly = fminf(ly, S.ppy[j]); hy = fmaxf(hy, S.ppy[j]);
-    }
-    lx = L.min(lx); ly = L.min(ly);
-    hx = L.max(hx); hy = L.max(hy);
-    const float e = reach + cull_d;
-    const float x0 = lx - e, x1 = hx + e, y0 = ly - e, y1 = hy + e;
-    // finite and below 1e6 px (f32 spacing <= 1/16 px there, so the 1 px in
-    // reach covers the rounding of the point positions and of these bounds)
-    if (x0 <= x1 && y0 <= y1 && fmaxf(fmaxf(fabsf(x0), fabsf(x1)), fmaxf(fabsf(y0), fabsf(y1))) < 1e6f) {
-      bool near = false;
-      for (int base = 0; base < nR && !near; base += G) {
-        const int i = base + L.lane;
-        bool keep = false;
-        if (i < nR) {
-          const float4 r = __ldg(rects + i);
-          keep = !(r.z < x0 || r.x > x1 || r.w < y0 || r.y > y1);
-        }
-        near = L.ballot(keep) != 0u;
-      }
-      if (!near) return;
-    }
-  }
+  if (reach >= 0.f && collide_bodies<G>(S, rects, nR, cull_d, L, reach)) return;
   for (int j = L.lane; j < S.nb; j += G) {
     float s, c;
     sincos_r(S.angP[j], &s, &c);
