@@ -57,6 +57,7 @@ struct StepArgs {
   const float4 *rects;     // nR x (x, y, x+w, y+h)
   int nR;
   float cull_d;            // rect culling distance of a collision pass
+  float reach;             // bound on a collision point's distance from its body (+1 px), < 0: none
   int nI;
   int maxB, maxC, maxP;    // smem carve sizes (per warp)
   DeviceTables T;
@@ -151,7 +152,7 @@ __device__ __forceinline__ void plain_step_body(const StepArgs &A) {
   }
   __syncwarp();
 
-  kr::island_step<kr::SlotAccess, 32>(A.K, S, A.rects, A.nR, A.cull_d, kr::Lanes<32>(lane), -1.f);
+  kr::island_step<kr::SlotAccess, 32>(A.K, S, A.rects, A.nR, A.cull_d, kr::Lanes<32>(lane), A.reach);
 
   // write back bodies, consumed forces and constraint multipliers / flags
   for (int i = lane; i < S.nb; i += 32) {
@@ -215,6 +216,7 @@ struct kr_world {
   size_t c_isl = 0, c_ibodies = 0, c_icons = 0, c_iab = 0, c_ipts = 0, c_lvl = 0, c_bpt = 0;
   float max_half_thick = 0.f;  // largest min(w, h) / 2 of the map's rects
   float cull_d = 0.f;
+  float reach = -1.f;          // largest collision-point offset + 1 px (kr_solver.cuh collide_bodies)
   int nI = 0, maxB = 1, maxC = 1, maxP = 1, maxLv = 0;
   bool uploaded = false;
   cudaStream_t stream = nullptr;
@@ -358,12 +360,20 @@ extern "C" int kr_create(const kr_solver_params *params, uint32_t n_bodies, uint
     if (std::isfinite(ht)) half_thick = std::max(half_thick, ht);
     else half_thick = HUGE_VAL;
   }
+  double off_max = 0.0;
   for (uint32_t i = 0; i < n_coll_pts; i++) {
-    float r;
+    float r, lx, ly;
+    std::memcpy(&lx, &coll_pts[4 * i + 1], sizeof(float));
+    std::memcpy(&ly, &coll_pts[4 * i + 2], sizeof(float));
     std::memcpy(&r, &coll_pts[4 * i + 3], sizeof(float));
     if (std::isfinite(r)) r_max = std::max(r_max, std::fabs((double)r));
     else r_max = HUGE_VAL;
+    const double off = std::sqrt((double)lx * lx + (double)ly * ly);
+    off_max = std::isfinite(off) ? std::max(off_max, off) : HUGE_VAL;
   }
+  // every collision point lies within off_max of its body's centre: the
+  // collision pass may skip bodies with no rect nearby (collide_bodies)
+  w->reach = off_max < 1e5 ? (float)off_max + 1.f : -1.f;
   // D = max(radius, half thickness) + 2, plus the slack of the culling box;
   // the f32 rounding of the box test is covered by the +1
   const double cull = std::max(r_max, half_thick) + 2.0 + kr::kCullSlack + 1.0;
@@ -612,6 +622,7 @@ extern "C" int kr_step(kr_world *w, int32_t n_steps) {
   A.maxB = w->maxB; A.maxC = w->maxC; A.maxP = w->maxP;
   A.T = DeviceTables{w->d_isl, w->d_ibodies, w->d_icons, w->d_iab, w->d_ipts, w->d_bpt, w->d_lvl};
   A.cull_d = w->cull_d;
+  A.reach = w->reach;
   const size_t smem = w->smem_bytes;
   cudaError_t e;
   const int grid = (w->nI + kWarpsPerBlock - 1) / kWarpsPerBlock;
@@ -931,6 +942,7 @@ extern "C" int kr_step_noalloc(const kr_solver_params *params, uint32_t n_bodies
   A.rects = reinterpret_cast<const float4 *>(W + kOffRects);
   A.nR = (int)n_rects;
   A.cull_d = 0.f;
+  A.reach = -1.f;
   A.nI = 0;
   // shared memory for the largest island the world can hold
   A.maxB = ((int)std::min<uint32_t>(n_bodies, KR_MAX_ISLAND_BODIES) + 3) & ~3;
