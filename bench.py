@@ -45,9 +45,9 @@ sys.path.insert(0, ROOT)
 
 METRIC = "creature-steps/s at 16k mixed envs, served vs plain launch; p50/p99 rollout ms"
 # DRAM bytes (read + write) of one persistent launch per creature, from an ncu
-# capture of the full 16,384-creature launch (37.81 MB read + 0.25 MB written):
-# the state copied in and out, independent of the step count
-NCU_DRAM_BYTES_PER_CREATURE = (37.81e6 + 248.06e3) / 16384
+# capture of the full 16,384-creature launch (40.86 MB read + 54.30 MB written):
+# the state, grips and slot records in and out, independent of the step count
+NCU_DRAM_BYTES_PER_CREATURE = (40.86e6 + 54.30e6) / 16384
 UNIT = "creature-steps/s"
 
 
@@ -547,7 +547,8 @@ def main():
                     "unit": "TFLOP/s", "frac": achieved / fma_rate,
                     "traffic": args.traffic if args.traffic is not None else NCU_DRAM_BYTES_PER_CREATURE * w.n,
                     "traffic_note": "ncu dram__bytes_read.sum + dram__bytes_write.sum of the full launch "
-                                    "(state in and out, ~2.3 KB per creature); algorithmic bytes ~2.5 KB",
+                                    "(state, grips and slot records in and out, ~5.8 KB per creature); "
+                                    "algorithmic bytes ~2.5 KB",
                     "ops_per_creature_step": ops, "kernel_ms": kms,
                     "peak_note": "measured dependent-free f32 FMA issue rate (lane-ops/s) of this GPU; "
                                  "MEASURED_PEAKS.json has no f32 figure"}
