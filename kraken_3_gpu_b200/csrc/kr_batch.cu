@@ -352,7 +352,9 @@ __device__ __noinline__ float net_control(NetArgs N, int arms, int segs, const f
   // device layout (net_transpose): W1T, b1, W2T, b2, W3T, b3 -- lane j of a
   // row reads word j, so a warp's loads are consecutive words.  Each lane
   // carries its units j = lane + u G as independent f64 chains; every sum
-  // still runs over i in ascending order from its bias.
+  // still runs over i in ascending order from its bias.  A product of two
+  // f32 values is exact in f64, so fma(x, w, acc) rounds once exactly as
+  // the reference's acc + x * w does.
   const float *w1 = N.pw + (size_t)N.pw_idx[slot] * N.pw_stride;
   const float *b1 = w1 + (size_t)ni * H, *w2 = b1 + H, *b2 = w2 + H * H, *w3 = b2 + H, *b3 = w3 + H * no;
   constexpr int U = (KR_NET_HIDDEN + G - 1) / G, UO = (KR_NET_OUT_STRIDE + G - 1) / G;
@@ -364,7 +366,7 @@ __device__ __noinline__ float net_control(NetArgs N, int arms, int segs, const f
     const float *r = w1 + i * H;
 #pragma unroll
     for (int u = 0; u < U; u++)
-      if (lane + u * G < H) acc[u] += xi * (double)r[lane + u * G];
+      if (lane + u * G < H) acc[u] = fma(xi, (double)r[lane + u * G], acc[u]);
   }
 #pragma unroll
   for (int u = 0; u < U; u++)
@@ -377,7 +379,7 @@ __device__ __noinline__ float net_control(NetArgs N, int arms, int segs, const f
     const float *r = w2 + i * H;
 #pragma unroll
     for (int u = 0; u < U; u++)
-      if (lane + u * G < H) acc[u] += hi * (double)r[lane + u * G];
+      if (lane + u * G < H) acc[u] = fma(hi, (double)r[lane + u * G], acc[u]);
   }
 #pragma unroll
   for (int u = 0; u < U; u++)
@@ -390,7 +392,7 @@ __device__ __noinline__ float net_control(NetArgs N, int arms, int segs, const f
     const float *r = w3 + i * no;
 #pragma unroll
     for (int u = 0; u < UO; u++)
-      if (lane + u * G < no) acc[u] += hi * (double)r[lane + u * G];
+      if (lane + u * G < no) acc[u] = fma(hi, (double)r[lane + u * G], acc[u]);
   }
 #pragma unroll
   for (int u = 0; u < UO; u++)
