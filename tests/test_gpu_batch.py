@@ -221,3 +221,49 @@ def test_autotune_leaves_slots_as_they_were():
     assert np.array_equal(ref.read_metrics(), eng.read_metrics())
     ref.close()
     eng.close()
+
+
+@pytest.mark.parametrize("lanes", [8, 16, 32])
+def test_creatures_against_walls_bit_exact_vs_f32_oracle(lanes):
+    """Creatures spawned with their arms across the walls of their map, so
+    that collision passes correct many points every step (the culled list,
+    the per-body skip and the sequential commit all active): body state equal
+    to the f32 oracle bit for bit after 30 steps, under every lane count."""
+    w = _small_uneven(n=12, n_maps=3, h=30)
+    rng = np.random.default_rng(17)
+    for i in range(w.n):
+        r = w.maps[w.map_id[i]]
+        # an inner wall where the map has one (the first four rects are the border)
+        k = 4 + int(rng.integers(0, len(r) - 4)) if len(r) > 4 else int(rng.integers(0, 4))
+        x, y, rw, rh = (float(v) for v in r[k])
+        reach = 24 + 13.5 * int(w.segs[i])
+        if rw < rh:   # vertical wall: mantle beside it on the map's side, arms across it
+            w.x[i] = x - 0.6 * reach if x > 720 else x + rw + 0.6 * reach
+            w.y[i] = y + 0.5 * rh
+        else:
+            w.x[i] = x + 0.5 * rw
+            w.y[i] = y - 0.6 * reach if y > 405 else y + rh + 0.6 * reach
+    eng = batch.BatchEngine(w.maps, w.n)
+    workloads.spawn_all(eng, w)
+    eng.set_launch(4 if lanes == 32 else 8, 0, lanes_per_creature=lanes)
+    eng.run(30)
+    st = eng.read_state()
+    eng.close()
+    moved_by_walls = 0
+    for i in range(w.n):
+        sim, grips, _ = _oracle_run(w, i, 30)
+        nb = sim.world.n
+        for f in ("px", "py", "ang", "vx", "vy", "av"):
+            assert np.array_equal(st[f][i, :nb], sim.world.arr(f).astype(np.float32)), (i, f)
+        free = ob.Sim(rects=np.zeros((0, 4)))  # the same creature with no map: how far walls moved it
+        free.add_creature(w.x[i], w.y[i], w.angle[i], int(w.arms[i]), int(w.segs[i]))
+        free.world.f32ify()
+        free.world.round_state()
+        cs = ControlStream(int(w.arms[i]), int(w.segs[i]), seed=int(w.seed[i]))
+        for s in range(30):
+            t, a = cs.at(s)
+            t32, a32 = (v.astype(np.float32).astype(np.float64) for v in (t, a))
+            free.apply_control_motors(0, TONE, t32, a32)
+            free.step32()
+        moved_by_walls += not np.array_equal(free.world.arr("px"), sim.world.arr("px"))
+    assert moved_by_walls >= w.n // 2, moved_by_walls  # the walls acted on most creatures
