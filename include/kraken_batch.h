@@ -197,6 +197,11 @@ int kr_batch_restore(kr_batch *b);
  * second over every SM), the issue-rate ceiling of the f32 path. */
 int kr_probe_fp32_rate(double *fma_per_s);
 
+/* The solver's sin / cos of f32 angles (Math.fround of the f64 sin / cos, as
+ * f32solver.mjs evaluates them) for n host values: s[i], c[i] of x[i].
+ * Synchronous; for checking the device's trig against a reference. */
+int kr_probe_sincos(const float *x, int32_t n, float *s, float *c);
+
 /* Launch shape: lanes per creature (32, 16 or 8: a warp carries 32 / lanes
  * creatures), warps per CTA (1..16, at most 64 creatures per CTA) and CTAs
  * per SM (0 = 16 / warps).  A CTA gets an equal share of the SM's shared

@@ -107,6 +107,7 @@ def _lib():
         "kr_batch_snapshot": (C.c_int, [vp]),
         "kr_batch_restore": (C.c_int, [vp]),
         "kr_probe_fp32_rate": (C.c_int, [_F64P]),
+        "kr_probe_sincos": (C.c_int, [_F32P, i32, _F32P, _F32P]),
     }
     for name, (res, args) in sigs.items():
         fn = getattr(L, name)
@@ -333,3 +334,14 @@ def probe_fp32_rate() -> float:
     r = C.c_double()
     _check(_lib().kr_probe_fp32_rate(C.byref(r)), None)
     return r.value
+
+
+def probe_sincos(x):
+    """The solver's device sin / cos of f32 angles (each the f64 value
+    rounded once to f32): (sin, cos) arrays."""
+    x = np.ascontiguousarray(x, dtype=np.float32)
+    s = np.zeros_like(x)
+    c = np.zeros_like(x)
+    _check(_lib().kr_probe_sincos(x.ctypes.data_as(_F32P), len(x), s.ctypes.data_as(_F32P),
+                                  c.ctypes.data_as(_F32P)), None)
+    return s, c

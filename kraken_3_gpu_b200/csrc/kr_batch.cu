@@ -1988,6 +1988,30 @@ __global__ void fma_probe_kernel(float *out, int iters) {
 }
 }  // namespace
 
+namespace {
+__global__ void sincos_probe_kernel(const float *x, int n, float *s, float *c) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) kr::sincos_r(x[i], s + i, c + i);
+}
+}  // namespace
+
+extern "C" int kr_probe_sincos(const float *x, int32_t n, float *s, float *c) {
+  if (!x || !s || !c || n < 0) { g_batch_error = "kr_probe_sincos: bad arguments"; return KR_ERR_INVALID; }
+  if (n == 0) return KR_OK;
+  float *d = nullptr;
+  cudaError_t e = cudaMalloc(&d, (size_t)n * 3 * sizeof(float));
+  if (e == cudaSuccess) e = cudaMemcpy(d, x, (size_t)n * sizeof(float), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) {
+    sincos_probe_kernel<<<(n + 255) / 256, 256>>>(d, n, d + n, d + 2 * (size_t)n);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaMemcpy(s, d + n, (size_t)n * sizeof(float), cudaMemcpyDeviceToHost);
+  if (e == cudaSuccess) e = cudaMemcpy(c, d + 2 * (size_t)n, (size_t)n * sizeof(float), cudaMemcpyDeviceToHost);
+  cudaFree(d);
+  if (e != cudaSuccess) { g_batch_error = cudaGetErrorString(e); return KR_ERR_CUDA; }
+  return KR_OK;
+}
+
 extern "C" int kr_probe_fp32_rate(double *fma_per_s) {
   if (!fma_per_s) return KR_ERR_INVALID;
   int dev = 0, n_sm = 0;

@@ -267,3 +267,20 @@ def test_creatures_against_walls_bit_exact_vs_f32_oracle(lanes):
             free.step32()
         moved_by_walls += not np.array_equal(free.world.arr("px"), sim.world.arr("px"))
     assert moved_by_walls >= w.n // 2, moved_by_walls  # the walls acted on most creatures
+
+
+def test_device_sincos_is_the_rounded_f64_value():
+    """The solver's f64 sin / cos rounded to f32 against numpy's f64 sin / cos
+    rounded to f32, on 2 M angles up to 2^20 rad and the ones the bodies
+    meet (|x| < 60): equal except where both f64 values straddle an f32
+    rounding midpoint (a few in 1e9), and within one f32 ulp everywhere."""
+    rng = np.random.default_rng(3)
+    x = np.concatenate([rng.uniform(-60, 60, 1_500_000), rng.uniform(-2.0 ** 20, 2.0 ** 20, 500_000),
+                        np.arange(-64, 65) * (np.pi / 32)]).astype(np.float32)
+    s, c = batch.probe_sincos(x)
+    want_s = np.sin(x.astype(np.float64)).astype(np.float32)
+    want_c = np.cos(x.astype(np.float64)).astype(np.float32)
+    diff = int(np.sum(s != want_s) + np.sum(c != want_c))
+    assert diff <= 3, diff
+    assert np.all(np.abs(s.view(np.int32).astype(np.int64) - want_s.view(np.int32)) <= 1)
+    assert np.all(np.abs(c.view(np.int32).astype(np.int64) - want_c.view(np.int32)) <= 1)
