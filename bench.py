@@ -471,18 +471,22 @@ def main():
 
     sampler = ClockSampler(local)
     sampler.start()
-    time.sleep(0.3)
+    # one more rollout while the sampler starts: the GPU stays busy (and its
+    # clocks up) until the timed region begins
+    eng.restore()
+    eng.run(max_h)
     barrier()
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    for _ in range(args.steps):
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
+    ev[0].record(stream)
+    for k in range(args.steps):
         flush.zero_()
         eng.restore()
         eng.run(max_h)
-    e1.record(stream)
-    e1.synchronize()
+        ev[k + 1].record(stream)
+    ev[-1].synchronize()
     barrier()
+    e0, e1 = ev[0], ev[-1]
+    rollout_ms = [ev[k].elapsed_time(ev[k + 1]) for k in range(args.steps)]
     elapsed_ms = e0.elapsed_time(e1)
     kms = eng.last_ms()  # the last rollout's kernel alone (events on its stream)
     t_max = all_max(elapsed_ms)
@@ -562,6 +566,7 @@ def main():
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
+            "rollout_ms": [round(x, 3) for x in rollout_ms],
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32", "data": "synthetic",
             "config": {"workload": "uneven-16k: 16,384 creatures, 64 maps, 4-8 arms x 5-9 segments, "
