@@ -160,3 +160,25 @@ def test_server_net_request_equals_engine_with_host_perturbed_genomes():
     eng.close()
     assert np.array_equal(got, want)
     assert not np.array_equal(got[0], got[1])  # the mirrored pair differs
+
+
+def test_net_restore_and_autotune_keep_the_sense_state():
+    """The net record (echo queue, lights, contact, recurrent outputs) is part
+    of a slot's state: a rollout restored from a snapshot repeats itself, and
+    the autotuner's trial launches leave the slots as they were."""
+    w = workloads.uneven(n=16, n_maps=2, seed=27, h_min=90, h_max=90, arms=(6, 6), segs=(5, 9))
+    G = _genomes(w, 9, echo_bias=1.5)
+    eng = batch.BatchEngine(w.maps, w.n, control="net", lights=w.lights)
+    workloads.spawn_all(eng, w)
+    eng.set_net(np.stack(G), np.arange(w.n, dtype=np.int32))
+    eng.run(30)
+    eng.snapshot()
+    eng.run(60)
+    first = (eng.read_net(), eng.read_metrics())
+    eng.restore()
+    eng.autotune(8)
+    eng.run(60)
+    second = (eng.read_net(), eng.read_metrics())
+    eng.close()
+    assert np.array_equal(first[0][0], second[0][0]) and np.array_equal(first[0][1], second[0][1])
+    assert np.array_equal(first[1], second[1])
