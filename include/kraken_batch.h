@@ -202,6 +202,12 @@ int kr_probe_fp32_rate(double *fma_per_s);
  * Synchronous; for checking the device's trig against a reference. */
 int kr_probe_sincos(const float *x, int32_t n, float *s, float *c);
 
+/* readProprio's atan2(sin d, cos d) of f64 angle differences as the device
+ * evaluates it (src/body/kraken.js:173 armCurl, src/sim/core.js:138 the
+ * shoulder angle): out[i] for d[i], d wrapped into (-pi, pi].
+ * Synchronous; for checking the device's wrap against a reference. */
+int kr_probe_wrap(const double *d, int32_t n, double *out);
+
 /* Launch shape: lanes per creature (32, 16 or 8: a warp carries 32 / lanes
  * creatures), warps per CTA (1..16, at most 64 creatures per CTA) and CTAs
  * per SM (0 = 16 / warps).  A CTA gets an equal share of the SM's shared

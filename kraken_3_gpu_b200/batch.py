@@ -108,6 +108,7 @@ def _lib():
         "kr_batch_restore": (C.c_int, [vp]),
         "kr_probe_fp32_rate": (C.c_int, [_F64P]),
         "kr_probe_sincos": (C.c_int, [_F32P, i32, _F32P, _F32P]),
+        "kr_probe_wrap": (C.c_int, [_F64P, i32, _F64P]),
     }
     for name, (res, args) in sigs.items():
         fn = getattr(L, name)
@@ -334,6 +335,15 @@ def probe_fp32_rate() -> float:
     r = C.c_double()
     _check(_lib().kr_probe_fp32_rate(C.byref(r)), None)
     return r.value
+
+
+def probe_wrap(d):
+    """readProprio's atan2(sin d, cos d) of f64 angle differences as the
+    device evaluates it (d wrapped into (-pi, pi])."""
+    d = np.ascontiguousarray(d, dtype=np.float64)
+    out = np.zeros_like(d)
+    _check(_lib().kr_probe_wrap(d.ctypes.data_as(_F64P), len(d), out.ctypes.data_as(_F64P)), None)
+    return out
 
 
 def probe_sincos(x):

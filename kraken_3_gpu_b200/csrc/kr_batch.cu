@@ -163,6 +163,34 @@ __device__ inline double mulberry_next(uint32_t &s) {
 
 __device__ inline double clamp_sym(double v, double m) { return v > m ? m : (v < -m ? -m : v); }
 
+// Math.atan2(Math.sin(d), Math.cos(d)) (kraken.js:173 armCurl, core.js:138
+// the shoulder angle) for the f64 difference d of two angles, as the exact
+// value that chain of f64 calls approximates to within a few ulp: d wrapped
+// into (-pi, pi].  For |d| <= pi that is d itself;
+// otherwise d - 2 pi k with k = rint(d / 2 pi) and 2 pi in three parts
+// (k times each of the first two exact for |k| < 2^24, d - k p1 exact by
+// Sterbenz), moved by one period more when the rounded quotient left the
+// remainder outside [-pi, pi].  Beyond |d| = 2^20, and for non-finite d,
+// the chain itself is evaluated.
+__device__ __forceinline__ double wrap_pi(double d) {
+  if (fabs(d) <= kPiD) return d;
+  if (!(fabs(d) <= 1048576.0)) {
+    double s, c;
+    sincos(d, &s, &c);
+    return atan2(s, c);
+  }
+  auto rem = [d](double k) {
+    double r = fma(-k, 0x1.921fb54000000p+2, d);
+    r = fma(-k, 0x1.10b4611000000p-28, r);
+    return fma(-k, 0x1.4c4c6628b80dcp-57, r);
+  };
+  const double k = rint(d * 0.15915494309189535);  // 1 / (2 pi)
+  double r = rem(k);
+  if (r > kPiD) r = rem(k + 1);
+  else if (r < -kPiD) r = rem(k - 1);
+  return r;
+}
+
 // proprioception of the current state, readProprio (core.js:129-175), f64;
 // writes 6A+6 values into X.obs and returns the attached-arm bitmask.  The
 // grip load divides by the arm's break force in f64, cdp[a].y (the JS
@@ -175,14 +203,12 @@ __device__ unsigned proprio(const BatchArgs &A, const TplDev &td, const TplSmem 
   const float4 *grip_st = reinterpret_cast<const float4 *>(S.anc);
   const double cx = S.px[0], cy = S.py[0], cvx = S.vx[0], cvy = S.vy[0];
   const double angle = S.ang[0], cav = S.av[0];
-  // armCurl terms: atan2(sin d, cos d) per adjacent segment pair
+  // armCurl terms: atan2(sin d, cos d) per adjacent segment pair, as wrap_pi
   const int npair = arms * (segs - 1);
   for (int q = lane; q < npair; q += G) {
     const int a = q / (segs - 1), i = q % (segs - 1) + 1;
     const double d = (double)S.ang[P.arm_segs[a * segs + i]] - (double)S.ang[P.arm_segs[a * segs + i - 1]];
-    double sd, cd;
-    sincos(d, &sd, &cd);
-    X.pair[q] = atan2(sd, cd);
+    X.pair[q] = wrap_pi(d);
   }
   L.sync();
   double ext = 0.0, curl = 0.0, sh = 0.0, tx = 0.0, ty = 0.0;
@@ -194,9 +220,8 @@ __device__ unsigned proprio(const BatchArgs &A, const TplDev &td, const TplSmem 
     curl = segs > 1 ? s / (segs - 1) : 0.0;
     const int s0 = P.arm_seg0[a], tip = P.arm_tip[a];
     const double d = (double)S.ang[s0] - angle;
-    double sd, cd, st, ct;
-    sincos(d, &sd, &cd);
-    sh = atan2(sd, cd);
+    double st, ct;
+    sh = wrap_pi(d);
     sincos((double)S.ang[tip], &st, &ct);
     tx = (double)S.px[tip] + kSegHalf * ct;
     ty = (double)S.py[tip] + kSegHalf * st;
@@ -1993,6 +2018,11 @@ __global__ void sincos_probe_kernel(const float *x, int n, float *s, float *c) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) kr::sincos_r(x[i], s + i, c + i);
 }
+
+__global__ void wrap_probe_kernel(const double *d, int n, double *out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) out[i] = wrap_pi(d[i]);
+}
 }  // namespace
 
 extern "C" int kr_probe_sincos(const float *x, int32_t n, float *s, float *c) {
@@ -2008,6 +2038,22 @@ extern "C" int kr_probe_sincos(const float *x, int32_t n, float *s, float *c) {
   if (e == cudaSuccess) e = cudaMemcpy(s, d + n, (size_t)n * sizeof(float), cudaMemcpyDeviceToHost);
   if (e == cudaSuccess) e = cudaMemcpy(c, d + 2 * (size_t)n, (size_t)n * sizeof(float), cudaMemcpyDeviceToHost);
   cudaFree(d);
+  if (e != cudaSuccess) { g_batch_error = cudaGetErrorString(e); return KR_ERR_CUDA; }
+  return KR_OK;
+}
+
+extern "C" int kr_probe_wrap(const double *d, int32_t n, double *out) {
+  if (!d || !out || n < 0) { g_batch_error = "kr_probe_wrap: bad arguments"; return KR_ERR_INVALID; }
+  if (n == 0) return KR_OK;
+  double *buf = nullptr;
+  cudaError_t e = cudaMalloc(&buf, (size_t)n * 2 * sizeof(double));
+  if (e == cudaSuccess) e = cudaMemcpy(buf, d, (size_t)n * sizeof(double), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) {
+    wrap_probe_kernel<<<(n + 255) / 256, 256>>>(buf, n, buf + n);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaMemcpy(out, buf + n, (size_t)n * sizeof(double), cudaMemcpyDeviceToHost);
+  cudaFree(buf);
   if (e != cudaSuccess) { g_batch_error = cudaGetErrorString(e); return KR_ERR_CUDA; }
   return KR_OK;
 }

@@ -284,3 +284,29 @@ def test_device_sincos_is_the_rounded_f64_value():
     assert diff <= 3, diff
     assert np.all(np.abs(s.view(np.int32).astype(np.int64) - want_s.view(np.int32)) <= 1)
     assert np.all(np.abs(c.view(np.int32).astype(np.int64) - want_c.view(np.int32)) <= 1)
+
+
+def test_device_wrap_is_atan2_of_sin_and_cos():
+    """readProprio's Math.atan2(Math.sin(d), Math.cos(d)), which the device
+    evaluates as d wrapped into (-pi, pi], against numpy's f64 chain: 3 M
+    differences of f32 angles up to 1e5 rad apart, values next to odd
+    multiples of pi and arguments beyond 2^20 (where the device evaluates
+    the chain itself).  Within 4 f64 ulp, and the same f32 after the
+    proprioception's scalings (/ 0.42 pi for the curl, / 0.62 pi for the
+    shoulder); NaN for non-finite input."""
+    rng = np.random.default_rng(11)
+    parts = []
+    for r in (1.0, 4.0, 60.0, 1e3, 1e5):
+        a = rng.uniform(-r, r, 600_000).astype(np.float32)
+        b = rng.uniform(-r, r, 600_000).astype(np.float32)
+        parts.append(a.astype(np.float64) - b.astype(np.float64))
+    odd = (2 * np.arange(-2000, 2001) + 1) * np.pi
+    parts.append((odd[:, None] + np.linspace(-1e-9, 1e-9, 11)[None, :] * (np.abs(odd[:, None]) + 1)).ravel())
+    parts.append(rng.uniform(2.0 ** 20, 2.0 ** 30, 1000) * rng.choice([-1.0, 1.0], 1000))
+    d = np.concatenate(parts)
+    got = batch.probe_wrap(d)
+    want = np.arctan2(np.sin(d), np.cos(d))
+    assert np.all(np.abs(got - want) <= 4 * np.spacing(np.abs(want)))
+    for scale in (0.42 * np.pi, 0.62 * np.pi):
+        assert np.array_equal((got / scale).astype(np.float32), (want / scale).astype(np.float32))
+    assert np.all(np.isnan(batch.probe_wrap(np.array([np.nan, np.inf, -np.inf]))))
