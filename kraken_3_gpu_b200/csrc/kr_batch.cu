@@ -163,6 +163,22 @@ __device__ inline double mulberry_next(uint32_t &s) {
 
 __device__ inline double clamp_sym(double v, double m) { return v > m ? m : (v < -m ? -m : v); }
 
+// One out-of-line copy of each f64 libm function that the reflex, postStep's
+// accumulators, the proprioception, the net and the senses call (the same
+// functions, with the same results): their call sites are many, and inlined
+// at every one they made the NET kernel's per-step code larger than the
+// instruction caches hold -- fetch stalls were its largest stall reason.
+__device__ __noinline__ double2 lib_sincos(double x) {
+  double s, c;
+  sincos(x, &s, &c);
+  return make_double2(s, c);
+}
+__device__ __noinline__ double lib_sin(double x) { return sin(x); }
+__device__ __noinline__ double lib_cos(double x) { return cos(x); }
+__device__ __noinline__ double lib_hypot(double x, double y) { return hypot(x, y); }
+__device__ __noinline__ double lib_tanh(double x) { return tanh(x); }
+__device__ __noinline__ double lib_atan2(double y, double x) { return atan2(y, x); }
+
 // Math.atan2(Math.sin(d), Math.cos(d)) (kraken.js:173 armCurl, core.js:138
 // the shoulder angle) for the f64 difference d of two angles, as the exact
 // value that chain of f64 calls approximates to within a few ulp: d wrapped
@@ -175,9 +191,8 @@ __device__ inline double clamp_sym(double v, double m) { return v > m ? m : (v <
 __device__ __forceinline__ double wrap_pi(double d) {
   if (fabs(d) <= kPiD) return d;
   if (!(fabs(d) <= 1048576.0)) {
-    double s, c;
-    sincos(d, &s, &c);
-    return atan2(s, c);
+    const double2 sc = lib_sincos(d);
+    return lib_atan2(sc.x, sc.y);
   }
   auto rem = [d](double k) {
     double r = fma(-k, 0x1.921fb54000000p+2, d);
@@ -220,20 +235,19 @@ __device__ unsigned proprio(const BatchArgs &A, const TplDev &td, const TplSmem 
     curl = segs > 1 ? s / (segs - 1) : 0.0;
     const int s0 = P.arm_seg0[a], tip = P.arm_tip[a];
     const double d = (double)S.ang[s0] - angle;
-    double st, ct;
     sh = wrap_pi(d);
-    sincos((double)S.ang[tip], &st, &ct);
-    tx = (double)S.px[tip] + kSegHalf * ct;
-    ty = (double)S.py[tip] + kSegHalf * st;
-    ext = fmin(1.0, hypot(tx - (double)S.px[s0], ty - (double)S.py[s0]) / fmax(1.0, td.reach));
+    const double2 t = lib_sincos((double)S.ang[tip]);
+    tx = (double)S.px[tip] + kSegHalf * t.y;
+    ty = (double)S.py[tip] + kSegHalf * t.x;
+    ext = fmin(1.0, lib_hypot(tx - (double)S.px[s0], ty - (double)S.py[s0]) / fmax(1.0, td.reach));
     attached = grip_st[a].w == 0.f;
   }
   const unsigned att = L.ballot(attached) & ((1u << arms) - 1u);
   // sums in arm order, like the sequential loop
   double ext_sum = 0.0;
   for (int a = 0; a < arms; a++) ext_sum += __shfl_sync(L.mask, ext, a, G);
-  double ca, sa;
-  sincos(-angle, &sa, &ca);
+  const double2 na = lib_sincos(-angle);
+  const double sa = na.x, ca = na.y;
   const double SL = kPiD * 0.62, JL = kPiD * 0.42;
   if (lane < arms) {
     const int a = lane;
@@ -244,7 +258,7 @@ __device__ unsigned proprio(const BatchArgs &A, const TplDev &td, const TplSmem 
     X.obs[2 * arms + 2 * a + 1] = (float)clamp_sym((dx * sa + dy * ca) / td.reach, 1.2);
     const float4 g = grip_st[a];
     double force = 0.0;
-    if (g.w == 0.f) force = hypot((double)S.lamX[P.arm_grip[a]], (double)S.lamY[P.arm_grip[a]]) * A.inv_h64;
+    if (g.w == 0.f) force = lib_hypot((double)S.lamX[P.arm_grip[a]], (double)S.lamY[P.arm_grip[a]]) * A.inv_h64;
     X.obs[4 * arms + a] = g.w != 0.f ? 0.f : (float)fmin(1.0, force / fmax(1.0, cdp[a].y));
     X.obs[5 * arms + a] = g.w != 0.f ? 0.f : 1.f;
   }
@@ -256,7 +270,7 @@ __device__ unsigned proprio(const BatchArgs &A, const TplDev &td, const TplSmem 
     m.prev_vy = cvy;
     X.obs[6 * arms + 2] = (float)((double)__popc(att) / arms);
     X.obs[6 * arms + 3] = (float)(ext_sum / arms);
-    X.obs[6 * arms + 4] = (float)fmin(1.0, hypot(cvx, cvy) / 300);
+    X.obs[6 * arms + 4] = (float)fmin(1.0, lib_hypot(cvx, cvy) / 300);
     X.obs[6 * arms + 5] = (float)fmax(-1.0, fmin(1.0, cav / 18));
   }
   L.sync();
@@ -324,7 +338,7 @@ __device__ void policy(const BatchArgs &A, const TplDev &td, CreatureSmem &X, in
 }
 
 // net.js's activation: tanh, clamped to +-1 beyond +-20, stored in a Float32Array
-__device__ __forceinline__ float net_act(double s) { return (float)(s > 20 ? 1.0 : (s < -20 ? -1.0 : tanh(s))); }
+__device__ __forceinline__ float net_act(double s) { return (float)(s > 20 ? 1.0 : (s < -20 ? -1.0 : lib_tanh(s))); }
 
 // What the KR_CTRL_NET steps read of BatchArgs, passed by value so that the
 // non-inlined calls take no address of the kernel's arguments or state.
@@ -468,18 +482,18 @@ __device__ __noinline__ void net_senses(NetArgs N, int arms, const int *arm_tip,
     const int l = lane;
     const double mw = N.map_size[2 * map], mh = N.map_size[2 * map + 1];
     const double a = time * lp[6 * l + 5] + lp[6 * l + 4];
-    R.light_xy[2 * l] = fmax(60.0, fmin(mw - 60, R.light_xy[2 * l] + cos(a) * 18 * dt));
-    R.light_xy[2 * l + 1] = fmax(60.0, fmin(mh - 60, R.light_xy[2 * l + 1] + sin(a * 0.8) * 18 * dt));
+    R.light_xy[2 * l] = fmax(60.0, fmin(mw - 60, R.light_xy[2 * l] + lib_cos(a) * 18 * dt));
+    R.light_xy[2 * l + 1] = fmax(60.0, fmin(mh - 60, R.light_xy[2 * l + 1] + lib_sin(a * 0.8) * 18 * dt));
   }
   L.sync();
   {
-    double sp, cp;
-    sincos(heading + kPiD / 2, &sp, &cp);  // light.js: receptors 26 px across the heading
+    const double2 hp = lib_sincos(heading + kPiD / 2);  // light.js: receptors 26 px across the heading
+    const double sp = hp.x, cp = hp.y;
     for (int q = lane; q < 3 * nl; q += G) {
       const int s = q / nl, l = q % nl;
       const double qx = s == 0 ? x + cp * 26 : (s == 1 ? x - cp * 26 : x);
       const double qy = s == 0 ? y + sp * 26 : (s == 1 ? y - sp * 26 : y);
-      const double d = hypot(qx - R.light_xy[2 * l], qy - R.light_xy[2 * l + 1]);
+      const double d = lib_hypot(qx - R.light_xy[2 * l], qy - R.light_xy[2 * l + 1]);
       R.lc[q] = fmax(0.0, 1 - d / lp[6 * l + 2]) * lp[6 * l + 3];
     }
   }
@@ -515,9 +529,8 @@ __device__ __noinline__ void net_senses(NetArgs N, int arms, const int *arm_tip,
     for (int i = lane; i < KR_NET_RAYS; i += G) {
       const double t = (double)i / (KR_NET_RAYS - 1);
       const double a = heading + (t - 0.5) * (kPiD * 0.85);
-      double sa, ca;
-      sincos(a, &sa, &ca);
-      R.ray_d[i] = echo_march(rects, nR, x, y, ca, sa, kEchoRange);
+      const double2 ra = lib_sincos(a);
+      R.ray_d[i] = echo_march(rects, nR, x, y, ra.y, ra.x, kEchoRange);
     }
     L.sync();
     if (lane == 0) {
@@ -543,9 +556,8 @@ __device__ __noinline__ void net_senses(NetArgs N, int arms, const int *arm_tip,
   // tip contact: near = max(0, 1 - d / 9) of the map's SDF at the tip point
   for (int a = lane; a < arms; a += G) {
     const int tip = arm_tip[a];
-    double st, ct;
-    sincos((double)ang[tip], &st, &ct);
-    const double tx = (double)px[tip] + kSegHalf * ct, ty = (double)py[tip] + kSegHalf * st;
+    const double2 t = lib_sincos((double)ang[tip]);
+    const double tx = (double)px[tip] + kSegHalf * t.y, ty = (double)py[tip] + kSegHalf * t.x;
     // near is 0 unless a rect lies within 9 px: a rect whose box is 10 px
     // away or more cannot make it positive, so the SDF runs only when some
     // box is closer (the result is the same either way)
@@ -638,11 +650,11 @@ __device__ void run_creature(const BatchArgs &A, const TplDev &td, int nlv, cons
       if (c > 0) c -= A.dt;
       if (an[3] != 0.f) {
         if (adh > 0.08 && c <= 0) {
-          const double slip = hypot((double)S.vx[tip], (double)S.vy[tip]);
+          const double slip = lib_hypot((double)S.vx[tip], (double)S.vy[tip]);
           if (slip < A.slip_max) {
             const double ta = (double)S.ang[tip];
-            an[0] = (float)((double)S.px[tip] + kSegHalf * cos(ta));
-            an[1] = (float)((double)S.py[tip] + kSegHalf * sin(ta));
+            an[0] = (float)((double)S.px[tip] + kSegHalf * lib_cos(ta));
+            an[1] = (float)((double)S.py[tip] + kSegHalf * lib_sin(ta));
             const double brk = 40.0 + 860.0 * adh;
             cdp[a].y = brk;
             an[2] = (float)brk;
@@ -671,19 +683,19 @@ __device__ void run_creature(const BatchArgs &A, const TplDev &td, int nlv, cons
       SlotMeta &g = A.meta[slot];
       const double x = S.px[0], y = S.py[0], angle = S.ang[0], av = S.av[0];
       const double dx = x - g.last_x, dy = y - g.last_y;
-      const double step_dist = hypot(dx, dy);
+      const double step_dist = lib_hypot(dx, dy);
       g.path_len += step_dist;
       g.angular_accum += fabs(av) * A.h64 * A.substeps;
       const double fa = angle - kPiD * 0.5;
-      double sf, cf;
-      sincos(fa, &sf, &cf);
+      const double2 fsc = lib_sincos(fa);
+      const double sf = fsc.x, cf = fsc.y;
       const double fwd = dx * cf + dy * sf;
       if (fwd > 0) g.forward_prog += fwd;
       int anchored = 0;
       unsigned now = 0;
       for (int a = 0; a < arms; a++)
         if (S.anc[4 * a + 3] == 0.f) { anchored++; now |= 1u << a; }
-      const double d_spawn = hypot(x - g.spawn_x, y - g.spawn_y);
+      const double d_spawn = lib_hypot(x - g.spawn_x, y - g.spawn_y);
       if (anchored > 0) {
         g.anchored_steps++;
         if (d_spawn > g.spawn_dist_max) { g.grip_pull_prog += d_spawn - g.spawn_dist_max; g.spawn_dist_max = d_spawn; }

@@ -116,13 +116,21 @@ __device__ const double2 kSinCosTab[64] = {
     {-0.0980171403295606, 0.9951847266721969}
 };
 
+// sin / cos beyond 2^20 and of non-finite arguments: CUDA's f64 sincos
+// rounded to f32, out of line -- a cold path kept out of the instruction
+// stream of the solve loops.
+static __device__ __noinline__ float2 sincos_far(double x) {
+  double sd, cd;
+  sincos(x, &sd, &cd);
+  return make_float2(static_cast<float>(sd), static_cast<float>(cd));
+}
+
 __device__ __forceinline__ void sincos_r(float a, float *s, float *c) {
   const double x = static_cast<double>(a);
   if (!(fabs(x) <= 1048576.0)) {
-    double sd, cd;
-    sincos(x, &sd, &cd);
-    *s = static_cast<float>(sd);
-    *c = static_cast<float>(cd);
+    const float2 f = sincos_far(x);
+    *s = f.x;
+    *c = f.y;
     return;
   }
   // x = k pi/32 + r, |r| <= pi/64: pi/32 in three parts (29, 29 and 53
