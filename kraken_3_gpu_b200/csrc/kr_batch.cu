@@ -456,6 +456,17 @@ __device__ __noinline__ float net_control(NetArgs N, int arms, int segs, const f
   return (float)(1.0 / (2000.0 + tone * (400000.0 - 2000.0)));  // toneToCompliance
 }
 
+// The echo's ray march and the contact's SDF out of line: one copy each of
+// the f64 rect loop (instruction-cache footprint of the per-step path).
+__device__ __noinline__ double net_echo_ray(const double *rects, int n, double x, double y, double cx, double cy) {
+  return echo_march(rects, n, x, y, cx, cy, kEchoRange);
+}
+__device__ __noinline__ double2 net_sdf(const double *rects, int n, double px, double py) {
+  double d = 0.0;
+  const bool ok = sdf64(rects, n, px, py, &d);
+  return make_double2(ok ? 1.0 : 0.0, d);
+}
+
 // KR_CTRL_NET, after postStep: sim.time += dt, tickMapLights (map.js:75-83)
 // on the creature's copy of its map's lights, then tickSenses (core.js:
 // 245-267) without entities: the echo's tick (echo.js:120-127) and, when
@@ -530,7 +541,7 @@ __device__ __noinline__ void net_senses(NetArgs N, int arms, const int *arm_tip,
       const double t = (double)i / (KR_NET_RAYS - 1);
       const double a = heading + (t - 0.5) * (kPiD * 0.85);
       const double2 ra = lib_sincos(a);
-      R.ray_d[i] = echo_march(rects, nR, x, y, ra.y, ra.x, kEchoRange);
+      R.ray_d[i] = net_echo_ray(rects, nR, x, y, ra.y, ra.x);
     }
     L.sync();
     if (lane == 0) {
@@ -568,8 +579,8 @@ __device__ __noinline__ void net_senses(NetArgs N, int arms, const int *arm_tip,
                        (tx <= r[0] - 10 || tx >= r[0] + r[2] + 10 || ty <= r[1] - 10 || ty >= r[1] + r[3] + 10);
       close = !far;  // NaN coordinates or extents count as close: the SDF then decides
     }
-    double d;
-    const double near = close && sdf64(rects, nR, tx, ty, &d) ? fmax(0.0, 1 - d / 9) : 0.0;
+    const double2 sd = close ? net_sdf(rects, nR, tx, ty) : make_double2(0.0, 0.0);
+    const double near = sd.x != 0.0 ? fmax(0.0, 1 - sd.y / 9) : 0.0;
     R.contact[a] = R.contact[a] * 0.7 + near * 0.3;
   }
   L.sync();

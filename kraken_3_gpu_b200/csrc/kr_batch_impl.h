@@ -86,7 +86,7 @@ __host__ __device__ inline int policy_device_index(int arms, int segs, int p) {
 // this same code (IEEE f64 add, multiply and sqrt; min / max as std::min /
 // std::max).
 __host__ __device__ inline bool sdf64(const double *rects, int n, double px, double py, double *out) {
-  double best = INFINITY;
+  double best = INFINITY, thr = INFINITY;  // thr = best * best, the JS's per-rect product
   const double *r = rects;
   for (int i = 0; i < n; i++, r += 4) {
     const double xr = r[0] + r[2], yb = r[1] + r[3];
@@ -94,11 +94,17 @@ __host__ __device__ inline bool sdf64(const double *rects, int n, double px, dou
     const double cx = r[0] < mx ? mx : r[0], cy = r[1] < my ? my : r[1];
     const double dx = px - cx, dy = py - cy, d2 = dx * dx + dy * dy;
     if (d2 > 1e-12) {
-      if (d2 < best * best) best = sqrt(d2);
+      if (d2 < thr) {
+        best = sqrt(d2);
+        thr = best * best;
+      }
     } else {
       const double a = px - r[0], b = xr - px, e = py - r[1], f = yb - py;
       const double ab = b < a ? b : a, ef = f < e ? f : e, m = ef < ab ? ef : ab;
-      if (-m < best) best = -m;
+      if (-m < best) {
+        best = -m;
+        thr = best * best;
+      }
     }
   }
   if (!(best < INFINITY && best > -INFINITY)) return false;
