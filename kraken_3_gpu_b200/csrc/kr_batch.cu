@@ -63,6 +63,8 @@ struct BatchArgs {
   const double *lights;  // x y r ir ph sp per light
   const int *light_off;  // n_maps + 1, or null: no lights
   const double *map_size;
+  const double2 *light_tab;  // per light, its position after env step t < light_T (or null)
+  int light_T;
 };
 
 // --- shared-memory layout, carved per template ------------------------------
@@ -353,12 +355,42 @@ struct NetArgs {
   const double *lights;
   const int *light_off;
   const double *map_size;
+  const double2 *light_tab;
+  int light_T;
   double dt;
 };
 
 __device__ __forceinline__ NetArgs net_args(const BatchArgs &A) {
   return NetArgs{A.net, A.meta, A.pw, A.pw_idx, A.pw_stride, A.rects64, A.map_off, A.lights, A.light_off,
-                 A.map_size, A.dt};
+                 A.map_size, A.light_tab, A.light_T, A.dt};
+}
+
+// tickMapLights (map.js:75-83) for one light (x y r ir ph sp at lp) at sim
+// time `time`: its position after the tick
+__device__ __forceinline__ double2 light_tick(double2 p, const double *lp, double time, double mw, double mh,
+                                              double dt) {
+  const double a = time * lp[5] + lp[4];
+  return make_double2(fmax(60.0, fmin(mw - 60, p.x + lib_cos(a) * 18 * dt)),
+                      fmax(60.0, fmin(mh - 60, p.y + lib_sin(a * 0.8) * 18 * dt)));
+}
+
+// The light-position table (light_table_steps): block = map, thread = light;
+// the sim clock summed step by step from 0 as each creature's record sums it.
+__global__ void light_table_kernel(const double *lights, const int *light_off, const double *map_size, double dt,
+                                   int T, double2 *tab) {
+  const int map = blockIdx.x, lo = light_off[map], nl = light_off[map + 1] - lo;
+  const double mw = map_size[2 * map], mh = map_size[2 * map + 1];
+  for (int l = threadIdx.x; l < nl; l += blockDim.x) {
+    const double *lp = lights + 6 * (size_t)(lo + l);
+    double2 p = make_double2(lp[0], lp[1]);
+    double time = 0.0;
+    double2 *out = tab + (size_t)(lo + l) * T;
+    for (int t = 0; t < T; t++) {
+      time = time + dt;
+      p = light_tick(p, lp, time, mw, mh, dt);
+      out[t] = p;
+    }
+  }
 }
 
 // KR_CTRL_NET, before the step: the trainer's input vector (train.js:236-241:
@@ -473,10 +505,12 @@ __device__ __noinline__ double2 net_sdf(const double *rects, int n, double px, d
 // the net asked for it and the cooldown allows, an emission (echo.js:67-85:
 // 12 rays over the fan, lanes strided, arrivals inserted in arrival order
 // after equal times, as the stable sort after the push orders them); the
-// light sense (light.js:90-97) and the tip contact per arm.
+// light sense (light.js:90-97) and the tip contact per arm.  t: the env
+// step this is the end of (the slot's step counter, from 0 at its spawn):
+// below light_T the lights' positions come from the engine's table.
 template <int G>
 __device__ __noinline__ void net_senses(NetArgs N, int arms, const int *arm_tip, const float *px, const float *py,
-                                        const float *ang, int map, int slot, kr::Lanes<G> L) {
+                                        const float *ang, int map, int slot, int t, kr::Lanes<G> L) {
   NetRec &R = N.net[slot];
   const int lane = L.lane;
   const int ro = N.map_off[map], nR = N.map_off[map + 1] - ro;
@@ -491,10 +525,15 @@ __device__ __noinline__ void net_senses(NetArgs N, int arms, const int *arm_tip,
   // contribution on its own lane; lane 0 sums them in light order below
   if (lane < nl) {
     const int l = lane;
-    const double mw = N.map_size[2 * map], mh = N.map_size[2 * map + 1];
-    const double a = time * lp[6 * l + 5] + lp[6 * l + 4];
-    R.light_xy[2 * l] = fmax(60.0, fmin(mw - 60, R.light_xy[2 * l] + lib_cos(a) * 18 * dt));
-    R.light_xy[2 * l + 1] = fmax(60.0, fmin(mh - 60, R.light_xy[2 * l + 1] + lib_sin(a * 0.8) * 18 * dt));
+    double2 p;
+    if (t < N.light_T) {
+      p = N.light_tab[(size_t)(lo + l) * N.light_T + t];
+    } else {
+      p = light_tick(make_double2(R.light_xy[2 * l], R.light_xy[2 * l + 1]), lp + 6 * l, time,
+                     N.map_size[2 * map], N.map_size[2 * map + 1], dt);
+    }
+    R.light_xy[2 * l] = p.x;
+    R.light_xy[2 * l + 1] = p.y;
   }
   L.sync();
   {
@@ -723,7 +762,7 @@ __device__ void run_creature(const BatchArgs &A, const TplDev &td, int nlv, cons
       g.last_x = x; g.last_y = y;
     }
     if constexpr (NET) {
-      if (m.ctrl == KR_CTRL_NET) net_senses<G>(net_args(A), arms, P.arm_tip, S.px, S.py, S.ang, m.map, slot, L);
+      if (m.ctrl == KR_CTRL_NET) net_senses<G>(net_args(A), arms, P.arm_tip, S.px, S.py, S.ang, m.map, slot, t, L);
     }
     m.step = t + 1;
   }
@@ -1228,6 +1267,7 @@ int launch_part(kr_batch *b, Part &p, int max_steps, bool timed) {
   A.pw = b->d_pw; A.pw_idx = b->d_pw_idx; A.pw_stride = b->pw_stride;
   A.net = b->d_net; A.rects64 = b->d_rects64; A.lights = b->d_lights; A.light_off = b->d_light_off;
   A.map_size = b->d_map_size;
+  A.light_tab = b->d_light_tab; A.light_T = b->light_T;
   cudaError_t e;
   if ((e = cudaMemsetAsync(p.d_queue, 0, sizeof(int), st)) != cudaSuccess) return b->cuda_fail(e, "queue reset");
   if (timed) cudaEventRecord(p.ev0, st);
@@ -1442,6 +1482,15 @@ extern "C" int kr_batch_create(const kr_batch_desc *desc, kr_batch **out) {
       if ((e = upload_vec(&b->d_lights, lv)) != cudaSuccess) return bail(e, "upload(lights)");
       if ((e = upload_vec(&b->d_light_off, lo)) != cudaSuccess) return bail(e, "upload(light offsets)");
       if ((e = upload_vec(&b->d_map_size, ms)) != cudaSuccess) return bail(e, "upload(map sizes)");
+      b->light_T = light_table_steps(nl);
+      if (b->light_T > 0) {
+        if ((e = cudaMalloc(&b->d_light_tab, (size_t)nl * b->light_T * sizeof(double2))) != cudaSuccess)
+          return bail(e, "cudaMalloc(light table)");
+        light_table_kernel<<<d.n_maps, 32>>>(b->d_lights, b->d_light_off, b->d_map_size,
+                                             d.solver.h * d.solver.substeps, b->light_T, b->d_light_tab);
+        if ((e = cudaGetLastError()) == cudaSuccess) e = cudaDeviceSynchronize();
+        if (e != cudaSuccess) return bail(e, "light table");
+      }
     }
   }
   b->h_meta.assign(C, SlotMeta{});
@@ -1948,7 +1997,7 @@ extern "C" void kr_batch_destroy(kr_batch *b) {
                   b->d_state, b->d_grip, b->d_glam, b->d_cd, b->d_ctrl, b->d_meta, b->d_obs,
                   b->d_pw, b->d_pw_idx, b->s_state, b->s_grip, b->s_glam, b->s_cd,
                   b->s_ctrl, b->s_meta, b->s_groups, b->d_net, b->s_net, b->d_lights, b->d_light_off,
-                  b->d_map_size};
+                  b->d_map_size, b->d_light_tab};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   if (b->own_stream && b->stream) cudaStreamDestroy(b->stream);

@@ -144,6 +144,17 @@ __host__ __device__ inline double echo_march(const double *rects, int n, double 
   return maxd;
 }
 
+// Env steps of the light-position table of an engine with n_lights map
+// lights: a map's lights move by the sim's clock alone (tickMapLights), so
+// every creature of a map sees the same positions after its step t, and the
+// engine tabulates them once (16 bytes per light and step, at most 64 MB,
+// at most 4,096 steps; later steps move the lights per creature as before).
+inline int light_table_steps(long n_lights) {
+  if (n_lights <= 0) return 0;
+  const long cap = (64L << 20) / (16L * n_lights);
+  return (int)(cap < 4096 ? cap : 4096);
+}
+
 // net.js weightCount for an arms-armed body: n_in = 10 arms + 45 inputs,
 // KR_NET_HIDDEN twice, 3 arms + 2 outputs
 __host__ __device__ inline int net_inputs(int arms) { return 10 * arms + 45; }
@@ -266,6 +277,8 @@ struct kr_batch {
   double *d_lights = nullptr;
   int *d_light_off = nullptr;
   double *d_map_size = nullptr;
+  double2 *d_light_tab = nullptr;      // per light, its position after env step t < light_T
+  int light_T = 0;
   krb::NetRec *d_net = nullptr, *s_net = nullptr;
   std::vector<int> h_pw_arms;          // arms of each net individual (-1: unused)
   // slots

@@ -153,7 +153,10 @@ uint64_t fixed_bytes(const kr_server_desc &d) {
   uint64_t b = kFixedBytes;
   if (d.n_maps > 0 && d.map_rect_off) b += (uint64_t)d.map_rect_off[d.n_maps] * 16 + (uint64_t)d.n_maps * 8;
   if (d.policy || d.net) b += 2ull * kMaxThetaPerRound * weight_stride(d) * 4;
-  if (d.net && d.lights && d.map_light_off) b += (uint64_t)d.map_light_off[d.n_maps] * 48 + (uint64_t)d.n_maps * 20;
+  if (d.net && d.lights && d.map_light_off) {
+    const long nl = d.map_light_off[d.n_maps];
+    b += (uint64_t)nl * 48 + (uint64_t)d.n_maps * 20 + (uint64_t)nl * light_table_steps(nl) * 16;
+  }
   return b;
 }
 

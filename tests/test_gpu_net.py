@@ -182,3 +182,60 @@ def test_net_restore_and_autotune_keep_the_sense_state():
     eng.close()
     assert np.array_equal(first[0][0], second[0][0]) and np.array_equal(first[0][1], second[0][1])
     assert np.array_equal(first[1], second[1])
+
+
+def _host_light_sense(lights, steps, dt, x, y, ang0, mw=1440.0, mh=810.0):
+    """light.js sampleAt for the three receptors after `steps` ticks of the
+    map's lights (map.js tickMapLights), in numpy f64 from the map's initial
+    positions; (x, y, ang0) the creature's mantle."""
+    L = np.asarray(lights, np.float64).reshape(-1, 6)
+    px, py = L[:, 0].copy(), L[:, 1].copy()
+    time = 0.0
+    for _ in range(steps):
+        time = time + dt
+        a = time * L[:, 5] + L[:, 4]
+        px = np.maximum(60.0, np.minimum(mw - 60, px + np.cos(a) * 18 * dt))
+        py = np.maximum(60.0, np.minimum(mh - 60, py + np.sin(a * 0.8) * 18 * dt))
+    heading = float(ang0) - np.pi * 0.5
+    sp, cp = np.sin(heading + np.pi / 2), np.cos(heading + np.pi / 2)
+    pts = [(x + cp * 26, y + sp * 26), (x - cp * 26, y - sp * 26), (x, y)]
+    out = []
+    for qx, qy in pts:
+        v = 0.05
+        for k in range(len(L)):
+            d = np.hypot(qx - px[k], qy - py[k])
+            v += max(0.0, 1 - d / L[k, 2]) * L[k, 3]
+        out.append(min(1.0, v))
+    return np.asarray(out, np.float32)
+
+
+@pytest.mark.parametrize("steps", [100, 4200])
+def test_light_sense_from_the_table_and_past_it(steps):
+    """The lights' positions come from the engine's per-map table for the
+    first 4,096 env steps (every creature of a map sees the same lights after
+    its step t) and are ticked per creature after it.  The light inputs of
+    the last step, built from the senses at the end of the step before,
+    against the lights ticked on the host for as many steps and the
+    creature's pose then: within 1e-6 (libm cos / sin / hypot may differ in
+    the last f64 bit), before and after the end of the table."""
+    w = workloads.uneven(n=4, n_maps=2, seed=31, h_min=steps, h_max=steps, arms=(5, 5), segs=(5, 5))
+    G = _genomes(w, 6)
+    eng = batch.BatchEngine(w.maps, w.n, control="net", lights=w.lights)
+    workloads.spawn_all(eng, w)
+    width = max(len(g) for g in G)
+    padded = np.zeros((len(G), width), np.float32)
+    for k, g in enumerate(G):
+        padded[k, :len(g)] = g
+    eng.set_net(padded, np.arange(w.n, dtype=np.int32))
+    eng.run(steps - 1)
+    st = eng.read_state()
+    eng.run(1)
+    x, _ = eng.read_net()
+    eng.close()
+    dt = (1 / 120) * 2
+    for i in range(w.n):
+        A = int(w.arms[i])
+        at = 6 * A + 6 + 2 * batch.NET_RAYS + 6  # proprioception, echo, chemoreception, then light
+        want = _host_light_sense(w.lights[w.map_id[i]], steps - 1, dt, float(st["px"][i, 0]),
+                                 float(st["py"][i, 0]), st["ang"][i, 0])
+        assert np.allclose(x[i, at:at + 3], want, atol=1e-6, rtol=0), (i, x[i, at:at + 3], want)
