@@ -54,5 +54,10 @@ def test_plan_counts_net_genomes_and_records():
     assert with_net - without > 4 * stride + 4
     assert with_net - without - (4 * stride + 4) < 4096  # the record: sense state and the net's vectors
     lights = [[[100.0, 100.0, 250.0, 0.7, 0.0, 0.1]]] * len(maps)
+    cap_n, _ = serve.plan(maps, 1 << 30, net=True)
     cap_l, per_l = serve.plan(maps, 1 << 30, net=True, lights=lights)
     assert per_l == with_net
+    # the lights and their position table (16 B per light and step, 4,096
+    # steps here) are fixed bytes, taken from the budget before the slots
+    table = len(maps) * 4096 * 16
+    assert cap_n - cap_l >= 2 * (table // (2 * with_net))
