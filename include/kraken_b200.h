@@ -123,6 +123,10 @@ int kr_world_islands(const kr_world *w, int32_t *n_islands, int32_t *max_levels)
  *   bodies   n_bodies x 12 f32 (in/out)     cons   n_constraints x 20 words (in/out)
  *   forces   n_bodies x 4 f32 (in/out)      rects  n_rects x 4 f32 (x y w h)
  *   coll_pts n_coll_pts x 4 words and coll_range 2 x n_bodies u32, as for kr_create.
+ * Alignment: bodies, forces, cons and coll_pts must start on a 16-byte
+ * boundary (the kernel moves them as 16-byte vectors), rects and coll_range
+ * on a 4-byte one; a misaligned pointer is rejected with KR_ERR_INVALID
+ * before the device is touched.
  * The per-creature schedule is rebuilt on the device at every call into one
  * file-scope device array of fixed size (about 270 KB; every GPU that loads
  * the library holds it until the process exits), so the call allocates
@@ -134,11 +138,14 @@ int kr_world_islands(const kr_world *w, int32_t *n_islands, int32_t *max_levels)
  * builder and rejected with the same code before any step runs.  Other codes: KR_ERR_INVALID
  * (null pointer, implausible parameter, inconsistent coll_range),
  * KR_ERR_INDEX (a constraint's body index out of range), KR_ERR_CUDA.  No
- * message is recorded (recording one would allocate).
+ * message is recorded (recording one would allocate).  A rejected world
+ * leaves the caller's buffers untouched.
  * The first call on a device looks up the device address of the scratch
- * array; make that first call before any stream capture.  The call waits for
- * the schedule builder on `stream` (cudaStream_t as void*, NULL = the legacy
- * default stream), then enqueues the steps asynchronously.  Every call on a
+ * array; make that first call before any stream capture.  Every call then
+ * waits on the host for the schedule builder's verdict -- a 4-byte copy from
+ * the device into static host memory followed by a synchronize of `stream`
+ * (cudaStream_t as void*, NULL = the legacy default stream) -- and only then
+ * enqueues the steps asynchronously.  Every call on a
  * device shares the one scratch array: calls that overlap on the GPU (other
  * host threads, other streams) race and must not be issued. */
 #define KR_NOALLOC_MAX_BODIES 2048

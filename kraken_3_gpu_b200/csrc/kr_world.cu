@@ -20,6 +20,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdint>
 #include <cstdio>
 #include <cstring>
 #include <numeric>
@@ -749,13 +750,16 @@ __global__ void noalloc_schedule_kernel(int *W, const float *bodies, const uint3
   int *level = W + kOffLevel, *cur = W + kOffCur;
   W[kOffHdr + 0] = 0;
   W[kOffHdr + 2] = KR_OK;
-  // collRange must tile the points in body order (gpuworld.js:193-199)
-  uint32_t acc = 0;
+  // collRange must tile the points in body order (gpuworld.js:193-199).  The
+  // running sum is 64-bit and may never pass nP, so no count can wrap it and
+  // every range lies inside [0, nP): the point loops below stay in bounds.
+  uint64_t acc = 0;
   for (int g = 0; g < nB; g++) {
-    if (coll_range[g] != acc) { W[kOffHdr + 2] = KR_ERR_INVALID; return; }
+    if ((uint64_t)coll_range[g] != acc) { W[kOffHdr + 2] = KR_ERR_INVALID; return; }
     acc += coll_range[nB + g];
+    if (acc > (uint64_t)nP) { W[kOffHdr + 2] = KR_ERR_INVALID; return; }
   }
-  if (acc != (uint32_t)nP) { W[kOffHdr + 2] = KR_ERR_INVALID; return; }
+  if (acc != (uint64_t)nP) { W[kOffHdr + 2] = KR_ERR_INVALID; return; }
   for (int g = 0; g < nB; g++) { parent[g] = g; root_isl[g] = -1; }
   for (int k = 0; k < nC; k++) {
     const uint32_t a = cons[20 * (size_t)k], b = cons[20 * (size_t)k + 1];
@@ -842,8 +846,12 @@ __global__ void noalloc_schedule_kernel(int *W, const float *bodies, const uint3
     rec[I_LVL_OFF] = lvl_off;
     rec[I_NLV] = nlv;
     lvl_off += nlv + 1;
-    // collision points in local body order
+    // collision points in local body order; the island's count is checked
+    // against the kernel's capacity before any of its points is written
     rec[I_PT_OFF] = pt_off;
+    uint64_t np_isl = 0;
+    for (int j = 0; j < nb; j++) np_isl += coll_range[nB + ib[bo + j]];
+    if (np_isl > (uint64_t)KR_MAX_ISLAND_COLLPTS) { W[kOffHdr + 2] = KR_ERR_CAPACITY; return; }
     int np = 0;
     for (int j = 0; j < nb; j++) {
       const int g = ib[bo + j];
@@ -852,7 +860,6 @@ __global__ void noalloc_schedule_kernel(int *W, const float *bodies, const uint3
       for (uint32_t q = 0; q < cn; q++) ipts[pt_off + np + (int)q] = (int)(off + q);
       np += (int)cn;
     }
-    if (np > KR_MAX_ISLAND_COLLPTS) { W[kOffHdr + 2] = KR_ERR_CAPACITY; return; }
     rec[I_NP] = np;
     pt_off += np;
   }
@@ -892,6 +899,14 @@ extern "C" int kr_step_noalloc(const kr_solver_params *params, uint32_t n_bodies
                                const uint32_t *coll_range, int32_t n_steps, void *stream) {
   if (!params || !bodies || !forces || !rects || !coll_range || (n_constraints && !cons) ||
       (n_coll_pts && !coll_pts) || n_steps < 0)
+    return KR_ERR_INVALID;
+  // The kernels move bodies, forces, constraints and collision points as
+  // 16-byte vectors and read rects and collRange as 4-byte words; a caller's
+  // pool may hand out any address, so misaligned buffers are refused here,
+  // before the device is touched.
+  auto misaligned = [](const void *q, uintptr_t a) { return (reinterpret_cast<uintptr_t>(q) & (a - 1)) != 0; };
+  if (misaligned(bodies, 16) || misaligned(forces, 16) || (cons && misaligned(cons, 16)) ||
+      (coll_pts && misaligned(coll_pts, 16)) || misaligned(rects, 4) || misaligned(coll_range, 4))
     return KR_ERR_INVALID;
   const kr_solver_params &p = *params;
   const float hf = static_cast<float>(p.h);

@@ -131,3 +131,27 @@ def test_create_rejects_implausible_params_without_device():
     with pytest.raises(_native.KrError) as e:
         gpuworld.create(w, empty)
     assert "nRects" in str(e.value)
+
+
+def test_no_alloc_step_rejects_misaligned_buffers_without_device():
+    # kr_step_noalloc moves bodies, forces, constraints and collision points
+    # as 16-byte vectors and reads rects / collRange as words: a pointer off
+    # that alignment (a caller's pool may hand one out) is refused with
+    # KR_ERR_INVALID before any CUDA call.  The addresses are never
+    # dereferenced: the argument checks come first.
+    L = _native.lib()
+    L.kr_step_noalloc.restype = ctypes.c_int
+    L.kr_step_noalloc.argtypes = [ctypes.POINTER(_native.SolverParams), ctypes.c_uint32, ctypes.c_uint32,
+                                  ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                  ctypes.c_uint32, ctypes.c_void_p, ctypes.c_uint32, ctypes.c_void_p,
+                                  ctypes.c_int32, ctypes.c_void_p]
+    params = _native.SolverParams(1 / 120, 2, 4, 3.0, 3.0, 360.0, 18.0)
+    base = 1 << 20
+    ok = dict(bodies=base, cons=base + 4096, forces=base + 8192, rects=base + 12288,
+              coll=base + 16384, rng=base + 20480)
+    for name, off in (("bodies", 4), ("cons", 8), ("forces", 4), ("coll", 12), ("rects", 2), ("rng", 1)):
+        a = dict(ok)
+        a[name] += off
+        rc = L.kr_step_noalloc(ctypes.byref(params), 43, 90, a["bodies"], a["cons"], a["forces"], a["rects"],
+                               24, a["coll"], 92, a["rng"], 1, None)
+        assert rc == _native.KR_ERR_INVALID, f"{name} + {off}: status {rc}"
