@@ -35,7 +35,6 @@ import statistics
 import subprocess
 import sys
 import tempfile
-import threading
 import time
 
 import numpy as np
@@ -140,45 +139,40 @@ class ClockSampler:
 # ---------------------------------------------------------------------------
 # CPU oracle (the reported baseline and the reference arm)
 # ---------------------------------------------------------------------------
-def cpu_oracle_rate(w, seconds: float, threads: int, f32: bool = False, opcount: bool = False):
-    """FP64 oracle (the restated xpbd.js) on a sample of the workload: each
-    thread owns independent one-creature sims and steps them round robin
-    for `seconds`; ctypes releases the GIL, so threads run in parallel."""
-    from kraken_3_gpu_b200.workloads import TONE, ControlStream
+def host_threads() -> int:
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+def cpu_rollouts(w, every: int, offset: int, threads: int, limit_s: float):
+    """The FP64 oracle (the restated xpbd.js) on the host cores with no
+    Python in the loop (oracle/xpbd_bench.c): the creatures i = offset (mod
+    every) of the workload, each in its own one-creature world on its map,
+    driven by its own control stream (the same mulberry32 draws the device
+    makes), applyControl with the reflex, the step and postStep, to its
+    horizon or until limit_s; POSIX threads over contiguous ranges of about
+    equal work.  Returns (creature-steps / s, creature-steps, seconds, creatures)."""
     from oracle import binding as ob
+    sel = np.arange(offset % every, w.n, every)
+    steps, el = ob.bench_rollouts(w.maps, w.map_id[sel], w.arms[sel], w.segs[sel], w.x[sel], w.y[sel],
+                                  w.angle[sel], w.seed[sel], w.horizon[sel], threads, limit_s=limit_s)
+    return steps / el, steps, el, len(sel)
 
-    def make(i):
-        sim = ob.Sim(rects=w.maps[w.map_id[i]], opcount=opcount)
-        sim.add_creature(w.x[i], w.y[i], w.angle[i], int(w.arms[i]), int(w.segs[i]))
-        if f32:
-            sim.world.f32ify()
-            sim.world.round_state()
-        return [sim, ControlStream(int(w.arms[i]), int(w.segs[i]), seed=int(w.seed[i])), 0]
 
-    per_thread = 8
-    counts = [0] * threads
-    stop = time.perf_counter() + seconds
-
-    def work(t):
-        sims = [make((t * per_thread + k) % w.n) for k in range(per_thread)]
-        n = 0
-        while time.perf_counter() < stop:
-            for s in sims:
-                tg, ad = s[1].at(s[2])
-                s[0].apply_control_motors(0, TONE, tg, ad)
-                (s[0].step32 if f32 else s[0].step)()
-                s[2] += 1
-                n += 1
-        counts[t] = n
-
-    t0 = time.perf_counter()
-    ths = [threading.Thread(target=work, args=(t,)) for t in range(threads)]
-    for th in ths:
-        th.start()
-    for th in ths:
-        th.join()
-    el = time.perf_counter() - t0
-    return sum(counts) / el, sum(counts), el
+def cpu_baseline_line(w, threads: int, seconds: float):
+    """cpu_baseline of the bench line: every 32nd creature of the workload on
+    all host threads (bounded by `seconds`), and the single-thread rate on
+    every 512th for the per-core scaling."""
+    v1, n1, e1, c1 = cpu_rollouts(w, 512, 0, 1, max(2.0, seconds / 3))
+    vt, nt, et, ct = cpu_rollouts(w, 32, 0, threads, seconds)
+    return {"value": vt, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"{nt} creature-steps in {et:.1f} s: {ct} creatures (every 32nd) of the same workload "
+                      "at their own horizons, each in its own world, controls + reflex + FP64 step + postStep "
+                      "(C restatement of src/physics/xpbd.js and core.js, POSIX threads, no Python in the loop)",
+            "single_thread": {"value": v1, "creature_steps": n1, "seconds": round(e1, 3), "creatures": c1},
+            "scaling_vs_single_thread": vt / (threads * v1)}
 
 
 def ops_per_creature_step(w, sample: int = 48, steps: int = 60) -> float:
@@ -217,36 +211,52 @@ def dist_env():
     return replicas.dist_env()
 
 
+def bench_config(args, w, world: int) -> dict:
+    """The workload description both arms print (the same dict, so the two
+    lines describe one configuration)."""
+    return {"workload": f"uneven-{w.n}: {w.n:,} creatures, {len(w.maps)} maps, 4-8 arms x 5-9 segments, "
+                        f"horizons {args.hmin}-{args.hmax}",
+            "creatures": w.n, "maps": len(w.maps), "creature_steps_per_rollout": w.creature_steps(),
+            "seed": args.seed, "substeps": 2, "iterations": 4,
+            "controls": "per-creature mulberry32 streams, redraw every 6 steps, reflex on",
+            "parallelism": f"replicas x{world}",
+            "l2": "GPU arm: flushed between timed rollouts (256 MB write), state restored from a device "
+                  "snapshot inside the timed region"}
+
+
 def reference_arm(args):
+    """The reference's algorithm on the host cores: the FP64 oracle (the
+    reference is browser JavaScript; no JS runtime here) driven as the GPU
+    arm drives its creatures, on the same workload realisation.  One bench
+    step = one bounded sample of it: the creatures i = step (mod 32) at their
+    own horizons, on every host thread, at most 20 s."""
     rank, world, _ = dist_env()
     if rank != 0:
         return
-    from kraken_3_gpu_b200 import workloads
-    w = workloads.uneven(n=min(args.n, 4096), n_maps=args.maps, seed=args.seed,
+    from kraken_3_gpu_b200 import replicas, workloads
+    w = workloads.uneven(n=args.n, n_maps=args.maps, seed=replicas.shard_seed(args.seed, 0),
                          h_min=args.hmin, h_max=args.hmax)
-    threads = os.cpu_count() or 1
-    per = max(2.0, min(20.0, 60.0 / max(1, args.steps + args.warmup)))
-    for _ in range(args.warmup):
-        cpu_oracle_rate(w, per / 4, threads)
-    vals, total, el = [], 0, 0.0
-    for _ in range(args.steps):
-        v, n, e = cpu_oracle_rate(w, per, threads)
-        vals.append(v)
+    threads = host_threads()
+    for k in range(args.warmup):
+        cpu_rollouts(w, 32, 31 - k, threads, 2.0)
+    total, el, ms = 0, 0.0, []
+    for k in range(args.steps):
+        _, n, e, _ = cpu_rollouts(w, 32, k, threads, 20.0)
         total += n
         el += e
+        ms.append(e * 1000)
     value = total / el
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT,
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": per * 1000, "higher_is_better": True, "scaling": "weak",
+        "ms_per_step": float(np.mean(ms)), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": "uneven-16k", "creatures": args.n, "maps": args.maps,
-                   "bodies": "4-8 arms x 5-9 segs", "horizons": f"{args.hmin}-{args.hmax}",
-                   "substeps": 2, "iterations": 4, "parallelism": "host threads"},
+        "config": bench_config(args, w, world),
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
-                         "sample": f"{threads} threads x 8 one-creature worlds of the workload, "
-                                   f"{per:.1f} s per step (FP64 restatement of src/physics/xpbd.js; "
-                                   "the reference is browser JavaScript, no JS runtime on the box)"},
+                         "sample": f"per step the creatures i = step (mod 32) of the workload ({w.n // 32:,}) at "
+                                   "their own horizons, at most 20 s; FP64 restatement of src/physics/xpbd.js with "
+                                   "core.js's applyControl and postStep in C on POSIX threads (the reference is "
+                                   "browser JavaScript, no JS runtime on the box)"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -590,11 +600,7 @@ def main():
                     "ops_per_creature_step": ops, "kernel_ms": kms,
                     "peak_note": "measured dependent-free f32 FMA issue rate (lane-ops/s) of this GPU; "
                                  "MEASURED_PEAKS.json has no f32 figure"}
-            threads = os.cpu_count() or 1
-            cv, cn, ce = cpu_oracle_rate(w, args.cpu_seconds, threads)
-            cpu = {"value": cv, "unit": UNIT, "cores": threads, "kind": "port",
-                   "sample": f"{cn} creature-steps in {ce:.1f} s: {threads} threads x 8 one-creature "
-                             "worlds of the workload, FP64 restatement of src/physics/xpbd.js"}
+            cpu = cpu_baseline_line(w, host_threads(), args.cpu_seconds)
 
     if rank == 0:
         line = {
@@ -603,18 +609,10 @@ def main():
             "rollout_ms": [round(x, 3) for x in rollout_ms],
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32", "data": "synthetic",
-            "config": {"workload": "uneven-16k: 16,384 creatures, 64 maps, 4-8 arms x 5-9 segments, "
-                                   f"horizons {args.hmin}-{args.hmax}",
-                       "creatures": w.n, "maps": args.maps, "creature_steps_per_rollout": units,
-                       "substeps": 2, "iterations": 4,
-                       "controls": "device mulberry32 streams, redraw every 6 steps",
-                       "form": "persistent kernel, one launch per rollout, state resident in HBM",
-                       "launch_shape": {"lanes_per_creature": best[0], "warps_per_cta": best[1],
-                                        "ctas_per_sm": best[2]},
-                       "autotune_ms": {",".join(map(str, k)): round(v, 3) for k, v in tune.items()},
-                       "parallelism": f"replicas x{world}",
-                       "l2": "flushed between timed rollouts (256 MB write); state restored from a device "
-                             "snapshot inside the timed region"},
+            "config": bench_config(args, w, world),
+            "form": "persistent kernel, one launch per rollout, state resident in HBM",
+            "launch": {"lanes_per_creature": best[0], "warps_per_cta": best[1], "ctas_per_sm": best[2],
+                       "autotune_ms": {",".join(map(str, k)): round(v, 3) for k, v in tune.items()}},
             "roofline": roof, "cpu_baseline": cpu, "clocks": clocks, "e2e": e2e,
             "gpu_launches": gpu_launches, **extra,
         }

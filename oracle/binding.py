@@ -118,6 +118,8 @@ def lib(opcount: bool = False) -> C.CDLL:
         "or_sim_set_spawn_reach": (None, [vp, i, d]),
         "or_sim_pre_step": (None, [vp]), "or_sim_post_step": (None, [vp]),
         "or_sim_metrics": (None, [vp, i, C.POINTER(Metrics)]),
+        "or_bench_rollouts": (i, [i, dp, ip, ip, ip, ip, dp, dp, dp, u32p, ip, d, i, i, i, d, d, d, i, d,
+                                  C.POINTER(C.c_longlong), dp, dp]),
         "or_score": (d, [C.POINTER(Metrics)]),
         "or_net_new": (vp, [vp, dp, i]),
         "or_net_free": (None, [vp]),
@@ -541,3 +543,33 @@ class NetSim:
         e, p = C.c_int(), C.c_int()
         self.L.or_net_echo(self.ptr, ci, C.byref(e), C.byref(p))
         return e.value, p.value
+
+
+def bench_rollouts(maps, map_id, arms, segs, x, y, angle, seed, horizon, threads, limit_s=0.0,
+                   tone=0.5, period=6, substeps=2, iterations=4, h=1 / 120, width=1440.0, height=810.0,
+                   metrics=False):
+    """The timed CPU baseline (xpbd_bench.c): every creature in its own
+    one-creature world, driven per env step by its mulberry32 control stream,
+    applyControl, preStep, the FP64 step and postStep, on `threads` POSIX
+    threads over contiguous creature ranges, with no Python in the loop.
+    Returns (creature-steps done, seconds) and, with metrics, each creature's
+    final mantle x, y and path length (n, 3)."""
+    L = lib()
+    rects = np.ascontiguousarray(np.concatenate([np.asarray(m, np.float64).reshape(-1, 4) for m in maps]))
+    off = np.zeros(len(maps) + 1, np.int32)
+    off[1:] = np.cumsum([len(np.asarray(m).reshape(-1, 4)) for m in maps])
+    ii = [np.ascontiguousarray(a, dtype=np.int32) for a in (map_id, arms, segs, horizon)]
+    dd = [np.ascontiguousarray(a, dtype=np.float64) for a in (x, y, angle)]
+    sd = np.ascontiguousarray(seed, dtype=np.uint32)
+    n = len(sd)
+    out = np.zeros((n, 3)) if metrics else None
+    steps, el = C.c_longlong(), C.c_double()
+    ipp = C.POINTER(C.c_int)
+    rc = L.or_bench_rollouts(n, _dp(rects), off.ctypes.data_as(ipp), ii[0].ctypes.data_as(ipp),
+                             ii[1].ctypes.data_as(ipp), ii[2].ctypes.data_as(ipp), _dp(dd[0]), _dp(dd[1]),
+                             _dp(dd[2]), sd.ctypes.data_as(C.POINTER(C.c_uint32)), ii[3].ctypes.data_as(ipp),
+                             tone, period, substeps, iterations, h, width, height, threads, limit_s,
+                             C.byref(steps), C.byref(el), _dp(out) if metrics else None)
+    if rc != 0:
+        raise RuntimeError(f"or_bench_rollouts: status {rc}")
+    return (steps.value, el.value, out) if metrics else (steps.value, el.value)

@@ -161,6 +161,21 @@ int or_net_step(or_net_sim *n, const float *genomes, int n_params, const int *in
 void or_net_io(const or_net_sim *n, int ci, float *x, float *out);
 void or_net_echo(const or_net_sim *n, int ci, int *emits, int *pending);
 double or_score(const or_metrics *m);
+
+/* The timed CPU baseline (xpbd_bench.c): creatures [0, n), each in its own
+ * one-creature world on map map_id[c] (rects of all maps x y w h, map_off
+ * n_maps + 1), driven per env step by its mulberry32 control stream (redrawn
+ * every `period` steps), applyControl, preStep, step (FP64) and postStep, to
+ * its horizon or until limit_s seconds (0: none) have passed; `threads`
+ * POSIX threads over contiguous ranges of about equal work.  Returns 0 and
+ * the creature-steps done and the seconds from the start of the first
+ * thread to the end of the last; out (n x 3, may be NULL) receives each
+ * creature's final mantle x, y and path length. */
+int or_bench_rollouts(int n, const double *rects, const int *map_off, const int *map_id, const int *arms,
+                      const int *segs, const double *x, const double *y, const double *angle,
+                      const uint32_t *seed, const int *horizon, double tone, int period, int substeps,
+                      int iterations, double h, double width, double height, int threads, double limit_s,
+                      long long *steps_done, double *elapsed_s, double *out);
 void or_sim_metrics(const or_sim *s, int ci, or_metrics *out);
 
 #ifdef __cplusplus
