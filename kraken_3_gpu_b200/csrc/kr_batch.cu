@@ -155,9 +155,12 @@ __device__ inline void carve_creature(kr::Island &S, CreatureSmem &X, const TplS
   S.nb = td.nb; S.nc = td.nc; S.np = td.np;
 }
 
-__device__ inline double mulberry_next(uint32_t &s) {
-  s += 0x6D2B79F5u;
-  uint32_t t = s;
+// mulberry32 (src/world/map.js:11-20): the draw is a hash of the state, and
+// the state only advances by a constant, so the d-th draw after state s
+// (d = 1, 2, ...) is mulberry_at(s + d * kMulberryStep): lanes draw their
+// share of a redraw at once.
+constexpr uint32_t kMulberryStep = 0x6D2B79F5u;
+__device__ inline double mulberry_at(uint32_t t) {
   t = (t ^ (t >> 15)) * (t | 1u);
   t ^= t + (t ^ (t >> 7)) * (t | 61u);
   return (double)(t ^ (t >> 14)) / 4294967296.0;
@@ -673,13 +676,17 @@ __device__ void run_creature(const BatchArgs &A, const TplDev &td, int nlv, cons
     }
     // 2. controls
     if (m.ctrl == KR_CTRL_STREAM) {
-      if (t % A.ctrl_period == 0 && lane == 0) {
-        uint32_t r = m.rng;
-        for (int a = 0; a < arms; a++) {
-          for (int j = 0; j < td.segs; j++) X.ctrl[a * td.segs + j] = (float)(mulberry_next(r) * 2 - 1);
-          X.ctrl[AS + a] = (float)mulberry_next(r);
+      if (t % A.ctrl_period == 0) {
+        // the redraw's arms x (segs + 1) draws, in the stream's order (per
+        // arm its motors, then its adhesion), split over the lanes
+        const int per = td.segs + 1, nd = arms * per;
+        for (int d = lane; d < nd; d += G) {
+          const double r = mulberry_at(m.rng + (uint32_t)(d + 1) * kMulberryStep);
+          const int a = d / per, j = d - a * per;
+          if (j < td.segs) X.ctrl[a * td.segs + j] = (float)(r * 2 - 1);
+          else X.ctrl[AS + a] = (float)r;
         }
-        m.rng = r;
+        m.rng += (uint32_t)nd * kMulberryStep;
       }
     } else if (m.ctrl == KR_CTRL_POLICY) {
       policy<G>(A, td, X, slot, L);
@@ -729,37 +736,47 @@ __device__ void run_creature(const BatchArgs &A, const TplDev &td, int nlv, cons
     //    reference's hybrid loop runs it on the mirrored state)
     //    The accumulators are read and written through the slot's HBM
     //    record by lane 0 (they do not live in every lane's registers).
-    if (lane == 0) {
-      SlotMeta &g = A.meta[slot];
-      const double x = S.px[0], y = S.py[0], angle = S.ang[0], av = S.av[0];
-      const double dx = x - g.last_x, dy = y - g.last_y;
-      const double step_dist = lib_hypot(dx, dy);
-      g.path_len += step_dist;
-      g.angular_accum += fabs(av) * A.h64 * A.substeps;
-      const double fa = angle - kPiD * 0.5;
-      const double2 fsc = lib_sincos(fa);
-      const double sf = fsc.x, cf = fsc.y;
-      const double fwd = dx * cf + dy * sf;
-      if (fwd > 0) g.forward_prog += fwd;
-      int anchored = 0;
-      unsigned now = 0;
-      for (int a = 0; a < arms; a++)
-        if (S.anc[4 * a + 3] == 0.f) { anchored++; now |= 1u << a; }
-      const double d_spawn = lib_hypot(x - g.spawn_x, y - g.spawn_y);
-      if (anchored > 0) {
-        g.anchored_steps++;
-        if (d_spawn > g.spawn_dist_max) { g.grip_pull_prog += d_spawn - g.spawn_dist_max; g.spawn_dist_max = d_spawn; }
+    //    The two distances (the step's and the spawn point's) come from one
+    //    call on two lanes, beside lane 0's sincos of the heading.
+    {
+      const SlotMeta &gr = A.meta[slot];
+      const double x = S.px[0], y = S.py[0];
+      const double hx = lane == 1 ? x - gr.spawn_x : x - gr.last_x;
+      const double hy = lane == 1 ? y - gr.spawn_y : y - gr.last_y;
+      const double hv = lib_hypot(hx, hy);
+      const double d_spawn_l = __shfl_sync(L.mask, hv, L.base + 1);
+      if (lane == 0) {
+        SlotMeta &g = A.meta[slot];
+        const double angle = S.ang[0], av = S.av[0];
+        const double dx = hx, dy = hy;
+        const double step_dist = hv;
+        g.path_len += step_dist;
+        g.angular_accum += fabs(av) * A.h64 * A.substeps;
+        const double fa = angle - kPiD * 0.5;
+        const double2 fsc = lib_sincos(fa);
+        const double sf = fsc.x, cf = fsc.y;
+        const double fwd = dx * cf + dy * sf;
+        if (fwd > 0) g.forward_prog += fwd;
+        int anchored = 0;
+        unsigned now = 0;
+        for (int a = 0; a < arms; a++)
+          if (S.anc[4 * a + 3] == 0.f) { anchored++; now |= 1u << a; }
+        const double d_spawn = d_spawn_l;
+        if (anchored > 0) {
+          g.anchored_steps++;
+          if (d_spawn > g.spawn_dist_max) { g.grip_pull_prog += d_spawn - g.spawn_dist_max; g.spawn_dist_max = d_spawn; }
+        }
+        if (anchored == 0 && step_dist > 0.3) g.free_move += step_dist;
+        g.energy += (g.tone_d * 0.0006 + step_dist * 0.0004) * arms;
+        const unsigned was = g.arm_anchored;
+        if (anchored > 0 && !(was & 0x100u)) g.grip_cycles++;
+        const int newly = __popc(now & ~was & 0xffu);
+        g.attach_events += newly;
+        if (newly > 0 && anchored - newly > 0) g.strides += newly;
+        g.arm_anchored = now | (anchored > 0 ? 0x100u : 0u);
+        g.max_disp = fmax(g.max_disp, d_spawn);
+        g.last_x = x; g.last_y = y;
       }
-      if (anchored == 0 && step_dist > 0.3) g.free_move += step_dist;
-      g.energy += (g.tone_d * 0.0006 + step_dist * 0.0004) * arms;
-      const unsigned was = g.arm_anchored;
-      if (anchored > 0 && !(was & 0x100u)) g.grip_cycles++;
-      const int newly = __popc(now & ~was & 0xffu);
-      g.attach_events += newly;
-      if (newly > 0 && anchored - newly > 0) g.strides += newly;
-      g.arm_anchored = now | (anchored > 0 ? 0x100u : 0u);
-      g.max_disp = fmax(g.max_disp, d_spawn);
-      g.last_x = x; g.last_y = y;
     }
     if constexpr (NET) {
       if (m.ctrl == KR_CTRL_NET) net_senses<G>(net_args(A), arms, P.arm_tip, S.px, S.py, S.ang, m.map, slot, t, L);
