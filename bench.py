@@ -219,7 +219,7 @@ def bench_config(args, w, world: int) -> dict:
             "creatures": w.n, "maps": len(w.maps), "creature_steps_per_rollout": w.creature_steps(),
             "seed": args.seed, "substeps": 2, "iterations": 4,
             "controls": "per-creature mulberry32 streams, redraw every 6 steps, reflex on",
-            "parallelism": f"replicas x{world}",
+            "parallelism": f"contiguous creature ranges of one workload x{world}" if world > 1 else "1 GPU",
             "l2": "GPU arm: flushed between timed rollouts (256 MB write), state restored from a device "
                   "snapshot inside the timed region"}
 
@@ -234,7 +234,7 @@ def reference_arm(args):
     if rank != 0:
         return
     from kraken_3_gpu_b200 import replicas, workloads
-    w = workloads.uneven(n=args.n, n_maps=args.maps, seed=replicas.shard_seed(args.seed, 0),
+    w = workloads.uneven(n=args.n, n_maps=args.maps, seed=args.seed,
                          h_min=args.hmin, h_max=args.hmax)
     threads = host_threads()
     for k in range(args.warmup):
@@ -453,8 +453,11 @@ def main():
     def all_max(x: float) -> float:
         return replicas.max_over_ranks(x, world)
 
-    w = workloads.uneven(n=args.n, n_maps=args.maps, seed=replicas.shard_seed(args.seed, rank),
-                         h_min=args.hmin, h_max=args.hmax)
+    # one workload of world x n creatures, contiguous ranges of n per rank
+    # (rank 0's range is the one-GPU workload)
+    w_all = workloads.uneven(n=args.n * world, n_maps=args.maps, seed=args.seed, h_min=args.hmin, h_max=args.hmax)
+    w, (lo, hi) = replicas.shard(w_all, rank, world)
+    del w_all
     if args.net_only:
         line = net_controller(torch.cuda.current_stream(), w)
         line.update({"metric": "creature-steps/s under the reference net controller", "n_gpus": 1,
@@ -520,6 +523,14 @@ def main():
     gpu_launches = args.steps
 
     extra = {}
+    # the edge of the partition: every rank's per-creature scores gathered in
+    # workload order (one all-gather, outside the timed region)
+    scores = eng.read_metrics()[:, 0]
+    counts = [replicas.contiguous_range(args.n * world, r, world)[1] - replicas.contiguous_range(args.n * world, r, world)[0]
+              for r in range(world)]
+    gathered = replicas.gather_fitness(scores, counts, world, device="cuda")
+    extra["partition"] = {"creatures": [lo, hi], "ranks": world, "gathered_scores": int(gathered.size),
+                          "gathered_score_sum": float(np.sum(gathered))}
     # plain form: the same kernel, one launch per env step
     if not args.no_plain:
         eng.restore()

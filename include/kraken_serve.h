@@ -87,6 +87,13 @@ typedef struct kr_request {
   float sigma;
   uint64_t seed;                /* eps (policy) or control streams (no theta) */
   double arrival;               /* server time the request arrives (< 0: now) */
+  /* Index of this request's first individual in a population split over
+   * several servers (one per GPU): individual i here is individual
+   * first_individual + i of the whole population -- its mirrored pair
+   * (first_individual + i) / 2, its sign, and without theta its control
+   * stream -- so the split population's results equal the whole one's.
+   * Even, >= 0; 0 for a whole population. */
+  int32_t first_individual;
 } kr_request;
 
 /* results per individual: the metrics record of kraken_batch.h

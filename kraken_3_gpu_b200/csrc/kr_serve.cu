@@ -305,7 +305,7 @@ int admit(kr_server *S, int p) {
     std::vector<uint32_t> seeds = q.seeds;
     if (seeds.empty()) {
       seeds.resize(pop);
-      for (int i = 0; i < pop; i++) seeds[i] = (uint32_t)splitmix64(q.r.seed + (uint64_t)i);
+      for (int i = 0; i < pop; i++) seeds[i] = (uint32_t)splitmix64(q.r.seed + (uint64_t)(q.r.first_individual + i));
     }
     const std::vector<float> tones(pop, q.r.tone);
     SpawnInit init;
@@ -324,8 +324,9 @@ int admit(kr_server *S, int p) {
       st.h_slots[n_new] = s;
       if (pol) {
         PJob &j = st.h_jobs[n_new];
-        j.slot = s; j.theta_off = theta_off; j.arms = q.r.arms; j.segs = q.r.segs; j.pair = i / 2;
-        j.sign = (i & 1) ? -1.f : 1.f; j.sigma = q.r.sigma; j.seed = q.r.seed;
+        const int gi = q.r.first_individual + i;  // the individual's index in the whole population
+        j.slot = s; j.theta_off = theta_off; j.arms = q.r.arms; j.segs = q.r.segs; j.pair = gi / 2;
+        j.sign = (gi & 1) ? -1.f : 1.f; j.sigma = q.r.sigma; j.seed = q.r.seed;
       } else {
         st.h_jobs[n_new] = PJob{s, 0, 0, 0, 0, 1.f, 0.f, 0};
       }
@@ -540,6 +541,8 @@ extern "C" int kr_server_submit(kr_server *S, const kr_request *r, int64_t *id) 
     return S->fail(KR_ERR_CAPACITY, "population " + std::to_string(r->population) + " outside 1.." +
                                         std::to_string(S->part_cap) + " (half the slots)");
   if (r->horizon < 1) return S->fail(KR_ERR_INVALID, "horizon < 1");
+  if (r->first_individual < 0 || (r->first_individual & 1))
+    return S->fail(KR_ERR_INVALID, "first_individual must be even and >= 0");
   if (r->arms < 1 || r->arms > KR_BATCH_MAX_ARMS || r->segs < 1 || r->segs > KR_BATCH_MAX_SEGS)
     return S->fail(KR_ERR_INVALID, "body shape outside 1..8 arms x 1..9 segments");
   if (r->map_id < 0 || r->map_id >= S->d.n_maps) return S->fail(KR_ERR_INDEX, "unknown map");

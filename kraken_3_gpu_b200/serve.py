@@ -47,7 +47,8 @@ class Request(C.Structure):
                 ("angle", C.c_double), ("xs", _F64P), ("ys", _F64P), ("angles", _F64P),
                 ("control_seeds", C.POINTER(C.c_uint32)),
                 ("tone", C.c_float), ("theta", _F32P), ("n_params", C.c_int32),
-                ("sigma", C.c_float), ("seed", C.c_uint64), ("arrival", C.c_double)]
+                ("sigma", C.c_float), ("seed", C.c_uint64), ("arrival", C.c_double),
+                ("first_individual", C.c_int32)]
 
 
 class _RequestRaw(C.Structure):
@@ -189,10 +190,13 @@ class Server:
 
     def submit(self, population, horizon, arms, segs, map_id, x=0.0, y=0.0, angle=0.0, theta=None,
                sigma=0.0, seed=0, tone=0.5, arrival=-1.0, xs=None, ys=None, angles=None,
-               control_seeds=None) -> int:
+               control_seeds=None, first_individual=0) -> int:
         """Queue a request; x, y, angle is the common spawn pose, or xs, ys,
         angles one pose per individual; control_seeds (no theta) one control
-        stream seed per individual."""
+        stream seed per individual; first_individual (even): the index of
+        this request's first individual when a population is split over
+        several servers (its pairs' eps and streams are then the whole
+        population's)."""
         th = None if theta is None else np.ascontiguousarray(theta, dtype=np.float32).ravel()
         per = None
         if xs is not None:
@@ -205,7 +209,7 @@ class Server:
                     float(tone),
                     th.ctypes.data_as(_F32P) if th is not None else None,
                     0 if th is None else th.size, float(sigma), int(seed) & (2**64 - 1),
-                    float(arrival))
+                    float(arrival), int(first_individual))
         rid = C.c_int64()
         _check(_lib().kr_server_submit(self.h, C.byref(r), C.byref(rid)), self.h)
         return rid.value
