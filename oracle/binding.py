@@ -118,7 +118,7 @@ def lib(opcount: bool = False) -> C.CDLL:
         "or_sim_set_spawn_reach": (None, [vp, i, d]),
         "or_sim_pre_step": (None, [vp]), "or_sim_post_step": (None, [vp]),
         "or_sim_metrics": (None, [vp, i, C.POINTER(Metrics)]),
-        "or_bench_rollouts": (i, [i, dp, ip, ip, ip, ip, dp, dp, dp, u32p, ip, d, i, i, i, d, d, d, i, d,
+        "or_bench_rollouts": (i, [i, dp, ip, ip, ip, ip, dp, dp, dp, u32p, ip, d, i, i, i, d, d, d, i, d, i,
                                   C.POINTER(C.c_longlong), dp, dp]),
         "or_score": (d, [C.POINTER(Metrics)]),
         "or_net_new": (vp, [vp, dp, i]),
@@ -547,13 +547,14 @@ class NetSim:
 
 def bench_rollouts(maps, map_id, arms, segs, x, y, angle, seed, horizon, threads, limit_s=0.0,
                    tone=0.5, period=6, substeps=2, iterations=4, h=1 / 120, width=1440.0, height=810.0,
-                   metrics=False):
+                   metrics=False, f32=False):
     """The timed CPU baseline (xpbd_bench.c): every creature in its own
     one-creature world, driven per env step by its mulberry32 control stream,
     applyControl, preStep, the FP64 step and postStep, on `threads` POSIX
     threads over contiguous creature ranges, with no Python in the loop.
     Returns (creature-steps done, seconds) and, with metrics, each creature's
-    final mantle x, y and path length (n, 3)."""
+    final mantle x, y, path length and score (n, 4); f32: the f32 emulation's
+    step instead of the FP64 one (for checks)."""
     L = lib()
     rects = np.ascontiguousarray(np.concatenate([np.asarray(m, np.float64).reshape(-1, 4) for m in maps]))
     off = np.zeros(len(maps) + 1, np.int32)
@@ -562,14 +563,14 @@ def bench_rollouts(maps, map_id, arms, segs, x, y, angle, seed, horizon, threads
     dd = [np.ascontiguousarray(a, dtype=np.float64) for a in (x, y, angle)]
     sd = np.ascontiguousarray(seed, dtype=np.uint32)
     n = len(sd)
-    out = np.zeros((n, 3)) if metrics else None
+    out = np.zeros((n, 4)) if metrics else None
     steps, el = C.c_longlong(), C.c_double()
     ipp = C.POINTER(C.c_int)
     rc = L.or_bench_rollouts(n, _dp(rects), off.ctypes.data_as(ipp), ii[0].ctypes.data_as(ipp),
                              ii[1].ctypes.data_as(ipp), ii[2].ctypes.data_as(ipp), _dp(dd[0]), _dp(dd[1]),
                              _dp(dd[2]), sd.ctypes.data_as(C.POINTER(C.c_uint32)), ii[3].ctypes.data_as(ipp),
                              tone, period, substeps, iterations, h, width, height, threads, limit_s,
-                             C.byref(steps), C.byref(el), _dp(out) if metrics else None)
+                             1 if f32 else 0, C.byref(steps), C.byref(el), _dp(out) if metrics else None)
     if rc != 0:
         raise RuntimeError(f"or_bench_rollouts: status {rc}")
     return (steps.value, el.value, out) if metrics else (steps.value, el.value)

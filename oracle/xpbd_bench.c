@@ -10,7 +10,8 @@
  *       stream (src/world/map.js:11-20), per arm its motors then its
  *       adhesion, targets as r * 2 - 1 and adhesion as r;
  *     applyControl (core.js:183-220: targets clamped, the suction-cup reflex),
- *     preStep, world.step() (xpbd.js:487-490), postStep (core.js:297-356).
+ *     preStep, world.step() (xpbd.js:487-490; or, for checks, the f32
+ *     emulation's step of tools/f32solver.mjs), postStep (core.js:297-356).
  * Every creature lives in its own one-creature world on its map, as the
  * reference's creatures never interact.  All worlds are built before the
  * clock starts; creatures are then split into contiguous ranges of about
@@ -40,7 +41,8 @@ typedef struct {
   const uint32_t *seed;
   double tone, deadline;
   int period;
-  double *out;                    /* per creature: mantle x, y, path length, or NULL */
+  double *out;                    /* per creature: mantle x, y, path length, score, or NULL */
+  int f32;                        /* 1: the f32 emulation's step (f32solver.mjs) instead of FP64 */
   long long steps;
   double t_end;
 } bench_job;
@@ -63,7 +65,8 @@ static void *bench_thread(void *arg) {
       }
       or_apply_control_motors(s, 0, J->tone, tg, ad);
       or_sim_pre_step(s);
-      or_sim_step(s);
+      if (J->f32) or_sim_step32(s);
+      else or_sim_step(s);
       or_sim_post_step(s);
       done++;
       if (J->deadline > 0 && (done & 15) == 0 && now_s() > J->deadline) stop = 1;
@@ -71,9 +74,10 @@ static void *bench_thread(void *arg) {
     if (J->out) {
       or_metrics m;
       or_sim_metrics(s, 0, &m);
-      J->out[3 * c] = m.x;
-      J->out[3 * c + 1] = m.y;
-      J->out[3 * c + 2] = m.pathLen;
+      J->out[4 * c] = m.x;
+      J->out[4 * c + 1] = m.y;
+      J->out[4 * c + 2] = m.pathLen;
+      J->out[4 * c + 3] = m.score;
     }
   }
   J->t_end = now_s();
@@ -85,7 +89,7 @@ int or_bench_rollouts(int n, const double *rects, const int *map_off, const int 
                       const int *segs, const double *x, const double *y, const double *angle,
                       const uint32_t *seed, const int *horizon, double tone, int period, int substeps,
                       int iterations, double h, double width, double height, int threads, double limit_s,
-                      long long *steps_done, double *elapsed_s, double *out) {
+                      int f32, long long *steps_done, double *elapsed_s, double *out) {
   if (n < 1 || threads < 1 || period < 1 || !steps_done || !elapsed_s) return -1;
   for (int c = 0; c < n; c++)
     if (arms[c] < 1 || arms[c] > OR_MAX_ARMS || segs[c] < 1 || segs[c] > OR_MAX_SEGS || horizon[c] < 0) return -1;
@@ -100,7 +104,17 @@ int or_bench_rollouts(int n, const double *rects, const int *map_off, const int 
     const int m = map_id[c];
     sims[c] = or_sim_new(width, height, rects + 4 * (size_t)map_off[m], map_off[m + 1] - map_off[m],
                          substeps, iterations, h);
-    if (!sims[c] || or_sim_add_creature(sims[c], x[c], y[c], angle[c], arms[c], segs[c]) < 0) rc = -2;
+    if (!sims[c] || or_sim_add_creature(sims[c], x[c], y[c], angle[c], arms[c], segs[c]) < 0) {
+      rc = -2;
+      continue;
+    }
+    /* measureReach at the spawn point, as createSim records it for score() */
+    or_sim_set_spawn_reach(sims[c], 0, or_measure_reach(rects + 4 * (size_t)map_off[m], map_off[m + 1] - map_off[m],
+                                                        or_arm_reach(segs[c]), x[c], y[c]));
+    if (f32) {
+      or_f32ify(or_sim_world(sims[c]));
+      or_f32_round_state(or_sim_world(sims[c]));
+    }
   }
   double t0 = 0, t_end = 0;
   long long steps = 0;
@@ -122,7 +136,7 @@ int or_bench_rollouts(int n, const double *rects, const int *map_off, const int 
       J[k].end = c;
       J[k].sims = sims + J[k].begin;
       J[k].arms = arms; J[k].segs = segs; J[k].horizon = horizon; J[k].seed = seed;
-      J[k].tone = tone; J[k].period = period; J[k].out = out;
+      J[k].tone = tone; J[k].period = period; J[k].out = out; J[k].f32 = f32;
       J[k].deadline = limit_s > 0 ? t0 + limit_s : 0;
     }
     for (int k = 0; k < threads; k++) {

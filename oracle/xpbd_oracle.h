@@ -169,13 +169,14 @@ double or_score(const or_metrics *m);
  * its horizon or until limit_s seconds (0: none) have passed; `threads`
  * POSIX threads over contiguous ranges of about equal work.  Returns 0 and
  * the creature-steps done and the seconds from the start of the first
- * thread to the end of the last; out (n x 3, may be NULL) receives each
- * creature's final mantle x, y and path length. */
+ * thread to the end of the last; out (n x 4, may be NULL) receives each
+ * creature's final mantle x, y, path length and score (fitness.js, spawn
+ * reach measured at the spawn point).  f32: step with the f32 emulation. */
 int or_bench_rollouts(int n, const double *rects, const int *map_off, const int *map_id, const int *arms,
                       const int *segs, const double *x, const double *y, const double *angle,
                       const uint32_t *seed, const int *horizon, double tone, int period, int substeps,
                       int iterations, double h, double width, double height, int threads, double limit_s,
-                      long long *steps_done, double *elapsed_s, double *out);
+                      int f32, long long *steps_done, double *elapsed_s, double *out);
 void or_sim_metrics(const or_sim *s, int ci, or_metrics *out);
 
 #ifdef __cplusplus

@@ -6,6 +6,7 @@ driven step by step from Python, bit for bit, whatever the thread count."""
 import numpy as np
 
 from kraken_3_gpu_b200 import workloads
+from kraken_3_gpu_b200.kraken import arm_reach
 from kraken_3_gpu_b200.workloads import TONE, ControlStream
 from oracle import binding as ob
 
@@ -13,6 +14,7 @@ from oracle import binding as ob
 def _python_loop(w, i, steps):
     s = ob.Sim(rects=w.maps[w.map_id[i]])
     s.add_creature(w.x[i], w.y[i], w.angle[i], int(w.arms[i]), int(w.segs[i]))
+    s.set_spawn_reach(0, ob.measure_reach(w.maps[w.map_id[i]], arm_reach(int(w.segs[i])), w.x[i], w.y[i]))
     cs = ControlStream(int(w.arms[i]), int(w.segs[i]), seed=int(w.seed[i]))
     for t in range(steps):
         tg, ad = cs.at(t)
@@ -21,7 +23,7 @@ def _python_loop(w, i, steps):
         s.step()
         s.post_step()
     m = s.metrics(0)
-    return m["x"], m["y"], m["pathLen"]
+    return m["x"], m["y"], m["pathLen"], m["score"]
 
 
 def test_threaded_c_loop_equals_python_driven_oracle():

@@ -3,13 +3,20 @@
 The dynamics are chaotic: after a few hundred steps the f32 GPU trajectory
 and the f64 oracle trajectory of the same creature part ways (the
 reference measured this with its chaos checks), so long rollouts are
-compared as populations.  256 default creatures on map seed 1 (spawn jitter
-+-20 px, heading U[0, 2 pi)), 600 env steps with control streams: the
-path length of every creature's mantle on the GPU (batched engine) and in
-its own one-creature FP64 oracle world, driven the same way.  Bars: mean
-path length within 2 %, two-sample KS p > 0.05 for path length and for
-net displacement."""
-import threading
+compared as populations, on the quantity ES selects by: the reference's
+fitness score (src/sim/fitness.js:115-172, the engine's on-device
+postStep accumulators and score) -- and on the mantle's path length and
+net displacement.  Every creature is driven the same way on both sides
+(its control stream, applyControl with the suction-cup reflex, step,
+postStep); the oracle runs each creature in its own FP64 world on the
+host's threads (oracle/xpbd_bench.c).  Bars: mean score within 2 %,
+two-sample KS p > 0.05 for score, path length and displacement.
+
+  * config-1 creatures: 256 default bodies on map seed 1 (spawn jitter
+    +-20 px, heading U[0, 2 pi)), 600 env steps;
+  * the mixed workload: 512 creatures of 4-8 arms x 5-9 segments on 16 maps,
+    horizons U{300..900}."""
+import os
 
 import numpy as np
 import pytest
@@ -17,58 +24,45 @@ from scipy import stats
 
 from kraken_3_gpu_b200 import batch, workloads
 from oracle import binding as ob
-from tests.scenarios import TONE, ControlStream
 
 pytestmark = pytest.mark.gpu
-N, STEPS = 256, 600
+F = batch.METRIC_FIELDS
 
 
-def _oracle_fitness(w):
-    path = np.zeros(w.n)
-    disp = np.zeros(w.n)
-
-    def run(idx):
-        for i in idx:
-            sim = ob.Sim(rects=w.maps[0])
-            k = sim.add_creature(w.x[i], w.y[i], w.angle[i])
-            cs = ControlStream(6, 7, seed=int(w.seed[i]))
-            m = k.mantle
-            x0, y0 = sim.world.px[m], sim.world.py[m]
-            lx, ly, pl = x0, y0, 0.0
-            for s in range(STEPS):
-                t, a = cs.at(s)
-                sim.apply_control_motors(0, TONE, t, a)
-                sim.step()
-                x, y = sim.world.px[m], sim.world.py[m]
-                pl += float(np.hypot(x - lx, y - ly))
-                lx, ly = x, y
-            path[i] = pl
-            disp[i] = float(np.hypot(lx - x0, ly - y0))
-
-    th = [threading.Thread(target=run, args=(range(t, w.n, 16),)) for t in range(16)]
-    for t in th:
-        t.start()
-    for t in th:
-        t.join()
-    return path, disp
-
-
-def test_600_step_fitness_distribution_vs_fp64_oracle():
-    w = workloads.uniform(n=N, steps=STEPS)
+def _gpu(w):
     eng = batch.BatchEngine(w.maps, w.n)
     workloads.spawn_all(eng, w)
-    eng.run(STEPS)
-    fit = eng.read_fitness()
+    eng.run(int(w.horizon.max()))
+    m = eng.read_metrics()
     eng.close()
-    g_path = fit[:, 0]
-    g_disp = np.hypot(fit[:, 1] - w.x.astype(np.float32), fit[:, 2] - w.y.astype(np.float32))
-    o_path, o_disp = _oracle_fitness(w)
-    assert np.all(np.isfinite(g_path)) and np.all(g_path > 0)
-    rel = abs(g_path.mean() - o_path.mean()) / o_path.mean()
-    p_path = stats.ks_2samp(g_path, o_path, method="asymp").pvalue
-    p_disp = stats.ks_2samp(g_disp, o_disp, method="asymp").pvalue
-    print(f"mean path GPU {g_path.mean():.3f} oracle {o_path.mean():.3f} px ({100 * rel:.3f} %), "
-          f"KS p path {p_path:.3f} displacement {p_disp:.3f}")
-    assert rel < 0.02, f"mean path length differs by {100 * rel:.2f} %"
-    assert p_path > 0.05
-    assert p_disp > 0.05
+    return m[:, F.index("score")], m[:, F.index("pathLen")], m[:, F.index("x")], m[:, F.index("y")]
+
+
+def _oracle(w):
+    _, _, out = ob.bench_rollouts(w.maps, w.map_id, w.arms, w.segs, w.x, w.y, w.angle, w.seed, w.horizon,
+                                  max(1, os.cpu_count() or 1), metrics=True)
+    return out[:, 3], out[:, 2], out[:, 0], out[:, 1]
+
+
+def _compare(w, label):
+    g_score, g_path, gx, gy = _gpu(w)
+    o_score, o_path, ox, oy = _oracle(w)
+    g_disp, o_disp = np.hypot(gx - w.x, gy - w.y), np.hypot(ox - w.x, oy - w.y)
+    assert np.all(np.isfinite(g_score)) and np.all(g_path > 0)
+    rel = abs(g_score.mean() - o_score.mean()) / abs(o_score.mean())
+    p = {k: stats.ks_2samp(a, b, method="asymp").pvalue
+         for k, a, b in (("score", g_score, o_score), ("path", g_path, o_path), ("disp", g_disp, o_disp))}
+    print(f"{label}: mean score GPU {g_score.mean():.3f} oracle {o_score.mean():.3f} ({100 * rel:.3f} %), "
+          f"mean path {g_path.mean():.2f} / {o_path.mean():.2f} px, KS p " +
+          ", ".join(f"{k} {v:.3f}" for k, v in p.items()))
+    assert rel < 0.02, f"mean score differs by {100 * rel:.2f} %"
+    for k, v in p.items():
+        assert v > 0.05, f"KS p of {k} = {v:.4f}"
+
+
+def test_600_step_es_fitness_distribution_vs_fp64_oracle():
+    _compare(workloads.uniform(n=256, steps=600), "config-1 creatures x 600 steps")
+
+
+def test_mixed_bodies_es_fitness_distribution_vs_fp64_oracle():
+    _compare(workloads.uneven(n=512, n_maps=16, seed=7, h_min=300, h_max=900), "mixed workload, 512 creatures")
