@@ -3,7 +3,10 @@
     python -m kraken_3_gpu_b200.build
 
 Output: kraken_3_gpu_b200/libkraken_b200.so (kept out of git, shipped with the
-tree).  -fmad=false keeps every f32 multiply and add separately rounded, as
+tree), and the Node N-API addon's object napi/kraken_napi.o (compiled with
+gcc against the Node-API declarations of napi/node_api_decls.h: a compile
+check of the addon where no Node toolchain exists; node-gyp with
+napi/binding.gyp builds the loadable addon).  -fmad=false keeps every f32 multiply and add separately rounded, as
 the reference's per-op f32 semantics require; the kernels use explicit
 non-fusing intrinsics as well.
 """
@@ -47,5 +50,21 @@ def build(verbose: bool = False, force: bool = False) -> str:
     return OUT
 
 
+
+
+NAPI_SRC = os.path.join(HERE, "napi", "kraken_napi.c")
+NAPI_OBJ = os.path.join(HERE, "napi", "kraken_napi.o")
+
+
+def build_napi_object() -> str:
+    """Compile the N-API addon source to an object file (gcc, -Werror)."""
+    inc = os.path.join(os.path.dirname(HERE), "include")
+    cmd = [os.environ.get("CC", "gcc"), "-std=c11", "-O2", "-fPIC", "-Wall", "-Wextra", "-Werror",
+           "-I", inc, "-I", os.path.dirname(NAPI_SRC), "-c", NAPI_SRC, "-o", NAPI_OBJ]
+    subprocess.run(cmd, check=True)
+    return NAPI_OBJ
+
+
 if __name__ == "__main__":
     print(build(verbose="-v" in sys.argv, force=True))
+    print(build_napi_object())
