@@ -64,7 +64,7 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
-    ap.add_argument("--shape", default="", help="lanes,warps,ctas launch shape (empty: autotune)")
+    ap.add_argument("--shape", default="", help="lanes,warps,ctas[,unroll] launch shape (empty: autotune)")
     ap.add_argument("--chunk", type=int, default=64, help="server env steps per round")
     ap.add_argument("--no-es", action="store_true", help="skip the ES request stream")
     ap.add_argument("--es-requests", type=int, default=200)
@@ -429,7 +429,8 @@ def net_controller(stream, w, seed=7):
     eng.close()
     return {"value": w.creature_steps() / (ms / 1000.0), "unit": UNIT, "kernel_ms": ms,
             "controller": "net.js 10A+45 -> 24 -> 24 -> 3A+2 per creature, senses and recurrent outputs on the device",
-            "launch_shape": [shape["lanes_per_creature"], shape["warps_per_cta"], shape["ctas_per_sm"]]}
+            "launch_shape": [shape["lanes_per_creature"], shape["warps_per_cta"], shape["ctas_per_sm"],
+                             shape["substep_unroll"]]}
 
 
 def main():
@@ -485,10 +486,14 @@ def main():
     if args.shape:
         best = tuple(int(v) for v in args.shape.split(","))
         eng.set_launch(best[1], best[2], lanes_per_creature=best[0])
+        if len(best) > 3:
+            eng.set_unroll(best[3])
+        best = best[:3]
     else:
         g, wp, c, ms = eng.autotune(64)  # the library's autotuner: slots left as they were
         best = (g, wp, c)
         tune = {best: ms}
+    unroll = eng.get_launch()["substep_unroll"]
 
     # warm-up: full rollouts, each as a timed one runs
     for _ in range(args.warmup):
@@ -623,6 +628,7 @@ def main():
             "config": bench_config(args, w, world),
             "form": "persistent kernel, one launch per rollout, state resident in HBM",
             "launch": {"lanes_per_creature": best[0], "warps_per_cta": best[1], "ctas_per_sm": best[2],
+                       "substep_unroll": unroll,
                        "autotune_ms": {",".join(map(str, k)): round(v, 3) for k, v in tune.items()}},
             "roofline": roof, "cpu_baseline": cpu, "clocks": clocks, "e2e": e2e,
             "gpu_launches": gpu_launches, **extra,

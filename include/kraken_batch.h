@@ -219,17 +219,26 @@ int kr_probe_wrap(const double *d, int32_t n, double *out);
 int kr_batch_set_launch(kr_batch *b, int32_t lanes_per_creature, int32_t warps_per_cta,
                         int32_t ctas_per_sm);
 
+/* Substep unroll: the kernel's substep loop runs as a loop (1) or with its
+ * body twice per trip (2); the same operations in the same order, so the
+ * results do not depend on it -- only the instruction stream does.  Default
+ * 1; kr_batch_autotune picks it with the launch shape. */
+int kr_batch_set_unroll(kr_batch *b, int32_t substep_unroll);
+int kr_batch_get_unroll(kr_batch *b, int32_t *substep_unroll);
+
 /* The current launch shape and the dynamic shared memory of a CTA (bytes;
  * 0 before the first spawn).  Any pointer may be NULL. */
 int kr_batch_get_launch(kr_batch *b, int32_t *lanes_per_creature, int32_t *warps_per_cta,
                         int32_t *ctas_per_sm, int32_t *smem_bytes);
 
 /* Autotuner: runs `steps` env steps of the live slots with each candidate
- * launch shape (8, 16 and 32 lanes per creature with 4-16 warps per CTA),
- * puts every slot's state back after each trial (slots end as they were;
- * the kr_batch_snapshot copy is not touched) and keeps the fastest shape
- * (kr_batch_set_launch).  The chosen shape and its time are returned; any
- * pointer may be NULL.  Synchronous. */
+ * launch shape (8, 16 and 32 lanes per creature with 4-16 warps per CTA,
+ * each with the substep loop rolled or unrolled by 2), puts every slot's
+ * state back after each trial (slots end as they were; the
+ * kr_batch_snapshot copy is not touched) and keeps the fastest shape
+ * (kr_batch_set_launch, kr_batch_set_unroll).  The chosen shape and its time
+ * are returned (the unroll through kr_batch_get_unroll); any pointer may be
+ * NULL.  Synchronous. */
 int kr_batch_autotune(kr_batch *b, int32_t steps, int32_t *lanes_per_creature, int32_t *warps_per_cta,
                       int32_t *ctas_per_sm, float *best_ms);
 

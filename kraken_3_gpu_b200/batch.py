@@ -99,6 +99,8 @@ def _lib():
         "kr_batch_set_launch": (C.c_int, [vp, i32, i32, i32]),
         "kr_batch_get_launch": (C.c_int, [vp, _I32P, _I32P, _I32P, _I32P]),
         "kr_batch_autotune": (C.c_int, [vp, i32, _I32P, _I32P, _I32P, _F32P]),
+        "kr_batch_set_unroll": (C.c_int, [vp, i32]),
+        "kr_batch_get_unroll": (C.c_int, [vp, _I32P]),
         "kr_batch_last_ms": (C.c_int, [vp, _F32P]),
         "kr_batch_sync": (C.c_int, [vp]),
         "kr_batch_set_stream": (C.c_int, [vp, vp]),
@@ -243,20 +245,27 @@ class BatchEngine:
         _check(_lib().kr_batch_set_launch(self.h, lanes_per_creature, warps_per_cta, ctas_per_sm),
                self.h)
 
+    def set_unroll(self, substep_unroll):
+        """Unroll factor of the kernel's substep loop (1 or 2); results do
+        not depend on it."""
+        _check(_lib().kr_batch_set_unroll(self.h, substep_unroll), self.h)
+
     def autotune(self, steps=64):
-        """Time every candidate launch shape on `steps` env steps of the live
-        slots (state put back after each trial), keep the fastest; returns
-        (lanes_per_creature, warps_per_cta, ctas_per_sm, ms)."""
+        """Time every candidate launch shape (lanes, warps, CTAs per SM,
+        substep unroll) on `steps` env steps of the live slots (state put back
+        after each trial), keep the fastest; returns (lanes_per_creature,
+        warps_per_cta, ctas_per_sm, ms) -- the unroll is in get_launch()."""
         v = [C.c_int32() for _ in range(3)]
         ms = C.c_float()
         _check(_lib().kr_batch_autotune(self.h, steps, *[C.byref(x) for x in v], C.byref(ms)), self.h)
         return v[0].value, v[1].value, v[2].value, ms.value
 
     def get_launch(self):
-        v = [C.c_int32() for _ in range(4)]
-        _check(_lib().kr_batch_get_launch(self.h, *[C.byref(x) for x in v]), self.h)
+        v = [C.c_int32() for _ in range(5)]
+        _check(_lib().kr_batch_get_launch(self.h, *[C.byref(x) for x in v[:4]]), self.h)
+        _check(_lib().kr_batch_get_unroll(self.h, C.byref(v[4])), self.h)
         return {"lanes_per_creature": v[0].value, "warps_per_cta": v[1].value,
-                "ctas_per_sm": v[2].value, "smem_bytes": v[3].value}
+                "ctas_per_sm": v[2].value, "smem_bytes": v[3].value, "substep_unroll": v[4].value}
 
     def run(self, max_steps):
         _check(_lib().kr_batch_run(self.h, max_steps), self.h)

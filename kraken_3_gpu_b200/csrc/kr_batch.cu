@@ -631,7 +631,7 @@ __device__ __noinline__ void net_senses(NetArgs N, int arms, const int *arm_tip,
 // One creature (slot) advanced by its G lanes for up to A.max_steps env steps.
 // NET: the kernel instance of engines in KR_CTRL_NET mode (the other modes'
 // kernels carry none of the net's code).
-template <int G, bool NET>
+template <int G, bool NET, int U>
 __device__ void run_creature(const BatchArgs &A, const TplDev &td, int nlv, const TplSmem &P, float *base,
                              int slot, const kr::Lanes<G> &L) {
   const int lane = L.lane;
@@ -731,7 +731,7 @@ __device__ void run_creature(const BatchArgs &A, const TplDev &td, int nlv, cons
     }
     L.sync();
     // 4. the XPBD step
-    kr::island_step<kr::CompactAccess, G>(A.K, S, rects, nR, cull_d, L, td.off_max + 1.f);
+    kr::island_step<kr::CompactAccess, G, U>(A.K, S, rects, nR, cull_d, L, td.off_max + 1.f);
     // 5. postStep, core.js:297-356 (f64 on the f32 state, as the
     //    reference's hybrid loop runs it on the mirrored state)
     //    The accumulators are read and written through the slot's HBM
@@ -801,7 +801,7 @@ __device__ void run_creature(const BatchArgs &A, const TplDev &td, int nlv, cons
   }
 }
 
-template <int G, bool NET>
+template <int G, bool NET, int U>
 __global__ void __launch_bounds__(32 * kMaxW, 1) batch_kernel(BatchArgs A) {
   constexpr int CPW = 32 / G;  // creatures per warp
   constexpr int V = G == 32 ? 0 : G == 16 ? 1 : 2;  // kr::schedule_index(G): the schedule for G lanes
@@ -846,7 +846,7 @@ __global__ void __launch_bounds__(32 * kMaxW, 1) batch_kernel(BatchArgs A) {
     if (slot >= 0) {
       float *base = smem + tpl_smem_words(td.nb, td.nc, td.np) +
                     c * creature_smem_words(td.nb, td.nc, td.np, td.arms, td.segs);
-      run_creature<G, NET>(A, td, td.nlv[V], P, base, slot, L);
+      run_creature<G, NET, U>(A, td, td.nlv[V], P, base, slot, L);
     }
   }
 }
@@ -1213,7 +1213,8 @@ int build_groups(kr_batch *b, Part &p, int max_steps) {
 namespace {
 template <int G>
 cudaError_t launch_g(const BatchArgs &A, kr_batch *b, cudaStream_t st, int n_groups, int *grid_out) {
-  auto *fn = b->d_net ? batch_kernel<G, true> : batch_kernel<G, false>;
+  auto *fn = b->unroll == 2 ? (b->d_net ? batch_kernel<G, true, 2> : batch_kernel<G, false, 2>)
+                            : (b->d_net ? batch_kernel<G, true, 1> : batch_kernel<G, false, 1>);
   cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b->smem_dyn);
   if (e != cudaSuccess) return e;
   int per_sm = 0;
@@ -1735,6 +1736,19 @@ extern "C" int kr_batch_set_launch(kr_batch *b, int32_t lanes_per_creature, int3
   return KR_OK;
 }
 
+extern "C" int kr_batch_set_unroll(kr_batch *b, int32_t substep_unroll) {
+  if (!b) return KR_ERR_INVALID;
+  if (substep_unroll != 1 && substep_unroll != 2) return b->fail(KR_ERR_INVALID, "substep_unroll must be 1 or 2");
+  b->unroll = substep_unroll;
+  return KR_OK;
+}
+
+extern "C" int kr_batch_get_unroll(kr_batch *b, int32_t *substep_unroll) {
+  if (!b || !substep_unroll) return KR_ERR_INVALID;
+  *substep_unroll = b->unroll;
+  return KR_OK;
+}
+
 extern "C" int kr_batch_get_launch(kr_batch *b, int32_t *lanes_per_creature, int32_t *warps_per_cta,
                                    int32_t *ctas_per_sm, int32_t *smem_bytes) {
   if (!b) return KR_ERR_INVALID;
@@ -1809,7 +1823,10 @@ extern "C" int kr_batch_autotune(kr_batch *b, int32_t steps, int32_t *lanes_out,
                                  int32_t *ctas_out, float *best_ms_out) {
   if (!b) return KR_ERR_INVALID;
   if (steps < 1) return b->fail(KR_ERR_INVALID, "autotune steps < 1");
-  static const int kCand[][3] = {{8, 8, 0}, {8, 16, 1}, {8, 4, 4}, {16, 8, 0}, {16, 16, 1}, {32, 4, 0}, {32, 8, 0}};
+  // (lanes per creature, warps per CTA, CTAs per SM, substep unroll)
+  static const int kCand[][4] = {{8, 8, 0, 1},  {8, 16, 1, 1},  {8, 4, 4, 1},  {16, 8, 0, 1}, {16, 16, 1, 1},
+                                 {32, 4, 0, 1}, {32, 8, 0, 1},  {8, 8, 0, 2},  {8, 16, 1, 2}, {16, 8, 0, 2},
+                                 {32, 4, 0, 2}};
   const size_t C = (size_t)b->capacity;
   // scratch copy of every slot (the trials run, then the state goes back)
   float *t_state = nullptr, *t_ctrl = nullptr;
@@ -1841,7 +1858,7 @@ extern "C" int kr_batch_autotune(kr_batch *b, int32_t steps, int32_t *lanes_out,
     return r;
   };
   const std::vector<int> rem0 = b->h_remaining;
-  const int G0 = b->G, W0 = b->W, C0 = b->ctas_per_sm;
+  const int G0 = b->G, W0 = b->W, C0 = b->ctas_per_sm, U0 = b->unroll;
   const bool auto0 = b->auto_shape;
   int best = -1, rc = KR_OK;
   float best_ms = 0.f;
@@ -1849,6 +1866,7 @@ extern "C" int kr_batch_autotune(kr_batch *b, int32_t steps, int32_t *lanes_out,
   for (int c = 0; c < (int)(sizeof(kCand) / sizeof(kCand[0])) && e == cudaSuccess && rc == KR_OK; c++) {
     rc = kr_batch_set_launch(b, kCand[c][0], kCand[c][1], kCand[c][2]);
     if (rc != KR_OK) break;
+    b->unroll = kCand[c][3];
     b->main.dirty = true;
     rc = launch_part(b, b->main, steps, true);
     if (rc == KR_ERR_CAPACITY) { rc = KR_OK; b->h_remaining = rem0; e = copy_slots(false); continue; }
@@ -1868,10 +1886,11 @@ extern "C" int kr_batch_autotune(kr_batch *b, int32_t steps, int32_t *lanes_out,
   if (rc != KR_OK) return rc;
   if (e != cudaSuccess) return b->cuda_fail(e, "kr_batch_autotune");
   if (best < 0) {  // nothing live: keep the shape as it was
-    b->G = G0; b->W = W0; b->ctas_per_sm = C0; b->auto_shape = auto0; b->shape_dirty = true;
+    b->G = G0; b->W = W0; b->ctas_per_sm = C0; b->unroll = U0; b->auto_shape = auto0; b->shape_dirty = true;
   } else {
     rc = kr_batch_set_launch(b, kCand[best][0], kCand[best][1], kCand[best][2]);
     if (rc != KR_OK) return rc;
+    b->unroll = kCand[best][3];
   }
   if (lanes_out) *lanes_out = b->G;
   if (warps_out) *warps_out = b->W;

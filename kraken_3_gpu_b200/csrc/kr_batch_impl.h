@@ -305,6 +305,7 @@ struct kr_batch {
   int s_n_groups = -1, s_cpc = 0, s_G = 0;
   // launch shape
   int G = 16, W = 8, ctas_per_sm = 0, n_sm = 0;
+  int unroll = 1;               // unroll factor of the kernel's substep loop (1 or 2)
   int smem_per_sm = 0, smem_reserved = 0, smem_optin = 0;
   bool auto_shape = true;       // until kr_batch_set_launch: G and W from the live count
   int cpc = 16;                 // creature entries per group: W * 32 / G

@@ -772,10 +772,14 @@ __device__ __forceinline__ void grip_break(const SolverConsts &K, Island &S, int
 // One env step of one island by a group of G lanes (xpbd.js:487-490 with the
 // substep of f32solver.mjs:419-428): substeps x (reset lambda, integrate,
 // iterations x (constraint levels, collisions), finalize), then grip break.
-template <class Acc, int G>
+// U: unroll factor of the substep loop (1: a loop; 2: its body twice per
+// trip, remainder handled) -- the same operations in the same order, so the
+// results do not depend on it; the batched engine's autotuner picks it.
+template <class Acc, int G, int U = 1>
 __device__ __forceinline__ void island_step(const SolverConsts &K, Island &S,
                                             const float4 *__restrict__ rects, int nR, float cull_d,
                                             const Lanes<G> &L, float reach) {
+#pragma unroll U
   for (int s = 0; s < K.substeps; s++) {
     for (int k = L.lane; k < S.nc; k += G) { S.lamX[k] = 0.f; S.lamY[k] = 0.f; S.lam[k] = 0.f; }
     for (int i = L.lane; i < S.nb; i += G) integrate_body(K, S, i);

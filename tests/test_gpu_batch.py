@@ -94,22 +94,24 @@ def test_chunked_runs_and_graph_equal_one_run():
         e.close()
 
 
-@pytest.mark.parametrize("lanes,warps,ctas", [(32, 1, 1), (32, 16, 1), (16, 4, 2), (16, 8, 0),
-                                               (8, 2, 4), (8, 16, 1), (16, 4, 5), (16, 4, 6),
-                                               (32, 8, 3)])
-def test_launch_shape_does_not_change_results(lanes, warps, ctas):
-    """One to four creatures per warp, any CTA size or CTAs per SM: the
-    same bits."""
+@pytest.mark.parametrize("lanes,warps,ctas,unroll", [(32, 1, 1, 1), (32, 16, 1, 2), (16, 4, 2, 1), (16, 8, 0, 2),
+                                                      (8, 2, 4, 1), (8, 16, 1, 1), (8, 8, 0, 2), (16, 4, 5, 1),
+                                                      (16, 4, 6, 2), (32, 8, 3, 1)])
+def test_launch_shape_does_not_change_results(lanes, warps, ctas, unroll):
+    """One to four creatures per warp, any CTA size or CTAs per SM, the
+    substep loop rolled or unrolled: the same bits."""
     w = _small_uneven(n=40, h=30)
     base = batch.BatchEngine(w.maps, w.n, obs_ring=32)
     workloads.spawn_all(base, w)
     base.run(30)
     other = batch.BatchEngine(w.maps, w.n, obs_ring=32)
     other.set_launch(warps, ctas, lanes_per_creature=lanes)
+    other.set_unroll(unroll)
     workloads.spawn_all(other, w)
     other.run(17)
     other.run(13)
     assert other.get_launch()["lanes_per_creature"] == lanes
+    assert other.get_launch()["substep_unroll"] == unroll
     s0, s1 = base.read_state(), other.read_state()
     for f in ("px", "py", "ang", "vx", "vy", "av", "grips", "steps"):
         assert np.array_equal(s0[f], s1[f]), f
