@@ -28,6 +28,7 @@ the host cores as a reported baseline.
 from __future__ import annotations
 
 import argparse
+import ctypes as C
 import json
 import math
 import os
@@ -318,80 +319,188 @@ def served_es_stream(serve, w, chunk, n_req, rate, seed=0, net=False):
     st = srv.stats()
     srv.close()
     lat = np.array([x["completed"] - x["arrival"] for x in res])
+    queue = np.array([x["admitted"] - x["arrival"] for x in res])
+    service = np.array([x["completed"] - x["admitted"] for x in res])
     span = max(x["completed"] for x in res) - min(x["arrival"] for x in res)
+    arrivals = reqs[-1]["arrival"] - reqs[0]["arrival"]
+
+    def pct(a, q):
+        return float(np.percentile(a, q) * 1e3)
+
     return {"value": units / span, "unit": UNIT, "requests": n_req, "rate_req_s": rate,
-            "creature_steps": units, "makespan_s": span,
-            "p50_rollout_ms": float(np.percentile(lat, 50) * 1e3),
-            "p99_rollout_ms": float(np.percentile(lat, 99) * 1e3),
+            "offered_rate": units / max(arrivals, 1e-9), "delivered_rate": units / span,
+            "creature_steps": units, "makespan_s": span, "arrivals_span_s": arrivals,
+            "p50_rollout_ms": pct(lat, 50), "p99_rollout_ms": pct(lat, 99),
+            "queue_p50_ms": pct(queue, 50), "queue_p99_ms": pct(queue, 99),
+            "service_p50_ms": pct(service, 50), "service_p99_ms": pct(service, 99),
             "slots": st["capacity"], "chunk_steps": chunk,
             "device_kernel_ms_summed": st["device_ms"]}
 
 
-def config1_forms(torch, stream, plain_steps=200, steps=1000):
+def served_es_streams(serve, w, chunk, n_req, rate, net=False):
+    """The configured stream (Poisson `rate` req/s: it offers more work than
+    one GPU delivers, so its latencies grow with the stream's length), and the
+    same request mix at a sustainable load: the Poisson rate scaled so that the
+    offered creature-steps/s are 0.8 x the rate the first stream delivered
+    (the server's capacity under this mix)."""
+    over = served_es_stream(serve, w, chunk, n_req, rate, net=net)
+    sus_rate = rate * 0.8 * over["delivered_rate"] / over["offered_rate"]
+    sus = served_es_stream(serve, w, chunk, n_req, sus_rate, net=net)
+    over["sustainable_load"] = sus
+    return over
+
+
+class HybridLoop:
+    """The reference's plain loop (src/sim/gputrain.js:72-128: per env step
+    applyControl with the suction-cup reflex on the mirrored state,
+    uploadControls, one step, download + mirror) through the drop-in C ABI,
+    for many creatures of one body shape at once: the host side runs over
+    numpy arrays -- control-stream draws (mulberry32, map.js:11-20), clamped
+    motor targets, the reflex of core.js:199-218 (slip gate, attach at the tip
+    point, break force, release) and packControls' fields -- so that the
+    loop's cost is the boundary's, not Python's."""
+
+    def __init__(self, w, stream_ptr):
+        from kraken_3_gpu_b200 import _native, core, gpuworld, kraken
+        self.n = w.n
+        self.sim = core.create_sim(seed=1, creatures=w.n, poses=list(zip(w.x, w.y, w.angle)))
+        world, crs = self.sim["world"], self.sim["creatures"]
+        self.g = gpuworld.create(world, self.sim["map"])
+        gpuworld.upload(self.g)
+        self.L, self.h = _native.lib(), self.g.handle
+        _native.check(self.L.kr_set_stream(self.h, C.c_void_p(stream_ptr)), self.h)
+        k_of = {id(c): k for k, c in enumerate(world.constraints)}
+        self.motors = np.array([[k_of[id(m)] for a in c.arms for m in a.motors] for c in crs])
+        self.grips = np.array([[k_of[id(a.grip)] for a in c.arms] for c in crs])
+        self.tips = np.array([[a.tip for a in c.arms] for c in crs])
+        self.A, self.S = len(crs[0].arms), len(crs[0].arms[0].motors)
+        B = kraken.BODY
+        self.lim = np.where(np.arange(self.A * self.S) % self.S == 0, B["shoulderLimit"], B["jointLimit"])
+        self.half_seg = B["segLen"] * 0.5
+        self.cons = self.g.consData.reshape(-1, 20)
+        self.consu = self.g.consData.view(np.uint32).reshape(-1, 20)
+        self.body = self.g.bodyData.reshape(-1, 12)
+        self.cons[self.motors, 8] = kraken.tone_to_compliance(0.5)
+        self.rng = np.ascontiguousarray(w.seed, dtype=np.uint32).copy()
+        self.targets = np.zeros((self.n, self.A * self.S))
+        self.adh = np.zeros((self.n, self.A))
+        self.cd = np.zeros((self.n, self.A))
+        self.dt = world.h * world.substeps
+        self.cp = self.g.consData.view(np.uint32).ctypes.data_as(C.POINTER(C.c_uint32))
+        self.bp = self.g.bodyData.ctypes.data_as(C.POINTER(C.c_float))
+        self.t = 0
+        self._check(self.L.kr_download(self.h, self.bp, self.cp))  # the mirrored f32 state
+
+    def _check(self, rc):
+        from kraken_3_gpu_b200 import _native
+        _native.check(rc, self.h)
+
+    def _draw(self):
+        r = np.empty((self.n, self.A * (self.S + 1)))
+        s = self.rng
+        for d in range(r.shape[1]):
+            s = s + np.uint32(0x6D2B79F5)
+            t = (s ^ (s >> np.uint32(15))) * (s | np.uint32(1))
+            t ^= t + (t ^ (t >> np.uint32(7))) * (t | np.uint32(61))
+            r[:, d] = (t ^ (t >> np.uint32(14))) / 4294967296.0
+        self.rng = s
+        r = r.reshape(self.n, self.A, self.S + 1)
+        self.targets = (r[:, :, :self.S] * 2 - 1).reshape(self.n, -1)
+        self.adh = r[:, :, self.S]
+
+    def control(self):
+        """applyControl for every creature on the mirrored state, packed."""
+        if self.t % 6 == 0:
+            self._draw()
+        self.cons[self.motors, 10] = np.clip(self.targets, -self.lim, self.lim)
+        adh = np.clip(self.adh, 0.0, 1.0)
+        self.cd = np.where(self.cd > 0, self.cd - self.dt, self.cd)
+        broken = self.consu[self.grips, 17] != 0
+        tb = self.body[self.tips].astype(np.float64)
+        cand = broken & (adh > 0.08) & (self.cd <= 0)
+        att = cand & (np.hypot(tb[..., 4], tb[..., 5]) < 150.0)
+        self.cd = np.where(cand & ~att, 0.05, self.cd)
+        held = ~broken
+        ga = self.grips[att]
+        self.cons[ga, 6] = tb[..., 0][att] + self.half_seg * np.cos(tb[..., 6][att])
+        self.cons[ga, 7] = tb[..., 1][att] + self.half_seg * np.sin(tb[..., 6][att])
+        upd = att | held
+        self.cons[self.grips[upd], 16] = (40.0 + 860.0 * adh)[upd]
+        nb = broken & ~att | (held & (adh < 0.04))
+        self.consu[self.grips, 17] = nb.astype(np.uint32)
+
+    def step(self, ev=None):
+        self.control()
+        self._check(self.L.kr_upload_controls(self.h, self.cp))
+        if ev is not None:
+            ev[0].record()
+        self._check(self.L.kr_step(self.h, 1))
+        if ev is not None:
+            ev[1].record()
+        self._check(self.L.kr_download(self.h, self.bp, self.cp))
+        self.t += 1
+
+    def close(self):
+        from kraken_3_gpu_b200 import gpuworld
+        gpuworld.destroy(self.g)
+
+
+def config1_forms(torch, stream, steps=1000):
     """The plain batched drop-in configuration: 1,024 default creatures on
-    map seed 1 (createSim spawn rule).  The reference's plain form -- per env
-    step the 80 B constraint blocks up (uploadControls), one step, bodies and
-    constraints down (download), gpuworld.js:312-396 -- through the drop-in C
-    ABI with host buffers (the CPU reflex the reference runs between steps is
-    not timed); the same drop-in with state resident (kr_step per env step
-    only); and the persistent batched engine on the same creatures."""
-    import ctypes as C
-    from kraken_3_gpu_b200 import _native, batch, core, gpuworld, workloads
-    sim = core.create_sim(seed=1, creatures=1024)
-    w = sim["world"]
-    n = len(sim["creatures"])
-    g = gpuworld.create(w, sim["map"])
-    gpuworld.upload(g)
-    L = _native.lib()
-    h = g.handle
-    _native.check(L.kr_set_stream(h, C.c_void_p(stream.cuda_stream)), h)
-    cons = np.ascontiguousarray(g.consData).view(np.uint32)
-    body = np.zeros(g.nB * gpuworld.BODY_STRIDE, dtype=np.float32)
-    cp, bp = cons.ctypes.data_as(C.POINTER(C.c_uint32)), body.ctypes.data_as(C.POINTER(C.c_float))
-    for _ in range(5):
-        L.kr_upload_controls(h, cp); L.kr_step(h, 1); L.kr_download(h, bp, cp)
+    map seed 1, spawn jitter U(+-20 px) around the map's spawn point, heading
+    U[0, 2 pi), 1,000 env steps, random controls per creature (its own
+    control stream, redrawn every 6 steps).  Two forms on the same creatures
+    and controls: the reference's plain loop through the drop-in (HybridLoop:
+    per env step the reflex on the host, the 80 B constraint blocks up, one
+    kr_step, bodies and constraints down), timed whole and by the kernel time
+    of its steps; and the persistent batched engine (reflex and controls on the
+    device, one launch).  The persistent engine runs the same arithmetic, so
+    the two forms' final states are compared bit for bit as well."""
+    from kraken_3_gpu_b200 import batch, workloads
+    w = workloads.uniform(n=1024, steps=steps)
+    loop = HybridLoop(w, stream.cuda_stream)
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    for _ in range(plain_steps):
-        _native.check(L.kr_upload_controls(h, cp), h)
-        _native.check(L.kr_step(h, 1), h)
-        _native.check(L.kr_download(h, bp, cp), h)
+    for k in range(steps):
+        loop.step(evs[k])
     loop_s = time.perf_counter() - t0
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    for _ in range(plain_steps):
-        L.kr_step(h, 1)
-    e1.record(stream)
-    e1.synchronize()
-    step_ms = e0.elapsed_time(e1)
-    gpuworld.destroy(g)
-    mant = [c.mantle for c in sim["creatures"]]
-    eng = batch.BatchEngine([workloads._rects(sim["map"])], n)
+    kernel_ms = sum(a.elapsed_time(b) for a, b in evs)
+    mant = [c.mantle for c in loop.sim["creatures"]]
+    dropin_xy = loop.body[mant][:, :2].copy()
+    cons_bytes, body_bytes = loop.g.consData.nbytes, loop.g.bodyData.nbytes
+    loop.close()
+    eng = batch.BatchEngine(w.maps, w.n)
     eng.set_stream(stream.cuda_stream)
-    ones = np.ones(n, np.int32)
-    eng.spawn(0, 6 * ones, 7 * ones, 0 * ones, w.px[mant], w.py[mant], w.ang[mant], steps * ones,
-              seed=np.arange(n, dtype=np.uint32))
+    workloads.spawn_all(eng, w)
     eng.snapshot()
-    pers_ms, shape = float("inf"), None
-    for shp in ((32, 4, 0), (16, 8, 0)):
-        eng.set_launch(shp[1], shp[2], lanes_per_creature=shp[0])
-        eng.restore()
-        eng.run(64)
-        eng.restore()
-        eng.run(steps)
-        eng.sync()
-        if eng.last_ms() < pers_ms:
-            pers_ms, shape = eng.last_ms(), shp
+    g, wp, c, _ = eng.autotune(64)
+    eng.restore()
+    eng.run(64)
+    eng.restore()
+    eng.run(steps)
+    eng.sync()
+    pers_ms = eng.last_ms()
+    st = eng.read_state()
+    shape = eng.get_launch()
     eng.close()
-    return {"creatures": n, "map_seed": 1,
-            "dropin_per_step_loop": {"value": n * plain_steps / loop_s, "unit": UNIT, "steps": plain_steps,
-                                     "h2d_bytes_per_step": int(cons.nbytes),
-                                     "d2h_bytes_per_step": int(cons.nbytes + body.nbytes)},
-            "dropin_per_step_kernel": {"value": n * plain_steps / (step_ms / 1000.0), "unit": UNIT,
-                                       "steps": plain_steps},
-            "persistent": {"value": n * steps / (pers_ms / 1000.0), "unit": UNIT, "steps": steps,
-                           "launch_shape": list(shape)}}
+    pers_xy = np.stack([st["px"][:, 0], st["py"][:, 0]], axis=1)
+    same = float(np.mean(np.all(pers_xy.astype(np.float32) == dropin_xy, axis=1)))
+    n = w.n
+    return {"creatures": n, "map_seed": 1, "steps": steps,
+            "dropin_per_step_loop": {"value": n * steps / loop_s, "unit": UNIT,
+                                     "form": "reference plain loop: host reflex + packControls, uploadControls, "
+                                             "kr_step, download, per env step",
+                                     "h2d_bytes_per_step": int(cons_bytes),
+                                     "d2h_bytes_per_step": int(cons_bytes + body_bytes)},
+            "dropin_per_step_kernel": {"value": n * steps / (kernel_ms / 1000.0), "unit": UNIT,
+                                       "kernel_ms": kernel_ms,
+                                       "form": "the kr_step launches of that loop alone (CUDA events)"},
+            "persistent": {"value": n * steps / (pers_ms / 1000.0), "unit": UNIT, "kernel_ms": pers_ms,
+                           "launch_shape": [shape["lanes_per_creature"], shape["warps_per_cta"],
+                                            shape["ctas_per_sm"], shape["substep_unroll"]]},
+            "persistent_over_dropin_kernel": (n * steps / (pers_ms / 1000.0)) / (n * steps / (kernel_ms / 1000.0)),
+            "final_mantles_bit_identical": same}
 
 
 def net_controller(stream, w, seed=7):
@@ -589,13 +698,13 @@ def main():
             "wall_s": [round(x, 4) for x in reps]}
 
     if not args.no_es and rank == 0:
-        extra["served_es_stream"] = served_es_stream(serve, w, chunk, args.es_requests, 200.0)
+        extra["served_es_stream"] = served_es_streams(serve, w, chunk, args.es_requests, 200.0)
     if not args.no_config1 and rank == 0:
         extra["plain_dropin_1024"] = config1_forms(torch, stream)
     if not args.no_net and rank == 0:
         extra["net_controller"] = net_controller(stream, w)
         if not args.no_es:
-            extra["served_es_stream_net"] = served_es_stream(serve, w, chunk, args.es_requests, 200.0, net=True)
+            extra["served_es_stream_net"] = served_es_streams(serve, w, chunk, args.es_requests, 200.0, net=True)
 
     # roofline: f32 rounding ops per creature-step of the restated f32
     # algorithm (op-counting oracle build) x creature-steps per launch /

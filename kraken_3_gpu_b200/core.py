@@ -74,8 +74,13 @@ def group_constraints_by_color(world: XpbdWorld):
 
 
 def create_sim(**opts):
-    """createSim, core.js:37-74 with prey 0 and an optional body shape."""
+    """createSim, core.js:37-74 with prey 0 and an optional body shape.
+    poses: optional (x, y, angle) per creature instead of findSpawn's points
+    and the seeded headings (the map is still makeMap of the seed)."""
     o = {**DEFAULTS, **opts}
+    poses = o.pop("poses", None)
+    if poses is not None:
+        o["creatures"] = len(poses)
     world = XpbdWorld(substeps=o["substeps"], iterations=o["iterations"], h=o["h"])
     m = make_map(o["width"], o["height"], seed=o["seed"])
     world.sdf = m["sdf"]
@@ -84,9 +89,12 @@ def create_sim(**opts):
     color_mask = np.zeros(1 << 16, dtype=np.uint32)
     colored_upto = 0
     for i in range(o["creatures"]):
-        sp = find_spawn(m, arm_reach(o["segsPerArm"]) + 20, rnd)
-        k = spawn_kraken(world, sp["x"], sp["y"], rnd() * math.pi * 2,
-                         arms=o["arms"], segs=o["segsPerArm"])
+        if poses is not None:
+            x, y, ang = (float(v) for v in poses[i])
+        else:
+            sp = find_spawn(m, arm_reach(o["segsPerArm"]) + 20, rnd)
+            x, y, ang = sp["x"], sp["y"], rnd() * math.pi * 2
+        k = spawn_kraken(world, x, y, ang, arms=o["arms"], segs=o["segsPerArm"])
         # core.js:51-58: colour this creature's constraints (global body mask)
         for c in world.constraints[colored_upto:]:
             if c.color < 0:
