@@ -405,8 +405,9 @@ class HybridLoop:
             r[:, d] = (t ^ (t >> np.uint32(14))) / 4294967296.0
         self.rng = s
         r = r.reshape(self.n, self.A, self.S + 1)
-        self.targets = (r[:, :, :self.S] * 2 - 1).reshape(self.n, -1)
-        self.adh = r[:, :, self.S]
+        # held as f32, as the controls of a Float32Array (the engine's control record)
+        self.targets = (r[:, :, :self.S] * 2 - 1).astype(np.float32).astype(np.float64).reshape(self.n, -1)
+        self.adh = r[:, :, self.S].astype(np.float32).astype(np.float64)
 
     def control(self):
         """applyControl for every creature on the mirrored state, packed."""

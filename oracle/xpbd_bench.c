@@ -8,7 +8,8 @@
  *   per env step t of a creature:
  *     if t % period == 0: draw the controls from the creature's mulberry32
  *       stream (src/world/map.js:11-20), per arm its motors then its
- *       adhesion, targets as r * 2 - 1 and adhesion as r;
+ *       adhesion, targets as r * 2 - 1 and adhesion as r, each held as f32
+ *       (the controls of a Float32Array, as the engine's control record);
  *     applyControl (core.js:183-220: targets clamped, the suction-cup reflex),
  *     preStep, world.step() (xpbd.js:487-490; or, for checks, the f32
  *     emulation's step of tools/f32solver.mjs), postStep (core.js:297-356).
@@ -59,8 +60,8 @@ static void *bench_thread(void *arg) {
     for (int t = 0; t < J->horizon[c] && !stop; t++) {
       if (t % J->period == 0) {
         for (int a = 0; a < A; a++) {
-          for (int j = 0; j < S; j++) tg[a * S + j] = or_rnd(&rng) * 2 - 1;
-          ad[a] = or_rnd(&rng);
+          for (int j = 0; j < S; j++) tg[a * S + j] = (double)(float)(or_rnd(&rng) * 2 - 1);
+          ad[a] = (double)(float)or_rnd(&rng);
         }
       }
       or_apply_control_motors(s, 0, J->tone, tg, ad);

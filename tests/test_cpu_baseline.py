@@ -17,7 +17,7 @@ def _python_loop(w, i, steps):
     s.set_spawn_reach(0, ob.measure_reach(w.maps[w.map_id[i]], arm_reach(int(w.segs[i])), w.x[i], w.y[i]))
     cs = ControlStream(int(w.arms[i]), int(w.segs[i]), seed=int(w.seed[i]))
     for t in range(steps):
-        tg, ad = cs.at(t)
+        tg, ad = (v.astype(np.float32).astype(np.float64) for v in cs.at(t))
         s.apply_control_motors(0, TONE, tg, ad)
         s.pre_step()
         s.step()
