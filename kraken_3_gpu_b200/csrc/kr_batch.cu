@@ -78,12 +78,12 @@ __host__ __device__ constexpr int r4(int n) { return (n + 3) & ~3; }
 __host__ __device__ inline int tpl_smem_words(int nb, int nc, int np) {
   return 5 * r4(nb) + 11 * r4(nc) + 4 * r4(np) + kLvlWords + kArmWords;
 }
-// one creature: predicted bodies and their sin/cos, grip and motor state,
-// lambda, collision scratch (the committed state -- positions, angles,
-// velocities -- is read and written in place in the slot's HBM block: it is
-// touched once per substep, not in the solver's inner loops)
+// one creature: the committed state (positions, angles, velocities: loaded
+// from the slot's HBM block when the creature starts, written back when its
+// run ends), predicted bodies and their sin/cos, grip and motor state,
+// lambda, collision scratch
 __host__ __device__ inline int creature_smem_words(int nb, int nc, int np, int arms, int segs) {
-  return 5 * r4(nb) + 2 * r4(nc) + r4(arms * segs) + r4(arms * segs + arms) + 4 * arms + 3 * r4(np) +
+  return 11 * r4(nb) + 2 * r4(nc) + r4(arms * segs) + r4(arms * segs + arms) + 4 * arms + 3 * r4(np) +
          kr::kMaxCulled / 2;
 }
 
@@ -124,11 +124,11 @@ struct CreatureSmem {
 };
 
 __device__ inline void carve_creature(kr::Island &S, CreatureSmem &X, const TplSmem &P, float *p,
-                                      float *state, const TplDev &td) {
+                                      const TplDev &td) {
   const int mb = r4(td.nb), mc = r4(td.nc), mp = r4(td.np), AS = td.arms * td.segs;
-  // committed state in place in the slot's block (SoA, kBodyPad per field)
-  S.px = state; S.py = state + kBodyPad; S.vx = state + 2 * kBodyPad; S.vy = state + 3 * kBodyPad;
-  S.ang = state + 4 * kBodyPad; S.av = state + 5 * kBodyPad;
+  // committed state, resident for the creature's whole run
+  S.px = p; p += mb; S.py = p; p += mb; S.vx = p; p += mb; S.vy = p; p += mb;
+  S.ang = p; p += mb; S.av = p; p += mb;
   S.ppx = p; p += mb; S.ppy = p; p += mb; S.angP = p; p += mb;
   S.bs = p; p += mb; S.bc = p; p += mb;
   S.lamX = p; p += mc; S.lamY = p; p += mc;
@@ -637,7 +637,7 @@ __device__ void run_creature(const BatchArgs &A, const TplDev &td, int nlv, cons
   const int lane = L.lane;
   kr::Island S;
   CreatureSmem X;
-  carve_creature(S, X, P, base, A.state + (size_t)slot * kStateStride, td);
+  carve_creature(S, X, P, base, td);
   S.nlv = nlv;
   SlotMeta m = A.meta[slot];
   const int steps = min(A.max_steps, m.horizon - m.step);
@@ -646,6 +646,12 @@ __device__ void run_creature(const BatchArgs &A, const TplDev &td, int nlv, cons
   float4 *gst = A.grip + (size_t)slot * KR_BATCH_MAX_ARMS;
   float2 *glam = A.glam + (size_t)slot * KR_BATCH_MAX_ARMS;
   double2 *cdp = A.cd + (size_t)slot * KR_BATCH_MAX_ARMS;
+  // the committed state into shared memory (the slot's block is SoA, kBodyPad per field)
+  float *hbm = A.state + (size_t)slot * kStateStride;
+  for (int i = lane; i < td.nb; i += G) {
+    S.px[i] = hbm[i]; S.py[i] = hbm[kBodyPad + i]; S.vx[i] = hbm[2 * kBodyPad + i];
+    S.vy[i] = hbm[3 * kBodyPad + i]; S.ang[i] = hbm[4 * kBodyPad + i]; S.av[i] = hbm[5 * kBodyPad + i];
+  }
   for (int k = lane; k < td.nc; k += G) { S.lamX[k] = 0.f; S.lamY[k] = 0.f; }
   S.comp_m = m.comp;
   double cd = 0.0;  // reflex cooldown of arm `lane` (its f64 break force stays in cdp)
@@ -783,7 +789,12 @@ __device__ void run_creature(const BatchArgs &A, const TplDev &td, int nlv, cons
     }
     m.step = t + 1;
   }
-  // write back (the committed state is already in place)
+  // write back: the committed state, grips, cooldowns, controls, the meta fields kept in registers
+  L.sync();
+  for (int i = lane; i < td.nb; i += G) {
+    hbm[i] = S.px[i]; hbm[kBodyPad + i] = S.py[i]; hbm[2 * kBodyPad + i] = S.vx[i];
+    hbm[3 * kBodyPad + i] = S.vy[i]; hbm[4 * kBodyPad + i] = S.ang[i]; hbm[5 * kBodyPad + i] = S.av[i];
+  }
   if (lane < arms) {
     const int k = P.arm_grip[lane];
     gst[lane] = reinterpret_cast<const float4 *>(S.anc)[lane];
