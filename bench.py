@@ -44,10 +44,11 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "creature-steps/s at 16k mixed envs, served vs plain launch; p50/p99 rollout ms"
-# DRAM bytes (read + write) of one persistent launch per creature, from an ncu
-# capture of the full 16,384-creature launch (40.86 MB read + 54.30 MB written):
-# the state, grips and slot records in and out, independent of the step count
-NCU_DRAM_BYTES_PER_CREATURE = (40.86e6 + 54.30e6) / 16384
+# DRAM bytes (read + write) of one persistent launch per creature, from a one-kernel,
+# one-launch ncu capture of an 8,192-creature case (20,806,656 B read + 381,184 B written):
+# the committed state, grips, controls and slot records in and out once, independent of the
+# step count
+NCU_DRAM_BYTES_PER_CREATURE = (20806656 + 381184) / 8192
 UNIT = "creature-steps/s"
 
 
@@ -720,9 +721,9 @@ def main():
             roof = {"bound": "fp32", "achieved": achieved / 1e12, "peak": fma_rate / 1e12,
                     "unit": "TFLOP/s", "frac": achieved / fma_rate,
                     "traffic": args.traffic if args.traffic is not None else NCU_DRAM_BYTES_PER_CREATURE * w.n,
-                    "traffic_note": "ncu dram__bytes_read.sum + dram__bytes_write.sum of the full launch "
-                                    "(state, grips and slot records in and out, ~5.8 KB per creature); "
-                                    "algorithmic bytes ~2.5 KB",
+                    "traffic_note": "ncu dram__bytes_read.sum + dram__bytes_write.sum per creature of a one-launch "
+                                    "capture (8,192 creatures: 2,587 B each: state, grips, controls and slot "
+                                    "records in and out once) x the creatures of this launch; algorithmic ~2.5 KB",
                     "ops_per_creature_step": ops, "kernel_ms": kms,
                     "peak_note": "measured dependent-free f32 FMA issue rate (lane-ops/s) of this GPU; "
                                  "MEASURED_PEAKS.json has no f32 figure"}
