@@ -67,7 +67,9 @@ def parse():
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--shape", default="", help="lanes,warps,ctas[,unroll] launch shape (empty: autotune)")
-    ap.add_argument("--chunk", type=int, default=64, help="server env steps per round")
+    ap.add_argument("--chunk", type=int, default=64, help="server env steps per round (two-partition rounds)")
+    ap.add_argument("--slice-ms", type=float, default=50.0,
+                    help="server slices (ms) of the one-partition scheduler; 0: two partitions in rounds")
     ap.add_argument("--no-es", action="store_true", help="skip the ES request stream")
     ap.add_argument("--es-requests", type=int, default=200)
     ap.add_argument("--no-config1", action="store_true", help="skip the 1,024-creature drop-in comparison")
@@ -264,12 +266,13 @@ def reference_arm(args):
     print(json.dumps(line), flush=True)
 
 
-def served_uneven(serve, w, chunk, sessions):
+def served_uneven(serve, w, chunk, sessions, slice_ms=0.0):
     """The mixed workload through the rollout server's C ABI with host
     buffers: one request per creature (its own pose, control stream and
     horizon), all submitted at once; results read back to the host.  The
     server picks each round's launch shape from its partition's live count."""
-    srv = serve.Server(w.maps, 8 << 30, max_slots=w.n, chunk_steps=chunk, policy=False)
+    srv = serve.Server(w.maps, 8 << 30, max_slots=w.n, chunk_steps=chunk if slice_ms <= 0 else 1 << 20,
+                       policy=False, slice_ms=slice_ms)
     xs, ys, an = (np.ascontiguousarray(v, dtype=np.float64) for v in (w.x, w.y, w.angle))
     seeds = np.ascontiguousarray(w.seed, dtype=np.uint32)
     out = []
@@ -288,7 +291,7 @@ def served_uneven(serve, w, chunk, sessions):
     return out
 
 
-def served_es_stream(serve, w, chunk, n_req, rate, seed=0, net=False):
+def served_es_stream(serve, w, chunk, n_req, rate, seed=0, net=False, slice_ms=0.0):
     """ES evaluation requests (mirrored populations 8-512, horizons
     300-3000, body shapes and maps of the mixed workload, fused policy with
     theta ~ N(0, 0.1^2), sigma 0.02) arriving as a Poisson stream.  net: the
@@ -307,8 +310,9 @@ def served_es_stream(serve, w, chunk, n_req, rate, seed=0, net=False):
                                           serve.policy_params(arms, segs)).astype(np.float32),
                          sigma=0.02, seed=k + 1, arrival=t))
     units = sum(r["population"] * r["horizon"] for r in reqs)
-    srv = (serve.Server(w.maps, 8 << 30, max_slots=16384, chunk_steps=chunk, net=True, lights=w.lights) if net
-           else serve.Server(w.maps, 8 << 30, max_slots=16384, chunk_steps=chunk, policy=True))
+    kw = dict(max_slots=16384, chunk_steps=chunk if slice_ms <= 0 else 1 << 20, slice_ms=slice_ms)
+    srv = (serve.Server(w.maps, 8 << 30, net=True, lights=w.lights, **kw) if net
+           else serve.Server(w.maps, 8 << 30, policy=True, **kw))
     t0 = srv.now() + 0.02
     ids = []
     for r in reqs:
@@ -334,19 +338,20 @@ def served_es_stream(serve, w, chunk, n_req, rate, seed=0, net=False):
             "p50_rollout_ms": pct(lat, 50), "p99_rollout_ms": pct(lat, 99),
             "queue_p50_ms": pct(queue, 50), "queue_p99_ms": pct(queue, 99),
             "service_p50_ms": pct(service, 50), "service_p99_ms": pct(service, 99),
-            "slots": st["capacity"], "chunk_steps": chunk,
+            "slots": st["capacity"], "chunk_steps": chunk if slice_ms <= 0 else None,
+            "slice_ms": slice_ms if slice_ms > 0 else None, "rounds_or_slices": st["rounds"],
             "device_kernel_ms_summed": st["device_ms"]}
 
 
-def served_es_streams(serve, w, chunk, n_req, rate, net=False):
+def served_es_streams(serve, w, chunk, n_req, rate, net=False, slice_ms=0.0):
     """The configured stream (Poisson `rate` req/s: it offers more work than
     one GPU delivers, so its latencies grow with the stream's length), and the
     same request mix at a sustainable load: the Poisson rate scaled so that the
     offered creature-steps/s are 0.8 x the rate the first stream delivered
     (the server's capacity under this mix)."""
-    over = served_es_stream(serve, w, chunk, n_req, rate, net=net)
+    over = served_es_stream(serve, w, chunk, n_req, rate, net=net, slice_ms=slice_ms)
     sus_rate = rate * 0.8 * over["delivered_rate"] / over["offered_rate"]
-    sus = served_es_stream(serve, w, chunk, n_req, sus_rate, net=net)
+    sus = served_es_stream(serve, w, chunk, n_req, sus_rate, net=net, slice_ms=slice_ms)
     over["sustainable_load"] = sus
     return over
 
@@ -668,17 +673,26 @@ def main():
 
     # end to end: the workload served through the rollout server's C ABI with
     # host buffers (requests in, results out), p50/p99 rollout latency
-    chunk = args.chunk
-    sess = served_uneven(serve, w, chunk, 1 + max(1, min(args.steps, 2)))[1:]
-    e2e_s = all_max(sum(x["wall_s"] for x in sess))
-    lat = np.concatenate([x["lat"] for x in sess])
+    chunk, sl = args.chunk, args.slice_ms
+
+    def served_line(slice_ms):
+        sess = served_uneven(serve, w, chunk, 1 + max(1, min(args.steps, 2)), slice_ms=slice_ms)[1:]
+        wall = all_max(sum(x["wall_s"] for x in sess))
+        lat = np.concatenate([x["lat"] for x in sess])
+        return {"value": world * units * len(sess) / wall, "unit": UNIT,
+                "h2d_bytes_per_step": int(np.mean([x["h2d"] for x in sess])),
+                "d2h_bytes_per_step": int(np.mean([x["d2h"] for x in sess])),
+                "p50_rollout_ms": float(np.percentile(lat, 50) * 1e3),
+                "p99_rollout_ms": float(np.percentile(lat, 99) * 1e3)}
+
+    e2e = served_line(sl)
     clocks = sampler.stop()
-    e2e = {"value": world * units * len(sess) / e2e_s, "unit": UNIT,
-           "h2d_bytes_per_step": int(np.mean([x["h2d"] for x in sess])),
-           "d2h_bytes_per_step": int(np.mean([x["d2h"] for x in sess])),
-           "form": "served: rollout server C ABI, one request per creature, host buffers in and out",
-           "p50_rollout_ms": float(np.percentile(lat, 50) * 1e3),
-           "p99_rollout_ms": float(np.percentile(lat, 99) * 1e3), "chunk_steps": chunk}
+    e2e["form"] = ("served: rollout server C ABI, one request per creature, host buffers in and out; " +
+                   (f"one partition in preemptible slices of {sl:g} ms" if sl > 0 else
+                    f"two partitions in rounds of {chunk} env steps"))
+    if sl > 0:
+        extra["served_two_partitions"] = dict(served_line(0.0), chunk_steps=chunk,
+                                              form="the same, two partitions in rounds of chunk_steps")
 
     # the engine's own host-buffer API: spawn from host arrays (poses,
     # shapes, horizons, seeds), one persistent launch, the metrics record read
@@ -700,13 +714,14 @@ def main():
             "wall_s": [round(x, 4) for x in reps]}
 
     if not args.no_es and rank == 0:
-        extra["served_es_stream"] = served_es_streams(serve, w, chunk, args.es_requests, 200.0)
+        extra["served_es_stream"] = served_es_streams(serve, w, chunk, args.es_requests, 200.0, slice_ms=sl)
     if not args.no_config1 and rank == 0:
         extra["plain_dropin_1024"] = config1_forms(torch, stream)
     if not args.no_net and rank == 0:
         extra["net_controller"] = net_controller(stream, w)
         if not args.no_es:
-            extra["served_es_stream_net"] = served_es_streams(serve, w, chunk, args.es_requests, 200.0, net=True)
+            extra["served_es_stream_net"] = served_es_streams(serve, w, chunk, args.es_requests, 200.0, net=True,
+                                                              slice_ms=sl)
 
     # roofline: f32 rounding ops per creature-step of the restated f32
     # algorithm (op-counting oracle build) x creature-steps per launch /

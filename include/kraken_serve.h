@@ -12,12 +12,15 @@
  * through its hybrid loop (src/sim/gputrain.js:72-150); here requests arrive
  * at any time and share the GPU:
  *
- *  - continuous batching: the slots are split into two partitions that run
+ *  - continuous batching (slice_ms = 0): the slots are split into two partitions that run
  *    alternately on two streams, chunk_steps env steps per round; a request
  *    that arrives while others run is admitted at the next round of a
  *    partition as soon as slots are free, and its creatures run in the same
  *    launches as everyone else's (one partition's launch fills the tail of
  *    the other's);
+ *  - or (slice_ms > 0) one partition in preemptible slices: a slice runs
+ *    every live creature to its horizon and ends early when an arrived
+ *    request fits the free slots or its time is up; the next slice admits;
  *  - admission against an HBM budget: every slot's device memory (state,
  *    grips, controls, observation ring, policy weights) is accounted for at
  *    creation; the budget fixes the slot count, requests wait in FIFO order
@@ -70,6 +73,15 @@ typedef struct kr_server_desc {
   const double *lights;
   const int32_t *map_light_off;
   const double *map_size;
+  /* > 0: sliced scheduling instead of the two partitions' rounds.  All
+   * slots form one partition and every creature runs to its horizon in one
+   * persistent launch (a slice, at most chunk_steps env steps), which the
+   * server preempts -- through a device word the kernel reads at each env
+   * step -- when an arrived request fits the free slots or slice_ms
+   * milliseconds have passed; it then completes the requests whose
+   * creatures reached their horizons, admits, and launches the next slice.
+   * 0: two partitions alternating chunk_steps rounds (above). */
+  double slice_ms;
 } kr_server_desc;
 
 typedef struct kr_request {

@@ -48,6 +48,15 @@ struct BatchArgs {
   int cpc;               // creature entries per group (W * 32 / G)
   int *queue;            // group counter
   int max_steps;
+  // Preemption (the rollout server's slices; null otherwise): once the word
+  // turns non-zero, CTAs take no further group and every running creature
+  // stops at its next env-step boundary, its state written back as after
+  // any launch.  Each creature's lane 0 loads the word one step ahead, so
+  // the load never stalls a step.
+  const int *stop;
+  // the rollout server's completion counts (null otherwise): a creature
+  // that reaches its horizon adds 1 to tag_done[its SlotMeta::pad]
+  int *tag_done;
   int ctrl_period;
   float *obs;            // capacity x ring x KR_OBS_STRIDE
   int obs_ring;
@@ -669,7 +678,12 @@ __device__ void run_creature(const BatchArgs &A, const TplDev &td, int nlv, cons
   const float4 *rects = A.rects + A.map_off[m.map];
   const int nR = A.map_off[m.map + 1] - A.map_off[m.map];
   const float cull_d = fmaxf(A.map_cull[m.map], td.r_max + 2.f + kr::kCullSlack + 1.f);
+  int halt_next = 0;  // the stop word as loaded during the previous step
   for (int s = 0; s < steps; s++) {
+    if (A.stop) {
+      if (s > 0 && __shfl_sync(L.mask, halt_next, L.base)) break;
+      if (lane == 0) halt_next = *reinterpret_cast<const volatile int *>(A.stop);
+    }
     const int t = m.step;
     // 1. proprioception of the current state
     if (A.obs_ring > 0 || m.ctrl == KR_CTRL_POLICY || (NET && m.ctrl == KR_CTRL_NET)) {
@@ -803,6 +817,7 @@ __device__ void run_creature(const BatchArgs &A, const TplDev &td, int nlv, cons
   }
   float *cout = A.ctrl_cur + (size_t)slot * kCtrlStride;
   for (int q = lane; q < AS + arms; q += G) cout[q] = X.ctrl[q];
+  if (A.tag_done && lane == 0 && m.step >= m.horizon) atomicAdd(A.tag_done + m.pad, 1);
   if (lane == 0) {  // the fields this loop keeps in registers; postStep's are in place
     SlotMeta &g = A.meta[slot];
     g.step = m.step;
@@ -823,7 +838,8 @@ __global__ void __launch_bounds__(32 * kMaxW, 1) batch_kernel(BatchArgs A) {
   const int c = warp * CPW + wl / G;  // creature entry of this lane group
   for (;;) {
     __syncthreads();
-    if (threadIdx.x == 0) s_group = atomicAdd(A.queue, 1);
+    if (threadIdx.x == 0)
+      s_group = A.stop && *reinterpret_cast<const volatile int *>(A.stop) ? A.n_groups : atomicAdd(A.queue, 1);
     __syncthreads();
     const int g = s_group;
     if (g >= A.n_groups) return;
@@ -1286,6 +1302,8 @@ int launch_part(kr_batch *b, Part &p, int max_steps, bool timed) {
   A.rects = b->d_rects; A.map_off = b->d_map_off; A.map_cull = b->d_map_cull;
   A.groups = p.d_groups; A.n_groups = p.n_groups; A.cpc = b->cpc; A.queue = p.d_queue;
   A.max_steps = max_steps;
+  A.stop = p.stop;
+  A.tag_done = p.tag_done;
   A.ctrl_period = std::max(1, b->d.control_period);
   A.obs = b->d_obs; A.obs_ring = b->d.obs_ring;
   A.slip_max = b->d.grip_slip_max; A.cooldown = b->d.grip_cooldown;

@@ -55,7 +55,7 @@ struct SlotMeta {
   float tone;
   int attach_events;  // arms newly anchored after a step
   int ctrl;         // KR_CTRL_* of this slot
-  int pad;
+  int pad;          // the rollout server's request tag (BatchArgs::tag_done)
   double prev_vx, prev_vy;
   double path_len;
   double last_x, last_y;
@@ -236,6 +236,8 @@ struct Part {
   bool dirty = true;
   int *d_queue = nullptr;         // work-queue counter
   cudaStream_t stream = nullptr;  // the engine's stream when null
+  const int *stop = nullptr;      // device word: non-zero ends the launch early (see BatchArgs::stop)
+  int *tag_done = nullptr;        // per tag (SlotMeta::pad): creatures that reached their horizon
   cudaEvent_t staged = nullptr;   // the groups' host-to-device copy has run
   bool staged_pending = false;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;  // launch timing

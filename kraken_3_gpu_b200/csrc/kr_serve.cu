@@ -103,6 +103,12 @@ __global__ void gather_kernel(const SlotMeta *meta, const int *slots, int n, Slo
   out[i] = meta[slots[i]];
 }
 
+// every slot's step counter into one contiguous array (read back after a slice)
+__global__ void steps_kernel(const SlotMeta *meta, int n, int *out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) out[i] = meta[i].step;
+}
+
 struct Req {
   int64_t id = 0;
   kr_request r{};
@@ -144,8 +150,10 @@ uint64_t slot_bytes(const kr_server_desc &d) {
   b += (uint64_t)d.obs_ring * KR_OBS_STRIDE * 4;
   if (d.policy) b += (uint64_t)kMaxParams * 4 + 4;
   if (d.net) b += (uint64_t)kMaxNetParams * 4 + 4 + sizeof(NetRec);
-  // partition staging and work groups (two partitions of half the slots)
+  // partition staging and work groups (two partitions of half the slots, or
+  // one of all slots), and a slice's step-counter readback
   b += (uint64_t)kStateStride * 4 + sizeof(SlotMeta) + 4 + sizeof(PJob) + 4 + sizeof(SlotMeta) + 2 * 4;
+  if (d.slice_ms > 0) b += 8;  // step readback, per-request completion count
   return b;
 }
 
@@ -183,6 +191,19 @@ struct kr_server {
   double creature_steps = 0, device_ms = 0;
   uint64_t h2d_bytes = 0, d2h_bytes = 0;
   std::chrono::steady_clock::time_point t0;
+  // sliced scheduling (slice_ms > 0): one partition, preemptible slices
+  bool sliced = false;
+  double slice_s = 0;
+  int *d_stop = nullptr;          // the kernel's stop word
+  int *h_flag = nullptr;          // pinned {0, 1}: the values the stop word is set to
+  int *h_steps = nullptr;         // pinned: every slot's step counter after a slice
+  int *d_steps = nullptr;
+  cudaStream_t ctl = nullptr;     // the stop word's copies while a slice runs
+  double slice_t0 = 0;
+  bool stop_sent = false;
+  int *d_done = nullptr;          // per request tag (its first slot): creatures that reached their horizon
+  int *h_done = nullptr;          // pinned copy of d_done, polled while a request waits
+  double polled = -1;             // server time of the last poll
   std::string err;
 
   double now() const {
@@ -208,6 +229,7 @@ int check_desc(const kr_server_desc *d, std::string *why) {
   if (d->max_slots < 0) { *why = "max_slots < 0"; return KR_ERR_INVALID; }
   if (d->n_maps < 1 || !d->rects || !d->map_rect_off) { *why = "need at least one map"; return KR_ERR_INVALID; }
   if (d->policy && d->net) { *why = "policy and net are exclusive (theta is one or the other)"; return KR_ERR_INVALID; }
+  if (!(d->slice_ms >= 0 && d->slice_ms < 1e9)) { *why = "slice_ms outside [0, 1e9)"; return KR_ERR_INVALID; }
   return KR_OK;
 }
 
@@ -321,6 +343,7 @@ int admit(kr_server *S, int p) {
       std::copy(init.pose.begin() + (size_t)i * kStateStride, init.pose.begin() + (size_t)(i + 1) * kStateStride,
                 st.h_pose + (size_t)n_new * kStateStride);
       st.h_meta[n_new] = init.meta[i];
+      st.h_meta[n_new].pad = q.slots[0];  // the request's tag: its first slot
       st.h_slots[n_new] = s;
       if (pol) {
         PJob &j = st.h_jobs[n_new];
@@ -340,6 +363,10 @@ int admit(kr_server *S, int p) {
       std::copy(q.theta.begin(), q.theta.end(), st.h_theta + theta_off);
       theta_off += (int)q.theta.size();
       n_theta++;
+    }
+    if (S->d_done) {  // the request's completion count starts at 0 (its tag may be a reused slot)
+      cudaError_t ez = cudaMemsetAsync(S->d_done + q.slots[0], 0, sizeof(int), stream);
+      if (ez != cudaSuccess) return S->cuda_fail(ez, "completion count");
     }
     q.part = p;
     q.admitted = t;
@@ -417,6 +444,126 @@ int run_round(kr_server *S, int p) {
   return KR_OK;
 }
 
+// Sliced scheduling.  After a slice: every slot's step counter from the
+// device (the slice may have been cut short, so the host does not know how
+// far each creature got), the requests whose creatures all reached their
+// horizons gathered and completed (finish_round), their slots freed.
+int finish_slice(kr_server *S) {
+  Round &R = S->round[0];
+  Part &P = S->parts[0];
+  Stage &st = S->stage[0];
+  cudaStream_t stream = S->streams[0];
+  steps_kernel<<<(S->capacity + 255) / 256, 256, 0, stream>>>(S->b->d_meta, S->capacity, S->d_steps);
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(S->h_steps, S->d_steps, (size_t)S->capacity * sizeof(int), cudaMemcpyDeviceToHost, stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+  if (e != cudaSuccess) return S->cuda_fail(e, "slice step counters");
+  S->d2h_bytes += (uint64_t)S->capacity * sizeof(int);
+  for (int s : P.slots) {
+    SlotMeta &m = S->b->h_meta[s];
+    const int done = std::min(S->h_steps[s], m.horizon);
+    S->creature_steps += done - m.step;
+    m.step = done;
+    S->b->h_remaining[s] = m.horizon - done;
+  }
+  int n_res = 0;
+  for (int64_t id : S->active[0]) {
+    Req &q = S->reqs[id];
+    bool ended = true;
+    for (int s : q.slots)
+      if (S->b->h_remaining[s] > 0) { ended = false; break; }
+    if (!ended) continue;
+    R.completing.push_back(id);
+    for (int s : q.slots) st.h_rslots[n_res++] = s;
+  }
+  if (n_res > 0) {
+    e = cudaMemcpyAsync(st.d_rslots, st.h_rslots, (size_t)n_res * sizeof(int), cudaMemcpyHostToDevice, stream);
+    if (e == cudaSuccess) {
+      gather_kernel<<<(n_res + 127) / 128, 128, 0, stream>>>(S->b->d_meta, st.d_rslots, n_res, st.d_res);
+      e = cudaGetLastError();
+    }
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(st.h_res, st.d_res, (size_t)n_res * sizeof(SlotMeta), cudaMemcpyDeviceToHost, stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+    if (e != cudaSuccess) return S->cuda_fail(e, "slice results");
+    S->h2d_bytes += (uint64_t)n_res * sizeof(int);
+    S->d2h_bytes += (uint64_t)n_res * sizeof(SlotMeta);
+  }
+  finish_round(S, 0);
+  return KR_OK;
+}
+
+// true when the queue's first request has arrived and fits the free slots
+// plus the slots of the running requests whose creatures have all reached
+// their horizons by now (the kernel counts them per request; the counts are
+// polled at most once per millisecond, only while a request waits)
+bool admissible(kr_server *S) {
+  if (S->queue.empty()) return false;
+  const Req &q = S->reqs.at(S->queue.front());
+  const double t = S->now();
+  if (q.arrival > t) return false;
+  long fit = (long)S->free_slots.size();
+  if (q.r.population <= fit) return true;
+  if (!S->round[0].inflight || t - S->polled < 1e-3) return false;
+  S->polled = t;
+  if (cudaMemcpyAsync(S->h_done, S->d_done, (size_t)S->capacity * sizeof(int), cudaMemcpyDeviceToHost, S->ctl) !=
+          cudaSuccess ||
+      cudaStreamSynchronize(S->ctl) != cudaSuccess)
+    return false;
+  for (int64_t id : S->active[0]) {
+    const Req &a = S->reqs.at(id);
+    if (S->h_done[a.slots[0]] >= (int)a.slots.size()) fit += (long)a.slots.size();
+  }
+  return q.r.population <= fit;
+}
+
+// One step of sliced scheduling: while a slice runs, preempt it if an
+// arrived request fits the free slots or its time is up (otherwise return
+// at once); after it, complete, admit and launch the next slice, every live
+// creature up to its horizon (at most chunk_steps env steps).
+int run_slice(kr_server *S) {
+  Round &R = S->round[0];
+  cudaError_t e;
+  if (R.inflight) {
+    if (!S->stop_sent) {
+      if (!admissible(S) && S->now() - S->slice_t0 < S->slice_s) {
+        e = cudaEventQuery(R.done);
+        if (e == cudaErrorNotReady) return KR_OK;
+        if (e != cudaSuccess) return S->cuda_fail(e, "slice query");
+      } else {
+        e = cudaMemcpyAsync(S->d_stop, S->h_flag + 1, sizeof(int), cudaMemcpyHostToDevice, S->ctl);
+        if (e != cudaSuccess) return S->cuda_fail(e, "slice stop");
+        S->stop_sent = true;
+      }
+    }
+    e = cudaEventSynchronize(R.done);
+    // the stop word's copy has landed before the next slice clears it
+    if (e == cudaSuccess && S->stop_sent) e = cudaStreamSynchronize(S->ctl);
+    if (e != cudaSuccess) return S->cuda_fail(e, "slice wait");
+    int rc = finish_slice(S);
+    if (rc != KR_OK) return rc;
+  }
+  int rc = admit(S, 0);
+  if (rc != KR_OK) return rc;
+  Part &P = S->parts[0];
+  if (P.slots.empty()) return KR_OK;
+  cudaStream_t stream = S->streams[0];
+  e = cudaMemcpyAsync(S->d_stop, S->h_flag, sizeof(int), cudaMemcpyHostToDevice, stream);
+  if (e != cudaSuccess) return S->cuda_fail(e, "slice start");
+  P.dirty = true;
+  rc = launch_part(S->b, P, S->chunk, true);
+  if (rc != KR_OK) return S->batch_fail(rc);
+  R.timed = true;
+  e = cudaEventRecord(R.done, stream);
+  if (e != cudaSuccess) return S->cuda_fail(e, "slice record");
+  R.inflight = true;
+  S->stop_sent = false;
+  S->slice_t0 = S->now();
+  S->rounds++;
+  return KR_OK;
+}
+
 bool busy(const kr_server *S) {
   return !S->queue.empty() || !S->active[0].empty() || !S->active[1].empty() || S->round[0].inflight ||
          S->round[1].inflight;
@@ -469,7 +616,9 @@ extern "C" int kr_server_create(const kr_server_desc *d, kr_server **out) {
   S->d.map_size = nullptr;
   S->b = b;
   S->capacity = cap;
-  S->part_cap = cap / 2;
+  S->sliced = d->slice_ms > 0;
+  S->slice_s = d->slice_ms * 1e-3;
+  S->part_cap = S->sliced ? cap : cap / 2;
   S->chunk = d->chunk_steps;
   S->bytes_per_slot = ps;
   S->t0 = std::chrono::steady_clock::now();
@@ -507,7 +656,21 @@ extern "C" int kr_server_create(const kr_server_desc *d, kr_server **out) {
     b->h_pw_arms.assign(cap, -1);
     if (e != cudaSuccess) { S->cuda_fail(e, "policy weights"); return bail(KR_ERR_CUDA); }
   }
-  for (int p = 0; p < 2; p++) {
+  if (S->sliced) {
+    if (e == cudaSuccess) e = cudaMalloc(&S->d_stop, sizeof(int));
+    if (e == cudaSuccess) e = cudaMemset(S->d_stop, 0, sizeof(int));
+    if (e == cudaSuccess) e = cudaMallocHost(&S->h_flag, 2 * sizeof(int));
+    if (e == cudaSuccess) { S->h_flag[0] = 0; S->h_flag[1] = 1; }
+    if (e == cudaSuccess) e = cudaMallocHost(&S->h_steps, (size_t)cap * sizeof(int));
+    if (e == cudaSuccess) e = cudaMalloc(&S->d_steps, (size_t)cap * sizeof(int));
+    if (e == cudaSuccess) e = cudaMalloc(&S->d_done, (size_t)cap * sizeof(int));
+    if (e == cudaSuccess) e = cudaMemset(S->d_done, 0, (size_t)cap * sizeof(int));
+    if (e == cudaSuccess) e = cudaMallocHost(&S->h_done, (size_t)cap * sizeof(int));
+    S->parts[0].tag_done = S->d_done;
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&S->ctl, cudaStreamNonBlocking);
+    S->parts[0].stop = S->d_stop;
+  }
+  for (int p = 0; p < (S->sliced ? 1 : 2); p++) {
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&S->streams[p], cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&S->round[p].done, cudaEventDisableTiming);
     S->parts[p].all = false;
@@ -539,7 +702,7 @@ extern "C" int kr_server_submit(kr_server *S, const kr_request *r, int64_t *id) 
   if (!S || !r) return KR_ERR_INVALID;
   if (r->population < 1 || r->population > S->part_cap)
     return S->fail(KR_ERR_CAPACITY, "population " + std::to_string(r->population) + " outside 1.." +
-                                        std::to_string(S->part_cap) + " (half the slots)");
+                                        std::to_string(S->part_cap) + (S->sliced ? " (the slots)" : " (half the slots)"));
   if (r->horizon < 1) return S->fail(KR_ERR_INVALID, "horizon < 1");
   if (r->first_individual < 0 || (r->first_individual & 1))
     return S->fail(KR_ERR_INVALID, "first_individual must be even and >= 0");
@@ -602,9 +765,14 @@ extern "C" int kr_server_submit_batch(kr_server *S, const kr_request *reqs, int3
 
 extern "C" int kr_server_pump(kr_server *S, int32_t *busy_out) {
   if (!S) return KR_ERR_INVALID;
-  const int p = S->next;
-  S->next ^= 1;
-  int rc = run_round(S, p);
+  int rc;
+  if (S->sliced) {
+    rc = run_slice(S);
+  } else {
+    const int p = S->next;
+    S->next ^= 1;
+    rc = run_round(S, p);
+  }
   if (busy_out) *busy_out = busy(S) ? 1 : 0;
   return rc;
 }
@@ -619,6 +787,9 @@ extern "C" int kr_server_drain(kr_server *S) {
     }
     int rc = kr_server_pump(S, nullptr);
     if (rc != KR_OK) return rc;
+    // a slice that runs on with nothing to preempt it: look again shortly
+    if (S->sliced && S->round[0].inflight && !S->stop_sent)
+      std::this_thread::sleep_for(std::chrono::microseconds(100));
   }
   return KR_OK;
 }
@@ -715,6 +886,13 @@ extern "C" void kr_server_destroy(kr_server *S) {
     if (S->round[p].done) cudaEventDestroy(S->round[p].done);
     if (S->streams[p]) cudaStreamDestroy(S->streams[p]);
   }
+  if (S->d_stop) cudaFree(S->d_stop);
+  if (S->h_flag) cudaFreeHost(S->h_flag);
+  if (S->h_steps) cudaFreeHost(S->h_steps);
+  if (S->d_steps) cudaFree(S->d_steps);
+  if (S->d_done) cudaFree(S->d_done);
+  if (S->h_done) cudaFreeHost(S->h_done);
+  if (S->ctl) cudaStreamDestroy(S->ctl);
   if (S->b) kr_batch_destroy(S->b);
   delete S;
 }

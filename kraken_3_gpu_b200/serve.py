@@ -38,7 +38,7 @@ class ServerDesc(C.Structure):
                 ("lanes_per_creature", C.c_int32), ("warps_per_cta", C.c_int32),
                 ("ctas_per_sm", C.c_int32), ("grip_slip_max", C.c_double),
                 ("grip_cooldown", C.c_double), ("net", C.c_int32), ("lights", _F64P),
-                ("map_light_off", _I32P), ("map_size", _F64P)]
+                ("map_light_off", _I32P), ("map_size", _F64P), ("slice_ms", C.c_double)]
 
 
 class Request(C.Structure):
@@ -111,7 +111,7 @@ def _check(rc, h):
 
 def _desc(maps, hbm_budget, max_slots, obs_ring, chunk_steps, policy, lanes, warps, ctas,
           substeps, iterations, h, lin_drag, ang_drag, max_speed, max_ang_speed, grip_slip_max,
-          grip_cooldown, net, lights, map_size):
+          grip_cooldown, net, lights, map_size, slice_ms):
     rect_list = [np.asarray(m, dtype=np.float32).reshape(-1, 4) for m in maps]
     off = np.zeros(len(rect_list) + 1, dtype=np.int32)
     for i, r in enumerate(rect_list):
@@ -123,6 +123,7 @@ def _desc(maps, hbm_budget, max_slots, obs_ring, chunk_steps, policy, lanes, war
                    len(rect_list), rects.ctypes.data_as(_F32P), off.ctypes.data_as(_I32P),
                    int(hbm_budget), int(max_slots), int(obs_ring), int(chunk_steps), int(policy),
                    int(lanes), int(warps), int(ctas), grip_slip_max, grip_cooldown)
+    d.slice_ms = float(slice_ms)
     keep = [rects, off]
     if net:
         d.net = 1
@@ -146,7 +147,7 @@ def _desc(maps, hbm_budget, max_slots, obs_ring, chunk_steps, policy, lanes, war
 _DEFAULTS = dict(max_slots=0, obs_ring=0, chunk_steps=32, policy=True, lanes=0, warps=0, ctas=0,
                  substeps=2, iterations=4, h=1 / 120, lin_drag=3.0, ang_drag=3.0, max_speed=360.0,
                  max_ang_speed=18.0, grip_slip_max=150.0, grip_cooldown=0.05, net=False, lights=None,
-                 map_size=(1440.0, 810.0))
+                 map_size=(1440.0, 810.0), slice_ms=0.0)
 
 
 def plan(maps, hbm_budget, **kw):

@@ -1,5 +1,8 @@
 """GPU tests of the rollout server: device eps, weights, results alone vs in
-the mix, queued admission under an HBM budget, repeatability."""
+the mix, queued admission under an HBM budget, repeatability -- under both
+schedulers: two partitions in alternating rounds (slice_ms = 0) and one
+partition in preemptible slices (slice_ms > 0; small slices here, so that
+slices are cut by arrivals and by time)."""
 import numpy as np
 import pytest
 
@@ -68,8 +71,12 @@ def test_server_equals_engine_with_explicit_mirrored_weights():
     assert not np.array_equal(got[0], got[1])  # the mirrored pair differs
 
 
-def _run(maps, reqs, max_slots, stagger=0.0, chunk=16, obs_ring=0):
-    srv = serve.Server(maps, 2 << 30, max_slots=max_slots, chunk_steps=chunk, obs_ring=obs_ring)
+MODES = [dict(slice_ms=0.0, chunk=16), dict(slice_ms=1.0, chunk=1 << 20)]
+
+
+def _run(maps, reqs, max_slots, stagger=0.0, chunk=16, obs_ring=0, slice_ms=0.0):
+    srv = serve.Server(maps, 2 << 30, max_slots=max_slots, chunk_steps=chunk, obs_ring=obs_ring,
+                       slice_ms=slice_ms)
     t0 = srv.now() + 0.01
     ids = [srv.submit(**r, arrival=t0 + k * stagger) for k, r in enumerate(reqs)]
     srv.drain()
@@ -79,11 +86,12 @@ def _run(maps, reqs, max_slots, stagger=0.0, chunk=16, obs_ring=0):
     return out, st
 
 
-def test_each_request_same_alone_and_in_the_mix():
+@pytest.mark.parametrize("mode", MODES)
+def test_each_request_same_alone_and_in_the_mix(mode):
     maps = _maps()
     reqs = _requests(maps)
-    alone = [_run(maps, [r], max_slots=64)[0][0] for r in reqs]
-    mixed, st = _run(maps, reqs, max_slots=96, stagger=0.004)
+    alone = [_run(maps, [r], max_slots=64, **mode)[0][0] for r in reqs]
+    mixed, st = _run(maps, reqs, max_slots=96, stagger=0.004, **mode)
     assert st["completed"] == len(reqs)
     for a, m in zip(alone, mixed):
         assert np.array_equal(a["results"], m["results"])
@@ -95,13 +103,14 @@ def test_each_request_same_alone_and_in_the_mix():
         assert m["arrival"] <= m["admitted"] <= m["completed"]
 
 
-def test_queued_admission_under_budget_bit_identical_three_runs():
+@pytest.mark.parametrize("mode", MODES)
+def test_queued_admission_under_budget_bit_identical_three_runs(mode):
     maps = _maps()
     reqs = _requests(maps, seed=3, n=16, pop_max=16, h_max=120)
     for r in reqs:
         r["theta"] = None  # control streams, as the memory-bound configuration
     budget_slots = 32
-    runs = [_run(maps, reqs, max_slots=budget_slots, obs_ring=128) for _ in range(3)]
+    runs = [_run(maps, reqs, max_slots=budget_slots, obs_ring=128, **mode) for _ in range(3)]
     total = sum(r["population"] for r in reqs)
     assert total > budget_slots
     for out, st in runs:
@@ -126,16 +135,20 @@ def test_server_rejects_bad_requests():
     srv.close()
 
 
-def test_served_uneven_workload_equals_batched_engine():
+@pytest.mark.parametrize("mode", [dict(slice_ms=0.0, chunk_steps=24), dict(slice_ms=0.5, chunk_steps=1 << 20),
+                                  dict(slice_ms=1000.0, chunk_steps=1 << 20)])
+def test_served_uneven_workload_equals_batched_engine(mode):
     """The mixed workload submitted as requests (one per creature, its own
-    pose, control stream and horizon) gives the batched engine's results."""
+    pose, control stream and horizon) gives the batched engine's results --
+    with slices cut every half millisecond, and with slices that run until
+    an arrival fits (here: a creature's slot frees only when its slice ends)."""
     w = workloads.uneven(n=60, n_maps=5, seed=13, h_min=30, h_max=120)
     eng = batch.BatchEngine(w.maps, w.n)
     workloads.spawn_all(eng, w)
     eng.run(int(w.horizon.max()))
     want = eng.read_metrics()
     eng.close()
-    srv = serve.Server(w.maps, 1 << 30, max_slots=40, chunk_steps=24, policy=False)
+    srv = serve.Server(w.maps, 1 << 30, max_slots=40, policy=False, **mode)
     half = w.n // 2
     ids = []
     for i in range(half):  # one call per request
