@@ -74,6 +74,7 @@ def parse():
     ap.add_argument("--es-requests", type=int, default=200)
     ap.add_argument("--no-config1", action="store_true", help="skip the 1,024-creature drop-in comparison")
     ap.add_argument("--no-net", action="store_true", help="skip the reference-net controller rollout")
+    ap.add_argument("--no-config4", action="store_true", help="skip the 65,536-creature memory-bound serving case")
     ap.add_argument("--net-only", action="store_true",
                     help="only the reference-net controller rollout of the workload (one JSON line)")
     ap.add_argument("--traffic", type=float, default=None,
@@ -286,7 +287,8 @@ def served_uneven(serve, w, chunk, sessions, slice_ms=0.0):
         s1 = srv.stats()
         out.append({"wall_s": wall, "lat": times[:, 2] - times[:, 0],
                     "h2d": s1["h2d_bytes"] - s0["h2d_bytes"], "d2h": s1["d2h_bytes"] - s0["d2h_bytes"],
-                    "device_ms": s1["device_ms"] - s0["device_ms"]})
+                    "device_ms": s1["device_ms"] - s0["device_ms"],
+                    "host_gap_ms": s1["host_gap_ms"] - s0["host_gap_ms"], "slices": s1["rounds"] - s0["rounds"]})
     srv.close()
     return out
 
@@ -340,6 +342,7 @@ def served_es_stream(serve, w, chunk, n_req, rate, seed=0, net=False, slice_ms=0
             "service_p50_ms": pct(service, 50), "service_p99_ms": pct(service, 99),
             "slots": st["capacity"], "chunk_steps": chunk if slice_ms <= 0 else None,
             "slice_ms": slice_ms if slice_ms > 0 else None, "rounds_or_slices": st["rounds"],
+            "host_gap_ms": st["host_gap_ms"],
             "device_kernel_ms_summed": st["device_ms"]}
 
 
@@ -508,6 +511,37 @@ def config1_forms(torch, stream, steps=1000):
                                             shape["ctas_per_sm"], shape["substep_unroll"]]},
             "persistent_over_dropin_kernel": (n * steps / (pers_ms / 1000.0)) / (n * steps / (kernel_ms / 1000.0)),
             "final_mantles_bit_identical": same}
+
+
+def config4_memory_bound(serve, slice_ms):
+    """The memory-bound configuration: 65,536 creatures of the mixed bodies
+    (64 maps, horizons U{200..4096}), each with a 128-step observation ring,
+    one request per creature submitted at once to a server whose slot count
+    comes from its HBM budget: 8 GB (every creature fits: 33.5 KB per slot
+    with the ring) and 1.5 GB (about 47,800 slots, so requests queue for
+    slots freed by completed ones).  Wall clock per run, results copied back."""
+    from kraken_3_gpu_b200 import workloads
+    w = workloads.uneven(n=65536, n_maps=64, seed=4, h_min=200, h_max=4096)
+    xs, ys, an = (np.ascontiguousarray(v, dtype=np.float64) for v in (w.x, w.y, w.angle))
+    out = {"creatures": w.n, "creature_steps": w.creature_steps(), "obs_ring": 128}
+    for name, budget in (("budget_8GB", 8 << 30), ("budget_1.5GB", int(1.5 * (1 << 30)))):
+        srv = serve.Server(w.maps, budget, policy=False, obs_ring=128, chunk_steps=1 << 20 if slice_ms > 0 else 128,
+                           slice_ms=slice_ms)
+        t0 = time.perf_counter()
+        ids = srv.submit_many(w.horizon, w.arms, w.segs, w.map_id, xs, ys, an, control_seeds=w.seed)
+        srv.drain()
+        res, times = srv.results_many(ids, release=True)
+        wall = time.perf_counter() - t0
+        st = srv.stats()
+        srv.close()
+        lat = times[:, 2] - times[:, 0]
+        out[name] = {"value": w.creature_steps() / wall, "unit": UNIT, "wall_s": wall, "slots": st["capacity"],
+                     # requests not admitted with the first ones: they waited for freed slots
+                     "queued_requests": int(np.sum(times[:, 1] > times[:, 1].min() + 1e-3)),
+                     "p50_rollout_ms": float(np.percentile(lat, 50) * 1e3),
+                     "p99_rollout_ms": float(np.percentile(lat, 99) * 1e3), "slices_or_rounds": st["rounds"],
+                     "host_gap_ms": st["host_gap_ms"], "device_bytes": st["device_bytes"]}
+    return out
 
 
 def net_controller(stream, w, seed=7):
@@ -683,7 +717,9 @@ def main():
                 "h2d_bytes_per_step": int(np.mean([x["h2d"] for x in sess])),
                 "d2h_bytes_per_step": int(np.mean([x["d2h"] for x in sess])),
                 "p50_rollout_ms": float(np.percentile(lat, 50) * 1e3),
-                "p99_rollout_ms": float(np.percentile(lat, 99) * 1e3)}
+                "p99_rollout_ms": float(np.percentile(lat, 99) * 1e3),
+                "slices_or_rounds_per_session": float(np.mean([x["slices"] for x in sess])),
+                "host_gap_ms_per_session": float(np.mean([x["host_gap_ms"] for x in sess]))}
 
     e2e = served_line(sl)
     clocks = sampler.stop()
@@ -717,6 +753,8 @@ def main():
         extra["served_es_stream"] = served_es_streams(serve, w, chunk, args.es_requests, 200.0, slice_ms=sl)
     if not args.no_config1 and rank == 0:
         extra["plain_dropin_1024"] = config1_forms(torch, stream)
+    if not args.no_config4 and rank == 0:
+        extra["memory_bound_65k"] = config4_memory_bound(serve, sl)
     if not args.no_net and rank == 0:
         extra["net_controller"] = net_controller(stream, w)
         if not args.no_es:

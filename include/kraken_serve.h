@@ -77,8 +77,10 @@ typedef struct kr_server_desc {
    * slots form one partition and every creature runs to its horizon in one
    * persistent launch (a slice, at most chunk_steps env steps), which the
    * server preempts -- through a device word the kernel reads at each env
-   * step -- when an arrived request fits the free slots or slice_ms
-   * milliseconds have passed; it then completes the requests whose
+   * step -- when an arrived request fits the free slots (counting requests
+   * the kernel reports complete; not before the slice has run 3 times the
+   * host's time between slices) or slice_ms milliseconds (at least 10 such
+   * host gaps) have passed; it then completes the requests whose
    * creatures reached their horizons, admits, and launches the next slice.
    * 0: two partitions alternating chunk_steps rounds (above). */
   double slice_ms;
@@ -125,6 +127,7 @@ typedef struct kr_server_stats {
   uint64_t device_bytes;        /* device bytes the server holds */
   uint64_t h2d_bytes;           /* host-to-device bytes copied so far (spawns, weights, schedules) */
   uint64_t d2h_bytes;           /* device-to-host bytes copied so far (results) */
+  double host_gap_ms;           /* sliced scheduling: summed host time between a slice's end and the next launch */
 } kr_server_stats;
 
 /* The slot count and per-slot bytes a descriptor yields (no device needed). */

@@ -1149,10 +1149,21 @@ int build_groups(kr_batch *b, Part &p, int max_steps) {
       return b->fail(KR_ERR_STATE, "slot " + std::to_string(s) + ": its individual's weights were laid out for "
                                        "another body shape (kr_batch_set_policy after the spawn)");
   }
-  std::stable_sort(live.begin(), live.end(), [&](int x, int y) {
-    if (b->h_meta[x].tpl != b->h_meta[y].tpl) return b->h_meta[x].tpl < b->h_meta[y].tpl;
-    return rem[x] > rem[y];
-  });
+  // by template, then longest remaining first, ties in slot-list order: one
+  // 64-bit key per live slot (template 8 bits, inverted remaining steps 31
+  // bits, list position 24 bits), sorted without touching the slot records
+  {
+    std::vector<uint64_t> keys(live.size());
+    for (size_t i = 0; i < live.size(); i++) {
+      const int s = live[i];
+      keys[i] = ((uint64_t)(uint32_t)b->h_meta[s].tpl << 55) | ((uint64_t)(0x7fffffffu - (uint32_t)rem[s]) << 24) |
+                (uint64_t)i;
+    }
+    std::sort(keys.begin(), keys.end());
+    std::vector<int> sorted(live.size());
+    for (size_t i = 0; i < live.size(); i++) sorted[i] = live[keys[i] & 0xffffffu];
+    live.swap(sorted);
+  }
   // Group size per template.  When the live creatures fill less than one
   // wave of the resident CTAs, smaller groups (whole warps) spread them over
   // every SM instead of packing a few SMs.

@@ -204,6 +204,8 @@ struct kr_server {
   int *d_done = nullptr;          // per request tag (its first slot): creatures that reached their horizon
   int *h_done = nullptr;          // pinned copy of d_done, polled while a request waits
   double polled = -1;             // server time of the last poll
+  double gap_s = 0;               // host time between a slice's end and the next launch (running mean)
+  double gap_sum = 0;             // ... summed
   std::string err;
 
   double now() const {
@@ -503,6 +505,9 @@ bool admissible(kr_server *S) {
   const Req &q = S->reqs.at(S->queue.front());
   const double t = S->now();
   if (q.arrival > t) return false;
+  // a slice runs at least 3 host gaps before an admission cuts it, so that
+  // the GPU idles at most a quarter of the time however often requests come
+  if (S->round[0].inflight && t - S->slice_t0 < 3 * S->gap_s) return false;
   long fit = (long)S->free_slots.size();
   if (q.r.population <= fit) return true;
   if (!S->round[0].inflight || t - S->polled < 1e-3) return false;
@@ -527,7 +532,9 @@ int run_slice(kr_server *S) {
   cudaError_t e;
   if (R.inflight) {
     if (!S->stop_sent) {
-      if (!admissible(S) && S->now() - S->slice_t0 < S->slice_s) {
+      // the time slice: slice_ms, or 10 host gaps when those are longer (large
+      // populations), so that the GPU idles at most about a tenth of the time
+      if (!admissible(S) && S->now() - S->slice_t0 < std::max(S->slice_s, 10 * S->gap_s)) {
         e = cudaEventQuery(R.done);
         if (e == cudaErrorNotReady) return KR_OK;
         if (e != cudaSuccess) return S->cuda_fail(e, "slice query");
@@ -537,10 +544,14 @@ int run_slice(kr_server *S) {
         S->stop_sent = true;
       }
     }
+  }
+  double ended = -1;
+  if (R.inflight) {
     e = cudaEventSynchronize(R.done);
     // the stop word's copy has landed before the next slice clears it
     if (e == cudaSuccess && S->stop_sent) e = cudaStreamSynchronize(S->ctl);
     if (e != cudaSuccess) return S->cuda_fail(e, "slice wait");
+    ended = S->now();
     int rc = finish_slice(S);
     if (rc != KR_OK) return rc;
   }
@@ -560,6 +571,11 @@ int run_slice(kr_server *S) {
   R.inflight = true;
   S->stop_sent = false;
   S->slice_t0 = S->now();
+  if (ended >= 0) {
+    const double gap = S->slice_t0 - ended;
+    S->gap_s = S->gap_s > 0 ? 0.75 * S->gap_s + 0.25 * gap : gap;
+    S->gap_sum += gap;
+  }
   S->rounds++;
   return KR_OK;
 }
@@ -859,6 +875,7 @@ extern "C" int kr_server_get_stats(kr_server *S, kr_server_stats *o) {
   o->device_bytes = S->device_bytes;
   o->h2d_bytes = S->h2d_bytes + S->parts[0].h2d_bytes + S->parts[1].h2d_bytes;
   o->d2h_bytes = S->d2h_bytes;
+  o->host_gap_ms = S->gap_sum * 1e3;
   return KR_OK;
 }
 

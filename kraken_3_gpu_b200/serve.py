@@ -66,7 +66,7 @@ class Stats(C.Structure):
                 ("queued", C.c_int32), ("submitted", C.c_int64), ("admitted", C.c_int64),
                 ("completed", C.c_int64), ("rounds", C.c_int64), ("creature_steps", C.c_double),
                 ("device_ms", C.c_double), ("bytes_per_slot", C.c_uint64), ("device_bytes", C.c_uint64),
-                ("h2d_bytes", C.c_uint64), ("d2h_bytes", C.c_uint64)]
+                ("h2d_bytes", C.c_uint64), ("d2h_bytes", C.c_uint64), ("host_gap_ms", C.c_double)]
 
 
 _bound = False
