@@ -359,102 +359,6 @@ def served_es_streams(serve, w, chunk, n_req, rate, net=False, slice_ms=0.0):
     return over
 
 
-class HybridLoop:
-    """The reference's plain loop (src/sim/gputrain.js:72-128: per env step
-    applyControl with the suction-cup reflex on the mirrored state,
-    uploadControls, one step, download + mirror) through the drop-in C ABI,
-    for many creatures of one body shape at once: the host side runs over
-    numpy arrays -- control-stream draws (mulberry32, map.js:11-20), clamped
-    motor targets, the reflex of core.js:199-218 (slip gate, attach at the tip
-    point, break force, release) and packControls' fields -- so that the
-    loop's cost is the boundary's, not Python's."""
-
-    def __init__(self, w, stream_ptr):
-        from kraken_3_gpu_b200 import _native, core, gpuworld, kraken
-        self.n = w.n
-        self.sim = core.create_sim(seed=1, creatures=w.n, poses=list(zip(w.x, w.y, w.angle)))
-        world, crs = self.sim["world"], self.sim["creatures"]
-        self.g = gpuworld.create(world, self.sim["map"])
-        gpuworld.upload(self.g)
-        self.L, self.h = _native.lib(), self.g.handle
-        _native.check(self.L.kr_set_stream(self.h, C.c_void_p(stream_ptr)), self.h)
-        k_of = {id(c): k for k, c in enumerate(world.constraints)}
-        self.motors = np.array([[k_of[id(m)] for a in c.arms for m in a.motors] for c in crs])
-        self.grips = np.array([[k_of[id(a.grip)] for a in c.arms] for c in crs])
-        self.tips = np.array([[a.tip for a in c.arms] for c in crs])
-        self.A, self.S = len(crs[0].arms), len(crs[0].arms[0].motors)
-        B = kraken.BODY
-        self.lim = np.where(np.arange(self.A * self.S) % self.S == 0, B["shoulderLimit"], B["jointLimit"])
-        self.half_seg = B["segLen"] * 0.5
-        self.cons = self.g.consData.reshape(-1, 20)
-        self.consu = self.g.consData.view(np.uint32).reshape(-1, 20)
-        self.body = self.g.bodyData.reshape(-1, 12)
-        self.cons[self.motors, 8] = kraken.tone_to_compliance(0.5)
-        self.rng = np.ascontiguousarray(w.seed, dtype=np.uint32).copy()
-        self.targets = np.zeros((self.n, self.A * self.S))
-        self.adh = np.zeros((self.n, self.A))
-        self.cd = np.zeros((self.n, self.A))
-        self.dt = world.h * world.substeps
-        self.cp = self.g.consData.view(np.uint32).ctypes.data_as(C.POINTER(C.c_uint32))
-        self.bp = self.g.bodyData.ctypes.data_as(C.POINTER(C.c_float))
-        self.t = 0
-        self._check(self.L.kr_download(self.h, self.bp, self.cp))  # the mirrored f32 state
-
-    def _check(self, rc):
-        from kraken_3_gpu_b200 import _native
-        _native.check(rc, self.h)
-
-    def _draw(self):
-        r = np.empty((self.n, self.A * (self.S + 1)))
-        s = self.rng
-        for d in range(r.shape[1]):
-            s = s + np.uint32(0x6D2B79F5)
-            t = (s ^ (s >> np.uint32(15))) * (s | np.uint32(1))
-            t ^= t + (t ^ (t >> np.uint32(7))) * (t | np.uint32(61))
-            r[:, d] = (t ^ (t >> np.uint32(14))) / 4294967296.0
-        self.rng = s
-        r = r.reshape(self.n, self.A, self.S + 1)
-        # held as f32, as the controls of a Float32Array (the engine's control record)
-        self.targets = (r[:, :, :self.S] * 2 - 1).astype(np.float32).astype(np.float64).reshape(self.n, -1)
-        self.adh = r[:, :, self.S].astype(np.float32).astype(np.float64)
-
-    def control(self):
-        """applyControl for every creature on the mirrored state, packed."""
-        if self.t % 6 == 0:
-            self._draw()
-        self.cons[self.motors, 10] = np.clip(self.targets, -self.lim, self.lim)
-        adh = np.clip(self.adh, 0.0, 1.0)
-        self.cd = np.where(self.cd > 0, self.cd - self.dt, self.cd)
-        broken = self.consu[self.grips, 17] != 0
-        tb = self.body[self.tips].astype(np.float64)
-        cand = broken & (adh > 0.08) & (self.cd <= 0)
-        att = cand & (np.hypot(tb[..., 4], tb[..., 5]) < 150.0)
-        self.cd = np.where(cand & ~att, 0.05, self.cd)
-        held = ~broken
-        ga = self.grips[att]
-        self.cons[ga, 6] = tb[..., 0][att] + self.half_seg * np.cos(tb[..., 6][att])
-        self.cons[ga, 7] = tb[..., 1][att] + self.half_seg * np.sin(tb[..., 6][att])
-        upd = att | held
-        self.cons[self.grips[upd], 16] = (40.0 + 860.0 * adh)[upd]
-        nb = broken & ~att | (held & (adh < 0.04))
-        self.consu[self.grips, 17] = nb.astype(np.uint32)
-
-    def step(self, ev=None):
-        self.control()
-        self._check(self.L.kr_upload_controls(self.h, self.cp))
-        if ev is not None:
-            ev[0].record()
-        self._check(self.L.kr_step(self.h, 1))
-        if ev is not None:
-            ev[1].record()
-        self._check(self.L.kr_download(self.h, self.bp, self.cp))
-        self.t += 1
-
-    def close(self):
-        from kraken_3_gpu_b200 import gpuworld
-        gpuworld.destroy(self.g)
-
-
 def config1_forms(torch, stream, steps=1000):
     """The plain batched drop-in configuration: 1,024 default creatures on
     map seed 1, spawn jitter U(+-20 px) around the map's spawn point, heading
@@ -466,9 +370,9 @@ def config1_forms(torch, stream, steps=1000):
     of its steps; and the persistent batched engine (reflex and controls on the
     device, one launch).  The persistent engine runs the same arithmetic, so
     the two forms' final states are compared bit for bit as well."""
-    from kraken_3_gpu_b200 import batch, workloads
+    from kraken_3_gpu_b200 import batch, hybrid, workloads
     w = workloads.uniform(n=1024, steps=steps)
-    loop = HybridLoop(w, stream.cuda_stream)
+    loop = hybrid.HybridLoop(w, stream.cuda_stream)
     evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
     torch.cuda.synchronize()
     t0 = time.perf_counter()
