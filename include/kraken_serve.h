@@ -146,14 +146,18 @@ int kr_server_submit(kr_server *s, const kr_request *r, int64_t *id);
 int kr_server_submit_batch(kr_server *s, const kr_request *reqs, int32_t n, int64_t *ids,
                            int32_t *n_submitted);
 
-/* One scheduling round of the next partition: wait for its previous round,
- * complete the requests that ended there, admit arrived requests into free
- * slots, launch chunk_steps env steps of its creatures.  *busy = 1 while any
- * request is queued or running. */
+/* One scheduling step.  Two partitions (slice_ms = 0): the next partition's
+ * round -- wait for its previous round, complete the requests that ended
+ * there, admit arrived requests into free slots, launch chunk_steps env
+ * steps of its creatures.  Slices (slice_ms > 0): while a slice runs and
+ * neither an admissible request nor the slice's time calls for preemption,
+ * return at once; otherwise end the slice (preempting it if needed),
+ * complete, admit and launch the next one.  *busy = 1 while any request is
+ * queued or running. */
 int kr_server_pump(kr_server *s, int32_t *busy);
 
 /* Pump until every submitted request has completed (sleeps while the next
- * request has not arrived yet). */
+ * request has not arrived yet, and 0.1 ms between looks at a running slice). */
 int kr_server_drain(kr_server *s);
 
 /* Ids of requests completed since the last poll (up to cap). */
