@@ -69,7 +69,10 @@ def parse():
     ap.add_argument("--shape", default="", help="lanes,warps,ctas[,unroll] launch shape (empty: autotune)")
     ap.add_argument("--chunk", type=int, default=64, help="server env steps per round (two-partition rounds)")
     ap.add_argument("--slice-ms", type=float, default=50.0,
-                    help="server slices (ms) of the one-partition scheduler; 0: two partitions in rounds")
+                    help="server time slices (ms) of the one-partition scheduler; 0: two partitions in rounds")
+    ap.add_argument("--engine-slice-ms", type=float, default=50.0,
+                    help="persistent rollouts in preemptible time slices of this many ms, the creatures regrouped "
+                         "between them (0: one launch per rollout)")
     ap.add_argument("--no-es", action="store_true", help="skip the ES request stream")
     ap.add_argument("--es-requests", type=int, default=200)
     ap.add_argument("--no-config1", action="store_true", help="skip the 1,024-creature drop-in comparison")
@@ -448,13 +451,13 @@ def config4_memory_bound(serve, slice_ms):
     return out
 
 
-def net_controller(stream, w, seed=7):
+def net_controller(stream, w, seed=7, slice_ms=0.0):
     """The same workload driven by the reference trainer's own controller
     (KR_CTRL_NET: net.js's recurrent net on proprioception + echo, light and
     contact senses), one randomGenome-initialised genome per creature (net.js:
-    41-55: N(0, 1/fan_in) weights, zero biases); one persistent launch over the
-    whole horizons with the autotuned launch shape, kernel time by CUDA
-    events."""
+    41-55: N(0, 1/fan_in) weights, zero biases); the whole horizons with the
+    autotuned launch shape, in time slices of slice_ms (0: one launch), device
+    time by CUDA events."""
     from kraken_3_gpu_b200 import batch, workloads
     rng = np.random.default_rng(seed)
     width = batch.net_param_count(int(w.arms.max()))
@@ -474,17 +477,20 @@ def net_controller(stream, w, seed=7):
     eng.set_net(genomes, np.arange(w.n, dtype=np.int32))
     eng.snapshot()
     eng.autotune(64)  # the launch shape, as the persistent bench picks it; slots left as they were
+    eng.set_slice(slice_ms)
     eng.run(64)
     eng.restore()
     eng.run(int(w.horizon.max()))
     eng.sync()
     ms = eng.last_ms()
     shape = eng.get_launch()
+    slices = eng.last_slices()
     eng.close()
     return {"value": w.creature_steps() / (ms / 1000.0), "unit": UNIT, "kernel_ms": ms,
             "controller": "net.js 10A+45 -> 24 -> 24 -> 3A+2 per creature, senses and recurrent outputs on the device",
             "launch_shape": [shape["lanes_per_creature"], shape["warps_per_cta"], shape["ctas_per_sm"],
-                             shape["substep_unroll"]]}
+                             shape["substep_unroll"]],
+            "time_slices": slices, "slice_ms": slice_ms if slice_ms > 0 else None}
 
 
 def main():
@@ -514,7 +520,7 @@ def main():
     w, (lo, hi) = replicas.shard(w_all, rank, world)
     del w_all
     if args.net_only:
-        line = net_controller(torch.cuda.current_stream(), w)
+        line = net_controller(torch.cuda.current_stream(), w, slice_ms=args.engine_slice_ms)
         line.update({"metric": "creature-steps/s under the reference net controller", "n_gpus": 1,
                      "config": {"workload": f"uneven: {w.n} creatures, {len(w.maps)} maps, horizons "
                                             f"{args.hmin}-{args.hmax}"}})
@@ -548,6 +554,7 @@ def main():
         best = (g, wp, c)
         tune = {best: ms}
     unroll = eng.get_launch()["substep_unroll"]
+    eng.set_slice(args.engine_slice_ms)
 
     # warm-up: full rollouts, each as a timed one runs
     for _ in range(args.warmup):
@@ -565,21 +572,25 @@ def main():
     barrier()
     ev = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
     ev[0].record(stream)
+    gpu_launches = 0
     for k in range(args.steps):
         flush.zero_()
         eng.restore()
         eng.run(max_h)
         ev[k + 1].record(stream)
+        slices, kernels = eng.last_run_launches()
+        gpu_launches += kernels
     ev[-1].synchronize()
     barrier()
     e0, e1 = ev[0], ev[-1]
     rollout_ms = [ev[k].elapsed_time(ev[k + 1]) for k in range(args.steps)]
     elapsed_ms = e0.elapsed_time(e1)
-    kms = eng.last_ms()  # the last rollout's kernel alone (events on its stream)
+    # the last rollout's launches (events on its stream; under time slices
+    # from its first slice to its last, the host time between them included)
+    kms = eng.last_ms()
     t_max = all_max(elapsed_ms)
     value = replicas.job_rate(units * args.steps, world, t_max / 1000.0)
     ms_per_step = t_max / args.steps
-    gpu_launches = args.steps
 
     extra = {}
     # the edge of the partition: every rank's per-creature scores gathered in
@@ -628,7 +639,8 @@ def main():
     e2e = served_line(sl)
     clocks = sampler.stop()
     e2e["form"] = ("served: rollout server C ABI, one request per creature, host buffers in and out; " +
-                   (f"one partition in preemptible slices of {sl:g} ms" if sl > 0 else
+                   (f"one partition in preemptible slices of {sl:g} ms, completions polled every 1 ms"
+                    if sl > 0 else
                     f"two partitions in rounds of {chunk} env steps"))
     if sl > 0:
         extra["served_two_partitions"] = dict(served_line(0.0), chunk_steps=chunk,
@@ -660,7 +672,7 @@ def main():
     if not args.no_config4 and rank == 0:
         extra["memory_bound_65k"] = config4_memory_bound(serve, sl)
     if not args.no_net and rank == 0:
-        extra["net_controller"] = net_controller(stream, w)
+        extra["net_controller"] = net_controller(stream, w, slice_ms=args.engine_slice_ms)
         if not args.no_es:
             extra["served_es_stream_net"] = served_es_streams(serve, w, chunk, args.es_requests, 200.0, net=True,
                                                               slice_ms=sl)
@@ -682,6 +694,9 @@ def main():
                                     "capture (8,192 creatures: 2,587 B each: state, grips, controls and slot "
                                     "records in and out once) x the creatures of this launch; algorithmic ~2.5 KB",
                     "ops_per_creature_step": ops, "kernel_ms": kms,
+                    "kernel_ms_note": (f"the rollout's {slices} time-slice launches of batch_kernel, first to last, "
+                                       "the host time between them included" if slices > 1 else
+                                       "the rollout's one launch of batch_kernel"),
                     "peak_note": "measured dependent-free f32 FMA issue rate (lane-ops/s) of this GPU; "
                                  "MEASURED_PEAKS.json has no f32 figure"}
             cpu = cpu_baseline_line(w, host_threads(), args.cpu_seconds)
@@ -694,9 +709,12 @@ def main():
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32", "data": "synthetic",
             "config": bench_config(args, w, world),
-            "form": "persistent kernel, one launch per rollout, state resident in HBM",
+            "form": ("persistent kernel, state resident in HBM; " +
+                     (f"each rollout in preemptible time slices of {args.engine_slice_ms:g} ms, the live creatures "
+                      "regrouped between slices" if slices > 1 else "one launch per rollout")),
             "launch": {"lanes_per_creature": best[0], "warps_per_cta": best[1], "ctas_per_sm": best[2],
-                       "substep_unroll": unroll,
+                       "substep_unroll": unroll, "time_slices_per_rollout": slices,
+                       "slice_ms": args.engine_slice_ms if slices > 1 else None,
                        "autotune_ms": {",".join(map(str, k)): round(v, 3) for k, v in tune.items()}},
             "roofline": roof, "cpu_baseline": cpu, "clocks": clocks, "e2e": e2e,
             "gpu_launches": gpu_launches, **extra,

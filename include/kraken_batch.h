@@ -137,8 +137,27 @@ int kr_batch_set_net(kr_batch *b, const float *genomes, int32_t n_individuals, i
 int kr_batch_read_net(kr_batch *b, int32_t first, int32_t n, float *inputs, float *outputs);
 
 /* Advance every live slot by min(max_steps, horizon - step) env steps with
- * one persistent launch.  Asynchronous; returns once enqueued. */
+ * one persistent launch.  Asynchronous; returns once enqueued -- except
+ * under time slices (kr_batch_set_slice) when max_steps covers every live
+ * slot's remaining steps: then the run is a sequence of launches and the
+ * call returns when every creature has reached its horizon. */
 int kr_batch_run(kr_batch *b, int32_t max_steps);
+
+/* Time slices.  slice_ms > 0: a kr_batch_run that takes every live slot to
+ * its horizon runs as preemptible slices -- a persistent launch, stopped
+ * through a device word after slice_ms (creatures stop at an env-step
+ * boundary, state written back), the step counters read back, the live
+ * creatures regrouped by their remaining steps and launched again.  The
+ * regrouping spreads the longest creatures over every SM as the short ones
+ * finish, so the tail of uneven horizons runs with shorter steps; the
+ * results are bit-identical to one launch.  A slice that advanced no
+ * creature doubles the next one's time.  0 (default): one launch.
+ * kr_batch_last_ms then covers the whole run, host time between slices
+ * included; kr_batch_last_slices gives the slices it took and the kernels
+ * it launched (slices and step-counter readbacks; 1 and 1 for one launch).
+ * Either pointer may be NULL. */
+int kr_batch_set_slice(kr_batch *b, float slice_ms);
+int kr_batch_last_slices(kr_batch *b, int32_t *slices, int32_t *kernels);
 
 /* `launches` back-to-back launches of steps_per_launch env steps each over
  * the same creature groups, no host work between them (with

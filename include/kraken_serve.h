@@ -20,13 +20,16 @@
  *    the other's);
  *  - or (slice_ms > 0) one partition in preemptible slices: a slice runs
  *    every live creature to its horizon and ends early when an arrived
- *    request fits the free slots or its time is up; the next slice admits;
+ *    request fits the free slots or its time is up; the next slice admits
+ *    and regroups the creatures by their remaining steps.  Requests whose
+ *    creatures have all ended complete while the slice runs;
  *  - admission against an HBM budget: every slot's device memory (state,
  *    grips, controls, observation ring, policy weights) is accounted for at
  *    creation; the budget fixes the slot count, requests wait in FIFO order
  *    until enough slots are free;
  *  - per-request completion: a request's results are gathered on the device
- *    and copied back when its last round ends; its slots return to the pool.
+ *    and copied back when its last round ends (slices: within about a
+ *    millisecond of its last creature's end); its slots return to the pool.
  *
  * Every creature's trajectory depends only on its own request (body, map,
  * pose, parameters, seed), so a request's results are bit-identical whether
@@ -75,13 +78,18 @@ typedef struct kr_server_desc {
   const double *map_size;
   /* > 0: sliced scheduling instead of the two partitions' rounds.  All
    * slots form one partition and every creature runs to its horizon in one
-   * persistent launch (a slice, at most chunk_steps env steps), which the
-   * server preempts -- through a device word the kernel reads at each env
-   * step -- when an arrived request fits the free slots (counting requests
-   * the kernel reports complete; not before the slice has run 3 times the
-   * host's time between slices) or slice_ms milliseconds (at least 10 such
-   * host gaps) have passed; it then completes the requests whose
-   * creatures reached their horizons, admits, and launches the next slice.
+   * persistent launch (a slice, at most chunk_steps env steps).  While it
+   * runs, the server copies back the kernel's per-request counts of
+   * creatures at their horizons once a millisecond and completes the
+   * requests whose creatures have all ended (their records copied back
+   * beside the running kernel).  It preempts the slice -- through a device
+   * word the kernel reads at each env step -- when an arrived request fits
+   * the free slots plus those of the completed requests (not before the
+   * slice has run 3 times the host's time between slices) or slice_ms
+   * milliseconds (at least 10 such host gaps) have passed, then frees the
+   * completed requests' slots, admits, and launches the next slice, its
+   * creatures regrouped by their remaining steps (the longest spread over
+   * every SM: a shorter tail than one launch).
    * 0: two partitions alternating chunk_steps rounds (above). */
   double slice_ms;
 } kr_server_desc;
@@ -149,11 +157,12 @@ int kr_server_submit_batch(kr_server *s, const kr_request *reqs, int32_t n, int6
 /* One scheduling step.  Two partitions (slice_ms = 0): the next partition's
  * round -- wait for its previous round, complete the requests that ended
  * there, admit arrived requests into free slots, launch chunk_steps env
- * steps of its creatures.  Slices (slice_ms > 0): while a slice runs and
- * neither an admissible request nor the slice's time calls for preemption,
- * return at once; otherwise end the slice (preempting it if needed),
- * complete, admit and launch the next one.  *busy = 1 while any request is
- * queued or running. */
+ * steps of its creatures.  Slices (slice_ms > 0): while a slice runs,
+ * complete the requests it has finished (at most one poll a millisecond)
+ * and, unless an arrived request fits or the slice's time is up, return;
+ * otherwise end the slice (preempting it if needed), free, admit and
+ * launch the next one.
+ * *busy = 1 while any request is queued or running. */
 int kr_server_pump(kr_server *s, int32_t *busy);
 
 /* Pump until every submitted request has completed (sleeps while the next

@@ -102,6 +102,8 @@ def _lib():
         "kr_batch_set_unroll": (C.c_int, [vp, i32]),
         "kr_batch_get_unroll": (C.c_int, [vp, _I32P]),
         "kr_batch_last_ms": (C.c_int, [vp, _F32P]),
+        "kr_batch_set_slice": (C.c_int, [vp, C.c_float]),
+        "kr_batch_last_slices": (C.c_int, [vp, _I32P, _I32P]),
         "kr_batch_sync": (C.c_int, [vp]),
         "kr_batch_set_stream": (C.c_int, [vp, vp]),
         "kr_batch_destroy": (None, [vp]),
@@ -269,6 +271,21 @@ class BatchEngine:
 
     def run(self, max_steps):
         _check(_lib().kr_batch_run(self.h, max_steps), self.h)
+
+    def set_slice(self, slice_ms):
+        """Time slices (ms) for runs that take every live slot to its horizon:
+        preemptible launches, the creatures regrouped between them (0: one
+        launch).  Results do not depend on it."""
+        _check(_lib().kr_batch_set_slice(self.h, float(slice_ms)), self.h)
+
+    def last_slices(self) -> int:
+        return self.last_run_launches()[0]
+
+    def last_run_launches(self):
+        """(slices, kernels launched) of the last run."""
+        n, k = C.c_int32(), C.c_int32()
+        _check(_lib().kr_batch_last_slices(self.h, C.byref(n), C.byref(k)), self.h)
+        return n.value, k.value
 
     def run_launches(self, steps_per_launch, launches):
         _check(_lib().kr_batch_run_launches(self.h, steps_per_launch, launches), self.h)

@@ -16,13 +16,16 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstring>
 #include <map>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "kr_batch_impl.h"
+#include "kr_order.h"
 
 namespace {
 using namespace krb;
@@ -817,13 +820,18 @@ __device__ void run_creature(const BatchArgs &A, const TplDev &td, int nlv, cons
   }
   float *cout = A.ctrl_cur + (size_t)slot * kCtrlStride;
   for (int q = lane; q < AS + arms; q += G) cout[q] = X.ctrl[q];
-  if (A.tag_done && lane == 0 && m.step >= m.horizon) atomicAdd(A.tag_done + m.pad, 1);
   if (lane == 0) {  // the fields this loop keeps in registers; postStep's are in place
     SlotMeta &g = A.meta[slot];
     g.step = m.step;
     g.rng = m.rng;
     g.prev_vx = m.prev_vx;
     g.prev_vy = m.prev_vy;
+    // the record is final once the count includes this creature: the server
+    // copies a request's records back (copy engine) while the launch still runs
+    if (A.tag_done && m.step >= m.horizon) {
+      __threadfence_system();
+      atomicAdd(A.tag_done + m.pad, 1);
+    }
   }
 }
 
@@ -928,6 +936,13 @@ __global__ void spawn_kernel(float *state, float4 *grip, float2 *glam, double2 *
     m.spawn_reach = 70.0 < v ? v : 70.0;
     meta[slot] = m;
   }
+}
+
+// every slot's step counter into one contiguous array (read back after a
+// time slice: a preempted slice leaves each creature at its own step)
+__global__ void step_counts_kernel(const SlotMeta *meta, int n, int *out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) out[i] = meta[i].step;
 }
 
 }  // namespace
@@ -1149,19 +1164,18 @@ int build_groups(kr_batch *b, Part &p, int max_steps) {
       return b->fail(KR_ERR_STATE, "slot " + std::to_string(s) + ": its individual's weights were laid out for "
                                        "another body shape (kr_batch_set_policy after the spawn)");
   }
-  // by template, then longest remaining first, ties in slot-list order: one
-  // 64-bit key per live slot (template 8 bits, inverted remaining steps 31
-  // bits, list position 24 bits), sorted without touching the slot records
+  // by template, then longest remaining first, ties in slot-list order
   {
-    std::vector<uint64_t> keys(live.size());
-    for (size_t i = 0; i < live.size(); i++) {
-      const int s = live[i];
-      keys[i] = ((uint64_t)(uint32_t)b->h_meta[s].tpl << 55) | ((uint64_t)(0x7fffffffu - (uint32_t)rem[s]) << 24) |
-                (uint64_t)i;
+    const int n = (int)live.size();
+    std::vector<int> lt(n), lr(n), perm, perm2;
+    std::vector<uint64_t> keys, keys2;
+    for (int i = 0; i < n; i++) {
+      lt[i] = b->h_meta[live[i]].tpl;
+      lr[i] = rem[live[i]];
     }
-    std::sort(keys.begin(), keys.end());
-    std::vector<int> sorted(live.size());
-    for (size_t i = 0; i < live.size(); i++) sorted[i] = live[keys[i] & 0xffffffu];
+    lpt_order(n, lt.data(), lr.data(), perm, keys, keys2, perm2);
+    std::vector<int> sorted(n);
+    for (int i = 0; i < n; i++) sorted[i] = live[perm[i]];
     live.swap(sorted);
   }
   // Group size per template.  When the live creatures fill less than one
@@ -1269,16 +1283,21 @@ cudaError_t launch_g(const BatchArgs &A, kr_batch *b, cudaStream_t st, int n_gro
 
 namespace krb {
 
+// Few creatures (under 16 per SM): one per warp, the shortest step latency;
+// up to 96 per SM two per warp; beyond, four per warp, the most
+// creature-steps per issue slot (measured on the 16k workload).
+// Proprioception and the fused policy run per arm, so creatures that need
+// them pack four per warp from 16 per SM on.
+int auto_lanes(const kr_batch *b, long live, long per_arm) {
+  const bool arm_heavy = b->d.obs_ring > 0 || 2 * per_arm > live;
+  return live < 16L * b->n_sm ? 32 : (arm_heavy || live >= 96L * b->n_sm) ? 8 : 16;
+}
+
 int launch_part(kr_batch *b, Part &p, int max_steps, bool timed) {
   if (b->tpls.empty()) return KR_OK;
   if (b->d.control_mode == KR_CTRL_POLICY && !b->d_pw)
     return b->fail(KR_ERR_STATE, "policy control without kr_batch_set_policy");
   if (b->auto_shape && p.dirty) {
-    // few creatures (under 16 per SM): one per warp, the shortest step
-    // latency; up to 96 per SM two per warp; beyond, four per warp, the
-    // most creature-steps per issue slot (measured on the 16k workload).
-    // Proprioception and the fused policy run per arm, so creatures that
-    // need them pack four per warp from 16 per SM on.
     long live = 0, per_arm = 0;
     auto count = [&](int s) {
       if (b->h_remaining[s] <= 0 || b->h_meta[s].horizon <= 0) return;
@@ -1290,8 +1309,7 @@ int launch_part(kr_batch *b, Part &p, int max_steps, bool timed) {
     } else {
       for (int s : p.slots) count(s);
     }
-    const bool arm_heavy = b->d.obs_ring > 0 || 2 * per_arm > live;
-    const int g = live < 16L * b->n_sm ? 32 : (arm_heavy || live >= 96L * b->n_sm) ? 8 : 16;
+    const int g = auto_lanes(b, live, per_arm);
     const int w = g == 32 ? 4 : 8;
     if (g != b->G || w != b->W) {
       b->G = g;
@@ -1401,6 +1419,97 @@ cudaError_t launch_spawn(kr_batch *b, const int *d_slots, const float *d_pose, c
                                       d_slots, d_pose, d_meta, n, b->d_rects64, b->d_map_off, b->rays,
                                       b->d_net, b->d_lights, b->d_light_off);
   return cudaGetLastError();
+}
+
+// kr_batch_run under time slices, every live slot to its horizon: launches
+// preempted through the stop word after slice_ms, each followed by the
+// step counters' readback and a regrouping of the creatures still live.
+// The whole run's device time goes to the part's ev0 / ev1.
+int run_sliced(kr_batch *b, int max_steps) {
+  Part &p = b->main;
+  cudaStream_t st = part_stream(b, p);
+  cudaError_t e = cudaSuccess;
+  if (!b->slice_ready) {
+    if (!b->d_stop) e = cudaMalloc(&b->d_stop, sizeof(int));
+    if (e == cudaSuccess && !b->h_flag) e = cudaMallocHost(&b->h_flag, 2 * sizeof(int));
+    if (e == cudaSuccess && !b->d_steps) e = cudaMalloc(&b->d_steps, (size_t)b->capacity * sizeof(int));
+    if (e == cudaSuccess && !b->h_steps) e = cudaMallocHost(&b->h_steps, (size_t)b->capacity * sizeof(int));
+    if (e == cudaSuccess && !b->ctl) e = cudaStreamCreateWithFlags(&b->ctl, cudaStreamNonBlocking);
+    if (e == cudaSuccess && !b->slice_start) e = cudaEventCreateWithFlags(&b->slice_start, cudaEventDisableTiming);
+    if (e == cudaSuccess && !b->slice_end) e = cudaEventCreateWithFlags(&b->slice_end, cudaEventDisableTiming);
+    if (e != cudaSuccess) return b->cuda_fail(e, "time-slice setup");
+    b->h_flag[0] = 0;
+    b->h_flag[1] = 1;
+    b->slice_ready = true;
+  }
+  std::vector<int> run;  // the slots live when the run starts
+  for (int s = 0; s < b->capacity; s++)
+    if (b->h_remaining[s] > 0) run.push_back(s);
+  using clk = std::chrono::steady_clock;
+  double slice_s = b->slice_ms * 1e-3;
+  long long steps_before = -1;
+  b->last_slices = b->last_kernels = 0;
+  for (int k = 0;; k++) {
+    e = cudaMemcpyAsync(b->d_stop, b->h_flag, sizeof(int), cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaEventRecord(b->slice_start, st);
+    // the stop word's copy on the control stream comes after its reset
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(b->ctl, b->slice_start, 0);
+    if (e != cudaSuccess) return b->cuda_fail(e, "slice start");
+    p.stop = b->d_stop;
+    p.dirty = true;
+    int rc = launch_part(b, p, max_steps, k == 0);
+    p.stop = nullptr;
+    if (rc != KR_OK) return rc;
+    if (p.n_groups == 0) break;
+    b->last_slices++;
+    b->last_kernels++;
+    e = cudaEventRecord(b->slice_end, st);
+    if (e != cudaSuccess) return b->cuda_fail(e, "slice record");
+    // the slice's time counts from when its launch is next on the stream
+    bool started = false, stopped = false;
+    clk::time_point t0{};
+    for (;;) {
+      e = cudaEventQuery(b->slice_end);
+      if (e == cudaSuccess) break;
+      if (e != cudaErrorNotReady) return b->cuda_fail(e, "slice query");
+      if (!started) {
+        const cudaError_t q = cudaEventQuery(b->slice_start);
+        if (q == cudaSuccess) {
+          started = true;
+          t0 = clk::now();
+        } else if (q != cudaErrorNotReady) {
+          return b->cuda_fail(q, "slice query");
+        }
+      } else if (!stopped && std::chrono::duration<double>(clk::now() - t0).count() >= slice_s) {
+        e = cudaMemcpyAsync(b->d_stop, b->h_flag + 1, sizeof(int), cudaMemcpyHostToDevice, b->ctl);
+        if (e != cudaSuccess) return b->cuda_fail(e, "slice stop");
+        stopped = true;
+      }
+      std::this_thread::sleep_for(std::chrono::microseconds(20));
+    }
+    // the stop word's copy has landed before the next slice resets it
+    if (stopped && (e = cudaStreamSynchronize(b->ctl)) != cudaSuccess) return b->cuda_fail(e, "slice stop wait");
+    if (!stopped) break;  // every creature reached its horizon inside the slice
+    step_counts_kernel<<<(b->capacity + 255) / 256, 256, 0, st>>>(b->d_meta, b->capacity, b->d_steps);
+    b->last_kernels++;
+    e = cudaGetLastError();
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(b->h_steps, b->d_steps, (size_t)b->capacity * sizeof(int), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return b->cuda_fail(e, "slice step counters");
+    long live = 0;
+    long long steps = 0;
+    for (int s : run) {
+      b->h_remaining[s] = std::max(0, b->h_meta[s].horizon - b->h_steps[s]);
+      live += b->h_remaining[s] > 0;
+      steps += b->h_steps[s];
+    }
+    if (live == 0) break;
+    if (steps == steps_before) slice_s *= 2;  // no creature advanced: a longer slice
+    steps_before = steps;
+  }
+  if (b->last_slices > 0 && (e = cudaEventRecord(p.ev1, st)) != cudaSuccess) return b->cuda_fail(e, "slice timing");
+  return KR_OK;
 }
 
 }  // namespace krb
@@ -1808,7 +1917,28 @@ extern "C" int kr_batch_run(kr_batch *b, int32_t max_steps) {
   if (max_steps < 0) return b->fail(KR_ERR_INVALID, "max_steps < 0");
   if (max_steps == 0) return KR_OK;
   b->main.dirty = true;  // finished slots leave the queue, work estimates change
-  return launch_part(b, b->main, max_steps, true);
+  if (b->slice_ms > 0.f) {
+    bool to_horizon = true;
+    for (int s = 0; s < b->capacity && to_horizon; s++) to_horizon = b->h_remaining[s] <= max_steps;
+    if (to_horizon) return run_sliced(b, max_steps);
+  }
+  const int rc = launch_part(b, b->main, max_steps, true);
+  b->last_slices = b->last_kernels = b->main.n_groups > 0 ? 1 : 0;
+  return rc;
+}
+
+extern "C" int kr_batch_set_slice(kr_batch *b, float slice_ms) {
+  if (!b) return KR_ERR_INVALID;
+  if (!(slice_ms >= 0.f && slice_ms < 1e7f)) return b->fail(KR_ERR_INVALID, "slice_ms outside [0, 1e7)");
+  b->slice_ms = slice_ms;
+  return KR_OK;
+}
+
+extern "C" int kr_batch_last_slices(kr_batch *b, int32_t *slices, int32_t *kernels) {
+  if (!b) return KR_ERR_INVALID;
+  if (slices) *slices = b->last_slices;
+  if (kernels) *kernels = b->last_kernels;
+  return KR_OK;
 }
 
 extern "C" int kr_batch_run_launches(kr_batch *b, int32_t steps_per_launch, int32_t launches) {
@@ -2073,9 +2203,14 @@ extern "C" void kr_batch_destroy(kr_batch *b) {
                   b->d_state, b->d_grip, b->d_glam, b->d_cd, b->d_ctrl, b->d_meta, b->d_obs,
                   b->d_pw, b->d_pw_idx, b->s_state, b->s_grip, b->s_glam, b->s_cd,
                   b->s_ctrl, b->s_meta, b->s_groups, b->d_net, b->s_net, b->d_lights, b->d_light_off,
-                  b->d_map_size, b->d_light_tab};
+                  b->d_map_size, b->d_light_tab, b->d_stop, b->d_steps};
   for (void *p : ptrs)
     if (p) cudaFree(p);
+  if (b->h_flag) cudaFreeHost(b->h_flag);
+  if (b->h_steps) cudaFreeHost(b->h_steps);
+  if (b->ctl) cudaStreamDestroy(b->ctl);
+  if (b->slice_start) cudaEventDestroy(b->slice_start);
+  if (b->slice_end) cudaEventDestroy(b->slice_end);
   if (b->own_stream && b->stream) cudaStreamDestroy(b->stream);
   delete b;
 }

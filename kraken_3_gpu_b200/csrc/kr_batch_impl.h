@@ -321,6 +321,15 @@ struct kr_batch {
   size_t pw_capacity = 0;
   int pw_stride = 0, n_individuals = 0;
   std::vector<int> h_pw_idx, h_pw_tpl;
+  // time-sliced runs (kr_batch_set_slice)
+  float slice_ms = 0.f;
+  bool slice_ready = false;            // the buffers below exist
+  int *d_stop = nullptr;               // the kernel's stop word
+  int *h_flag = nullptr;               // pinned {0, 1}: the values it is set to
+  int *d_steps = nullptr, *h_steps = nullptr;  // every slot's step counter after a slice
+  cudaStream_t ctl = nullptr;          // the stop word's copy while a slice runs
+  cudaEvent_t slice_start = nullptr, slice_end = nullptr;
+  int last_slices = 0, last_kernels = 0;  // of the last kr_batch_run
 
   int fail(int code, const std::string &m) { err = m; return code; }
   int cuda_fail(cudaError_t e, const char *what) {
@@ -337,6 +346,10 @@ int ensure_template(kr_batch *b, int arms, int segs);
 int upload_templates(kr_batch *b);
 // creatures per group of every template and the CTA's shared memory
 int plan_shape(kr_batch *b);
+// lanes per creature the automatic launch shape gives `live` creatures, of
+// which `per_arm` run the policy or net controller (their proprioception
+// and controller run per arm)
+int auto_lanes(const kr_batch *b, long live, long per_arm);
 // groups of the part's live slots, longest work first, staged to the device
 int build_groups(kr_batch *b, Part &p, int max_steps);
 // one persistent launch over the part's groups, min(max_steps, remaining)

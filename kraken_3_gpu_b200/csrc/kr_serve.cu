@@ -120,6 +120,8 @@ struct Req {
   int rounds_left = 0;
   double arrival = 0, admitted = -1, completed = -1;
   std::vector<double> results;
+  int pending = 0;                      // sliced scheduling: creatures not yet at their horizon
+  int64_t seq = 0;                      // admission order
   bool done = false;
 };
 
@@ -137,7 +139,7 @@ struct Stage {
 struct Round {
   bool inflight = false;
   cudaEvent_t done = nullptr;
-  std::vector<int64_t> completing;
+  std::vector<Req *> completing;
   bool timed = false;
 };
 
@@ -177,7 +179,10 @@ struct kr_server {
   Stage stage[2];
   Round round[2];
   cudaStream_t streams[2] = {nullptr, nullptr};
-  std::vector<int64_t> active[2];
+  // running requests per partition, in admission order (a running request
+  // cannot be released, so its map entry, and the pointer, stay valid)
+  std::vector<Req *> active[2];
+  std::vector<Req *> slot_req;   // the request holding each slot
   int part_used[2] = {0, 0};
   int next = 0;
   int capacity = 0, part_cap = 0, chunk = 1;
@@ -193,17 +198,22 @@ struct kr_server {
   std::chrono::steady_clock::time_point t0;
   // sliced scheduling (slice_ms > 0): one partition, preemptible slices
   bool sliced = false;
-  double slice_s = 0;
+  double slice_s = 0;            // the time slice (slice_ms)
   int *d_stop = nullptr;          // the kernel's stop word
   int *h_flag = nullptr;          // pinned {0, 1}: the values the stop word is set to
   int *h_steps = nullptr;         // pinned: every slot's step counter after a slice
   int *d_steps = nullptr;
-  cudaStream_t ctl = nullptr;     // the stop word's copies while a slice runs
+  cudaStream_t ctl = nullptr;     // the stop word's and completion counts' copies while a slice runs
+  cudaEvent_t staged = nullptr;   // a slice's admissions done: the control stream waits for it
   double slice_t0 = 0;
   bool stop_sent = false;
   int *d_done = nullptr;          // per request tag (its first slot): creatures that reached their horizon
-  int *h_done = nullptr;          // pinned copy of d_done, polled while a request waits
+  int *h_done = nullptr;          // pinned copy of d_done, polled while a slice runs
+  std::vector<int> prev_done;     // h_done as of the poll before
+  std::vector<int> gather_slots;  // slots whose records a poll copies back
+  std::vector<int> rec_pos;       // ... and where each record lands in the staging
   double polled = -1;             // server time of the last poll
+  long done_unfreed = 0;          // slots of requests completed while their slice runs
   double gap_s = 0;               // host time between a slice's end and the next launch (running mean)
   double gap_sum = 0;             // ... summed
   std::string err;
@@ -269,7 +279,20 @@ void free_stage(Stage &s) {
   s = Stage{};
 }
 
-// completes the requests of partition p whose last round just ended
+// a request's results from its creatures' records (rec[0..population))
+void complete(kr_server *S, Req &q, const SlotMeta *rec, double t) {
+  const size_t n = q.slots.size();
+  q.results.resize(n * KR_RESULT_WORDS);
+  for (size_t i = 0; i < n; i++) slot_metrics(rec[i], q.results.data() + i * KR_RESULT_WORDS);
+  q.completed = t;
+  q.done = true;
+  S->completed++;
+  S->done_ids.push_back(q.id);
+}
+
+// completes the requests of partition p whose last round just ended (those
+// completed while the slice ran have their results already) and frees
+// their slots
 void finish_round(kr_server *S, int p) {
   Round &R = S->round[p];
   const double t = S->now();
@@ -278,31 +301,29 @@ void finish_round(kr_server *S, int p) {
     if (cudaEventElapsedTime(&ms, S->parts[p].ev0, S->parts[p].ev1) == cudaSuccess) S->device_ms += ms;
   }
   size_t off = 0;
-  for (int64_t id : R.completing) {
-    Req &q = S->reqs[id];
+  for (Req *qp : R.completing) {
+    Req &q = *qp;
     const size_t n = q.slots.size();
-    q.results.resize(n * KR_RESULT_WORDS);
-    for (size_t i = 0; i < n; i++) slot_metrics(S->stage[p].h_res[off + i], q.results.data() + i * KR_RESULT_WORDS);
-    off += n;
-    q.completed = t;
-    q.done = true;
+    if (q.done) {
+      S->done_unfreed -= (long)n;
+    } else {
+      complete(S, q, S->stage[p].h_res + off, t);
+      off += n;
+    }
     for (int s : q.slots) {
       S->b->h_meta[s].horizon = 0;
       S->b->h_remaining[s] = 0;
       S->free_slots.push_back(s);
+      S->slot_req[s] = nullptr;
     }
     S->part_used[p] -= (int)n;
-    S->completed++;
-    S->done_ids.push_back(id);
   }
   if (!R.completing.empty()) {
     auto &act = S->active[p];
-    act.erase(std::remove_if(act.begin(), act.end(), [&](int64_t id) { return S->reqs[id].done; }), act.end());
-    std::vector<int> keep;
-    keep.reserve(S->part_used[p]);
-    for (int64_t id : S->active[p])
-      for (int s : S->reqs[id].slots) keep.push_back(s);
-    S->parts[p].slots.swap(keep);
+    act.erase(std::remove_if(act.begin(), act.end(), [](const Req *q) { return q->done; }), act.end());
+    // the slot list keeps its order (admission order) without the freed slots
+    auto &sl = S->parts[p].slots;
+    sl.erase(std::remove_if(sl.begin(), sl.end(), [&](int s) { return S->b->h_meta[s].horizon == 0; }), sl.end());
   }
   R.completing.clear();
   R.inflight = false;
@@ -369,13 +390,19 @@ int admit(kr_server *S, int p) {
     if (S->d_done) {  // the request's completion count starts at 0 (its tag may be a reused slot)
       cudaError_t ez = cudaMemsetAsync(S->d_done + q.slots[0], 0, sizeof(int), stream);
       if (ez != cudaSuccess) return S->cuda_fail(ez, "completion count");
+      S->prev_done[q.slots[0]] = 0;
     }
     q.part = p;
     q.admitted = t;
     q.rounds_left = (q.r.horizon + S->chunk - 1) / S->chunk;
+    q.pending = pop;
+    q.seq = S->admitted;
     S->part_used[p] += pop;
-    S->active[p].push_back(q.id);
-    for (int s : q.slots) S->parts[p].slots.push_back(s);
+    S->active[p].push_back(&q);
+    for (int s : q.slots) {
+      S->parts[p].slots.push_back(s);
+      S->slot_req[s] = &q;
+    }
     S->queue.pop_front();
     S->admitted++;
   }
@@ -420,10 +447,10 @@ int run_round(kr_server *S, int p) {
   // requests ending in this round: gather their results
   Stage &st = S->stage[p];
   int n_res = 0;
-  for (int64_t id : S->active[p]) {
-    Req &q = S->reqs[id];
+  for (Req *qp : S->active[p]) {
+    Req &q = *qp;
     if (--q.rounds_left > 0) continue;
-    R.completing.push_back(id);
+    R.completing.push_back(qp);
     for (int s : q.slots) st.h_rslots[n_res++] = s;
   }
   cudaStream_t stream = S->streams[p];
@@ -449,7 +476,8 @@ int run_round(kr_server *S, int p) {
 // Sliced scheduling.  After a slice: every slot's step counter from the
 // device (the slice may have been cut short, so the host does not know how
 // far each creature got), the requests whose creatures all reached their
-// horizons gathered and completed (finish_round), their slots freed.
+// horizons gathered and completed (finish_round) unless that happened while
+// the slice ran, their slots freed.
 int finish_slice(kr_server *S) {
   Round &R = S->round[0];
   Part &P = S->parts[0];
@@ -459,26 +487,29 @@ int finish_slice(kr_server *S) {
   cudaError_t e = cudaGetLastError();
   if (e == cudaSuccess)
     e = cudaMemcpyAsync(S->h_steps, S->d_steps, (size_t)S->capacity * sizeof(int), cudaMemcpyDeviceToHost, stream);
+  // the completion counts as the slice left them: the next slice's polls
+  // count from here
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(S->h_done, S->d_done, (size_t)S->capacity * sizeof(int), cudaMemcpyDeviceToHost, stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
   if (e != cudaSuccess) return S->cuda_fail(e, "slice step counters");
-  S->d2h_bytes += (uint64_t)S->capacity * sizeof(int);
+  S->d2h_bytes += 2 * (uint64_t)S->capacity * sizeof(int);
+  std::copy(S->h_done, S->h_done + S->capacity, S->prev_done.begin());
   for (int s : P.slots) {
     SlotMeta &m = S->b->h_meta[s];
     const int done = std::min(S->h_steps[s], m.horizon);
     S->creature_steps += done - m.step;
+    // a request ends with its last creature to reach its horizon
+    if (done == m.horizon && m.step < m.horizon && --S->slot_req[s]->pending == 0)
+      R.completing.push_back(S->slot_req[s]);
     m.step = done;
     S->b->h_remaining[s] = m.horizon - done;
   }
+  std::sort(R.completing.begin(), R.completing.end(), [](const Req *a, const Req *b) { return a->seq < b->seq; });
   int n_res = 0;
-  for (int64_t id : S->active[0]) {
-    Req &q = S->reqs[id];
-    bool ended = true;
-    for (int s : q.slots)
-      if (S->b->h_remaining[s] > 0) { ended = false; break; }
-    if (!ended) continue;
-    R.completing.push_back(id);
-    for (int s : q.slots) st.h_rslots[n_res++] = s;
-  }
+  for (const Req *q : R.completing)
+    if (!q->done)
+      for (int s : q->slots) st.h_rslots[n_res++] = s;
   if (n_res > 0) {
     e = cudaMemcpyAsync(st.d_rslots, st.h_rslots, (size_t)n_res * sizeof(int), cudaMemcpyHostToDevice, stream);
     if (e == cudaSuccess) {
@@ -496,10 +527,70 @@ int finish_slice(kr_server *S) {
   return KR_OK;
 }
 
+// While a slice runs: the device's per-request completion counts, copied
+// back at most once every kPollS seconds; the requests whose creatures all
+// reached their horizons since the poll before are completed at once --
+// their records copied back by the copy engine while the kernel goes on
+// (the kernel writes a creature's record before counting it).  Their slots
+// return to the pool when the slice ends.
+constexpr double kPollS = 1e-3;
+
+int poll_completions(kr_server *S) {
+  const double t = S->now();
+  if (!S->round[0].inflight || t - S->polled < kPollS) return KR_OK;
+  S->polled = t;
+  cudaError_t e = cudaMemcpyAsync(S->h_done, S->d_done, (size_t)S->capacity * sizeof(int), cudaMemcpyDeviceToHost,
+                                  S->ctl);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(S->ctl);
+  if (e != cudaSuccess) return S->cuda_fail(e, "completion counts");
+  S->d2h_bytes += (uint64_t)S->capacity * sizeof(int);
+  std::vector<Req *> ended;
+  for (int tag = 0; tag < S->capacity; tag++) {
+    if (S->h_done[tag] == S->prev_done[tag]) continue;
+    S->prev_done[tag] = S->h_done[tag];
+    Req *q = S->slot_req[tag];
+    if (q && !q->done && q->slots[0] == tag && S->h_done[tag] >= (int)q->slots.size()) ended.push_back(q);
+  }
+  if (ended.empty()) return KR_OK;
+  std::sort(ended.begin(), ended.end(), [](const Req *a, const Req *b) { return a->seq < b->seq; });
+  // the records, read by the copy engine (the running slice holds every SM):
+  // runs of nearby slots, one copy each, into the slice's result staging,
+  // which is idle until the slice ends (runs are disjoint ranges of the
+  // slots, so they fit its capacity records)
+  Stage &st = S->stage[0];
+  std::vector<int> &want = S->gather_slots;
+  want.clear();
+  for (const Req *q : ended) want.insert(want.end(), q->slots.begin(), q->slots.end());
+  std::sort(want.begin(), want.end());
+  constexpr int kRunGap = 16;  // records copied across a gap rather than a copy more
+  size_t off = 0;
+  for (size_t i = 0; i < want.size() && e == cudaSuccess;) {
+    const int a = want[i];
+    int b = a;
+    size_t j = i + 1;
+    while (j < want.size() && want[j] - b <= kRunGap) b = want[j++];
+    e = cudaMemcpyAsync(st.h_res + off, S->b->d_meta + a, (size_t)(b - a + 1) * sizeof(SlotMeta),
+                        cudaMemcpyDeviceToHost, S->ctl);
+    for (size_t k = i; k < j; k++) S->rec_pos[want[k]] = (int)(off + (size_t)(want[k] - a));
+    off += (size_t)(b - a + 1);
+    i = j;
+  }
+  if (e == cudaSuccess) e = cudaStreamSynchronize(S->ctl);
+  if (e != cudaSuccess) return S->cuda_fail(e, "streamed results");
+  S->d2h_bytes += (uint64_t)off * sizeof(SlotMeta);
+  const double tc = S->now();
+  std::vector<SlotMeta> rec;
+  for (Req *q : ended) {
+    rec.resize(q->slots.size());
+    for (size_t i = 0; i < q->slots.size(); i++) rec[i] = st.h_res[S->rec_pos[q->slots[i]]];
+    complete(S, *q, rec.data(), tc);
+    S->done_unfreed += (long)q->slots.size();
+  }
+  return KR_OK;
+}
+
 // true when the queue's first request has arrived and fits the free slots
-// plus the slots of the running requests whose creatures have all reached
-// their horizons by now (the kernel counts them per request; the counts are
-// polled at most once per millisecond, only while a request waits)
+// plus those of the requests completed while the slice runs
 bool admissible(kr_server *S) {
   if (S->queue.empty()) return false;
   const Req &q = S->reqs.at(S->queue.front());
@@ -508,41 +599,34 @@ bool admissible(kr_server *S) {
   // a slice runs at least 3 host gaps before an admission cuts it, so that
   // the GPU idles at most a quarter of the time however often requests come
   if (S->round[0].inflight && t - S->slice_t0 < 3 * S->gap_s) return false;
-  long fit = (long)S->free_slots.size();
-  if (q.r.population <= fit) return true;
-  if (!S->round[0].inflight || t - S->polled < 1e-3) return false;
-  S->polled = t;
-  if (cudaMemcpyAsync(S->h_done, S->d_done, (size_t)S->capacity * sizeof(int), cudaMemcpyDeviceToHost, S->ctl) !=
-          cudaSuccess ||
-      cudaStreamSynchronize(S->ctl) != cudaSuccess)
-    return false;
-  for (int64_t id : S->active[0]) {
-    const Req &a = S->reqs.at(id);
-    if (S->h_done[a.slots[0]] >= (int)a.slots.size()) fit += (long)a.slots.size();
-  }
-  return q.r.population <= fit;
+  return q.r.population <= (long)S->free_slots.size() + S->done_unfreed;
 }
 
-// One step of sliced scheduling: while a slice runs, preempt it if an
-// arrived request fits the free slots or its time is up (otherwise return
-// at once); after it, complete, admit and launch the next slice, every live
-// creature up to its horizon (at most chunk_steps env steps).
+// One step of sliced scheduling: while a slice runs, complete the requests
+// it has finished (poll_completions) and preempt it if an arrived request
+// fits or its time is up (otherwise return at once); after it, free the
+// completed requests' slots, admit and launch the next slice, every live
+// creature up to its horizon (at most chunk_steps env steps).  A relaunch
+// regroups the creatures by their remaining steps and spreads the longest
+// over every SM, so that the tail of long horizons runs with short steps:
+// slices make the rollouts' device time shorter, not only admissions sooner.
 int run_slice(kr_server *S) {
   Round &R = S->round[0];
   cudaError_t e;
-  if (R.inflight) {
-    if (!S->stop_sent) {
-      // the time slice: slice_ms, or 10 host gaps when those are longer (large
-      // populations), so that the GPU idles at most about a tenth of the time
-      if (!admissible(S) && S->now() - S->slice_t0 < std::max(S->slice_s, 10 * S->gap_s)) {
-        e = cudaEventQuery(R.done);
-        if (e == cudaErrorNotReady) return KR_OK;
-        if (e != cudaSuccess) return S->cuda_fail(e, "slice query");
-      } else {
-        e = cudaMemcpyAsync(S->d_stop, S->h_flag + 1, sizeof(int), cudaMemcpyHostToDevice, S->ctl);
-        if (e != cudaSuccess) return S->cuda_fail(e, "slice stop");
-        S->stop_sent = true;
-      }
+  if (R.inflight && !S->stop_sent) {
+    int rc = poll_completions(S);
+    if (rc != KR_OK) return rc;
+    // the time slice: slice_ms, or 10 host gaps when those are longer (large
+    // populations), so that the GPU idles at most about a tenth of the time
+    const bool time_up = S->now() - S->slice_t0 >= std::max(S->slice_s, 10 * S->gap_s);
+    if (!admissible(S) && !time_up) {
+      e = cudaEventQuery(R.done);
+      if (e == cudaErrorNotReady) return KR_OK;
+      if (e != cudaSuccess) return S->cuda_fail(e, "slice query");
+    } else {
+      e = cudaMemcpyAsync(S->d_stop, S->h_flag + 1, sizeof(int), cudaMemcpyHostToDevice, S->ctl);
+      if (e != cudaSuccess) return S->cuda_fail(e, "slice stop");
+      S->stop_sent = true;
     }
   }
   double ended = -1;
@@ -561,6 +645,9 @@ int run_slice(kr_server *S) {
   if (P.slots.empty()) return KR_OK;
   cudaStream_t stream = S->streams[0];
   e = cudaMemcpyAsync(S->d_stop, S->h_flag, sizeof(int), cudaMemcpyHostToDevice, stream);
+  // the slice's copies of the completion counts follow its admissions' resets
+  if (e == cudaSuccess) e = cudaEventRecord(S->staged, stream);
+  if (e == cudaSuccess) e = cudaStreamWaitEvent(S->ctl, S->staged, 0);
   if (e != cudaSuccess) return S->cuda_fail(e, "slice start");
   P.dirty = true;
   rc = launch_part(S->b, P, S->chunk, true);
@@ -684,6 +771,9 @@ extern "C" int kr_server_create(const kr_server_desc *d, kr_server **out) {
     if (e == cudaSuccess) e = cudaMallocHost(&S->h_done, (size_t)cap * sizeof(int));
     S->parts[0].tag_done = S->d_done;
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&S->ctl, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&S->staged, cudaEventDisableTiming);
+    S->prev_done.assign(cap, 0);
+    S->rec_pos.assign(cap, 0);
     S->parts[0].stop = S->d_stop;
   }
   for (int p = 0; p < (S->sliced ? 1 : 2); p++) {
@@ -707,6 +797,7 @@ extern "C" int kr_server_create(const kr_server_desc *d, kr_server **out) {
   if (e != cudaSuccess) { S->cuda_fail(e, "server setup"); return bail(KR_ERR_CUDA); }
   S->free_slots.resize(cap);
   for (int s = 0; s < cap; s++) S->free_slots[s] = cap - 1 - s;  // lowest slots first
+  S->slot_req.assign(cap, nullptr);
   S->device_bytes = ps * (uint64_t)cap + fixed_bytes(*d);
   *out = S;
   return KR_OK;
@@ -910,6 +1001,7 @@ extern "C" void kr_server_destroy(kr_server *S) {
   if (S->d_done) cudaFree(S->d_done);
   if (S->h_done) cudaFreeHost(S->h_done);
   if (S->ctl) cudaStreamDestroy(S->ctl);
+  if (S->staged) cudaEventDestroy(S->staged);
   if (S->b) kr_batch_destroy(S->b);
   delete S;
 }

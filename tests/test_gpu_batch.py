@@ -94,6 +94,34 @@ def test_chunked_runs_and_graph_equal_one_run():
         e.close()
 
 
+@pytest.mark.parametrize("slice_ms", [0.3, 2.0])
+def test_time_sliced_run_equals_one_launch(slice_ms):
+    """Preemptible time slices (creatures stopped mid-rollout, regrouped and
+    relaunched) end in the one launch's state and metrics, bit for bit; a
+    step-limited run (max_steps short of the horizons) stays one launch."""
+    w = workloads.uneven(n=700, n_maps=6, seed=21, h_min=40, h_max=900)
+    H = int(w.horizon.max())
+    ref = batch.BatchEngine(w.maps, w.n)
+    workloads.spawn_all(ref, w)
+    ref.run(H)
+    a, ma = ref.read_state(), ref.read_metrics()
+    ref.close()
+    eng = batch.BatchEngine(w.maps, w.n)
+    workloads.spawn_all(eng, w)
+    eng.set_slice(slice_ms)
+    eng.run(H // 3)
+    assert eng.last_slices() == 1
+    eng.run(H)
+    assert eng.last_slices() > 1
+    assert eng.last_ms() > 0
+    b, mb = eng.read_state(), eng.read_metrics()
+    eng.close()
+    for f in ("px", "py", "ang", "vx", "vy", "av", "steps"):
+        assert np.array_equal(a[f], b[f]), f
+    assert np.array_equal(ma, mb)
+    assert np.array_equal(b["steps"], w.horizon)
+
+
 @pytest.mark.parametrize("lanes,warps,ctas,unroll", [(32, 1, 1, 1), (32, 16, 1, 2), (16, 4, 2, 1), (16, 8, 0, 2),
                                                       (8, 2, 4, 1), (8, 16, 1, 1), (8, 8, 0, 2), (16, 4, 5, 1),
                                                       (16, 4, 6, 2), (32, 8, 3, 1)])

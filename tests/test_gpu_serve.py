@@ -2,7 +2,8 @@
 the mix, queued admission under an HBM budget, repeatability -- under both
 schedulers: two partitions in alternating rounds (slice_ms = 0) and one
 partition in preemptible slices (slice_ms > 0; small slices here, so that
-slices are cut by arrivals and by time)."""
+slices are cut by arrivals and by time; completions found by polling while
+a slice runs)."""
 import numpy as np
 import pytest
 
@@ -141,7 +142,7 @@ def test_served_uneven_workload_equals_batched_engine(mode):
     """The mixed workload submitted as requests (one per creature, its own
     pose, control stream and horizon) gives the batched engine's results --
     with slices cut every half millisecond, and with slices that run until
-    an arrival fits (here: a creature's slot frees only when its slice ends)."""
+    an arrival fits (a creature's slot frees only when its slice ends)."""
     w = workloads.uneven(n=60, n_maps=5, seed=13, h_min=30, h_max=120)
     eng = batch.BatchEngine(w.maps, w.n)
     workloads.spawn_all(eng, w)
@@ -163,3 +164,41 @@ def test_served_uneven_workload_equals_batched_engine(mode):
     srv.close()
     assert np.array_equal(np.concatenate([got, rest]), want)
     assert np.all(times[:, 0] <= times[:, 1]) and np.all(times[:, 1] <= times[:, 2])
+
+
+def test_sliced_requests_complete_while_their_slice_runs():
+    """Slices: a short request completes (its records copied back beside the
+    running kernel) while the slice that runs it still runs a long one --
+    one slice in all, its time (10 s) longer than the run -- and every
+    request's results equal the batched engine's."""
+    import time
+
+    w = workloads.uneven(n=6, n_maps=2, seed=17, h_min=20, h_max=30)
+    w.horizon[0] = 3000  # the long request
+    eng = batch.BatchEngine(w.maps, w.n)
+    workloads.spawn_all(eng, w)
+    eng.run(int(w.horizon.max()))
+    want = eng.read_metrics()
+    eng.close()
+    srv = serve.Server(w.maps, 1 << 30, max_slots=8, policy=False, slice_ms=10000.0, chunk_steps=1 << 20)
+    ids = list(srv.submit_many(w.horizon, w.arms, w.segs, w.map_id, w.x, w.y, w.angle, control_seeds=w.seed))
+    early = None
+    t_end = time.monotonic() + 60
+    while time.monotonic() < t_end:
+        busy = srv.pump()
+        done = set(srv.poll())
+        if done and early is None:
+            early = (srv.stats(), done)
+        if not busy:
+            break
+        time.sleep(0.0002)
+    srv.drain()
+    rest, times = srv.results_many(ids, release=True)
+    st = srv.stats()
+    srv.close()
+    assert early is not None
+    first_stats, first_done = early
+    assert ids[0] not in first_done and first_stats["rounds"] == 1
+    assert st["rounds"] == 1  # nothing preempted: the one slice ran every request
+    assert np.all(times[1:, 2] < times[0, 2])
+    assert np.array_equal(rest, want)
