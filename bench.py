@@ -555,6 +555,27 @@ def main():
         tune = {best: ms}
     unroll = eng.get_launch()["substep_unroll"]
     eng.set_slice(args.engine_slice_ms)
+    shape_choice = None
+    if args.engine_slice_ms > 0 and not args.shape:
+        # the autotuner times 64 steps of the whole population; a sliced
+        # rollout also runs the tail, where the automatic shape of each slice
+        # (more lanes per creature as creatures finish) may be faster: two
+        # whole rollouts with each, the faster kept (untimed, as warm-up)
+        def rollout_ms():
+            eng.restore()
+            eng.run(max_h)
+            eng.sync()
+            return eng.last_ms()
+
+        t_tuned = min(rollout_ms(), rollout_ms())
+        eng.set_launch(0, 0, lanes_per_creature=0)
+        t_auto = min(rollout_ms(), rollout_ms())
+        shape_choice = {"autotuned_ms": round(t_tuned, 3), "automatic_ms": round(t_auto, 3)}
+        if t_tuned <= t_auto:
+            eng.set_launch(best[1], best[2], lanes_per_creature=best[0])
+        else:
+            best = ("automatic per slice",) * 3
+        shape_choice["kept"] = "autotuned" if t_tuned <= t_auto else "automatic"
 
     # warm-up: full rollouts, each as a timed one runs
     for _ in range(args.warmup):
@@ -578,7 +599,7 @@ def main():
         eng.restore()
         eng.run(max_h)
         ev[k + 1].record(stream)
-        slices, kernels = eng.last_run_launches()
+        slices, kernels, creature_launches = eng.last_run_launches()
         gpu_launches += kernels
     ev[-1].synchronize()
     barrier()
@@ -647,8 +668,9 @@ def main():
                                               form="the same, two partitions in rounds of chunk_steps")
 
     # the engine's own host-buffer API: spawn from host arrays (poses,
-    # shapes, horizons, seeds), one persistent launch, the metrics record read
-    # back -- per rollout, wall-clock through the C ABI
+    # shapes, horizons, seeds), one kr_batch_run (in time slices, as the timed
+    # rollouts), the metrics record read back -- per rollout, wall-clock
+    # through the C ABI
     if rank == 0:
         reps = []
         for _ in range(3):
@@ -659,7 +681,8 @@ def main():
             reps.append(time.perf_counter() - t0)
         extra["engine_api_e2e"] = {
             "value": units / min(reps[1:]), "unit": UNIT,
-            "form": "batched engine C ABI: kr_batch_spawn from host arrays, kr_batch_run, kr_batch_read_metrics",
+            "form": "batched engine C ABI: kr_batch_spawn from host arrays, kr_batch_run (time slices as the timed "
+                    "rollouts), kr_batch_read_metrics",
             # the library's staging of each spawned creature: its pose block (6 x 76 f32), slot record
             # (184 B) and slot index; the metrics record back
             "h2d_bytes_per_step": int(w.n * (6 * 76 * 4 + 184 + 4)), "d2h_bytes_per_step": int(m.nbytes),
@@ -689,10 +712,13 @@ def main():
             achieved = ops * units / (kms / 1000.0)
             roof = {"bound": "fp32", "achieved": achieved / 1e12, "peak": fma_rate / 1e12,
                     "unit": "TFLOP/s", "frac": achieved / fma_rate,
-                    "traffic": args.traffic if args.traffic is not None else NCU_DRAM_BYTES_PER_CREATURE * w.n,
-                    "traffic_note": "ncu dram__bytes_read.sum + dram__bytes_write.sum per creature of a one-launch "
-                                    "capture (8,192 creatures: 2,587 B each: state, grips, controls and slot "
-                                    "records in and out once) x the creatures of this launch; algorithmic ~2.5 KB",
+                    "traffic": (args.traffic if args.traffic is not None
+                                else NCU_DRAM_BYTES_PER_CREATURE * creature_launches),
+                    "traffic_note": "per rollout, as achieved: ncu dram__bytes_read.sum + dram__bytes_write.sum per "
+                                    "creature of a one-launch capture (8,192 creatures: 2,587 B each: state, grips, "
+                                    "controls and slot records in and out once per launch) x the creatures the "
+                                    f"rollout's {slices} launch(es) ran ({creature_launches}); algorithmic ~2.5 KB "
+                                    "per creature per launch",
                     "ops_per_creature_step": ops, "kernel_ms": kms,
                     "kernel_ms_note": (f"the rollout's {slices} time-slice launches of batch_kernel, first to last, "
                                        "the host time between them included" if slices > 1 else
@@ -713,7 +739,7 @@ def main():
                      (f"each rollout in preemptible time slices of {args.engine_slice_ms:g} ms, the live creatures "
                       "regrouped between slices" if slices > 1 else "one launch per rollout")),
             "launch": {"lanes_per_creature": best[0], "warps_per_cta": best[1], "ctas_per_sm": best[2],
-                       "substep_unroll": unroll, "time_slices_per_rollout": slices,
+                       "substep_unroll": unroll, "time_slices_per_rollout": slices, "shape_choice": shape_choice,
                        "slice_ms": args.engine_slice_ms if slices > 1 else None,
                        "autotune_ms": {",".join(map(str, k)): round(v, 3) for k, v in tune.items()}},
             "roofline": roof, "cpu_baseline": cpu, "clocks": clocks, "e2e": e2e,

@@ -153,11 +153,13 @@ int kr_batch_run(kr_batch *b, int32_t max_steps);
  * results are bit-identical to one launch.  A slice that advanced no
  * creature doubles the next one's time.  0 (default): one launch.
  * kr_batch_last_ms then covers the whole run, host time between slices
- * included; kr_batch_last_slices gives the slices it took and the kernels
- * it launched (slices and step-counter readbacks; 1 and 1 for one launch).
- * Either pointer may be NULL. */
+ * included; kr_batch_last_slices gives the slices it took, the kernels it
+ * launched (slices and step-counter readbacks; 1 and 1 for one launch) and
+ * the creatures its slices launched, summed over the slices (each slice
+ * loads and writes back the state of the creatures it runs).  Any pointer
+ * may be NULL. */
 int kr_batch_set_slice(kr_batch *b, float slice_ms);
-int kr_batch_last_slices(kr_batch *b, int32_t *slices, int32_t *kernels);
+int kr_batch_last_slices(kr_batch *b, int32_t *slices, int32_t *kernels, int64_t *creature_launches);
 
 /* `launches` back-to-back launches of steps_per_launch env steps each over
  * the same creature groups, no host work between them (with
@@ -234,7 +236,9 @@ int kr_probe_wrap(const double *d, int32_t n, double *out);
  * Until this is called the engine picks the shape per launch: 32 lanes x 4
  * warps below 16 live creatures per SM, 16 lanes x 8 warps below 96 (8
  * lanes when most creatures run the fused policy or an observation ring is
- * kept), else 8 lanes x 8 warps.  Results do not depend on the launch shape. */
+ * kept), else 8 lanes x 8 warps; lanes_per_creature = 0 returns to that
+ * (the other arguments are ignored).  Results do not depend on the launch
+ * shape. */
 int kr_batch_set_launch(kr_batch *b, int32_t lanes_per_creature, int32_t warps_per_cta,
                         int32_t ctas_per_sm);
 

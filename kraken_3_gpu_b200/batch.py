@@ -58,6 +58,7 @@ METRIC_WORDS = len(METRIC_FIELDS)
 _F32P = C.POINTER(C.c_float)
 _F64P = C.POINTER(C.c_double)
 _I32P = C.POINTER(C.c_int32)
+_I64P = C.POINTER(C.c_int64)
 _U32P = C.POINTER(C.c_uint32)
 
 
@@ -103,7 +104,7 @@ def _lib():
         "kr_batch_get_unroll": (C.c_int, [vp, _I32P]),
         "kr_batch_last_ms": (C.c_int, [vp, _F32P]),
         "kr_batch_set_slice": (C.c_int, [vp, C.c_float]),
-        "kr_batch_last_slices": (C.c_int, [vp, _I32P, _I32P]),
+        "kr_batch_last_slices": (C.c_int, [vp, _I32P, _I32P, _I64P]),
         "kr_batch_sync": (C.c_int, [vp]),
         "kr_batch_set_stream": (C.c_int, [vp, vp]),
         "kr_batch_destroy": (None, [vp]),
@@ -242,8 +243,9 @@ class BatchEngine:
         _check(_lib().kr_batch_restore(self.h), self.h)
 
     def set_launch(self, warps_per_cta, ctas_per_sm=0, lanes_per_creature=32):
-        """Launch shape: G lanes per creature (32, 16 or 8), warps per CTA,
-        CTAs per SM (0: 16 / warps).  Results do not depend on it."""
+        """Launch shape: G lanes per creature (32, 16 or 8; 0: the automatic
+        shape of every launch again), warps per CTA, CTAs per SM (0: 16 /
+        warps).  Results do not depend on it."""
         _check(_lib().kr_batch_set_launch(self.h, lanes_per_creature, warps_per_cta, ctas_per_sm),
                self.h)
 
@@ -282,10 +284,11 @@ class BatchEngine:
         return self.last_run_launches()[0]
 
     def last_run_launches(self):
-        """(slices, kernels launched) of the last run."""
-        n, k = C.c_int32(), C.c_int32()
-        _check(_lib().kr_batch_last_slices(self.h, C.byref(n), C.byref(k)), self.h)
-        return n.value, k.value
+        """(slices, kernels launched, creatures launched summed over the
+        slices) of the last run."""
+        n, k, c = C.c_int32(), C.c_int32(), C.c_int64()
+        _check(_lib().kr_batch_last_slices(self.h, C.byref(n), C.byref(k), C.byref(c)), self.h)
+        return n.value, k.value, c.value
 
     def run_launches(self, steps_per_launch, launches):
         _check(_lib().kr_batch_run_launches(self.h, steps_per_launch, launches), self.h)

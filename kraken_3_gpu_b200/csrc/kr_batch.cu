@@ -1449,6 +1449,8 @@ int run_sliced(kr_batch *b, int max_steps) {
   double slice_s = b->slice_ms * 1e-3;
   long long steps_before = -1;
   b->last_slices = b->last_kernels = 0;
+  b->last_creature_launches = 0;
+  long live = (long)run.size();
   for (int k = 0;; k++) {
     e = cudaMemcpyAsync(b->d_stop, b->h_flag, sizeof(int), cudaMemcpyHostToDevice, st);
     if (e == cudaSuccess) e = cudaEventRecord(b->slice_start, st);
@@ -1463,6 +1465,7 @@ int run_sliced(kr_batch *b, int max_steps) {
     if (p.n_groups == 0) break;
     b->last_slices++;
     b->last_kernels++;
+    b->last_creature_launches += live;
     e = cudaEventRecord(b->slice_end, st);
     if (e != cudaSuccess) return b->cuda_fail(e, "slice record");
     // the slice's time counts from when its launch is next on the stream
@@ -1497,7 +1500,7 @@ int run_sliced(kr_batch *b, int max_steps) {
       e = cudaMemcpyAsync(b->h_steps, b->d_steps, (size_t)b->capacity * sizeof(int), cudaMemcpyDeviceToHost, st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     if (e != cudaSuccess) return b->cuda_fail(e, "slice step counters");
-    long live = 0;
+    live = 0;
     long long steps = 0;
     for (int s : run) {
       b->h_remaining[s] = std::max(0, b->h_meta[s].horizon - b->h_steps[s]);
@@ -1868,8 +1871,17 @@ extern "C" int kr_batch_read_net(kr_batch *b, int32_t first, int32_t n, float *i
 extern "C" int kr_batch_set_launch(kr_batch *b, int32_t lanes_per_creature, int32_t warps_per_cta,
                                    int32_t ctas_per_sm) {
   if (!b) return KR_ERR_INVALID;
+  if (lanes_per_creature == 0) {  // back to the automatic shape of every launch
+    if (!b->auto_shape || b->ctas_per_sm != 0) {
+      b->main.dirty = true;
+      b->shape_dirty = true;
+    }
+    b->ctas_per_sm = 0;
+    b->auto_shape = true;
+    return KR_OK;
+  }
   if (lanes_per_creature != 32 && lanes_per_creature != 16 && lanes_per_creature != 8)
-    return b->fail(KR_ERR_INVALID, "lanes_per_creature must be 32, 16 or 8");
+    return b->fail(KR_ERR_INVALID, "lanes_per_creature must be 32, 16 or 8 (0: automatic)");
   if (warps_per_cta < 1 || warps_per_cta > kMaxW) return b->fail(KR_ERR_INVALID, "warps_per_cta outside 1..16");
   if (warps_per_cta * (32 / lanes_per_creature) > kMaxCPC)
     return b->fail(KR_ERR_INVALID, "more than 64 creatures per CTA");
@@ -1922,8 +1934,11 @@ extern "C" int kr_batch_run(kr_batch *b, int32_t max_steps) {
     for (int s = 0; s < b->capacity && to_horizon; s++) to_horizon = b->h_remaining[s] <= max_steps;
     if (to_horizon) return run_sliced(b, max_steps);
   }
+  long long live = 0;
+  for (int s = 0; s < b->capacity; s++) live += b->h_remaining[s] > 0;
   const int rc = launch_part(b, b->main, max_steps, true);
   b->last_slices = b->last_kernels = b->main.n_groups > 0 ? 1 : 0;
+  b->last_creature_launches = b->main.n_groups > 0 ? live : 0;
   return rc;
 }
 
@@ -1934,10 +1949,11 @@ extern "C" int kr_batch_set_slice(kr_batch *b, float slice_ms) {
   return KR_OK;
 }
 
-extern "C" int kr_batch_last_slices(kr_batch *b, int32_t *slices, int32_t *kernels) {
+extern "C" int kr_batch_last_slices(kr_batch *b, int32_t *slices, int32_t *kernels, int64_t *creature_launches) {
   if (!b) return KR_ERR_INVALID;
   if (slices) *slices = b->last_slices;
   if (kernels) *kernels = b->last_kernels;
+  if (creature_launches) *creature_launches = b->last_creature_launches;
   return KR_OK;
 }
 

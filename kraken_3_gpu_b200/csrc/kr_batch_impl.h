@@ -330,6 +330,7 @@ struct kr_batch {
   cudaStream_t ctl = nullptr;          // the stop word's copy while a slice runs
   cudaEvent_t slice_start = nullptr, slice_end = nullptr;
   int last_slices = 0, last_kernels = 0;  // of the last kr_batch_run
+  long long last_creature_launches = 0;    // ... live creatures per slice, summed
 
   int fail(int code, const std::string &m) { err = m; return code; }
   int cuda_fail(cudaError_t e, const char *what) {
