@@ -109,10 +109,14 @@ def test_time_sliced_run_equals_one_launch(slice_ms):
     eng = batch.BatchEngine(w.maps, w.n)
     workloads.spawn_all(eng, w)
     eng.set_slice(slice_ms)
+    eng.set_launch(8, 0, lanes_per_creature=16)
     eng.run(H // 3)
-    assert eng.last_slices() == 1
+    assert eng.last_run_launches() == (1, 1, w.n)
+    eng.set_launch(0, 0, lanes_per_creature=0)  # the automatic shape of every slice
+    live = int(np.sum(w.horizon > H // 3))
     eng.run(H)
-    assert eng.last_slices() > 1
+    slices, kernels, launched = eng.last_run_launches()
+    assert slices > 1 and kernels in (2 * slices - 1, 2 * slices) and launched >= live + slices - 1
     assert eng.last_ms() > 0
     b, mb = eng.read_state(), eng.read_metrics()
     eng.close()
