@@ -21,6 +21,7 @@
 #include <cstring>
 #include <map>
 #include <string>
+#include <system_error>
 #include <thread>
 #include <vector>
 
@@ -1364,14 +1365,13 @@ int launch_part(kr_batch *b, Part &p, int max_steps, bool timed) {
   return KR_OK;
 }
 
-int prepare_spawn(kr_batch *b, int n, const int32_t *arms, const int32_t *segs, const int32_t *map_id,
-                  const double *x, const double *y, const double *angle, const int32_t *horizon,
-                  const uint32_t *control_seed, const float *tone, int ctrl_mode, SpawnInit *out,
-                  int *first_bad) {
+int prepare_spawn_into(kr_batch *b, int n, const int32_t *arms, const int32_t *segs, const int32_t *map_id,
+                       const double *x, const double *y, const double *angle, const int32_t *horizon,
+                       const uint32_t *control_seed, const float *tone, int ctrl_mode, const int32_t *ctrl,
+                       float *pose, SlotMeta *meta, int *first_bad) {
+  // checks and body templates, in order (a template is built on first use)
   const size_t tpl_before = b->tpls.size();
-  out->pose.assign((size_t)n * kStateStride, 0.f);
-  out->meta.assign(n, SlotMeta{});
-  std::vector<double> px(kr::kMaxTplBodies), py(kr::kMaxTplBodies), pa(kr::kMaxTplBodies);
+  std::vector<int> tid(n);
   for (int i = 0; i < n; i++) {
     *first_bad = i;
     const int t = ensure_template(b, arms[i], segs[i]);
@@ -1381,35 +1381,76 @@ int prepare_spawn(kr_batch *b, int n, const int32_t *arms, const int32_t *segs, 
     if (map_id[i] < 0 || map_id[i] >= b->n_maps)
       return b->fail(KR_ERR_INDEX, "map " + std::to_string(map_id[i]) + " of " + std::to_string(b->n_maps));
     if (horizon[i] < 0) return b->fail(KR_ERR_INVALID, "negative horizon");
-    const kr::Template &T = b->tpls[t];
-    kr::spawn_pose(T, x[i], y[i], angle[i], 0.28, px.data(), py.data(), pa.data());
-    float *dst = out->pose.data() + (size_t)i * kStateStride;
-    for (int j = 0; j < T.nb; j++) {
-      dst[j] = (float)px[j];
-      dst[kBodyPad + j] = (float)py[j];
-      dst[4 * kBodyPad + j] = (float)pa[j];
-    }
-    SlotMeta &m = out->meta[i];
-    m = SlotMeta{};
-    m.tpl = t;
-    m.map = map_id[i];
-    m.horizon = horizon[i];
-    m.step = 0;
-    m.ctrl = ctrl_mode;
-    m.rng = control_seed ? control_seed[i] : 0u;
-    const double tn = std::max(0.0, std::min(1.0, tone ? (double)tone[i] : 0.5));
-    m.tone = (float)tn;
-    m.comp = (float)(1.0 / (2000.0 + tn * (400000.0 - 2000.0)));
-    m.last_x = (double)(float)x[i];
-    m.last_y = (double)(float)y[i];
-    m.tone_d = tn;
-    m.spawn_x = x[i];
-    m.spawn_y = y[i];
-    m.spawn_reach = T.reach;  // replaced by measureReach in spawn_kernel
+    tid[i] = t;
   }
   *first_bad = -1;
+  // spawn poses (spawnKraken: a cos and a sin per segment, in f64) and slot
+  // records of creatures [lo, hi); creatures are independent, so large
+  // batches are split over host threads
+  auto fill = [&](int lo, int hi) {
+    double px[kr::kMaxTplBodies], py[kr::kMaxTplBodies], pa[kr::kMaxTplBodies];
+    for (int i = lo; i < hi; i++) {
+      const kr::Template &T = b->tpls[tid[i]];
+      kr::spawn_pose(T, x[i], y[i], angle[i], 0.28, px, py, pa);
+      float *dst = pose + (size_t)i * kStateStride;
+      std::fill(dst, dst + kStateStride, 0.f);
+      for (int j = 0; j < T.nb; j++) {
+        dst[j] = (float)px[j];
+        dst[kBodyPad + j] = (float)py[j];
+        dst[4 * kBodyPad + j] = (float)pa[j];
+      }
+      SlotMeta &m = meta[i];
+      m = SlotMeta{};
+      m.tpl = tid[i];
+      m.map = map_id[i];
+      m.horizon = horizon[i];
+      m.step = 0;
+      m.ctrl = ctrl ? ctrl[i] : ctrl_mode;
+      m.rng = control_seed ? control_seed[i] : 0u;
+      const double tn = std::max(0.0, std::min(1.0, tone ? (double)tone[i] : 0.5));
+      m.tone = (float)tn;
+      m.comp = (float)(1.0 / (2000.0 + tn * (400000.0 - 2000.0)));
+      m.last_x = (double)(float)x[i];
+      m.last_y = (double)(float)y[i];
+      m.tone_d = tn;
+      m.spawn_x = x[i];
+      m.spawn_y = y[i];
+      m.spawn_reach = T.reach;  // replaced by measureReach in spawn_kernel
+    }
+  };
+  constexpr int kPerThread = 1024;
+  const int hw = (int)std::max(1u, std::thread::hardware_concurrency());
+  const int nt = std::min({16, hw, n / kPerThread});
+  if (nt <= 1) {
+    fill(0, n);
+  } else {
+    std::vector<std::thread> th;
+    int started = 0;
+    for (int k = 1; k < nt; k++) {
+      const int lo = (int)((long)n * k / nt), hi = (int)((long)n * (k + 1) / nt);
+      try {
+        th.emplace_back(fill, lo, hi);
+        started = k;
+      } catch (const std::system_error &) {
+        break;  // no more threads: this thread fills the rest
+      }
+    }
+    fill(0, (int)((long)n * 1 / nt));
+    if (started < nt - 1) fill((int)((long)n * (started + 1) / nt), n);
+    for (auto &t : th) t.join();
+  }
   if (b->tpls.size() != tpl_before) return upload_templates(b);
   return KR_OK;
+}
+
+int prepare_spawn(kr_batch *b, int n, const int32_t *arms, const int32_t *segs, const int32_t *map_id,
+                  const double *x, const double *y, const double *angle, const int32_t *horizon,
+                  const uint32_t *control_seed, const float *tone, int ctrl_mode, SpawnInit *out,
+                  int *first_bad) {
+  out->pose.resize((size_t)n * kStateStride);
+  out->meta.resize(n);
+  return prepare_spawn_into(b, n, arms, segs, map_id, x, y, angle, horizon, control_seed, tone, ctrl_mode, nullptr,
+                            out->pose.data(), out->meta.data(), first_bad);
 }
 
 cudaError_t launch_spawn(kr_batch *b, const int *d_slots, const float *d_pose, const SlotMeta *d_meta,

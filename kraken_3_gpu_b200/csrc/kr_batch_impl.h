@@ -356,6 +356,13 @@ int build_groups(kr_batch *b, Part &p, int max_steps);
 // one persistent launch over the part's groups, min(max_steps, remaining)
 // env steps per slot; asynchronous on the part's stream
 int launch_part(kr_batch *b, Part &p, int max_steps, bool timed);
+// host-side initial data of n creatures into pose (n x kStateStride f32,
+// every word written) and meta (n records); ctrl: per-creature control mode
+// (NULL: ctrl_mode for all).  Fails on a bad body shape, map or horizon.
+int prepare_spawn_into(kr_batch *b, int n, const int32_t *arms, const int32_t *segs, const int32_t *map_id,
+                       const double *x, const double *y, const double *angle, const int32_t *horizon,
+                       const uint32_t *control_seed, const float *tone, int ctrl_mode, const int32_t *ctrl,
+                       float *pose, SlotMeta *meta, int *first_bad);
 // host-side initial data of n creatures (spawn pose, meta); fails on a bad
 // body shape or map
 int prepare_spawn(kr_batch *b, int n, const int32_t *arms, const int32_t *segs, const int32_t *map_id,

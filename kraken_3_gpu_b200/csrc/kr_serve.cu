@@ -103,6 +103,13 @@ __global__ void gather_kernel(const SlotMeta *meta, const int *slots, int n, Slo
   out[i] = meta[slots[i]];
 }
 
+// the completion count of every request admitted in a staging starts at 0:
+// its tag (the request's first slot) may have counted an earlier request
+__global__ void clear_done_kernel(const SlotMeta *meta, const int *slots, int n, int *done) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n && meta[i].pad == slots[i]) done[slots[i]] = 0;
+}
+
 // every slot's step counter into one contiguous array (read back after a slice)
 __global__ void steps_kernel(const SlotMeta *meta, int n, int *out) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -123,6 +130,15 @@ struct Req {
   int pending = 0;                      // sliced scheduling: creatures not yet at their horizon
   int64_t seq = 0;                      // admission order
   bool done = false;
+};
+
+// admission's per-creature inputs, reused between admissions
+struct AdmitScratch {
+  std::vector<Req *> reqs;
+  std::vector<int32_t> arms, segs, maps, hor, ctrl;
+  std::vector<double> xs, ys, an;
+  std::vector<uint32_t> seeds;
+  std::vector<float> tones;
 };
 
 // staging of one partition (pinned host + device), reused every round
@@ -188,6 +204,7 @@ struct kr_server {
   int capacity = 0, part_cap = 0, chunk = 1;
   uint64_t bytes_per_slot = 0, device_bytes = 0;
   std::deque<int64_t> queue;
+  AdmitScratch adm;
   std::unordered_map<int64_t, Req> reqs;
   std::vector<int> free_slots;
   std::vector<int64_t> done_ids;
@@ -334,64 +351,85 @@ int admit(kr_server *S, int p) {
   Stage &st = S->stage[p];
   cudaStream_t stream = S->streams[p];
   const double t = S->now();
+  // the arrived requests that fit, in FIFO order
+  AdmitScratch &A = S->adm;
+  A.reqs.clear();
   int n_new = 0, n_theta = 0, theta_off = 0;
-  while (!S->queue.empty()) {
-    Req &q = S->reqs[S->queue.front()];
-    if (q.arrival > t) break;
-    const int pop = q.r.population;
-    if (pop > (int)S->free_slots.size() || S->part_used[p] + pop > S->part_cap) break;
-    const bool pol = !q.theta.empty();
-    const int ctrl = !pol ? KR_CTRL_STREAM : S->d.net ? KR_CTRL_NET : KR_CTRL_POLICY;
-    if (pol && n_theta >= kMaxThetaPerRound) break;
-    // the creatures' initial data
-    const std::vector<int32_t> arms(pop, q.r.arms), segs(pop, q.r.segs), maps(pop, q.r.map_id), hor(pop, q.r.horizon);
-    std::vector<double> xs = q.xs, ys = q.ys, an = q.angles;
-    if (xs.empty()) { xs.assign(pop, q.r.x); ys.assign(pop, q.r.y); an.assign(pop, q.r.angle); }
-    std::vector<uint32_t> seeds = q.seeds;
-    if (seeds.empty()) {
-      seeds.resize(pop);
-      for (int i = 0; i < pop; i++) seeds[i] = (uint32_t)splitmix64(q.r.seed + (uint64_t)(q.r.first_individual + i));
+  {
+    long free_left = (long)S->free_slots.size();
+    int used = S->part_used[p];
+    for (int64_t id : S->queue) {
+      Req &q = S->reqs[id];
+      if (q.arrival > t) break;
+      const int pop = q.r.population;
+      if (pop > free_left || used + pop > S->part_cap) break;
+      if (!q.theta.empty()) {
+        if (n_theta >= kMaxThetaPerRound) break;
+        n_theta++;
+      }
+      free_left -= pop;
+      used += pop;
+      n_new += pop;
+      A.reqs.push_back(&q);
     }
-    const std::vector<float> tones(pop, q.r.tone);
-    SpawnInit init;
-    int bad = -1;
-    int rc = prepare_spawn(S->b, pop, arms.data(), segs.data(), maps.data(), xs.data(), ys.data(), an.data(),
-                           hor.data(), seeds.data(), tones.data(), ctrl, &init, &bad);
-    if (rc != KR_OK) return S->batch_fail(rc);
+  }
+  if (A.reqs.empty()) return KR_OK;
+  // every admitted creature's initial data, one call, written into the staging
+  A.arms.resize(n_new); A.segs.resize(n_new); A.maps.resize(n_new); A.hor.resize(n_new); A.ctrl.resize(n_new);
+  A.xs.resize(n_new); A.ys.resize(n_new); A.an.resize(n_new); A.seeds.resize(n_new); A.tones.resize(n_new);
+  int k = 0;
+  for (const Req *qp : A.reqs) {
+    const Req &q = *qp;
+    const int pop = q.r.population;
+    const int ctrl = q.theta.empty() ? KR_CTRL_STREAM : S->d.net ? KR_CTRL_NET : KR_CTRL_POLICY;
+    for (int i = 0; i < pop; i++, k++) {
+      A.arms[k] = q.r.arms; A.segs[k] = q.r.segs; A.maps[k] = q.r.map_id; A.hor[k] = q.r.horizon; A.ctrl[k] = ctrl;
+      A.xs[k] = q.xs.empty() ? q.r.x : q.xs[i];
+      A.ys[k] = q.xs.empty() ? q.r.y : q.ys[i];
+      A.an[k] = q.xs.empty() ? q.r.angle : q.angles[i];
+      A.seeds[k] = q.seeds.empty() ? (uint32_t)splitmix64(q.r.seed + (uint64_t)(q.r.first_individual + i)) : q.seeds[i];
+      A.tones[k] = q.r.tone;
+    }
+  }
+  int bad = -1;
+  int rc = prepare_spawn_into(S->b, n_new, A.arms.data(), A.segs.data(), A.maps.data(), A.xs.data(), A.ys.data(),
+                              A.an.data(), A.hor.data(), A.seeds.data(), A.tones.data(), KR_CTRL_STREAM, A.ctrl.data(),
+                              st.h_pose, st.h_meta, &bad);
+  if (rc != KR_OK) return S->batch_fail(rc);
+  // slots, request tags, weight jobs and the host mirrors
+  k = 0;
+  for (Req *qp : A.reqs) {
+    Req &q = *qp;
+    const int pop = q.r.population;
+    const bool pol = !q.theta.empty();
     q.slots.resize(pop);
     for (int i = 0; i < pop; i++) {
       const int s = S->free_slots.back();
       S->free_slots.pop_back();
       q.slots[i] = s;
-      std::copy(init.pose.begin() + (size_t)i * kStateStride, init.pose.begin() + (size_t)(i + 1) * kStateStride,
-                st.h_pose + (size_t)n_new * kStateStride);
-      st.h_meta[n_new] = init.meta[i];
-      st.h_meta[n_new].pad = q.slots[0];  // the request's tag: its first slot
-      st.h_slots[n_new] = s;
+    }
+    for (int i = 0; i < pop; i++, k++) {
+      const int s = q.slots[i];
+      S->b->h_meta[s] = st.h_meta[k];
+      S->b->h_remaining[s] = st.h_meta[k].horizon;
+      st.h_meta[k].pad = q.slots[0];  // the request's tag: its first slot
+      st.h_slots[k] = s;
       if (pol) {
-        PJob &j = st.h_jobs[n_new];
+        PJob &j = st.h_jobs[k];
         const int gi = q.r.first_individual + i;  // the individual's index in the whole population
         j.slot = s; j.theta_off = theta_off; j.arms = q.r.arms; j.segs = q.r.segs; j.pair = gi / 2;
         j.sign = (gi & 1) ? -1.f : 1.f; j.sigma = q.r.sigma; j.seed = q.r.seed;
+        if (S->d.net) S->b->h_pw_arms[s] = q.r.arms;
+        else S->b->h_pw_tpl[s] = st.h_meta[k].tpl;
       } else {
-        st.h_jobs[n_new] = PJob{s, 0, 0, 0, 0, 1.f, 0.f, 0};
+        st.h_jobs[k] = PJob{s, 0, 0, 0, 0, 1.f, 0.f, 0};
       }
-      S->b->h_meta[s] = init.meta[i];
-      S->b->h_remaining[s] = init.meta[i].horizon;
-      if (pol && S->d.net) S->b->h_pw_arms[s] = q.r.arms;
-      else if (pol) S->b->h_pw_tpl[s] = init.meta[i].tpl;
-      n_new++;
     }
     if (pol) {
       std::copy(q.theta.begin(), q.theta.end(), st.h_theta + theta_off);
       theta_off += (int)q.theta.size();
-      n_theta++;
     }
-    if (S->d_done) {  // the request's completion count starts at 0 (its tag may be a reused slot)
-      cudaError_t ez = cudaMemsetAsync(S->d_done + q.slots[0], 0, sizeof(int), stream);
-      if (ez != cudaSuccess) return S->cuda_fail(ez, "completion count");
-      S->prev_done[q.slots[0]] = 0;
-    }
+    if (S->d_done) S->prev_done[q.slots[0]] = 0;  // its count is cleared on the device below
     q.part = p;
     q.admitted = t;
     q.rounds_left = (q.r.horizon + S->chunk - 1) / S->chunk;
@@ -412,6 +450,10 @@ int admit(kr_server *S, int p) {
   if (e == cudaSuccess) e = cudaMemcpyAsync(st.d_meta, st.h_meta, (size_t)n_new * sizeof(SlotMeta), cudaMemcpyHostToDevice, stream);
   if (e == cudaSuccess) e = cudaMemcpyAsync(st.d_slots, st.h_slots, (size_t)n_new * sizeof(int), cudaMemcpyHostToDevice, stream);
   if (e == cudaSuccess) e = launch_spawn(S->b, st.d_slots, st.d_pose, st.d_meta, n_new, stream);
+  if (e == cudaSuccess && S->d_done) {
+    clear_done_kernel<<<(n_new + 255) / 256, 256, 0, stream>>>(st.d_meta, st.d_slots, n_new, S->d_done);
+    e = cudaGetLastError();
+  }
   const bool weights = S->d.policy || S->d.net;
   if (e == cudaSuccess && weights && theta_off > 0) {
     e = cudaMemcpyAsync(st.d_theta, st.h_theta, (size_t)theta_off * sizeof(float), cudaMemcpyHostToDevice, stream);
