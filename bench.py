@@ -169,13 +169,26 @@ def cpu_rollouts(w, every: int, offset: int, threads: int, limit_s: float):
     return steps / el, steps, el, len(sel)
 
 
+def cpu_model() -> str:
+    """The host CPU's model name (Linux /proc/cpuinfo), or the platform's."""
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    import platform
+    return platform.processor() or "unknown"
+
+
 def cpu_baseline_line(w, threads: int, seconds: float):
     """cpu_baseline of the bench line: every 32nd creature of the workload on
     all host threads (bounded by `seconds`), and the single-thread rate on
     every 512th for the per-core scaling."""
     v1, n1, e1, c1 = cpu_rollouts(w, 512, 0, 1, max(2.0, seconds / 3))
     vt, nt, et, ct = cpu_rollouts(w, 32, 0, threads, seconds)
-    return {"value": vt, "unit": UNIT, "cores": threads, "kind": "port",
+    return {"value": vt, "unit": UNIT, "cores": threads, "kind": "port", "cpu_model": cpu_model(),
             "sample": f"{nt} creature-steps in {et:.1f} s: {ct} creatures (every 32nd) of the same workload "
                       "at their own horizons, each in its own world, controls + reflex + FP64 step + postStep "
                       "(C restatement of src/physics/xpbd.js and core.js, POSIX threads, no Python in the loop)",
@@ -710,8 +723,15 @@ def main():
         if not args.no_cpu_baseline and world == 1:
             ops = ops_per_creature_step(w)
             achieved = ops * units / (kms / 1000.0)
+            n_sm = torch.cuda.get_device_properties(local).multi_processor_count
+            nominal = {f"{mhz:g}_mhz": n_sm * 128 * mhz * 1e6 / 1e12
+                       for mhz in sorted({clocks["sm_max_mhz"] or 1965.0, clocks["sm_mhz"] or 1965.0})}
             roof = {"bound": "fp32", "achieved": achieved / 1e12, "peak": fma_rate / 1e12,
                     "unit": "TFLOP/s", "frac": achieved / fma_rate,
+                    "peak_nominal": nominal,
+                    "frac_nominal": {k: achieved / (v * 1e12) for k, v in nominal.items()},
+                    "peak_nominal_note": f"{n_sm} SMs x 128 FP32 lanes x SM clock, at the maximum and at the median "
+                                         "clock sampled under load",
                     "traffic": (args.traffic if args.traffic is not None
                                 else NCU_DRAM_BYTES_PER_CREATURE * creature_launches),
                     "traffic_note": "per rollout, as achieved: ncu dram__bytes_read.sum + dram__bytes_write.sum per "
