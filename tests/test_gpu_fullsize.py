@@ -1,7 +1,8 @@
 """Size-independent properties at the full sizes of the measured
 configurations, where the oracle cannot follow (it runs ~5e4 creature-steps/s
-on a whole host): determinism, launch-shape invariance, chunking, the served
-form against the persistent form, queued admission under a memory budget.
+on a whole host): determinism, launch-shape and time-slice invariance,
+chunking, the served form (both schedulers) against the persistent form,
+queued admission under a memory budget.
 Every comparison is bit for bit."""
 import numpy as np
 import pytest
@@ -27,10 +28,16 @@ def test_mixed_16k_deterministic_and_shape_invariant(mixed16k):
     workloads.spawn_all(eng, w)
     eng.snapshot()
     runs = []
-    for shape in ((8, 8, 0), (8, 8, 0), (16, 8, 0), (32, 8, 0)):
+    # (lanes, warps, CTAs per SM, time slice ms): the last two runs are cut
+    # into 50 ms slices, regrouped between them (the automatic per-slice
+    # shape in the last)
+    for shape in ((8, 8, 0, 0), (8, 8, 0, 0), (16, 8, 0, 0), (32, 8, 0, 0), (8, 16, 1, 50), (0, 0, 0, 50)):
         eng.set_launch(shape[1], shape[2], lanes_per_creature=shape[0])
+        eng.set_slice(shape[3])
         eng.restore()
         eng.run(int(w.horizon.max()))
+        if shape[3] > 0:
+            assert eng.last_slices() > 1
         runs.append(_state(eng))
     eng.close()
     st0, fit0 = runs[0]
@@ -43,18 +50,27 @@ def test_mixed_16k_deterministic_and_shape_invariant(mixed16k):
         assert np.array_equal(fit0, fit)
 
 
-def test_mixed_16k_served_equals_persistent(mixed16k):
+SCHEDULERS = [dict(chunk_steps=64), dict(chunk_steps=1 << 20, slice_ms=50.0)]
+
+
+@pytest.mark.parametrize("sched", SCHEDULERS, ids=["two_partitions", "slices"])
+def test_mixed_16k_served_equals_persistent(mixed16k, sched):
+    """The 16k workload as one request per creature equals the persistent
+    engine's metrics under both schedulers (slices: requests completing while
+    their slice runs, their records copied back beside the kernel)."""
     w = mixed16k
     eng = batch.BatchEngine(w.maps, w.n)
     workloads.spawn_all(eng, w)
     eng.run(int(w.horizon.max()))
     want = eng.read_metrics()
     eng.close()
-    srv = serve.Server(w.maps, 8 << 30, max_slots=w.n, chunk_steps=64, policy=False)
+    srv = serve.Server(w.maps, 8 << 30, max_slots=w.n, policy=False, **sched)
     ids = srv.submit_many(w.horizon, w.arms, w.segs, w.map_id, w.x, w.y, w.angle, control_seeds=w.seed)
     srv.drain()
     got, times = srv.results_many(ids, release=True)
+    st = srv.stats()
     srv.close()
+    assert st["completed"] == w.n
     assert np.array_equal(got, want)
     assert np.all(times[:, 2] >= times[:, 1])
 
@@ -76,17 +92,20 @@ def test_uniform_1024_chunked_equals_one_launch():
     chunked.close()
 
 
-def test_65k_queued_under_budget_bit_identical_three_runs():
+@pytest.mark.parametrize("sched", [dict(chunk_steps=128), dict(chunk_steps=1 << 20, slice_ms=50.0)],
+                         ids=["two_partitions", "slices"])
+def test_65k_queued_under_budget_bit_identical_three_runs(sched):
     """65,536 mixed creatures (horizons up to 4,096, 128-step observation
     rings) through a server whose memory budget holds fewer slots than
-    creatures, so requests queue for slots; three runs, same bits."""
+    creatures, so requests queue for slots; three runs, same bits, under
+    either scheduler."""
     w = workloads.uneven(n=65536, n_maps=64, seed=4, h_min=200, h_max=4096)
     budget = int(1.5 * (1 << 30))
-    cap, per_slot = serve.plan(w.maps, budget, policy=False, obs_ring=128)
+    cap, per_slot = serve.plan(w.maps, budget, policy=False, obs_ring=128, **sched)
     assert cap < w.n
     out = []
     for _ in range(3):
-        srv = serve.Server(w.maps, budget, policy=False, obs_ring=128, chunk_steps=128)
+        srv = serve.Server(w.maps, budget, policy=False, obs_ring=128, **sched)
         ids = srv.submit_many(w.horizon, w.arms, w.segs, w.map_id, w.x, w.y, w.angle, control_seeds=w.seed)
         srv.drain()
         res, times = srv.results_many(ids, release=True)
