@@ -141,11 +141,12 @@ int kr_world_islands(const kr_world *w, int32_t *n_islands, int32_t *max_levels)
  * message is recorded (recording one would allocate).  A rejected world
  * leaves the caller's buffers untouched.
  * The first call on a device looks up the device address of the scratch
- * array; make that first call before any stream capture.  Every call then
- * waits on the host for the schedule builder's verdict -- a 4-byte copy from
- * the device into static host memory followed by a synchronize of `stream`
- * (cudaStream_t as void*, NULL = the legacy default stream) -- and only then
- * enqueues the steps asynchronously.  Every call on a
+ * array.  Every call waits on the host for the schedule builder's verdict --
+ * a 4-byte copy from the device into static host memory followed by a
+ * synchronize of `stream` (cudaStream_t as void*, NULL = the legacy default
+ * stream) -- and only then enqueues the steps asynchronously; so no call can
+ * be made inside a stream capture (the copy and the synchronize are not
+ * capturable, and the capture would be invalidated).  Every call on a
  * device shares the one scratch array: calls that overlap on the GPU (other
  * host threads, other streams) race and must not be issued. */
 #define KR_NOALLOC_MAX_BODIES 2048
