@@ -130,6 +130,9 @@ struct Req {
   int pending = 0;                      // sliced scheduling: creatures not yet at their horizon
   int64_t seq = 0;                      // admission order
   bool done = false;
+  bool holding = false;                 // its slots are still its own (a request completed while its
+                                        // slice runs keeps them until the slice ends)
+  bool release_pending = false;         // released while holding: erased when its slots are freed
 };
 
 // admission's per-creature inputs, reused between admissions
@@ -333,6 +336,7 @@ void finish_round(kr_server *S, int p) {
       S->free_slots.push_back(s);
       S->slot_req[s] = nullptr;
     }
+    q.holding = false;
     S->part_used[p] -= (int)n;
   }
   if (!R.completing.empty()) {
@@ -341,6 +345,9 @@ void finish_round(kr_server *S, int p) {
     // the slot list keeps its order (admission order) without the freed slots
     auto &sl = S->parts[p].slots;
     sl.erase(std::remove_if(sl.begin(), sl.end(), [&](int s) { return S->b->h_meta[s].horizon == 0; }), sl.end());
+    // requests released while their slice still held their slots
+    for (const Req *q : R.completing)
+      if (q->release_pending) S->reqs.erase(q->id);
   }
   R.completing.clear();
   R.inflight = false;
@@ -435,6 +442,7 @@ int admit(kr_server *S, int p) {
     q.rounds_left = (q.r.horizon + S->chunk - 1) / S->chunk;
     q.pending = pop;
     q.seq = S->admitted;
+    q.holding = true;
     S->part_used[p] += pop;
     S->active[p].push_back(&q);
     for (int s : q.slots) {
@@ -952,11 +960,26 @@ extern "C" int kr_server_poll(kr_server *S, int64_t *ids, int32_t cap, int32_t *
   return KR_OK;
 }
 
+namespace {
+// the request `id` as the caller sees it (a released request is gone)
+Req *find_req(kr_server *S, int64_t id) {
+  auto it = S->reqs.find(id);
+  return it == S->reqs.end() || it->second.release_pending ? nullptr : &it->second;
+}
+
+// releases a completed request: erased at once or, while the slice that
+// completed it still holds its slots, when the slice frees them
+void release_req(kr_server *S, Req &q) {
+  if (q.holding) q.release_pending = true;
+  else S->reqs.erase(q.id);
+}
+}  // namespace
+
 extern "C" int kr_server_result(kr_server *S, int64_t id, double *results, double *times) {
   if (!S) return KR_ERR_INVALID;
-  auto it = S->reqs.find(id);
-  if (it == S->reqs.end()) return S->fail(KR_ERR_INDEX, "unknown request " + std::to_string(id));
-  const Req &q = it->second;
+  const Req *qp = find_req(S, id);
+  if (!qp) return S->fail(KR_ERR_INDEX, "unknown request " + std::to_string(id));
+  const Req &q = *qp;
   if (!q.done) return S->fail(KR_ERR_STATE, "request " + std::to_string(id) + " has not completed");
   if (results) std::copy(q.results.begin(), q.results.end(), results);
   if (times) { times[0] = q.arrival; times[1] = q.admitted; times[2] = q.completed; }
@@ -967,28 +990,28 @@ extern "C" int kr_server_result_batch(kr_server *S, const int64_t *ids, int32_t 
                                       double *times, int32_t release) {
   if (!S || (n > 0 && !ids)) return KR_ERR_INVALID;
   for (int k = 0; k < n; k++) {
-    auto it = S->reqs.find(ids[k]);
-    if (it == S->reqs.end()) return S->fail(KR_ERR_INDEX, "unknown request " + std::to_string(ids[k]));
-    if (!it->second.done) return S->fail(KR_ERR_STATE, "request " + std::to_string(ids[k]) + " has not completed");
+    const Req *q = find_req(S, ids[k]);
+    if (!q) return S->fail(KR_ERR_INDEX, "unknown request " + std::to_string(ids[k]));
+    if (!q->done) return S->fail(KR_ERR_STATE, "request " + std::to_string(ids[k]) + " has not completed");
   }
   size_t off = 0;
   for (int k = 0; k < n; k++) {
-    auto it = S->reqs.find(ids[k]);
-    const Req &q = it->second;
-    if (results) std::copy(q.results.begin(), q.results.end(), results + off);
-    off += q.results.size();
-    if (times) { times[3 * k] = q.arrival; times[3 * k + 1] = q.admitted; times[3 * k + 2] = q.completed; }
-    if (release) S->reqs.erase(it);
+    Req *q = find_req(S, ids[k]);
+    if (!q) return S->fail(KR_ERR_INDEX, "request " + std::to_string(ids[k]) + " listed twice after its release");
+    if (results) std::copy(q->results.begin(), q->results.end(), results + off);
+    off += q->results.size();
+    if (times) { times[3 * k] = q->arrival; times[3 * k + 1] = q->admitted; times[3 * k + 2] = q->completed; }
+    if (release) release_req(S, *q);
   }
   return KR_OK;
 }
 
 extern "C" int kr_server_release(kr_server *S, int64_t id) {
   if (!S) return KR_ERR_INVALID;
-  auto it = S->reqs.find(id);
-  if (it == S->reqs.end()) return S->fail(KR_ERR_INDEX, "unknown request " + std::to_string(id));
-  if (!it->second.done) return S->fail(KR_ERR_STATE, "request " + std::to_string(id) + " has not completed");
-  S->reqs.erase(it);
+  Req *q = find_req(S, id);
+  if (!q) return S->fail(KR_ERR_INDEX, "unknown request " + std::to_string(id));
+  if (!q->done) return S->fail(KR_ERR_STATE, "request " + std::to_string(id) + " has not completed");
+  release_req(S, *q);
   return KR_OK;
 }
 

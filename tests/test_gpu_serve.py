@@ -170,8 +170,12 @@ def test_sliced_requests_complete_while_their_slice_runs():
     """Slices: a short request completes (its records copied back beside the
     running kernel) while the slice that runs it still runs a long one --
     one slice in all, its time (10 s) longer than the run -- and every
-    request's results equal the batched engine's."""
+    request's results equal the batched engine's.  A request released while
+    its slice still holds its slots is gone for the caller at once and is
+    freed when the slice ends."""
     import time
+
+    from kraken_3_gpu_b200 import _native
 
     w = workloads.uneven(n=6, n_maps=2, seed=17, h_min=20, h_max=30)
     w.horizon[0] = 3000  # the long request
@@ -183,22 +187,31 @@ def test_sliced_requests_complete_while_their_slice_runs():
     srv = serve.Server(w.maps, 1 << 30, max_slots=8, policy=False, slice_ms=10000.0, chunk_steps=1 << 20)
     ids = list(srv.submit_many(w.horizon, w.arms, w.segs, w.map_id, w.x, w.y, w.angle, control_seeds=w.seed))
     early = None
+    released = None
     t_end = time.monotonic() + 60
     while time.monotonic() < t_end:
         busy = srv.pump()
         done = set(srv.poll())
         if done and early is None:
             early = (srv.stats(), done)
+            released = min(done)
+            kept = srv.result(released, 1)["results"]
+            srv.release(released)  # its slice still runs and holds its slot
+            with pytest.raises(_native.KrError):
+                srv.result(released, 1)
         if not busy:
             break
         time.sleep(0.0002)
     srv.drain()
-    rest, times = srv.results_many(ids, release=True)
+    others = [i for i in ids if i != released]
+    rest, times = srv.results_many(others, release=True)
     st = srv.stats()
     srv.close()
     assert early is not None
     first_stats, first_done = early
     assert ids[0] not in first_done and first_stats["rounds"] == 1
-    assert st["rounds"] == 1  # nothing preempted: the one slice ran every request
-    assert np.all(times[1:, 2] < times[0, 2])
-    assert np.array_equal(rest, want)
+    assert st["rounds"] == 1 and st["completed"] == w.n  # the one slice ran every request
+    k = ids.index(released)
+    assert np.array_equal(kept, want[k:k + 1])
+    assert np.array_equal(rest, np.delete(want, k, axis=0))
+    assert times[others.index(ids[0]), 2] == times[:, 2].max()
