@@ -192,6 +192,9 @@ int kr_server_get_stats(kr_server *s, kr_server_stats *out);
  * mirrored pair `pair` of a request (synchronous; for checking). */
 int kr_policy_eps(uint64_t seed, int32_t pair, int32_t n, float *out);
 
+/* Stops a running slice at its creatures' next env step (a round of two
+ * partitions runs to its end), waits for the device and frees everything;
+ * requests not yet completed are dropped.  NULL is a no-op. */
 void kr_server_destroy(kr_server *s);
 const char *kr_server_last_error(const kr_server *s);
 

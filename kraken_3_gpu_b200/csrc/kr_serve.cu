@@ -1052,6 +1052,10 @@ extern "C" int kr_policy_eps(uint64_t seed, int32_t pair, int32_t n, float *out)
 
 extern "C" void kr_server_destroy(kr_server *S) {
   if (!S) return;
+  // a running slice stops at its creatures' next env step instead of running
+  // them to their horizons
+  if (S->sliced && S->round[0].inflight && !S->stop_sent)
+    cudaMemcpyAsync(S->d_stop, S->h_flag + 1, sizeof(int), cudaMemcpyHostToDevice, S->ctl);
   cudaDeviceSynchronize();
   for (int p = 0; p < 2; p++) {
     free_part(S->parts[p]);

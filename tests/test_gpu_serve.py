@@ -215,3 +215,20 @@ def test_sliced_requests_complete_while_their_slice_runs():
     assert np.array_equal(kept, want[k:k + 1])
     assert np.array_equal(rest, np.delete(want, k, axis=0))
     assert times[others.index(ids[0]), 2] == times[:, 2].max()
+
+
+def test_sliced_server_closes_without_running_its_slice_out():
+    """Destroying a server with a slice in flight stops the slice at its
+    creatures' next env step: closing takes a small fraction of the time the
+    running request needs (100,000 env steps)."""
+    import time
+
+    w = workloads.uneven(n=8, n_maps=2, seed=19, h_min=20, h_max=30)
+    srv = serve.Server(w.maps, 1 << 30, max_slots=8, policy=False, slice_ms=10000.0, chunk_steps=1 << 20)
+    srv.submit_many(np.full(w.n, 100000, np.int32), w.arms, w.segs, w.map_id, w.x, w.y, w.angle,
+                    control_seeds=w.seed)
+    srv.pump()  # admits and launches the slice
+    time.sleep(0.05)
+    t0 = time.monotonic()
+    srv.close()
+    assert time.monotonic() - t0 < 1.0
