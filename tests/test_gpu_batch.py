@@ -344,3 +344,25 @@ def test_device_wrap_is_atan2_of_sin_and_cos():
     for scale in (0.42 * np.pi, 0.62 * np.pi):
         assert np.array_equal((got / scale).astype(np.float32), (want / scale).astype(np.float32))
     assert np.all(np.isnan(batch.probe_wrap(np.array([np.nan, np.inf, -np.inf]))))
+
+
+@pytest.mark.parametrize("slice_ms", [0.0, 0.5])
+def test_engine_rollouts_equal_oracle_rollout_loop_f32(slice_ms):
+    """The engine's rollouts (control streams, reflex, step, postStep on the
+    device; uneven horizons) against the oracle's C rollout loop with the f32
+    emulation's step (xpbd_bench.c): final mantle positions bit for bit, path
+    length and score within 1e-9 (f64 libm calls on both sides), in one
+    launch and in time slices."""
+    w = workloads.uneven(n=48, n_maps=6, seed=23, h_min=100, h_max=200)
+    eng = batch.BatchEngine(w.maps, w.n)
+    workloads.spawn_all(eng, w)
+    eng.set_slice(slice_ms)
+    eng.run(int(w.horizon.max()))
+    met = eng.read_metrics()
+    eng.close()
+    _, _, ref = ob.bench_rollouts(w.maps, w.map_id, w.arms, w.segs, w.x, w.y, w.angle, w.seed, w.horizon, 2,
+                                  metrics=True, f32=True)
+    F = batch.METRIC_FIELDS
+    assert np.array_equal(met[:, [F.index("x"), F.index("y")]], ref[:, :2])
+    got = met[:, [F.index("pathLen"), F.index("score")]]
+    assert np.all(np.abs(got - ref[:, 2:4]) <= 1e-9 * np.maximum(1.0, np.abs(ref[:, 2:4])))
