@@ -85,7 +85,7 @@ typedef struct kr_server_desc {
    * beside the running kernel).  It preempts the slice -- through a device
    * word the kernel reads at each env step -- when an arrived request fits
    * the free slots plus those of the completed requests (not before the
-   * slice has run 3 times the host's time between slices) or slice_ms
+   * slice has run 10 times the host's time between slices) or slice_ms
    * milliseconds (at least 10 such host gaps) have passed, then frees the
    * completed requests' slots, admits, and launches the next slice, its
    * creatures regrouped by their remaining steps (the longest spread over

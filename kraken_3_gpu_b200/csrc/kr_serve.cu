@@ -646,9 +646,11 @@ bool admissible(kr_server *S) {
   const Req &q = S->reqs.at(S->queue.front());
   const double t = S->now();
   if (q.arrival > t) return false;
-  // a slice runs at least 3 host gaps before an admission cuts it, so that
-  // the GPU idles at most a quarter of the time however often requests come
-  if (S->round[0].inflight && t - S->slice_t0 < 3 * S->gap_s) return false;
+  // a slice runs at least 10 host gaps before an admission cuts it, so that
+  // the GPU idles at most about a tenth of the time however often requests
+  // come (with 3, queued single-creature requests cut slices so often that
+  // the host gaps took 8 % of a 65k memory-bound run)
+  if (S->round[0].inflight && t - S->slice_t0 < 10 * S->gap_s) return false;
   return q.r.population <= (long)S->free_slots.size() + S->done_unfreed;
 }
 
