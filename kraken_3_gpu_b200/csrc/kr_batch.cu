@@ -1134,51 +1134,66 @@ int plan_shape(kr_batch *b) {
 // are sorted by remaining steps, so the creatures that share a warp finish
 // together; groups are queued by their work (steps this launch x template
 // cost), largest first, so the launch ends on short groups.
+void gather_live(kr_batch *b, Part &p) {
+  p.g_live.clear();
+  p.g_tpl.clear();
+  p.g_rem.clear();
+  p.g_ctrl.clear();
+  p.g_per_arm = 0;
+  auto take = [&](int s) {
+    const int r = b->h_remaining[s];
+    if (r <= 0) return;
+    const SlotMeta &m = b->h_meta[s];
+    if (m.horizon <= 0) return;
+    p.g_live.push_back(s);
+    p.g_tpl.push_back(m.tpl);
+    p.g_rem.push_back(r);
+    p.g_ctrl.push_back(m.ctrl);
+    p.g_per_arm += m.ctrl == KR_CTRL_POLICY || m.ctrl == KR_CTRL_NET;
+  };
+  if (p.all) {
+    for (int s = 0; s < b->capacity; s++) take(s);
+  } else {
+    for (int s : p.slots) take(s);
+  }
+  p.gathered = true;
+}
+
 int build_groups(kr_batch *b, Part &p, int max_steps) {
+  // the live slots, gathered once (by launch_part's shape choice just
+  // before, or here); a gather is used by one build only
+  const bool fresh = p.gathered;
+  p.gathered = false;
   if (b->shape_dirty) {
     int rc = plan_shape(b);
     if (rc != KR_OK) return rc;
   }
-  const std::vector<int> &rem = b->h_remaining;
-  std::vector<int> live;
-  if (p.all) {
-    for (int s = 0; s < b->capacity; s++)
-      if (b->h_meta[s].horizon > 0 && rem[s] > 0) live.push_back(s);
-  } else {
-    for (int s : p.slots)
-      if (rem[s] > 0) live.push_back(s);
-  }
-  for (int s : live) {
-    const SlotMeta &m = b->h_meta[s];
-    if (m.ctrl == KR_CTRL_NET) {
+  if (!fresh) gather_live(b, p);
+  p.gathered = false;
+  const int n_live = (int)p.g_live.size();
+  for (int i = 0; i < n_live; i++) {
+    const int ctrl = p.g_ctrl[i];
+    if (ctrl != KR_CTRL_NET && ctrl != KR_CTRL_POLICY) continue;
+    const int s = p.g_live[i];
+    if (ctrl == KR_CTRL_NET) {
       if (!b->d_pw || b->h_pw_idx.size() != (size_t)b->capacity)
         return b->fail(KR_ERR_STATE, "slot " + std::to_string(s) + ": net control without kr_batch_set_net");
-      if (b->h_pw_arms[b->h_pw_idx[s]] != b->tpls[m.tpl].arms)
+      if (b->h_pw_arms[b->h_pw_idx[s]] != b->tpls[p.g_tpl[i]].arms)
         return b->fail(KR_ERR_STATE, "slot " + std::to_string(s) + ": its genome was set for another arm "
                                          "count (kr_batch_set_net after the spawn)");
       continue;
     }
-    if (m.ctrl != KR_CTRL_POLICY) continue;
     if (!b->d_pw || b->h_pw_idx.size() != (size_t)b->capacity)
       return b->fail(KR_ERR_STATE, "slot " + std::to_string(s) + ": policy control without kr_batch_set_policy");
-    if (b->h_pw_tpl[b->h_pw_idx[s]] != m.tpl)
+    if (b->h_pw_tpl[b->h_pw_idx[s]] != p.g_tpl[i])
       return b->fail(KR_ERR_STATE, "slot " + std::to_string(s) + ": its individual's weights were laid out for "
                                        "another body shape (kr_batch_set_policy after the spawn)");
   }
   // by template, then longest remaining first, ties in slot-list order
-  {
-    const int n = (int)live.size();
-    std::vector<int> lt(n), lr(n), perm, perm2;
-    std::vector<uint64_t> keys, keys2;
-    for (int i = 0; i < n; i++) {
-      lt[i] = b->h_meta[live[i]].tpl;
-      lr[i] = rem[live[i]];
-    }
-    lpt_order(n, lt.data(), lr.data(), perm, keys, keys2, perm2);
-    std::vector<int> sorted(n);
-    for (int i = 0; i < n; i++) sorted[i] = live[perm[i]];
-    live.swap(sorted);
-  }
+  lpt_order(n_live, p.g_tpl.data(), p.g_rem.data(), p.perm, p.keys, p.keys2, p.perm2);
+  std::vector<int> &live = p.s_live;
+  live.resize(n_live);
+  for (int i = 0; i < n_live; i++) live[i] = p.g_live[p.perm[i]];
   // Group size per template.  When the live creatures fill less than one
   // wave of the resident CTAs, smaller groups (whole warps) spread them over
   // every SM instead of packing a few SMs.
@@ -1186,28 +1201,28 @@ int build_groups(kr_batch *b, Part &p, int max_steps) {
   const int ctas = b->ctas_per_sm > 0 ? b->ctas_per_sm : std::max(1, 16 / b->W);
   const long slots = (long)b->n_sm * ctas;
   std::vector<int> n_t(b->h_tpl.size(), 0), size_t_(b->h_tpl.size(), 0);
-  for (int s : live) n_t[b->h_meta[s].tpl]++;
+  for (int i = 0; i < n_live; i++) n_t[p.g_tpl[i]]++;
   long full_groups = 0;
   for (size_t t = 0; t < n_t.size(); t++)
     if (n_t[t]) full_groups += (n_t[t] + b->tpl_cpg[t] - 1) / b->tpl_cpg[t];
   for (size_t t = 0; t < n_t.size(); t++) {
     size_t_[t] = b->tpl_cpg[t];
-    if (!n_t[t] || full_groups >= slots || live.empty()) continue;
-    const long want = std::max<long>(1, (long)((double)slots * n_t[t] / (double)live.size()));
+    if (!n_t[t] || full_groups >= slots || n_live == 0) continue;
+    const long want = std::max<long>(1, (long)((double)slots * n_t[t] / (double)n_live));
     int sz = (int)((n_t[t] + want - 1) / want);
     sz = ((sz + cpw - 1) / cpw) * cpw;
     size_t_[t] = std::max(cpw, std::min(b->tpl_cpg[t], sz));
   }
   std::vector<std::pair<double, int>> order;  // (work, first index into live)
   std::vector<int> starts, sizes;
-  for (size_t i = 0; i < live.size();) {
-    const int t = b->h_meta[live[i]].tpl;
-    const size_t st = i;
+  for (int i = 0; i < n_live;) {
+    const int t = p.g_tpl[p.perm[i]];
+    const int st = i;
     int n = 0;
-    while (i < live.size() && n < size_t_[t] && b->h_meta[live[i]].tpl == t) { i++; n++; }
-    const double work = (double)std::min(max_steps, rem[live[st]]) * tpl_cost(b->h_tpl[t]);
+    while (i < n_live && n < size_t_[t] && p.g_tpl[p.perm[i]] == t) { i++; n++; }
+    const double work = (double)std::min(max_steps, p.g_rem[p.perm[st]]) * tpl_cost(b->h_tpl[t]);
     order.push_back({work, (int)starts.size()});
-    starts.push_back((int)st);
+    starts.push_back(st);
     sizes.push_back(n);
   }
   std::stable_sort(order.begin(), order.end(),
@@ -1299,18 +1314,8 @@ int launch_part(kr_batch *b, Part &p, int max_steps, bool timed) {
   if (b->d.control_mode == KR_CTRL_POLICY && !b->d_pw)
     return b->fail(KR_ERR_STATE, "policy control without kr_batch_set_policy");
   if (b->auto_shape && p.dirty) {
-    long live = 0, per_arm = 0;
-    auto count = [&](int s) {
-      if (b->h_remaining[s] <= 0 || b->h_meta[s].horizon <= 0) return;
-      live++;
-      per_arm += b->h_meta[s].ctrl == KR_CTRL_POLICY || b->h_meta[s].ctrl == KR_CTRL_NET;
-    };
-    if (p.all) {
-      for (int s = 0; s < b->capacity; s++) count(s);
-    } else {
-      for (int s : p.slots) count(s);
-    }
-    const int g = auto_lanes(b, live, per_arm);
+    gather_live(b, p);  // build_groups below takes the same gather
+    const int g = auto_lanes(b, (long)p.g_live.size(), p.g_per_arm);
     const int w = g == 32 ? 4 : 8;
     if (g != b->G || w != b->W) {
       b->G = g;

@@ -242,6 +242,13 @@ struct Part {
   bool staged_pending = false;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;  // launch timing
   uint64_t h2d_bytes = 0;         // group uploads so far
+  // the live slots with their template, remaining steps and control mode,
+  // gathered in one pass over the slot records (gather_live) and used by
+  // the next build_groups; then the launch order's scratch
+  std::vector<int> g_live, g_tpl, g_rem, g_ctrl, s_live, perm, perm2;
+  std::vector<uint64_t> keys, keys2;
+  long g_per_arm = 0;
+  bool gathered = false;
 };
 
 // slot data a spawn writes, built on the host
@@ -351,6 +358,9 @@ int plan_shape(kr_batch *b);
 // which `per_arm` run the policy or net controller (their proprioception
 // and controller run per arm)
 int auto_lanes(const kr_batch *b, long live, long per_arm);
+// the part's live slots (remaining steps > 0) with their template, remaining
+// steps and control mode, in slot-list order, into p.g_*
+void gather_live(kr_batch *b, Part &p);
 // groups of the part's live slots, longest work first, staged to the device
 int build_groups(kr_batch *b, Part &p, int max_steps);
 // one persistent launch over the part's groups, min(max_steps, remaining)
