@@ -235,9 +235,11 @@ int kr_probe_wrap(const double *d, int32_t n, double *out);
  * memory; a group of one body template holds as many creatures as fit in it.
  * Until this is called the engine picks the shape per launch: 32 lanes x 4
  * warps below 16 live creatures per SM, 16 lanes x 8 warps below 96 (8
- * lanes when most creatures run the fused policy or an observation ring is
- * kept), else 8 lanes x 8 warps; lanes_per_creature = 0 returns to that
- * (the other arguments are ignored).  Results do not depend on the launch
+ * lanes when most creatures run the fused policy or the net, or an
+ * observation ring is kept), else 8 lanes x 8 warps -- x 16 warps in one CTA
+ * per SM when most creatures run the net or a ring is kept;
+ * lanes_per_creature = 0 returns to that (the other arguments are
+ * ignored).  Results do not depend on the launch
  * shape. */
 int kr_batch_set_launch(kr_batch *b, int32_t lanes_per_creature, int32_t warps_per_cta,
                         int32_t ctas_per_sm);

@@ -1140,6 +1140,7 @@ void gather_live(kr_batch *b, Part &p) {
   p.g_rem.clear();
   p.g_ctrl.clear();
   p.g_per_arm = 0;
+  p.g_net = 0;
   auto take = [&](int s) {
     const int r = b->h_remaining[s];
     if (r <= 0) return;
@@ -1150,6 +1151,7 @@ void gather_live(kr_batch *b, Part &p) {
     p.g_rem.push_back(r);
     p.g_ctrl.push_back(m.ctrl);
     p.g_per_arm += m.ctrl == KR_CTRL_POLICY || m.ctrl == KR_CTRL_NET;
+    p.g_net += m.ctrl == KR_CTRL_NET;
   };
   if (p.all) {
     for (int s = 0; s < b->capacity; s++) take(s);
@@ -1316,7 +1318,13 @@ int launch_part(kr_batch *b, Part &p, int max_steps, bool timed) {
   if (b->auto_shape && p.dirty) {
     gather_live(b, p);  // build_groups below takes the same gather
     const int g = auto_lanes(b, (long)p.g_live.size(), p.g_per_arm);
-    const int w = g == 32 ? 4 : 8;
+    // at 8 lanes, creatures under the reference net or keeping an
+    // observation ring run faster as one CTA of 16 warps per SM than as two
+    // of 8 (served net ES stream 2.60e7 -> 2.90e7 creature-steps/s; 65k
+    // creatures with 128-step rings 4.32e7 -> 4.54e7); under the fused
+    // policy the two are within noise, and stream controls keep 8
+    const bool wide = b->d.obs_ring > 0 || 2 * p.g_net > (long)p.g_live.size();
+    const int w = g == 32 ? 4 : (g == 8 && wide) ? 16 : 8;
     if (g != b->G || w != b->W) {
       b->G = g;
       b->W = w;

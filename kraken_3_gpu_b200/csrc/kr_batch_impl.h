@@ -247,7 +247,7 @@ struct Part {
   // the next build_groups; then the launch order's scratch
   std::vector<int> g_live, g_tpl, g_rem, g_ctrl, s_live, perm, perm2;
   std::vector<uint64_t> keys, keys2;
-  long g_per_arm = 0;
+  long g_per_arm = 0, g_net = 0;   // live slots under the policy or the net / under the net
   bool gathered = false;
 };
 
