@@ -167,7 +167,11 @@ def policy_eps(seed, pair, n):
 
 
 class Server:
-    """One rollout server handle (kr_server)."""
+    """One rollout server handle (kr_server).  Keywords as kr_server_desc:
+    max_slots, chunk_steps, obs_ring, policy, net, lights, ... and slice_ms
+    (> 0: one partition in preemptible time slices of that many ms, requests
+    completing while their slice runs; 0: two partitions in rounds of
+    chunk_steps env steps)."""
 
     def __init__(self, maps, hbm_budget, **kw):
         o = dict(_DEFAULTS, **kw)
