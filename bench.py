@@ -80,6 +80,9 @@ def parse():
     ap.add_argument("--no-config4", action="store_true", help="skip the 65,536-creature memory-bound serving case")
     ap.add_argument("--net-only", action="store_true",
                     help="only the reference-net controller rollout of the workload (one JSON line)")
+    ap.add_argument("--no-policy", action="store_true", help="skip the fused-policy controller rollout")
+    ap.add_argument("--policy-only", action="store_true",
+                    help="only the fused-policy controller rollout of the workload (one JSON line)")
     ap.add_argument("--traffic", type=float, default=None,
                     help="ncu DRAM bytes per launch of the captured kernel, if measured")
     return ap.parse_args()
@@ -464,6 +467,49 @@ def config4_memory_bound(serve, slice_ms):
     return out
 
 
+def policy_controller(stream, w, seed=8, slice_ms=0.0, shape=None):
+    """The same workload driven by the fused policy MLP (KR_CTRL_POLICY, the
+    ES requests' controller: proprioception -> 64 tanh -> motor targets and
+    adhesion), one individual per creature with its own weights theta ~
+    N(0, 0.1^2) in its body shape's layout -- every creature reads its own
+    weights each env step, as an ES population's individuals do; the whole
+    horizons with the autotuned launch shape (or `shape`: lanes, warps, CTAs
+    per SM[, unroll]), in time slices of slice_ms (0: one launch), device time
+    by CUDA events."""
+    from kraken_3_gpu_b200 import batch, workloads
+    rng = np.random.default_rng(seed)
+    width = max(batch.policy_params(int(a), int(g)) for a, g in zip(w.arms, w.segs))
+    weights = np.zeros((w.n, width), np.float32)
+    for i in range(w.n):
+        k = batch.policy_params(int(w.arms[i]), int(w.segs[i]))
+        weights[i, :k] = rng.normal(0, 0.1, k)
+    eng = batch.BatchEngine(w.maps, w.n, control="policy")
+    eng.set_stream(stream.cuda_stream)
+    workloads.spawn_all(eng, w)
+    eng.set_policy(weights, np.arange(w.n, dtype=np.int32))
+    eng.snapshot()
+    if shape:
+        eng.set_launch(shape[1], shape[2], lanes_per_creature=shape[0])
+        if len(shape) > 3:
+            eng.set_unroll(shape[3])
+    else:
+        eng.autotune(64)  # the launch shape, as the persistent bench picks it; slots left as they were
+    eng.set_slice(slice_ms)
+    eng.run(64)
+    eng.restore()
+    eng.run(int(w.horizon.max()))
+    eng.sync()
+    ms = eng.last_ms()
+    shape = eng.get_launch()
+    slices = eng.last_slices()
+    eng.close()
+    return {"value": w.creature_steps() / (ms / 1000.0), "unit": UNIT, "kernel_ms": ms,
+            "controller": "fused policy MLP 6A+6 -> 64 tanh -> A*S+A per creature, its own weights (theta ~ N(0, 0.1^2))",
+            "launch_shape": [shape["lanes_per_creature"], shape["warps_per_cta"], shape["ctas_per_sm"],
+                             shape["substep_unroll"]],
+            "time_slices": slices, "slice_ms": slice_ms if slice_ms > 0 else None}
+
+
 def net_controller(stream, w, seed=7, slice_ms=0.0):
     """The same workload driven by the reference trainer's own controller
     (KR_CTRL_NET: net.js's recurrent net on proprioception + echo, light and
@@ -532,11 +578,16 @@ def main():
     w_all = workloads.uneven(n=args.n * world, n_maps=args.maps, seed=args.seed, h_min=args.hmin, h_max=args.hmax)
     w, (lo, hi) = replicas.shard(w_all, rank, world)
     del w_all
-    if args.net_only:
-        line = net_controller(torch.cuda.current_stream(), w, slice_ms=args.engine_slice_ms)
-        line.update({"metric": "creature-steps/s under the reference net controller", "n_gpus": 1,
-                     "config": {"workload": f"uneven: {w.n} creatures, {len(w.maps)} maps, horizons "
-                                            f"{args.hmin}-{args.hmax}"}})
+    if args.net_only or args.policy_only:
+        if args.net_only:
+            line = net_controller(torch.cuda.current_stream(), w, slice_ms=args.engine_slice_ms)
+            line["metric"] = "creature-steps/s under the reference net controller"
+        else:
+            shape = tuple(int(v) for v in args.shape.split(",")) if args.shape else None
+            line = policy_controller(torch.cuda.current_stream(), w, slice_ms=args.engine_slice_ms, shape=shape)
+            line["metric"] = "creature-steps/s under the fused policy controller"
+        line.update({"n_gpus": 1, "config": {"workload": f"uneven: {w.n} creatures, {len(w.maps)} maps, horizons "
+                                                         f"{args.hmin}-{args.hmax}"}})
         if rank == 0:
             print(json.dumps(line))
         replicas.finish(world)
@@ -707,6 +758,8 @@ def main():
         extra["plain_dropin_1024"] = config1_forms(torch, stream)
     if not args.no_config4 and rank == 0:
         extra["memory_bound_65k"] = config4_memory_bound(serve, sl)
+    if not args.no_policy and rank == 0:
+        extra["policy_controller"] = policy_controller(stream, w, slice_ms=args.engine_slice_ms)
     if not args.no_net and rank == 0:
         extra["net_controller"] = net_controller(stream, w, slice_ms=args.engine_slice_ms)
         if not args.no_es:
